@@ -1,0 +1,133 @@
+/*
+ * libmjmlx: batched MuJoCo physics step, B200 CUDA engine.
+ *
+ * This header keeps the batched-simulation entry points of the reference's
+ * include/mjmlx/mjmlx.h with the same names, argument meaning and error
+ * behaviour, so an existing caller relinks against this library unchanged.
+ * Every declaration cites the reference declaration it replaces.
+ *
+ * Differences a caller can observe (all deliberate):
+ *  - There is no CPU fallback.  mjmlx_batched_create returns NULL and prints
+ *    to stderr when the CUDA engine cannot be built (reference: batched.cpp
+ *    falls back to a MuJoCo C thread pool when use_gpu == 0).
+ *  - Getter pointers point into host staging buffers owned by the sim; they
+ *    stay valid until the next getter call of the same quantity or the next
+ *    step (reference: mjmlx.h:137-138, same lifetime rule).
+ *  - Arrays at this boundary are env-major: qpos is float[num_envs * nq], etc.
+ */
+#ifndef MJMLX_H
+#define MJMLX_H
+
+#include "mjmlx_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Library version string.  Replaces mjmlx.h:37. */
+MJMLX_API const char* mjmlx_version(void);
+
+/* Load an MJCF model from a file / string.  NULL + stderr message on error.
+ * Replaces mjmlx.h:44 and mjmlx.h:47.  The built-in compiler reads the MJCF
+ * subset: option, compiler(angle), default (unnamed), worldbody/body/
+ * inertial/joint/freejoint/geom, asset/mesh(vertex), actuator/position|motor|
+ * general, contact/exclude|pair.  Unknown elements are an error. */
+MJMLX_API MjmlxModel* mjmlx_load_model(const char* xml_path);
+MJMLX_API MjmlxModel* mjmlx_load_model_from_string(const char* xml_string);
+
+/* Load-time options: self_collision = 0 clears conaffinity of the robot's
+ * geoms (bodies with joints and their descendants); max_condim > 0 caps the
+ * robot geoms' condim.  Replaces mjmlx.h:53-59. */
+typedef struct MjmlxModelOptions {
+    int self_collision;
+    int max_condim;
+} MjmlxModelOptions;
+MJMLX_API MjmlxModelOptions mjmlx_default_model_options(void);
+MJMLX_API MjmlxModel* mjmlx_load_model_ex(const char* xml_path, const MjmlxModelOptions* options);
+MJMLX_API MjmlxModel* mjmlx_load_model_from_string_ex(const char* xml_string, const MjmlxModelOptions* options);
+
+/* Replaces mjmlx.h:62. */
+MJMLX_API void mjmlx_free_model(MjmlxModel* model);
+/* Replaces mjmlx.h:65. */
+MJMLX_API MjmlxModelInfo mjmlx_model_info(const MjmlxModel* model);
+/* Replaces mjmlx.h:72 / mjmlx.h:75. */
+MJMLX_API float mjmlx_model_opt_timestep(const MjmlxModel* model);
+MJMLX_API void mjmlx_model_set_opt_timestep(MjmlxModel* model, float dt);
+/* Replaces mjmlx.h:78.  Returns 0 for an out-of-range id. */
+MJMLX_API float mjmlx_model_body_mass(const MjmlxModel* model, int body_id);
+/* Replaces mjmlx.h:83.  obj_type: 1 body, 3 joint, 5 geom, 19 actuator
+ * (MuJoCo mjtObj numbering).  Returns -1 if not found. */
+MJMLX_API int mjmlx_name2id(const MjmlxModel* model, int obj_type, const char* name);
+
+/* ---------------------------------------------------------------- batched */
+
+/* Create a batched simulation of config->num_envs copies of the model, all
+ * at qpos0 with zero velocity.  Replaces mjmlx.h:171. */
+MJMLX_API MjmlxBatchedSim* mjmlx_batched_create(const MjmlxModel* model, const MjmlxBatchedConfig* config);
+/* Replaces mjmlx.h:176. */
+MJMLX_API void mjmlx_batched_free(MjmlxBatchedSim* sim);
+/* One physics step of every env with ctrl float[num_envs * nu] (NULL = zero
+ * controls).  Asynchronous: getters synchronise.  Replaces mjmlx.h:181. */
+MJMLX_API void mjmlx_batched_step(MjmlxBatchedSim* sim, const float* ctrl);
+/* n physics steps with the same ctrl; ctrl crosses host->device once.
+ * Replaces mjmlx.h:186. */
+MJMLX_API void mjmlx_batched_step_n(MjmlxBatchedSim* sim, const float* ctrl, int n);
+/* Reset envs with mask[i] != 0 to qpos0 / zero velocity.  Replaces mjmlx.h:193. */
+MJMLX_API void mjmlx_batched_reset(MjmlxBatchedSim* sim, const int* reset_mask);
+/* Copy qpos / qvel of all envs out with one synchronisation.  Replaces mjmlx.h:198. */
+MJMLX_API void mjmlx_batched_get_state(const MjmlxBatchedSim* sim, float* qpos_out, float* qvel_out, int* nq_out, int* nv_out);
+/* Overwrite the whole qpos / qvel batch (either may be NULL).  Replaces mjmlx.h:203. */
+MJMLX_API void mjmlx_batched_set_state(MjmlxBatchedSim* sim, const float* qpos, const float* qvel);
+
+/* Batched getters, float[num_envs * dim].  Replace mjmlx.h:208-216.
+ * xpos/xquat/subtree_com/cinert/cvel/qfrc_actuator/cfrc_ext are the values
+ * computed during the last physics step (from the state at its start, as in
+ * the reference and in MuJoCo's mj_step). */
+MJMLX_API const float* mjmlx_batched_get_qpos(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_qvel(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_xpos(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_xquat(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_subtree_com(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_cinert(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_cvel(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_qfrc_actuator(const MjmlxBatchedSim* sim, int* n_out);
+MJMLX_API const float* mjmlx_batched_get_cfrc_ext(const MjmlxBatchedSim* sim, int* n_out);
+
+/* Per-env state setters.  Replace mjmlx.h:224-225. */
+MJMLX_API void mjmlx_batched_set_env_qpos(MjmlxBatchedSim* sim, int env_idx, const float* qpos, int nq);
+MJMLX_API void mjmlx_batched_set_env_qvel(MjmlxBatchedSim* sim, int env_idx, const float* qvel, int nv);
+
+/* Per-env physics randomisation (config->domain_rand == 1 only).  For each
+ * env_idx[i] (env_idx == NULL: n == num_envs, all envs) update the non-NULL
+ * arrays: mass_scale[n*nbody], com_delta[n*nbody*3], friction_scale[n],
+ * gain_scale[n*nu].  Returns 0 ok, -1 bad handle / domain_rand off / bad n,
+ * -2 env index out of range.  Replaces mjmlx.h:233. */
+MJMLX_API int mjmlx_batched_set_env_params(MjmlxBatchedSim* sim, const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale);
+/* Quadratic drag F = -k|v|v on free joints, drag_k[n * nfree].  Returns as
+ * above, -3 if the model has no free joint.  Replaces mjmlx.h:237-238. */
+MJMLX_API int mjmlx_batched_set_free_drag(MjmlxBatchedSim* sim, const int* env_idx, int n, const float* drag_k);
+MJMLX_API int mjmlx_batched_num_free_joints(const MjmlxBatchedSim* sim);
+
+/* Packed read-back: one row per env of [qpos(nq), qvel(nv), |contact force|
+ * of each selected body (nbody_sel), sum of qfrc_actuator^2 over dofs
+ * [dof_lo, dof_lo+ndof), sum of |qfrc_actuator| over the same dofs].
+ * set_pack_spec returns the row stride (or -1); get_pack fills
+ * out[num_envs * stride] and returns 0 (or -1).  Replaces mjmlx.h:241-242. */
+MJMLX_API int mjmlx_batched_set_pack_spec(MjmlxBatchedSim* sim, const int* body_ids, int nbody_sel, int dof_lo, int ndof);
+MJMLX_API int mjmlx_batched_get_pack(MjmlxBatchedSim* sim, float* out);
+
+/* Batched ray casting against the geoms of every env at the pose of the last
+ * step (mj_ray semantics).  pnt/vec float[B*nray*3]; dist_out float[B*nray]
+ * (-1 = no hit), geomid_out int[B*nray] (-1 = no hit).  Plane, sphere,
+ * capsule, ellipsoid, cylinder and box geoms are hit.  Returns 0 / -1.
+ * Replaces mjmlx.h:248. */
+MJMLX_API int mjmlx_batched_raycast(MjmlxBatchedSim* sim, const float* pnt, const float* vec, int nray, int bodyexclude, const unsigned char* geomgroup, int flg_static, float* dist_out, int* geomid_out);
+
+/* Wait for the last step.  Replaces mjmlx.h:252. */
+MJMLX_API void mjmlx_batched_eval_state(const MjmlxBatchedSim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MJMLX_H */

@@ -1,0 +1,467 @@
+/*
+ * Oracle (test infrastructure): constraint rows, Newton solver, Euler.
+ *   oracle_make_constraints <- solver.hpp:259-587 (rows in the order
+ *        frictionloss -> limits -> contacts; impedance efc_kbi solver.hpp:122-138;
+ *        pyramid rows J_n +- mu_k J_k with R = 2 mu0^2 / impratio * R_first,
+ *        R_first from invw_t (1 + mu0^2), solver.hpp:536-571)
+ *   oracle_solve            <- solver.hpp:592-854 (Newton on the primal cost,
+ *        Cholesky of H = M + J' D J), here with MuJoCo's previous-step warm
+ *        start (smooth vs warm by total cost), an exact line search on the
+ *        piecewise-quadratic cost, and termination by improvement or gradient
+ *        below tolerance scaled by 1/(meaninertia * nv)
+ *   oracle_integrate        <- euler.hpp:26-110 (semi-implicit Euler,
+ *        quaternion exp-map for free/ball joints), batched.cpp:712-745 for the
+ *        implicit joint-damping fold
+ */
+#include <pthread.h>
+#include <stdlib.h>
+
+#include "mjoracle.h"
+#include "o_util.h"
+
+enum { T_FRICTION = 0, T_LIMIT = 1, T_PYRAMID = 2, T_FRICTIONLESS = 3 };
+
+static void impedance(const OModel* m, const double* solref, const double* solimp, double pos, double* k, double* b, double* imp) {
+  double tc = solref[0], dr = solref[1];
+  if (!(m->disableflags & (1 << 11)) && tc > 0 && tc < 2 * m->timestep) tc = 2 * m->timestep;
+  double dmin = solimp[0] < 1e-4 ? 1e-4 : solimp[0] > 0.9999 ? 0.9999 : solimp[0];
+  double dmax = solimp[1] < 1e-4 ? 1e-4 : solimp[1] > 0.9999 ? 0.9999 : solimp[1];
+  double width = solimp[2] < 1e-12 ? 1e-12 : solimp[2];
+  double mid = solimp[3] < 1e-4 ? 1e-4 : solimp[3] > 0.9999 ? 0.9999 : solimp[3];
+  double power = solimp[4] < 1 ? 1 : solimp[4];
+  *k = tc > 0 ? 1.0 / (dmax * dmax * tc * tc * dr * dr) : -tc / (dmax * dmax);
+  *b = dr > 0 ? 2.0 / (dmax * tc) : -dr / dmax;
+  double x = fabs(pos) / width;
+  if (x >= 1) { *imp = dmax; return; }
+  double y = x < mid ? pow(x, power) / pow(mid, power - 1) : 1 - pow(1 - x, power) / pow(1 - mid, power - 1);
+  double v = dmin + y * (dmax - dmin);
+  *imp = v < dmin ? dmin : v > dmax ? dmax : v;
+}
+
+static int add_row(OData* d, int nv, int type) {
+  int r = d->nefc++;
+  memset(&d->efc_J[r * nv], 0, nv * sizeof(double));
+  d->efc_type[r] = type;
+  d->efc_floss[r] = 0;
+  return r;
+}
+
+static double rowdot(const double* J, const double* v, int nv) {
+  double s = 0;
+  for (int i = 0; i < nv; i++) s += J[i] * v[i];
+  return s;
+}
+
+void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
+  int nv = m->nv;
+  d->nefc = 0;
+  d->nefc_dropped = 0;
+  if (m->disableflags & 1) return;
+  if (!(m->disableflags & (1 << 2))) {
+    for (int i = 0; i < nv; i++) {
+      if (m->dof_frictionloss[i] <= 0) continue;
+      if (d->nefc + 1 > d->nefc_max) { d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+      double k, b, imp;
+      impedance(m, &m->dof_solref[2 * i], &m->dof_solimp[5 * i], 0, &k, &b, &imp);
+      int r = add_row(d, nv, T_FRICTION);
+      d->efc_J[r * nv + i] = 1;
+      double R = (1 - imp) / imp * m->dof_invweight0[i];
+      d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+      d->efc_D[r] = 1 / d->efc_R[r];
+      d->efc_aref[r] = -b * d->qvel[i];
+      d->efc_floss[r] = m->dof_frictionloss[i];
+    }
+  }
+  if (!(m->disableflags & (1 << 3))) {
+    for (int j = 0; j < m->njnt; j++) {
+      if (!m->jnt_limited[j] || (m->jnt_type[j] != 2 && m->jnt_type[j] != 3)) continue;
+      int qa = m->jnt_qposadr[j], da = m->jnt_dofadr[j];
+      for (int side = 0; side < 2; side++) {
+        double dist = side == 0 ? d->qpos[qa] - m->jnt_range[2 * j] : m->jnt_range[2 * j + 1] - d->qpos[qa];
+        double margin = m->jnt_margin[j];
+        if (!(dist < margin)) continue;
+        if (d->nefc + 1 > d->nefc_max) { d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+        double k, b, imp, pos = dist - margin;
+        impedance(m, &m->jnt_solref[2 * j], &m->jnt_solimp[5 * j], pos, &k, &b, &imp);
+        int r = add_row(d, nv, T_LIMIT);
+        double sg = side == 0 ? 1.0 : -1.0;
+        d->efc_J[r * nv + da] = sg;
+        double R = (1 - imp) / imp * m->dof_invweight0[da];
+        d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+        d->efc_D[r] = 1 / d->efc_R[r];
+        d->efc_aref[r] = -b * sg * d->qvel[da] - k * imp * pos;
+      }
+    }
+  }
+  if (m->disableflags & (1 << 4)) return;
+  double* jacp = d->work;           /* 3 nv */
+  double* jacr = d->work + 3 * nv;  /* 3 nv */
+  for (int c = 0; c < d->ncon; c++) {
+    double* con = &d->contact[ORACLE_CONTACT_STRIDE * c];
+    con[19] = -1;
+    double dist = con[12], incl = con[18];
+    if (!(dist < incl)) continue;
+    int pair = (int)con[13];
+    const int* pi = &m->pair_int[6 * pair];
+    const double* pr = &m->pair_real[16 * pair];
+    int dim = pi[4];
+    int nrow = dim == 1 ? 1 : 2 * (dim - 1);
+    if (d->nefc + nrow > d->nefc_max) { d->nefc_dropped += nrow; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+    double fs = (rnd ? rnd->friction_scale : 1.0);
+    double mu[5];
+    for (int k = 0; k < 5; k++) mu[k] = pr[2 + k] * fs;
+    double pos = dist - incl, k, b, imp;
+    impedance(m, pr + 7, pr + 9, pos, &k, &b, &imp);
+    /* Jacobian difference body2 - body1 at the contact point */
+    memset(jacp, 0, 6 * nv * sizeof(double));
+    for (int side = 0; side < 2; side++) {
+      int body = side == 0 ? pi[3] : pi[2];
+      double sg = side == 0 ? 1.0 : -1.0;
+      const double* rc = &d->subtree_com[3 * m->body_rootid[body]];
+      double off[3] = {con[0] - rc[0], con[1] - rc[1], con[2] - rc[2]};
+      for (int i = 0; i < nv; i++) {
+        int db = m->dof_bodyid[i];
+        if (!(db <= body && body < db + m->body_subtreesize[db])) continue;
+        const double* cd = &d->cdof[6 * i];
+        double x[3];
+        o_cross(cd, off, x);
+        for (int a = 0; a < 3; a++) {
+          jacp[a * nv + i] += sg * (cd[3 + a] + x[a]);
+          jacr[a * nv + i] += sg * cd[a];
+        }
+      }
+    }
+    const double* fr = con + 3;  /* n, t1, t2 */
+    con[19] = d->nefc;
+    double* Jn = d->work + 6 * nv;  /* nv */
+    for (int i = 0; i < nv; i++) Jn[i] = fr[0] * jacp[i] + fr[1] * jacp[nv + i] + fr[2] * jacp[2 * nv + i];
+    if (dim == 1) {
+      int r = add_row(d, nv, T_FRICTIONLESS);
+      memcpy(&d->efc_J[r * nv], Jn, nv * sizeof(double));
+      double R = (1 - imp) / imp * pr[14];
+      d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+      d->efc_D[r] = 1 / d->efc_R[r];
+      d->efc_aref[r] = -b * rowdot(Jn, d->qvel, nv) - k * imp * pos;
+      continue;
+    }
+    double mu0 = mu[0];
+    double Rfirst = (1 - imp) / imp * pr[14] * (1 + mu0 * mu0);
+    if (Rfirst < O_MINVAL) Rfirst = O_MINVAL;
+    double Rpy = 2 * mu0 * mu0 / m->impratio * Rfirst;
+    if (Rpy < O_MINVAL) Rpy = O_MINVAL;
+    for (int dir = 0; dir < dim - 1; dir++) {
+      /* directions: t1, t2 (translation), n (spin), t1, t2 (rolling) */
+      const double* ax = dir == 0 || dir == 3 ? fr + 3 : dir == 1 || dir == 4 ? fr + 6 : fr;
+      const double* src = dir < 2 ? jacp : jacr;
+      for (int sgi = 0; sgi < 2; sgi++) {
+        double sg = sgi == 0 ? 1.0 : -1.0;
+        int r = add_row(d, nv, T_PYRAMID);
+        double* J = &d->efc_J[r * nv];
+        for (int i = 0; i < nv; i++) {
+          double jt = ax[0] * src[i] + ax[1] * src[nv + i] + ax[2] * src[2 * nv + i];
+          J[i] = Jn[i] + sg * mu[dir] * jt;
+        }
+        d->efc_R[r] = Rpy;
+        d->efc_D[r] = 1 / Rpy;
+        d->efc_aref[r] = -b * rowdot(J, d->qvel, nv) - k * imp * pos;
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ Newton */
+
+/* row cost s(y) and force -s'(y) */
+static double row_cost(int type, double D, double fl, double y) {
+  if (type == T_FRICTION) {
+    double R = 1 / D;
+    if (fabs(y) < fl * R) return 0.5 * D * y * y;
+    return fl * fabs(y) - 0.5 * fl * fl * R;
+  }
+  return y < 0 ? 0.5 * D * y * y : 0;
+}
+static double row_force(int type, double D, double fl, double y) {
+  if (type == T_FRICTION) {
+    double f = -D * y;
+    return f > fl ? fl : f < -fl ? -fl : f;
+  }
+  return y < 0 ? -D * y : 0;
+}
+static int row_quadratic(int type, double D, double fl, double y) {
+  if (type == T_FRICTION) return fabs(y) < fl / D;
+  return y < 0;
+}
+/* s(y + dy) - s(y), written to keep precision when dy is small */
+static double row_cost_delta(int type, double D, double fl, double y, double dy) {
+  int q0 = row_quadratic(type, D, fl, y), q1 = row_quadratic(type, D, fl, y + dy);
+  if (q0 && q1) return 0.5 * D * dy * (2 * y + dy);
+  if (type != T_FRICTION && !q0 && !q1) return 0;
+  if (type == T_FRICTION && !q0 && !q1 && (y > 0) == (y + dy > 0)) return fl * (fabs(y + dy) - fabs(y));
+  return row_cost(type, D, fl, y + dy) - row_cost(type, D, fl, y);
+}
+
+typedef struct {
+  int nv, nefc;
+  const double *M, *qfrc_smooth, *qacc_smooth, *J, *aref, *D, *floss;
+  const int* type;
+} Prob;
+
+/* total cost at x; fills y (jar), force, Ma, grad */
+static double eval_point(const Prob* P, const double* x, double* y, double* force, double* Ma, double* grad) {
+  int nv = P->nv;
+  double cost = 0;
+  for (int i = 0; i < nv; i++) {
+    double s = 0;
+    for (int j = 0; j < nv; j++) s += P->M[i * nv + j] * x[j];
+    Ma[i] = s;
+  }
+  /* Gauss term 0.5 (x - a0)' M (x - a0) = 0.5 x'Mx - x' f + 0.5 a0' f */
+  for (int i = 0; i < nv; i++) cost += 0.5 * x[i] * Ma[i] - x[i] * P->qfrc_smooth[i] + 0.5 * P->qacc_smooth[i] * P->qfrc_smooth[i];
+  for (int r = 0; r < P->nefc; r++) {
+    y[r] = rowdot(&P->J[r * nv], x, nv) - P->aref[r];
+    force[r] = row_force(P->type[r], P->D[r], P->floss[r], y[r]);
+    cost += row_cost(P->type[r], P->D[r], P->floss[r], y[r]);
+  }
+  for (int i = 0; i < nv; i++) {
+    double s = Ma[i] - P->qfrc_smooth[i];
+    for (int r = 0; r < P->nefc; r++) s -= P->J[r * nv + i] * force[r];
+    grad[i] = s;
+  }
+  return cost;
+}
+
+/* f'(a), f''(a) of the cost along p from the current point */
+static void ls_deriv(const Prob* P, double A, double B, const double* y, const double* q, double a, double* d1, double* d2) {
+  double g1 = a * A + B, g2 = A;
+  for (int r = 0; r < P->nefc; r++) {
+    double yr = y[r] + a * q[r];
+    double f = row_force(P->type[r], P->D[r], P->floss[r], yr);
+    g1 -= q[r] * f;
+    if (row_quadratic(P->type[r], P->D[r], P->floss[r], yr)) g2 += P->D[r] * q[r] * q[r];
+  }
+  *d1 = g1;
+  *d2 = g2;
+}
+
+/* exact minimiser of the piecewise-quadratic cost along p (safeguarded Newton
+ * on the monotone derivative); returns alpha and the cost change */
+static double linesearch(const Prob* P, const double* y, const double* q, double A, double B, int maxit, double* dcost) {
+  double d0, h0;
+  ls_deriv(P, A, B, y, q, 0, &d0, &h0);
+  *dcost = 0;
+  if (!(d0 < 0)) return 0;
+  double lo = 0, dlo = d0, hi = -1, dhi = 0;
+  double a = -d0 / h0;
+  for (int it = 0; it < maxit; it++) {
+    double dd, hh;
+    ls_deriv(P, A, B, y, q, a, &dd, &hh);
+    if (dd < 0) { lo = a; dlo = dd; } else { hi = a; dhi = dd; }
+    if (fabs(dd) <= 1e-10 * fabs(d0)) break;
+    double an = a - dd / hh;
+    if (hi >= 0 && !(an > lo && an < hi)) {
+      an = (dlo * hi - dhi * lo) / (dlo - dhi);
+      if (!(an > lo && an < hi)) an = 0.5 * (lo + hi);
+    }
+    if (fabs(an - a) <= 1e-12 * fabs(a)) { a = an; break; }
+    a = an;
+  }
+  double dc = 0.5 * a * a * A + a * B;
+  for (int r = 0; r < P->nefc; r++) dc += row_cost_delta(P->type[r], P->D[r], P->floss[r], y[r], a * q[r]);
+  *dcost = dc;
+  return a;
+}
+
+void oracle_solve(const OModel* m, OData* d, int max_iter) {
+  int nv = m->nv, ne = d->nefc;
+  Prob P = {nv, ne, d->M, d->qfrc_smooth, d->qacc_smooth, d->efc_J, d->efc_aref, d->efc_D, d->efc_floss, d->efc_type};
+  double* w = d->work;
+  double *x = w, *Ma = w + nv, *grad = w + 2 * nv, *p = w + 3 * nv, *Mp = w + 4 * nv, *xc = w + 5 * nv, *tmp = w + 6 * nv;
+  double* H = w + 8 * nv;
+  double* q = H + nv * nv;
+  double* yc = q + d->nefc_max;
+  double* fc = yc + d->nefc_max;
+  double scale = 1.0 / (m->meaninertia * (nv > 1 ? nv : 1));
+  /* warm start: the lowest-cost candidate of smooth / previous / predicted */
+  double best;
+  memcpy(x, d->qacc_smooth, nv * sizeof(double));
+  best = eval_point(&P, x, d->efc_jar, d->efc_force, Ma, grad);
+  d->warm_choice = 0;
+  if (!(m->disableflags & (1 << 8))) {
+    double c = eval_point(&P, d->qacc_warmstart, yc, fc, tmp, tmp + nv);
+    if (c < best) { best = c; memcpy(x, d->qacc_warmstart, nv * sizeof(double)); d->warm_choice = 1; }
+    if (d->qacc_predicted) {
+      double cp = eval_point(&P, d->qacc_predicted, yc, fc, tmp, tmp + nv);
+      if (cp <= best) { best = cp; memcpy(x, d->qacc_predicted, nv * sizeof(double)); d->warm_choice = 2; }
+    }
+  }
+  double cost = eval_point(&P, x, d->efc_jar, d->efc_force, Ma, grad);
+  d->cost_initial = cost;
+  d->niter = 0;
+  double gn = 0;
+  for (int i = 0; i < nv; i++) gn += grad[i] * grad[i];
+  if (ne > 0 && scale * sqrt(gn) >= m->tolerance) {
+    for (int it = 0; it < max_iter; it++) {
+      /* H = M + sum_quadratic D J'J */
+      memcpy(H, d->M, nv * nv * sizeof(double));
+      for (int r = 0; r < ne; r++) {
+        if (!row_quadratic(d->efc_type[r], d->efc_D[r], d->efc_floss[r], d->efc_jar[r])) continue;
+        const double* J = &d->efc_J[r * nv];
+        double Dr = d->efc_D[r];
+        for (int i = 0; i < nv; i++) {
+          if (J[i] == 0) continue;
+          for (int j = 0; j <= i; j++) H[i * nv + j] += Dr * J[i] * J[j];
+        }
+      }
+      for (int i = 0; i < nv; i++)
+        for (int j = i + 1; j < nv; j++) H[i * nv + j] = H[j * nv + i];
+      o_chol(H, nv);
+      for (int i = 0; i < nv; i++) p[i] = -grad[i];
+      o_chol_solve(H, nv, p);
+      double gp = 0;
+      for (int i = 0; i < nv; i++) gp += grad[i] * p[i];
+      if (!(gp < 0)) break;
+      /* line search coefficients */
+      double A = 0, B = 0;
+      for (int i = 0; i < nv; i++) {
+        double s = 0;
+        for (int j = 0; j < nv; j++) s += d->M[i * nv + j] * p[j];
+        Mp[i] = s;
+        A += p[i] * s;
+        B += p[i] * (Ma[i] - d->qfrc_smooth[i]);
+      }
+      for (int r = 0; r < ne; r++) q[r] = rowdot(&d->efc_J[r * nv], p, nv);
+      double dcost;
+      double alpha = linesearch(&P, d->efc_jar, q, A, B, m->ls_iterations, &dcost);
+      d->niter++;
+      if (alpha == 0) break;
+      for (int i = 0; i < nv; i++) x[i] += alpha * p[i];
+      cost = eval_point(&P, x, d->efc_jar, d->efc_force, Ma, grad);
+      double improvement = -scale * dcost;
+      gn = 0;
+      for (int i = 0; i < nv; i++) gn += grad[i] * grad[i];
+      if (improvement < m->tolerance || scale * sqrt(gn) < m->tolerance) break;
+    }
+  }
+  (void)xc;
+  d->cost_final = cost;
+  memcpy(d->qacc, x, nv * sizeof(double));
+  for (int i = 0; i < nv; i++) {
+    double s = 0;
+    for (int r = 0; r < ne; r++) s += d->efc_J[r * nv + i] * d->efc_force[r];
+    d->qfrc_constraint[i] = s;
+  }
+}
+
+void oracle_integrate(const OModel* m, OData* d) {
+  int nv = m->nv;
+  double h = m->timestep;
+  double* acc = d->work;  /* nv */
+  memcpy(acc, d->qacc, nv * sizeof(double));
+  /* implicit damping: (M + h D) qacc = qfrc_smooth + qfrc_constraint */
+  int implicit = 0;
+  double* damp = d->work + nv;
+  for (int i = 0; i < nv; i++) damp[i] = m->dof_damping[i];
+  if (m->integrator == 2 || m->integrator == 3) {
+    for (int a = 0; a < m->nu; a++) {
+      if (!m->actuator_biastype[a]) continue;
+      double gv = m->actuator_gaintype[a] ? m->actuator_gainprm[3 * a + 2] : 0;
+      double bv = m->actuator_biasprm[3 * a + 2];
+      if (gv != 0 || bv == 0) continue;
+      double g = m->actuator_gear[a];
+      damp[m->jnt_dofadr[m->actuator_trnid[a]]] += -bv * g * g;
+    }
+  } else if (m->disableflags & (1 << 15)) {
+    for (int i = 0; i < nv; i++) damp[i] = 0;
+  }
+  for (int i = 0; i < nv; i++)
+    if (damp[i] != 0) implicit = 1;
+  if (implicit) {
+    double* Md = d->work + 2 * nv;
+    memcpy(Md, d->M, nv * nv * sizeof(double));
+    for (int i = 0; i < nv; i++) Md[i * nv + i] += h * damp[i];
+    o_chol(Md, nv);
+    for (int i = 0; i < nv; i++) acc[i] = d->qfrc_smooth[i] + d->qfrc_constraint[i];
+    o_chol_solve(Md, nv, acc);
+  }
+  for (int i = 0; i < nv; i++) d->qvel[i] += h * acc[i];
+  for (int j = 0; j < m->njnt; j++) {
+    int qa = m->jnt_qposadr[j], da = m->jnt_dofadr[j], t = m->jnt_type[j];
+    double* q = d->qpos + qa;
+    const double* v = d->qvel + da;
+    if (t == 2 || t == 3) { q[0] += h * v[0]; continue; }
+    const double* w = v;
+    double* qq = q;
+    if (t == 0) {
+      for (int k = 0; k < 3; k++) q[k] += h * v[k];
+      w = v + 3;
+      qq = q + 3;
+    }
+    double wn = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    double ha = 0.5 * h * wn;
+    double s = wn > 1e-12 ? sin(ha) / wn : 0.5 * h;
+    double dq[4] = {cos(ha), s * w[0], s * w[1], s * w[2]};
+    o_quat_mul(qq, dq, qq);
+    o_quat_normalize(qq);
+  }
+}
+
+static int bad(double x) { return !(fabs(x) <= 1e10); }
+
+static void reset_env(const OModel* m, OData* d) {
+  memcpy(d->qpos, m->qpos0, m->nq * sizeof(double));
+  memset(d->qvel, 0, m->nv * sizeof(double));
+  memset(d->qacc_warmstart, 0, m->nv * sizeof(double));
+}
+
+void oracle_step(const OModel* m, OData* d, const ORand* r, int max_iter) {
+  if (max_iter <= 0) max_iter = m->iterations;
+  d->status = 0;
+  for (int i = 0; i < m->nq; i++)
+    if (bad(d->qpos[i])) { reset_env(m, d); d->status |= ORACLE_BADSTATE; break; }
+  for (int i = 0; i < m->nv; i++)
+    if (bad(d->qvel[i])) { reset_env(m, d); d->status |= ORACLE_BADSTATE; break; }
+  oracle_kinematics(m, d);
+  oracle_com(m, d, r);
+  oracle_crb(m, d, r);
+  oracle_rne(m, d, r);
+  oracle_smooth_forces(m, d, r);
+  oracle_collide(m, d);
+  oracle_make_constraints(m, d, r);
+  oracle_solve(m, d, max_iter);
+  for (int i = 0; i < m->nv; i++)
+    if (bad(d->qacc[i])) {
+      reset_env(m, d);
+      memset(d->qacc, 0, m->nv * sizeof(double));
+      d->status |= ORACLE_BADQACC;
+      return;
+    }
+  memcpy(d->qacc_warmstart, d->qacc, m->nv * sizeof(double));
+  oracle_integrate(m, d);
+}
+
+typedef struct {
+  const OModel* m;
+  OData* const* d;
+  int B, nsub, max_iter, tid, nthread;
+} Job;
+
+static void* worker(void* arg) {
+  Job* j = (Job*)arg;
+  for (int e = j->tid; e < j->B; e += j->nthread)
+    for (int s = 0; s < j->nsub; s++) oracle_step(j->m, j->d[e], NULL, j->max_iter);
+  return NULL;
+}
+
+void oracle_step_batch(const OModel* m, OData* const* d, int B, int nsub, int max_iter, int nthread) {
+  if (nthread < 1) nthread = 1;
+  if (nthread > B) nthread = B;
+  pthread_t th[256];
+  Job jobs[256];
+  if (nthread > 256) nthread = 256;
+  for (int t = 0; t < nthread; t++) {
+    jobs[t] = (Job){m, d, B, nsub, max_iter, t, nthread};
+    if (t > 0) pthread_create(&th[t], NULL, worker, &jobs[t]);
+  }
+  worker(&jobs[0]);
+  for (int t = 1; t < nthread; t++) pthread_join(th[t], NULL);
+}
