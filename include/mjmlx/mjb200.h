@@ -29,6 +29,72 @@ MJMLX_API int mjb200_model_dump(const MjmlxModel* model, char* buf, int bufsize)
 /* Last error message of the calling thread ("" if none). */
 MJMLX_API const char* mjb200_last_error(void);
 
+/* ------------------------------------------------------ engine configuration */
+
+typedef struct MjbEngineConfig {
+    int warps_per_block;   /* envs per CTA (one warp each); 0 = default */
+    int persistent;        /* -1 auto, 0 one warp per env, 1 persistent work queue */
+    int blocks_per_sm;     /* persistent grid size per SM; 0 = occupancy limit */
+    int ncon_max;          /* per-env contact capacity; 0 = automatic */
+    int nefc_max;          /* per-env constraint-row capacity; 0 = automatic */
+    int use_graph;         /* replay launches from captured CUDA graphs */
+    int record;            /* write xpos/xquat/cvel/cinert/... on the last substep */
+    int warmstart;         /* 0 previous-step qacc (MuJoCo), 1 learned prediction with fallback */
+    double tolerance;      /* > 0 overrides the model's solver tolerance */
+    int max_iter;          /* > 0 overrides the Newton iteration cap */
+    int lockstep;          /* 1: the warps of a CTA run each stage together */
+} MjbEngineConfig;
+
+/* Defaults of MjbEngineConfig. */
+MJMLX_API MjbEngineConfig mjb200_default_engine_config(void);
+
+/* Mixed-model batch: counts[i] envs of models[i], stored model by model
+ * (env-major records of varying size; see mjb200_batched_layout).  All envs
+ * step in one launch.  ecfg may be NULL.  NULL + stderr on failure. */
+MJMLX_API MjmlxBatchedSim* mjb200_batched_create_multi(const MjmlxModel* const* models, const int* counts, int nmodels,
+                                                       const MjmlxBatchedConfig* config, const MjbEngineConfig* ecfg);
+MJMLX_API int mjb200_batched_configure(MjmlxBatchedSim* sim, const MjbEngineConfig* ecfg);
+MJMLX_API int mjb200_batched_get_config(const MjmlxBatchedSim* sim, MjbEngineConfig* out);
+
+/* Record layout: num_envs, sum of nq / nv / nu over envs, and the per-env
+ * offsets (arrays of num_envs, each may be NULL). */
+MJMLX_API int mjb200_batched_layout(const MjmlxBatchedSim* sim, int* num_envs, int* total_q, int* total_v, int* total_u,
+                                    int* qadr, int* vadr, int* uadr);
+
+/* n physics steps with the controls already in device memory (no host copy). */
+MJMLX_API int mjb200_batched_step_device(MjmlxBatchedSim* sim, int n);
+/* Device pointers of the HBM-resident state (float, env-major records). */
+MJMLX_API int mjb200_batched_device_state(MjmlxBatchedSim* sim, float** qpos, float** qvel, float** ctrl, float** qacc_warmstart);
+/* The CUDA stream (cudaStream_t) every launch of the sim is ordered on. */
+MJMLX_API void* mjb200_batched_stream(MjmlxBatchedSim* sim);
+/* Launch shape chosen for the step kernel. */
+MJMLX_API int mjb200_batched_launch_shape(const MjmlxBatchedSim* sim, int* grid, int* warps_per_block, int* smem_bytes, int* persistent);
+
+/* Per-env statistics of the last step call (arrays of num_envs, each may be
+ * NULL): status bits (1 bad state reset, 2 bad acceleration reset, 4 contact
+ * overflow, 8 constraint-row overflow, 16 unsupported pair), Newton
+ * iterations summed / maximum over the substeps, contacts and rows of the
+ * last substep, warm-start choice (0 smooth, 1 previous, 2 predicted). */
+MJMLX_API int mjb200_batched_stats(MjmlxBatchedSim* sim, int* status, int* niter_sum, int* niter_max, int* ncon, int* nefc, int* warm_choice);
+
+/* Solver acceleration qacc of the last substep, float[total_v]. */
+MJMLX_API const float* mjb200_batched_get_qacc(MjmlxBatchedSim* sim, int* n_out);
+
+/* Capture contacts / constraint rows / solver vectors of the last substep.
+ * set_debug(ncon_max, nefc_max) enables capture (0 disables); get_debug fills
+ * contacts[num_envs*ncon_max*16] (pos3 frame9 dist pair dim includemargin),
+ * efc[num_envs*nefc_max*4] (type force D aref), vec[num_envs*4*nv_max]
+ * (qacc_smooth, qfrc_smooth, qacc, qfrc_constraint); returns nv_max. */
+/* Per-stage SM clock totals of the lockstep step kernel (8 stages: state check
+ * + kinematics, collision, COM + CRB, RNE + forces, unconstrained solve,
+ * constraint build, Newton, integration).  enable 1 starts (and zeroes) the
+ * counters, 0 stops them, -1 leaves them; cycles8 (may be NULL) receives the
+ * totals accumulated so far.  Returns 0 / -1. */
+MJMLX_API int mjb200_batched_stage_timing(MjmlxBatchedSim* sim, int enable, unsigned long long* cycles8);
+
+MJMLX_API int mjb200_batched_set_debug(MjmlxBatchedSim* sim, int ncon_max, int nefc_max);
+MJMLX_API int mjb200_batched_get_debug(MjmlxBatchedSim* sim, float* contacts, float* efc, float* vec);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,622 @@
+// Constraint rows, Newton solve and Euler integration for one env per warp.
+//   d_constraints <- solver.hpp:259-587 (rows: frictionloss -> limits ->
+//                    contacts; impedance efc_kbi :122-138; pyramid rows with
+//                    R = 2 mu0^2/impratio * R_first :536-571)
+//   d_newton      <- solver.hpp:592-854 (H = M + J'DJ, shared-memory Cholesky
+//                    :743-785), with previous-step / predicted warm start,
+//                    exact line search and tolerance-scaled termination
+//   d_integrate   <- euler.hpp:26-110, batched.cpp:712-745 (implicit damping)
+// Rows are added in order; the first row group that does not fit in
+// nefc_max is dropped together with every later group (status bit set).
+#pragma once
+#include "dev_stages.cuh"
+
+namespace mjbdev {
+
+// Cholesky of the n x n matrix A (row-major, in place, lower triangle = L).
+__device__ __noinline__ void d_chol(float* A, int n, int lane) {
+  #pragma unroll 1
+  for (int j = 0; j < n; j++) {
+    float s = A[j * n + j];
+    #pragma unroll 1
+    for (int k = 0; k < j; k++) s -= A[j * n + k] * A[j * n + k];
+    float d = sqrtf(fmaxf(s, 1e-30f));
+    float id = 1.f / d;
+    __syncwarp();
+    #pragma unroll 1
+    for (int i = j + 1 + lane; i < n; i += 32) {
+      float t = A[i * n + j];
+      #pragma unroll 1
+      for (int k = 0; k < j; k++) t -= A[i * n + k] * A[j * n + k];
+      A[i * n + j] = t * id;
+    }
+    if (lane == 0) A[j * n + j] = d;
+    __syncwarp();
+  }
+}
+
+// x := (L L')^-1 x
+__device__ __noinline__ void d_chol_solve(const float* L, int n, float* x, int lane) {
+  #pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    float xk = x[k] / L[k * n + k];
+    __syncwarp();
+    #pragma unroll 1
+    for (int i = k + 1 + lane; i < n; i += 32) x[i] -= L[i * n + k] * xk;
+    if (lane == 0) x[k] = xk;
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    float xk = x[k] / L[k * n + k];
+    __syncwarp();
+    #pragma unroll 1
+    for (int i = lane; i < k; i += 32) x[i] -= L[k * n + i] * xk;
+    if (lane == 0) x[k] = xk;
+    __syncwarp();
+  }
+}
+
+__device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
+  float tc = sr0, dr = sr1;
+  if (!(m.disableflags & (1 << 11)) && tc > 0 && tc < 2 * m.timestep) tc = 2 * m.timestep;
+  float dmin = clampf(si[0], 1e-4f, 0.9999f), dmax = clampf(si[1], 1e-4f, 0.9999f);
+  float width = fmaxf(si[2], 1e-12f), mid = clampf(si[3], 1e-4f, 0.9999f), power = fmaxf(si[4], 1.f);
+  k = tc > 0 ? 1.f / (dmax * dmax * tc * tc * dr * dr) : -tc / (dmax * dmax);
+  b = dr > 0 ? 2.f / (dmax * tc) : -dr / dmax;
+  float x = fabsf(pos) / width;
+  if (x >= 1.f) { imp = dmax; return; }
+  float y = x < mid ? powf(x, power) / powf(mid, power - 1.f) : 1.f - powf(1.f - x, power) / powf(1.f - mid, power - 1.f);
+  imp = clampf(dmin + y * (dmax - dmin), dmin, dmax);
+}
+
+__device__ __forceinline__ int rows_of(float dim) { int d = (int)dim; return d == 1 ? 1 : 2 * (d - 1); }
+
+// Builds efc rows; returns nefc.  Row metadata: EFC_AREF (b during the
+// build), EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y (k*imp*pos during the build),
+// EFC_CON (contact index or -1).
+__device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  const int nv = m.nv;
+  float* J = ws + m.w_J;
+  float* efc = ws + m.w_efc;
+  const int ne = m.nefc_max;
+  const float* qpos = ws + m.w_qpos;
+  const float* qvel = ws + m.w_qvel;
+  float* con = ws + m.w_con;
+  int nefc = 0;
+  bool stop = false;
+  if (m.disableflags & 1) return 0;
+  // --- frictionloss rows (static list)
+  if (!(m.disableflags & (1 << 2)) && m.nfloss > 0) {
+    int nf = m.nfloss;
+    if (nf > m.nefc_max) { nf = m.nefc_max; stop = true; }
+    #pragma unroll 1
+    for (int r = E.lane; r < nf; r += 32) {
+      int dof = ldi(it, m.i_floss + r);
+      const float* f = ft + m.f_floss + 8 * r;
+      float si[5] = {ldf(f, 3), ldf(f, 4), ldf(f, 5), ldf(f, 6), ldf(f, 7)};
+      float k, b, imp;
+      impedance(m, ldf(f, 1), ldf(f, 2), si, 0.f, k, b, imp);
+      float R = fmaxf((1.f - imp) / imp * ldf(ft, m.f_dof_invweight0 + dof), 1e-15f);
+      #pragma unroll 1
+      for (int c = 0; c < nv; c++) J[r * nv + c] = c == dof ? 1.f : 0.f;
+      EfcRef e{efc + r, ne};
+      e[EFC_D] = 1.f / R;
+      e[EFC_AREF] = -b * qvel[dof];
+      e[EFC_FLOSS] = ldf(f, 0);
+      e[EFC_TYPE] = ROW_FRICTION;
+      e[EFC_CON] = -1;
+    }
+    nefc = nf;
+  }
+  // --- joint limit rows (lower then upper side, joint order)
+  if (!stop && !(m.disableflags & (1 << 3))) {
+    #pragma unroll 1
+    for (int base = 0; base < m.nlimit; base += 32) {
+      int li = base + E.lane;
+      int act[2] = {0, 0};
+      float dist[2] = {0, 0};
+      if (li < m.nlimit) {
+        int qa = ldi(it, m.i_limit + 3 * li + 2);
+        const float* f = ft + m.f_limit + 10 * li;
+        float q = qpos[qa];
+        dist[0] = q - ldf(f, 0);
+        dist[1] = ldf(f, 1) - q;
+        float margin = ldf(f, 2);
+        act[0] = dist[0] < margin;
+        act[1] = dist[1] < margin;
+      }
+      int cnt = act[0] + act[1];
+      int incl = warp_incl_scan(cnt, E.lane);
+      int total = __shfl_sync(FULL_MASK, incl, 31);
+      int r = nefc + incl - cnt;
+      for (int s = 0; s < 2; s++) {
+        if (!act[s]) continue;
+        if (r >= m.nefc_max) break;
+        int dof = ldi(it, m.i_limit + 3 * li + 1);
+        const float* f = ft + m.f_limit + 10 * li;
+        float si[5] = {ldf(f, 5), ldf(f, 6), ldf(f, 7), ldf(f, 8), ldf(f, 9)};
+        float pos = dist[s] - ldf(f, 2), k, b, imp;
+        impedance(m, ldf(f, 3), ldf(f, 4), si, pos, k, b, imp);
+        float sg = s == 0 ? 1.f : -1.f;
+        #pragma unroll 1
+        for (int c = 0; c < nv; c++) J[r * nv + c] = c == dof ? sg : 0.f;
+        float R = fmaxf((1.f - imp) / imp * ldf(ft, m.f_dof_invweight0 + dof), 1e-15f);
+        EfcRef e{efc + r, ne};
+        e[EFC_D] = 1.f / R;
+        e[EFC_AREF] = -b * sg * qvel[dof] - k * imp * pos;
+        e[EFC_FLOSS] = 0;
+        e[EFC_TYPE] = ROW_LIMIT;
+        e[EFC_CON] = -1;
+        r++;
+      }
+      nefc += total;
+      if (nefc > m.nefc_max) { nefc = m.nefc_max; stop = true; break; }
+    }
+  }
+  // --- contact rows: offsets by scan, then per-contact impedance, then J by dof lanes
+  int row0 = nefc;
+  if (!stop && !(m.disableflags & (1 << 4))) {
+    #pragma unroll 1
+    for (int base = 0; base < ncon; base += 32) {
+      int c = base + E.lane;
+      int nr = 0;
+      float* cr = con + MJB_CONTACT_FLOATS * (c < ncon ? c : 0);
+      if (c < ncon) nr = (cr[12] < cr[15]) ? rows_of(cr[14]) : 0;
+      int incl = warp_incl_scan(nr, E.lane);
+      int total = __shfl_sync(FULL_MASK, incl, 31);
+      int r0 = nefc + incl - nr;
+      bool fits = r0 + nr <= m.nefc_max;
+      unsigned bad = __ballot_sync(FULL_MASK, nr > 0 && !fits);
+      if (bad) {
+        // drop the first group that does not fit and every later contact
+        int first = __ffs(bad) - 1;
+        int keep_rows = __shfl_sync(FULL_MASK, r0, first) - nefc;
+        if (c < ncon && E.lane >= first) nr = 0;
+        total = keep_rows;
+        stop = true;
+      }
+      if (c < ncon && nr > 0) {
+        int p = (int)cr[13];
+        const float* pf = ft + m.f_pair + 16 * p;
+        float si[5] = {ldf(pf, 9), ldf(pf, 10), ldf(pf, 11), ldf(pf, 12), ldf(pf, 13)};
+        float pos = cr[12] - cr[15], k, b, imp;
+        impedance(m, ldf(pf, 7), ldf(pf, 8), si, pos, k, b, imp);
+        float invw = ldf(pf, 14);
+        int dim = (int)cr[14];
+        float D;
+        if (dim == 1) {
+          D = 1.f / fmaxf((1.f - imp) / imp * invw, 1e-15f);
+        } else {
+          float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
+          float mu0 = ldf(pf, 2) * fs;
+          float Rf = fmaxf((1.f - imp) / imp * invw * (1.f + mu0 * mu0), 1e-15f);
+          D = 1.f / fmaxf(2.f * mu0 * mu0 / m.impratio * Rf, 1e-15f);
+        }
+        #pragma unroll 1
+        for (int q = 0; q < nr; q++) {
+          EfcRef e{efc + r0 + q, ne};
+          e[EFC_D] = D;
+          e[EFC_AREF] = b;
+          e[EFC_Y] = k * imp * pos;
+          e[EFC_FLOSS] = 0;
+          e[EFC_TYPE] = dim == 1 ? ROW_FRICTIONLESS : ROW_PYRAMID;
+          e[EFC_CON] = (float)c;
+        }
+      }
+      nefc += total;
+      if (stop) break;
+    }
+  }
+  if (stop) E.status |= MJB_STATUS_EFC_OVERFLOW;
+  __syncwarp();
+  // Jacobian rows of the contacts: one lane per dof
+  if (nefc > row0) {
+    const float* scom = ws + m.w_scom;
+    const float* cdof = ws + m.w_cdof;
+    #pragma unroll 1
+    for (int i = E.lane; i < nv; i += 32) {
+      int db = ldi(it, m.i_dof_bodyid + i);
+      int dsub = ldi(it, m.i_body_subtreesize + db);
+      const float* cd = cdof + 6 * i;
+      int r = row0;
+      #pragma unroll 1
+      for (int c = 0; c < ncon && r < nefc; c++) {
+        const float* cr = con + MJB_CONTACT_FLOATS * c;
+        if (!(cr[12] < cr[15])) continue;
+        int p = (int)cr[13];
+        int b1 = ldi(it, m.i_pair + 6 * p + 2), b2 = ldi(it, m.i_pair + 6 * p + 3);
+        float jp[3] = {0, 0, 0}, jr[3] = {0, 0, 0};
+        for (int side = 0; side < 2; side++) {
+          int body = side == 0 ? b2 : b1;
+          if (!(db <= body && body < db + dsub)) continue;
+          float sg = side == 0 ? 1.f : -1.f;
+          int root = ldi(it, m.i_body_rootid + body);
+          float off[3] = {cr[0] - scom[3 * root], cr[1] - scom[3 * root + 1], cr[2] - scom[3 * root + 2]}, x[3];
+          cross3(cd, off, x);
+          for (int a = 0; a < 3; a++) { jp[a] += sg * (cd[3 + a] + x[a]); jr[a] += sg * cd[a]; }
+        }
+        const float* fr = cr + 3;
+        float jn = fr[0] * jp[0] + fr[1] * jp[1] + fr[2] * jp[2];
+        int dim = (int)cr[14];
+        if (dim == 1) {
+          J[r * nv + i] = jn;
+          r++;
+          continue;
+        }
+        float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
+        const float* pf = ft + m.f_pair + 16 * p;
+        #pragma unroll 1
+        for (int dir = 0; dir < dim - 1; dir++) {
+          const float* ax = (dir == 0 || dir == 3) ? fr + 3 : (dir == 1 || dir == 4) ? fr + 6 : fr;
+          const float* src = dir < 2 ? jp : jr;
+          float jt = ax[0] * src[0] + ax[1] * src[1] + ax[2] * src[2];
+          float mu = ldf(pf, 2 + dir) * fs;
+          J[r * nv + i] = jn + mu * jt;
+          J[(r + 1) * nv + i] = jn - mu * jt;
+          r += 2;
+        }
+      }
+    }
+    __syncwarp();
+    // reference acceleration: aref = -b J v - k imp pos
+    #pragma unroll 1
+    for (int r = row0 + E.lane; r < nefc; r += 32) {
+      float jv = 0;
+      #pragma unroll 1
+      for (int c = 0; c < nv; c++) jv += J[r * nv + c] * qvel[c];
+      EfcRef e{efc + r, ne};
+      e[EFC_AREF] = -e[EFC_AREF] * jv - e[EFC_Y];
+    }
+    __syncwarp();
+  }
+  return nefc;
+}
+
+// ------------------------------------------------------------ Newton solver
+__device__ __forceinline__ bool row_quad(int type, float D, float fl, float y) {
+  if (type == ROW_FRICTION) return fabsf(y) < fl / D;
+  return y < 0.f;
+}
+__device__ __forceinline__ float row_force(int type, float D, float fl, float y) {
+  if (type == ROW_FRICTION) return clampf(-D * y, -fl, fl);
+  return y < 0.f ? -D * y : 0.f;
+}
+__device__ __forceinline__ float row_cost(int type, float D, float fl, float y) {
+  if (type == ROW_FRICTION) {
+    float R = 1.f / D;
+    if (fabsf(y) < fl * R) return 0.5f * D * y * y;
+    return fl * fabsf(y) - 0.5f * fl * fl * R;
+  }
+  return y < 0.f ? 0.5f * D * y * y : 0.f;
+}
+__device__ __forceinline__ float row_cost_delta(int type, float D, float fl, float y, float dy) {
+  bool q0 = row_quad(type, D, fl, y), q1 = row_quad(type, D, fl, y + dy);
+  if (q0 && q1) return 0.5f * D * dy * (2.f * y + dy);
+  if (type != ROW_FRICTION && !q0 && !q1) return 0.f;
+  if (type == ROW_FRICTION && !q0 && !q1 && ((y > 0) == (y + dy > 0))) return fl * (fabsf(y + dy) - fabsf(y));
+  return row_cost(type, D, fl, y + dy) - row_cost(type, D, fl, y);
+}
+
+// Cost of candidate x (Gauss term 0.5 d'M d with d = x - qacc_smooth, plus
+// row costs).  `tmp` is nv floats of scratch.  Warp-uniform result.
+__device__ __noinline__ float d_cost(Env& E, int nefc, const float* x, float* tmp) {
+  const DevModelDesc& m = *E.md;
+  const int nv = m.nv, ne = m.nefc_max, lane = E.lane;
+  const float* __restrict__ M = E.ws + m.w_M;
+  const float* __restrict__ qas = E.ws + m.w_qas;
+  const float* __restrict__ J = E.ws + m.w_J;
+  float* efc = E.ws + m.w_efc;
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) tmp[i] = x[i] - qas[i];
+  __syncwarp();
+  float c = 0;
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) {
+    float s = 0;
+    #pragma unroll 1
+    for (int j = 0; j < nv; j++) s += M[i * nv + j] * tmp[j];
+    c += 0.5f * tmp[i] * s;
+  }
+  #pragma unroll 1
+  for (int r = lane; r < nefc; r += 32) {
+    const EfcRef e{efc + r, ne};
+    float y = -e[EFC_AREF];
+    #pragma unroll 1
+    for (int j = 0; j < nv; j++) y += J[r * nv + j] * x[j];
+    c += row_cost((int)e[EFC_TYPE], e[EFC_D], e[EFC_FLOSS], y);
+  }
+  __syncwarp();
+  return warp_sum(c);
+}
+
+// g = Md - J'force; returns ||g||^2 and the magnitude of the summed terms
+// (||Md||^2 + ||J'force||^2) that sets the FP32 round-off floor of g.
+__device__ __forceinline__ float grad_update(const float* J, const float* force, const float* Md, float* grad, int nv, int nefc, int lane, float& terms) {
+  float gn = 0, tn = 0;
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) {
+    float f = 0;
+    #pragma unroll 1
+    for (int r = 0; r < nefc; r++) f += J[r * nv + i] * force[r];
+    float g = Md[i] - f;
+    grad[i] = g;
+    gn += g * g;
+    tn += Md[i] * Md[i] + f * f;
+  }
+  terms = warp_sum(tn);
+  return warp_sum(gn);
+}
+
+// Newton solve from the warm start; x (w_x) holds the result.  Returns the
+// iteration count.  vec: Md, grad, p, Mp, tmp (5 nv).
+// The Hessian factor is rebuilt only when the set of rows in their quadratic
+// zone changed since the last factorisation.  Termination: improvement or
+// gradient below tolerance * meaninertia * nv, where the gradient test also
+// accepts the FP32 round-off floor of the gradient (16 eps times the norm of
+// the terms it is summed from) -- below that floor FP32 cannot resolve it.
+__device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int max_iter, const float* xpred, int& choice) {
+  (void)P;
+  const DevModelDesc& m = *E.md;
+  const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations, i_tri = m.i_tri;
+  float* ws = E.ws;
+  const float* __restrict__ M = ws + m.w_M;
+  const float* __restrict__ qas = ws + m.w_qas;
+  const float* __restrict__ J = ws + m.w_J;
+  float* efc = ws + m.w_efc;
+  float* H = ws + m.w_H;
+  float* x = ws + m.w_x;
+  const float* xw = ws + m.w_xwarm;
+  float* vec = ws + m.w_vec;
+  float *Md = vec, *grad = vec + nv, *p = vec + 2 * nv, *Mp = vec + 3 * nv, *tmp = vec + 4 * nv;
+  float* eY = efc + EFC_Y * ne;
+  float* eF = efc + EFC_FORCE * ne;
+  float* eQ = efc + EFC_Q * ne;
+  const float* eD = efc + EFC_D * ne;
+  const float* eA = efc + EFC_AREF * ne;
+  const float* eL = efc + EFC_FLOSS * ne;
+  const float* eT = efc + EFC_TYPE * ne;
+  const float scale = m.scale, tol = m.tolerance;
+  const int* it = E.it;
+
+  // warm start: lowest cost of smooth / previous / predicted
+  choice = 0;
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) x[i] = qas[i];
+  __syncwarp();
+  if (!(m.disableflags & (1 << 8)) && nefc > 0) {
+    float best = d_cost(E, nefc, qas, tmp);
+    float cw = d_cost(E, nefc, xw, tmp);
+    if (cw < best) { best = cw; choice = 1; }
+    if (xpred) {
+      float cp = d_cost(E, nefc, xpred, tmp);
+      if (cp <= best) { best = cp; choice = 2; }
+    }
+    const float* src = choice == 1 ? xw : choice == 2 ? xpred : qas;
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) x[i] = src[i];
+    __syncwarp();
+  } else if (!(m.disableflags & (1 << 8)) && xpred) {
+    choice = 2;
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) x[i] = qas[i];
+    __syncwarp();
+  }
+  // state at x: d = x - a0, Md, y, force, grad
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) tmp[i] = x[i] - qas[i];
+  __syncwarp();
+  #pragma unroll 1
+  for (int i = lane; i < nv; i += 32) {
+    float s = 0;
+    #pragma unroll 1
+    for (int j = 0; j < nv; j++) s += M[i * nv + j] * tmp[j];
+    Md[i] = s;
+  }
+  #pragma unroll 1
+  for (int r = lane; r < nefc; r += 32) {
+    float y = -eA[r];
+    #pragma unroll 1
+    for (int j = 0; j < nv; j++) y += J[r * nv + j] * x[j];
+    eY[r] = y;
+    eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
+  }
+  __syncwarp();
+  float terms;
+  float gn = grad_update(J, eF, Md, grad, nv, nefc, lane, terms);
+  __syncwarp();
+  const float eps_floor = 16.f * 1.1920929e-7f;
+  if (nefc == 0 || scale * sqrtf(gn) < tol || gn <= eps_floor * eps_floor * terms) return 0;
+  const int ntri = nv * (nv + 1) / 2;
+  const int nwords = (nefc + 31) >> 5;
+  unsigned act_prev[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};  // impossible pattern: forces the first build
+  bool have_factor = false;
+  int niter = 0;
+  #pragma unroll 1
+  for (int iter = 0; iter < max_iter; iter++) {
+    // active (quadratic-zone) pattern of the rows; nefc <= 128 uses the fast path
+    bool same = have_factor && nefc <= 128;
+    unsigned act[4] = {0, 0, 0, 0};
+    #pragma unroll 1
+    for (int w = 0; w < nwords && w < 4; w++) {
+      int r = 32 * w + lane;
+      bool q = r < nefc && row_quad((int)eT[r], eD[r], eL[r], eY[r]);
+      act[w] = __ballot_sync(FULL_MASK, q);
+      if (act[w] != act_prev[w]) same = false;
+    }
+    if (nefc > 128) same = false;
+    if (!same) {
+      #pragma unroll 1
+      for (int t = lane; t < ntri; t += 32) {
+        int packed = ldi(it, i_tri + t);
+        int i = packed >> 16, j = packed & 0xffff;
+        float s = M[i * nv + j];
+        #pragma unroll 1
+        for (int r = 0; r < nefc; r++) {
+          bool q = nefc <= 128 ? ((act[r >> 5] >> (r & 31)) & 1u) : row_quad((int)eT[r], eD[r], eL[r], eY[r]);
+          if (q) s += eD[r] * J[r * nv + i] * J[r * nv + j];
+        }
+        H[i * nv + j] = s;
+      }
+      __syncwarp();
+      d_chol(H, nv, lane);
+      for (int w = 0; w < 4; w++) act_prev[w] = act[w];
+      have_factor = true;
+    }
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) p[i] = -grad[i];
+    __syncwarp();
+    d_chol_solve(H, nv, p, lane);
+    // line-search coefficients A = p'Mp, B = p'Md, q = J p
+    float A = 0, B = 0, gp = 0;
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) {
+      float s = 0;
+      #pragma unroll 1
+      for (int j = 0; j < nv; j++) s += M[i * nv + j] * p[j];
+      Mp[i] = s;
+      A += p[i] * s;
+      B += p[i] * Md[i];
+      gp += grad[i] * p[i];
+    }
+    #pragma unroll 1
+    for (int r = lane; r < nefc; r += 32) {
+      float s = 0;
+      #pragma unroll 1
+      for (int j = 0; j < nv; j++) s += J[r * nv + j] * p[j];
+      eQ[r] = s;
+    }
+    A = warp_sum(A);
+    B = warp_sum(B);
+    gp = warp_sum(gp);
+    __syncwarp();
+    if (!(gp < 0.f)) break;
+    // exact line search: safeguarded Newton on the monotone derivative
+    float d0, h0;
+    {
+      float g1 = 0, g2 = 0;
+      #pragma unroll 1
+      for (int r = lane; r < nefc; r += 32) {
+        int ty = (int)eT[r];
+        float q = eQ[r], y = eY[r], D = eD[r], fl = eL[r];
+        g1 -= q * row_force(ty, D, fl, y);
+        if (row_quad(ty, D, fl, y)) g2 += D * q * q;
+      }
+      d0 = B + warp_sum(g1);
+      h0 = A + warp_sum(g2);
+    }
+    niter++;
+    float alpha = 0;
+    if (d0 < 0.f) {
+      float lo = 0, dlo = d0, hi = -1, dhi = 0;
+      float a = -d0 / h0;
+      #pragma unroll 1
+      for (int it2 = 0; it2 < ls_iter; it2++) {
+        float g1 = 0, g2 = 0;
+        #pragma unroll 1
+        for (int r = lane; r < nefc; r += 32) {
+          int ty = (int)eT[r];
+          float q = eQ[r], y = eY[r] + a * q, D = eD[r], fl = eL[r];
+          g1 -= q * row_force(ty, D, fl, y);
+          if (row_quad(ty, D, fl, y)) g2 += D * q * q;
+        }
+        float dd = a * A + B + warp_sum(g1);
+        float hh = A + warp_sum(g2);
+        if (dd < 0.f) { lo = a; dlo = dd; } else { hi = a; dhi = dd; }
+        if (fabsf(dd) <= 1e-6f * fabsf(d0)) break;
+        float an = a - dd / hh;
+        if (hi >= 0.f && !(an > lo && an < hi)) {
+          an = (dlo * hi - dhi * lo) / (dlo - dhi);
+          if (!(an > lo && an < hi)) an = 0.5f * (lo + hi);
+        }
+        if (fabsf(an - a) <= 1e-6f * fabsf(a)) { a = an; break; }
+        a = an;
+      }
+      alpha = a;
+    }
+    if (alpha == 0.f) break;
+    // cost change along the step (accurate for small steps)
+    float dc = 0;
+    #pragma unroll 1
+    for (int r = lane; r < nefc; r += 32) dc += row_cost_delta((int)eT[r], eD[r], eL[r], eY[r], alpha * eQ[r]);
+    dc = warp_sum(dc) + 0.5f * alpha * alpha * A + alpha * B;
+    // update x, Md, y, force, grad
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) {
+      x[i] += alpha * p[i];
+      Md[i] += alpha * Mp[i];
+    }
+    #pragma unroll 1
+    for (int r = lane; r < nefc; r += 32) {
+      float y = eY[r] + alpha * eQ[r];
+      eY[r] = y;
+      eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
+    }
+    __syncwarp();
+    gn = grad_update(J, eF, Md, grad, nv, nefc, lane, terms);
+    __syncwarp();
+    float improvement = -scale * dc;
+    if (improvement < tol || scale * sqrtf(gn) < tol || gn <= eps_floor * eps_floor * terms) break;
+  }
+  return niter;
+}
+
+// qfrc_constraint = J' force into out
+__device__ __noinline__ void d_jtf(Env& E, int nefc, float* out) {
+  const DevModelDesc& m = *E.md;
+  const int nv = m.nv, ne = m.nefc_max;
+  const float* J = E.ws + m.w_J;
+  const float* eF = E.ws + m.w_efc + EFC_FORCE * ne;
+  #pragma unroll 1
+  for (int i = E.lane; i < nv; i += 32) {
+    float s = 0;
+    #pragma unroll 1
+    for (int r = 0; r < nefc; r++) s += J[r * nv + i] * eF[r];
+    out[i] = s;
+  }
+  __syncwarp();
+}
+
+// Semi-implicit Euler with optional implicit damping; returns false when the
+// acceleration is not finite (caller resets the env).
+__device__ __noinline__ void d_integrate(Env& E, const float* acc) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  float* ws = E.ws;
+  float* qpos = ws + m.w_qpos;
+  float* qvel = ws + m.w_qvel;
+  const float h = m.timestep;
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) qvel[i] += h * acc[i];
+  __syncwarp();
+  #pragma unroll 1
+  for (int j = E.lane; j < m.njnt; j += 32) {
+    int qa = ldi(it, m.i_jnt_qposadr + j), da = ldi(it, m.i_jnt_dofadr + j), t = ldi(it, m.i_jnt_type + j);
+    float* q = qpos + qa;
+    const float* v = qvel + da;
+    if (t == 2 || t == 3) { q[0] += h * v[0]; continue; }
+    const float* w = v;
+    float* qq = q;
+    if (t == 0) {
+      for (int k = 0; k < 3; k++) q[k] += h * v[k];
+      w = v + 3;
+      qq = q + 3;
+    }
+    float wn = sqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    float ha = 0.5f * h * wn;
+    float sn, cs;
+    sincosf(ha, &sn, &cs);
+    float s = wn > 1e-12f ? sn / wn : 0.5f * h;
+    float dq[4] = {cs, s * w[0], s * w[1], s * w[2]};
+    float cur[4] = {qq[0], qq[1], qq[2], qq[3]}, nq[4];
+    qmul(cur, dq, nq);
+    qnormalize(nq);
+    for (int k = 0; k < 4; k++) qq[k] = nq[k];
+  }
+  __syncwarp();
+}
+
+}  // namespace mjbdev

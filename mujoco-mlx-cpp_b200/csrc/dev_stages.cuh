@@ -1,0 +1,503 @@
+// Warp-cooperative stages of the physics step, one warp per env, all
+// intermediate state in the warp's shared-memory workspace.
+//   d_kinematics  <- kinematics.hpp:75-183 (bodies processed level by level,
+//                    one lane per body of the level)
+//   d_collide     <- collision.hpp:235-501 (one lane per candidate pair;
+//                    contacts compacted in pair order with a warp scan)
+//   d_com/d_crb   <- forward.hpp:143-279
+//   d_rne         <- forward.hpp:281-397
+//   d_forces      <- forward.hpp:399-469
+#pragma once
+#include "dev_collide.cuh"
+#include "step_params.h"
+
+namespace mjbdev {
+
+struct Env {
+  const DevModelDesc* md;  // shared-memory copy
+  const int* it;
+  const float* ft;
+  float* ws;
+  int lane;
+  int env;
+  int status;
+};
+
+__device__ __forceinline__ float msc(const StepParams& P, const Env& E, int b) {
+  return P.rand_mass ? P.rand_mass[P.env_badr[E.env] + b] : 1.f;
+}
+
+__device__ __noinline__ void d_kinematics(Env& E) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  const float* qpos = ws + m.w_qpos;
+  float* xpos = ws + m.w_xpos;
+  float* xquat = ws + m.w_xquat;
+  float* xmat = ws + m.w_xmat;
+  float* xipos = ws + m.w_xipos;
+  float* xanchor = ws + m.w_xanchor;
+  float* xaxis = ws + m.w_xaxis;
+  if (E.lane == 0) {
+    xpos[0] = xpos[1] = xpos[2] = 0;
+    xquat[0] = 1; xquat[1] = xquat[2] = xquat[3] = 0;
+  }
+  __syncwarp();
+  #pragma unroll 1
+  for (int l = 1; l < m.nlevel; l++) {
+    int s = ldi(it, m.i_level_start + l), e = ldi(it, m.i_level_start + l + 1);
+    #pragma unroll 1
+    for (int k = s + E.lane; k < e; k += 32) {
+      int b = ldi(it, m.i_level_body + k);
+      int p = ldi(it, m.i_body_parentid + b);
+      float pq[4] = {xquat[4 * p], xquat[4 * p + 1], xquat[4 * p + 2], xquat[4 * p + 3]};
+      float lp[3] = {ldf(ft, m.f_body_pos + 3 * b), ldf(ft, m.f_body_pos + 3 * b + 1), ldf(ft, m.f_body_pos + 3 * b + 2)};
+      float lq[4] = {ldf(ft, m.f_body_quat + 4 * b), ldf(ft, m.f_body_quat + 4 * b + 1), ldf(ft, m.f_body_quat + 4 * b + 2), ldf(ft, m.f_body_quat + 4 * b + 3)};
+      float pos[3], quat[4], r[3];
+      qrot(pq, lp, r);
+      for (int c = 0; c < 3; c++) pos[c] = xpos[3 * p + c] + r[c];
+      qmul(pq, lq, quat);
+      int ja = ldi(it, m.i_body_jntadr + b), jn = ldi(it, m.i_body_jntnum + b);
+      #pragma unroll 1
+      for (int j = ja; j >= 0 && j < ja + jn; j++) {
+        int t = ldi(it, m.i_jnt_type + j);
+        int qa = ldi(it, m.i_jnt_qposadr + j);
+        float* an = xanchor + 3 * j;
+        float* ax = xaxis + 3 * j;
+        if (t == 0) {
+          for (int c = 0; c < 3; c++) pos[c] = qpos[qa + c];
+          for (int c = 0; c < 4; c++) quat[c] = qpos[qa + 3 + c];
+          qnormalize(quat);
+          for (int c = 0; c < 3; c++) an[c] = pos[c];
+          ax[0] = 0; ax[1] = 0; ax[2] = 1;
+          continue;
+        }
+        float jp[3] = {ldf(ft, m.f_jnt_pos + 3 * j), ldf(ft, m.f_jnt_pos + 3 * j + 1), ldf(ft, m.f_jnt_pos + 3 * j + 2)};
+        float ja3[3] = {ldf(ft, m.f_jnt_axis + 3 * j), ldf(ft, m.f_jnt_axis + 3 * j + 1), ldf(ft, m.f_jnt_axis + 3 * j + 2)};
+        float rj[3], axw[3];
+        qrot(quat, jp, rj);
+        for (int c = 0; c < 3; c++) an[c] = pos[c] + rj[c];
+        qrot(quat, ja3, axw);
+        for (int c = 0; c < 3; c++) ax[c] = axw[c];
+        if (t == 3 || t == 1) {
+          float ql[4];
+          if (t == 3) {
+            float ang = qpos[qa] - ldf(ft, m.f_qpos0 + qa);
+            float sn, cs;
+            sincosf(0.5f * ang, &sn, &cs);
+            ql[0] = cs; ql[1] = ja3[0] * sn; ql[2] = ja3[1] * sn; ql[3] = ja3[2] * sn;
+          } else {
+            for (int c = 0; c < 4; c++) ql[c] = qpos[qa + c];
+            qnormalize(ql);
+          }
+          qmul(quat, ql, quat);
+          qrot(quat, jp, rj);
+          for (int c = 0; c < 3; c++) pos[c] = an[c] - rj[c];
+        } else {
+          float dist = qpos[qa] - ldf(ft, m.f_qpos0 + qa);
+          for (int c = 0; c < 3; c++) pos[c] += axw[c] * dist;
+        }
+      }
+      qnormalize(quat);
+      for (int c = 0; c < 3; c++) xpos[3 * b + c] = pos[c];
+      for (int c = 0; c < 4; c++) xquat[4 * b + c] = quat[c];
+    }
+    __syncwarp();
+  }
+  #pragma unroll 1
+  for (int b = E.lane; b < m.nbody; b += 32) {
+    float q[4] = {xquat[4 * b], xquat[4 * b + 1], xquat[4 * b + 2], xquat[4 * b + 3]};
+    q2mat(q, xmat + 9 * b);
+    float ip[3] = {ldf(ft, m.f_body_ipos + 3 * b), ldf(ft, m.f_body_ipos + 3 * b + 1), ldf(ft, m.f_body_ipos + 3 * b + 2)}, r[3];
+    qrot(q, ip, r);
+    for (int c = 0; c < 3; c++) xipos[3 * b + c] = xpos[3 * b + c] + r[c];
+  }
+  float* gxpos = ws + m.w_gxpos;
+  float* gxmat = ws + m.w_gxmat;
+  #pragma unroll 1
+  for (int g = E.lane; g < m.ngeom; g += 32) {
+    int b = ldi(it, m.i_geom_bodyid + g);
+    float q[4] = {xquat[4 * b], xquat[4 * b + 1], xquat[4 * b + 2], xquat[4 * b + 3]};
+    float gp[3] = {ldf(ft, m.f_geom_pos + 3 * g), ldf(ft, m.f_geom_pos + 3 * g + 1), ldf(ft, m.f_geom_pos + 3 * g + 2)}, r[3];
+    float gq[4] = {ldf(ft, m.f_geom_quat + 4 * g), ldf(ft, m.f_geom_quat + 4 * g + 1), ldf(ft, m.f_geom_quat + 4 * g + 2), ldf(ft, m.f_geom_quat + 4 * g + 3)}, cq[4];
+    qrot(q, gp, r);
+    for (int c = 0; c < 3; c++) gxpos[3 * g + c] = xpos[3 * b + c] + r[c];
+    qmul(q, gq, cq);
+    q2mat(cq, gxmat + 9 * g);
+  }
+  __syncwarp();
+}
+
+// Broadphase + narrowphase; contacts in pair order.  Returns ncon.
+__device__ __noinline__ int d_collide(Env& E) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  const float* gxpos = ws + m.w_gxpos;
+  const float* gxmat = ws + m.w_gxmat;
+  float* con = ws + m.w_con;
+  int ncon = 0;
+  if (m.disableflags & ((1 << 0) | (1 << 4))) return 0;
+  #pragma unroll 1
+  for (int base = 0; base < m.npair; base += 32) {
+    int p = base + E.lane;
+    DCon cs[4];
+    int n = 0;
+    bool unsup = false;
+    if (p < m.npair) {
+      int g1 = ldi(it, m.i_pair + 6 * p), g2 = ldi(it, m.i_pair + 6 * p + 1);
+      int t1 = ldi(it, m.i_geom_type + g1), t2 = ldi(it, m.i_geom_type + g2);
+      float margin = ldf(ft, m.f_pair + 16 * p);
+      float s1[3] = {ldf(ft, m.f_geom_size + 3 * g1), ldf(ft, m.f_geom_size + 3 * g1 + 1), ldf(ft, m.f_geom_size + 3 * g1 + 2)};
+      float s2[3] = {ldf(ft, m.f_geom_size + 3 * g2), ldf(ft, m.f_geom_size + 3 * g2 + 1), ldf(ft, m.f_geom_size + 3 * g2 + 2)};
+      const float* mesh2 = nullptr;
+      int nvert2 = 0;
+      if (t2 == 7) {
+        int md = ldi(it, m.i_geom_dataid + g2);
+        mesh2 = ft + m.f_mesh_vert + 3 * ldi(it, m.i_mesh + 2 * md);
+        nvert2 = ldi(it, m.i_mesh + 2 * md + 1);
+      }
+      n = c_collide_pair(t1, t2, gxpos + 3 * g1, gxmat + 9 * g1, s1, ldf(ft, m.f_geom_rbound + g1), gxpos + 3 * g2, gxmat + 9 * g2, s2,
+                         ldf(ft, m.f_geom_rbound + g2), mesh2, nvert2, margin, cs);
+      if (n < 0) { unsup = true; n = 0; }
+    }
+    if (__any_sync(FULL_MASK, unsup)) E.status |= MJB_STATUS_UNSUPPORTED_PAIR;
+    int incl = warp_incl_scan(n, E.lane);
+    int total = __shfl_sync(FULL_MASK, incl, 31);
+    int off = ncon + incl - n;
+    #pragma unroll 1
+    for (int i = 0; i < n; i++) {
+      int idx = off + i;
+      if (idx >= m.ncon_max) break;
+      float* c = con + MJB_CONTACT_FLOATS * idx;
+      for (int k = 0; k < 3; k++) c[k] = cs[i].pos[k];
+      c_make_frame(cs[i].n, c + 3);
+      c[12] = cs[i].dist;
+      c[13] = (float)p;
+      c[14] = (float)ldi(it, m.i_pair + 6 * p + 4);
+      c[15] = ldf(ft, m.f_pair + 16 * p + 1);
+    }
+    ncon += total;
+  }
+  if (ncon > m.ncon_max) {
+    E.status |= MJB_STATUS_CONTACT_OVERFLOW;
+    ncon = m.ncon_max;
+  }
+  __syncwarp();
+  return ncon;
+}
+
+// subtree COM, cinert (about the root's subtree COM), cdof
+__device__ __noinline__ void d_com(Env& E, const StepParams& P) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  float* tmp = ws + m.w_tmp;  // 4 per body: mass, mass*xipos
+  const float* xipos = ws + m.w_xipos;
+  const float* xquat = ws + m.w_xquat;
+  float* scom = ws + m.w_scom;
+  #pragma unroll 1
+  for (int b = E.lane; b < m.nbody; b += 32) {
+    float mb = ldf(ft, m.f_body_mass + b) * msc(P, E, b);
+    tmp[4 * b] = mb;
+    for (int c = 0; c < 3; c++) tmp[4 * b + 1 + c] = mb * xipos[3 * b + c];
+  }
+  __syncwarp();
+  for (int l = m.nlevel - 2; l >= 0; l--) {
+    int s = ldi(it, m.i_level_start + l), e = ldi(it, m.i_level_start + l + 1);
+    #pragma unroll 1
+    for (int k = s + E.lane; k < e; k += 32) {
+      int b = ldi(it, m.i_level_body + k);
+      int c0 = ldi(it, m.i_child_start + b), c1 = ldi(it, m.i_child_start + b + 1);
+      float a[4] = {tmp[4 * b], tmp[4 * b + 1], tmp[4 * b + 2], tmp[4 * b + 3]};
+      #pragma unroll 1
+      for (int ci = c0; ci < c1; ci++) {
+        int c = ldi(it, m.i_child_list + ci);
+        for (int q = 0; q < 4; q++) a[q] += tmp[4 * c + q];
+      }
+      for (int q = 0; q < 4; q++) tmp[4 * b + q] = a[q];
+    }
+    __syncwarp();
+  }
+  #pragma unroll 1
+  for (int b = E.lane; b < m.nbody; b += 32) {
+    float mass = tmp[4 * b];
+    for (int c = 0; c < 3; c++) scom[3 * b + c] = mass > 1e-8f ? tmp[4 * b + 1 + c] / mass : xipos[3 * b + c];
+  }
+  __syncwarp();
+  float* cinert = ws + m.w_cinert;
+  #pragma unroll 1
+  for (int b = E.lane; b < m.nbody; b += 32) {
+    float* ci = cinert + 10 * b;
+    if (b == 0) {
+      for (int k = 0; k < 10; k++) ci[k] = 0;
+      continue;
+    }
+    float s = msc(P, E, b);
+    float mb = ldf(ft, m.f_body_mass + b) * s;
+    float q[4] = {xquat[4 * b], xquat[4 * b + 1], xquat[4 * b + 2], xquat[4 * b + 3]};
+    float iq[4] = {ldf(ft, m.f_body_iquat + 4 * b), ldf(ft, m.f_body_iquat + 4 * b + 1), ldf(ft, m.f_body_iquat + 4 * b + 2), ldf(ft, m.f_body_iquat + 4 * b + 3)};
+    float cq[4], R[9];
+    qmul(q, iq, cq);
+    q2mat(cq, R);
+    float I0 = ldf(ft, m.f_body_inertia + 3 * b) * s, I1 = ldf(ft, m.f_body_inertia + 3 * b + 1) * s, I2 = ldf(ft, m.f_body_inertia + 3 * b + 2) * s;
+    float Ig[9];
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) Ig[r * 3 + c] = R[r * 3] * I0 * R[c * 3] + R[r * 3 + 1] * I1 * R[c * 3 + 1] + R[r * 3 + 2] * I2 * R[c * 3 + 2];
+    int root = ldi(it, m.i_body_rootid + b);
+    float off[3] = {xipos[3 * b] - scom[3 * root], xipos[3 * b + 1] - scom[3 * root + 1], xipos[3 * b + 2] - scom[3 * root + 2]};
+    float d2 = dot3(off, off);
+    ci[0] = Ig[0] + mb * (d2 - off[0] * off[0]);
+    ci[1] = Ig[4] + mb * (d2 - off[1] * off[1]);
+    ci[2] = Ig[8] + mb * (d2 - off[2] * off[2]);
+    ci[3] = Ig[1] - mb * off[0] * off[1];
+    ci[4] = Ig[2] - mb * off[0] * off[2];
+    ci[5] = Ig[5] - mb * off[1] * off[2];
+    ci[6] = mb * off[0]; ci[7] = mb * off[1]; ci[8] = mb * off[2];
+    ci[9] = mb;
+  }
+  float* cdof = ws + m.w_cdof;
+  const float* xmat = ws + m.w_xmat;
+  const float* xanchor = ws + m.w_xanchor;
+  const float* xaxis = ws + m.w_xaxis;
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) {
+    int b = ldi(it, m.i_dof_bodyid + i), j = ldi(it, m.i_dof_jntid + i), t = ldi(it, m.i_jnt_type + j);
+    int sub = i - ldi(it, m.i_jnt_dofadr + j);
+    float* c = cdof + 6 * i;
+    int root = ldi(it, m.i_body_rootid + b);
+    float ax[3];
+    bool rot = true;
+    if (t == 3) { ax[0] = xaxis[3 * j]; ax[1] = xaxis[3 * j + 1]; ax[2] = xaxis[3 * j + 2]; }
+    else if (t == 2) { rot = false; ax[0] = xaxis[3 * j]; ax[1] = xaxis[3 * j + 1]; ax[2] = xaxis[3 * j + 2]; }
+    else if (t == 0 && sub < 3) { rot = false; ax[0] = ax[1] = ax[2] = 0; ax[sub] = 1; }
+    else {
+      int col = (t == 0) ? sub - 3 : sub;
+      for (int k = 0; k < 3; k++) ax[k] = xmat[9 * b + 3 * k + col];
+    }
+    if (rot) {
+      float off[3] = {scom[3 * root] - xanchor[3 * j], scom[3 * root + 1] - xanchor[3 * j + 1], scom[3 * root + 2] - xanchor[3 * j + 2]};
+      c[0] = ax[0]; c[1] = ax[1]; c[2] = ax[2];
+      cross3(ax, off, c + 3);
+    } else {
+      c[0] = c[1] = c[2] = 0;
+      c[3] = ax[0]; c[4] = ax[1]; c[5] = ax[2];
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void cinert_mul(const float* ci, const float* v, float* f) {
+  const float *w = v, *l = v + 3;
+  f[0] = ci[0] * w[0] + ci[3] * w[1] + ci[4] * w[2] + (ci[7] * l[2] - ci[8] * l[1]);
+  f[1] = ci[3] * w[0] + ci[1] * w[1] + ci[5] * w[2] + (ci[8] * l[0] - ci[6] * l[2]);
+  f[2] = ci[4] * w[0] + ci[5] * w[1] + ci[2] * w[2] + (ci[6] * l[1] - ci[7] * l[0]);
+  f[3] = ci[9] * l[0] - (ci[7] * w[2] - ci[8] * w[1]);
+  f[4] = ci[9] * l[1] - (ci[8] * w[0] - ci[6] * w[2]);
+  f[5] = ci[9] * l[2] - (ci[6] * w[1] - ci[7] * w[0]);
+}
+
+// composite rigid bodies and the joint-space mass matrix
+__device__ __noinline__ void d_crb(Env& E) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  float* crb = ws + m.w_crb;
+  const float* cinert = ws + m.w_cinert;
+  #pragma unroll 1
+  for (int k = E.lane; k < 10 * m.nbody; k += 32) crb[k] = k < 10 ? 0.f : cinert[k];
+  __syncwarp();
+  for (int l = m.nlevel - 2; l >= 1; l--) {
+    int s = ldi(it, m.i_level_start + l), e = ldi(it, m.i_level_start + l + 1);
+    #pragma unroll 1
+    for (int k = s + E.lane; k < e; k += 32) {
+      int b = ldi(it, m.i_level_body + k);
+      int c0 = ldi(it, m.i_child_start + b), c1 = ldi(it, m.i_child_start + b + 1);
+      #pragma unroll 1
+      for (int ci = c0; ci < c1; ci++) {
+        int c = ldi(it, m.i_child_list + ci);
+        for (int q = 0; q < 10; q++) crb[10 * b + q] += crb[10 * c + q];
+      }
+    }
+    __syncwarp();
+  }
+  int nv = m.nv;
+  float* M = ws + m.w_M;
+  #pragma unroll 1
+  for (int k = E.lane; k < nv * nv; k += 32) M[k] = 0;
+  __syncwarp();
+  const float* cdof = ws + m.w_cdof;
+  #pragma unroll 1
+  for (int i = E.lane; i < nv; i += 32) {
+    float f[6];
+    cinert_mul(crb + 10 * ldi(it, m.i_dof_bodyid + i), cdof + 6 * i, f);
+    for (int j = i; j >= 0; j = ldi(it, m.i_dof_parentid + j)) {
+      const float* cj = cdof + 6 * j;
+      float s = f[0] * cj[0] + f[1] * cj[1] + f[2] * cj[2] + f[3] * cj[3] + f[4] * cj[4] + f[5] * cj[5];
+      if (j == i) s += ldf(ft, m.f_dof_armature + i);
+      M[i * nv + j] = s;
+      M[j * nv + i] = s;
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void cross_motion(const float* v, const float* u, float* r) {
+  float a[3], b[3], c[3];
+  cross3(v, u, c);
+  cross3(v + 3, u, a);
+  cross3(v, u + 3, b);
+  r[0] = c[0]; r[1] = c[1]; r[2] = c[2];
+  for (int k = 0; k < 3; k++) r[3 + k] = a[k] + b[k];
+}
+__device__ __forceinline__ void cross_force(const float* v, const float* f, float* r) {
+  float a[3], b[3], c[3];
+  cross3(v, f, a);
+  cross3(v + 3, f + 3, b);
+  cross3(v, f + 3, c);
+  for (int k = 0; k < 3; k++) { r[k] = a[k] + b[k]; r[3 + k] = c[k]; }
+}
+
+// com velocities, cdof_dot, and the bias force (RNE with qacc = 0) into `bias`
+__device__ __noinline__ void d_rne(Env& E, float* bias) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  float* ws = E.ws;
+  const float* qv = ws + m.w_qvel;
+  const float* cdof = ws + m.w_cdof;
+  float* cvel = ws + m.w_cvel;
+  float* cdd = ws + m.w_cdofdot;
+  float* cacc = ws + m.w_cacc;
+  float* cfrc = ws + m.w_crb;  // crb is dead after d_crb
+  const float* cinert = ws + m.w_cinert;
+  if (E.lane < 6) {
+    cvel[E.lane] = 0;
+    cacc[E.lane] = E.lane < 3 || (m.disableflags & (1 << 6)) ? 0.f : -m.gravity[E.lane - 3];
+  }
+  __syncwarp();
+  #pragma unroll 1
+  for (int l = 1; l < m.nlevel; l++) {
+    int s = ldi(it, m.i_level_start + l), e = ldi(it, m.i_level_start + l + 1);
+    #pragma unroll 1
+    for (int k = s + E.lane; k < e; k += 32) {
+      int b = ldi(it, m.i_level_body + k);
+      int p = ldi(it, m.i_body_parentid + b);
+      float cv[6], ca[6];
+      for (int c = 0; c < 6; c++) { cv[c] = cvel[6 * p + c]; ca[c] = cacc[6 * p + c]; }
+      int a = ldi(it, m.i_body_dofadr + b), n = ldi(it, m.i_body_dofnum + b);
+      #pragma unroll 1
+      for (int q = 0; q < n;) {
+        int i = a + q;
+        int t = ldi(it, m.i_jnt_type + ldi(it, m.i_dof_jntid + i));
+        if (t == 0) {
+          for (int s2 = 0; s2 < 3; s2++) {
+            for (int c = 0; c < 6; c++) cdd[6 * (i + s2) + c] = 0;
+            for (int c = 0; c < 6; c++) cv[c] += cdof[6 * (i + s2) + c] * qv[i + s2];
+          }
+          for (int s2 = 3; s2 < 6; s2++) cross_motion(cv, cdof + 6 * (i + s2), cdd + 6 * (i + s2));
+          for (int s2 = 3; s2 < 6; s2++)
+            for (int c = 0; c < 6; c++) cv[c] += cdof[6 * (i + s2) + c] * qv[i + s2];
+          q += 6;
+        } else if (t == 1) {
+          for (int s2 = 0; s2 < 3; s2++) cross_motion(cv, cdof + 6 * (i + s2), cdd + 6 * (i + s2));
+          for (int s2 = 0; s2 < 3; s2++)
+            for (int c = 0; c < 6; c++) cv[c] += cdof[6 * (i + s2) + c] * qv[i + s2];
+          q += 3;
+        } else {
+          cross_motion(cv, cdof + 6 * i, cdd + 6 * i);
+          for (int c = 0; c < 6; c++) cv[c] += cdof[6 * i + c] * qv[i];
+          q += 1;
+        }
+      }
+      #pragma unroll 1
+      for (int i = a; i < a + n; i++)
+        for (int c = 0; c < 6; c++) ca[c] += cdd[6 * i + c] * qv[i];
+      for (int c = 0; c < 6; c++) { cvel[6 * b + c] = cv[c]; cacc[6 * b + c] = ca[c]; }
+    }
+    __syncwarp();
+  }
+  #pragma unroll 1
+  for (int b = E.lane; b < m.nbody; b += 32) {
+    float Ia[6], Iv[6], vf[6];
+    cinert_mul(cinert + 10 * b, cacc + 6 * b, Ia);
+    cinert_mul(cinert + 10 * b, cvel + 6 * b, Iv);
+    cross_force(cvel + 6 * b, Iv, vf);
+    for (int c = 0; c < 6; c++) cfrc[6 * b + c] = Ia[c] + vf[c];
+  }
+  __syncwarp();
+  for (int l = m.nlevel - 2; l >= 1; l--) {
+    int s = ldi(it, m.i_level_start + l), e = ldi(it, m.i_level_start + l + 1);
+    #pragma unroll 1
+    for (int k = s + E.lane; k < e; k += 32) {
+      int b = ldi(it, m.i_level_body + k);
+      int c0 = ldi(it, m.i_child_start + b), c1 = ldi(it, m.i_child_start + b + 1);
+      #pragma unroll 1
+      for (int ci = c0; ci < c1; ci++) {
+        int c = ldi(it, m.i_child_list + ci);
+        for (int q = 0; q < 6; q++) cfrc[6 * b + q] += cfrc[6 * c + q];
+      }
+    }
+    __syncwarp();
+  }
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) {
+    const float* f = cfrc + 6 * ldi(it, m.i_dof_bodyid + i);
+    const float* c = cdof + 6 * i;
+    bias[i] = c[0] * f[0] + c[1] * f[1] + c[2] * f[2] + c[3] * f[3] + c[4] * f[4] + c[5] * f[5];
+  }
+  __syncwarp();
+}
+
+// passive + actuation + smooth force
+__device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* bias) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  const float* qpos = ws + m.w_qpos;
+  const float* qvel = ws + m.w_qvel;
+  const float* ctrl = ws + m.w_ctrl;
+  float* qfs = ws + m.w_qfs;
+  float* qfa = ws + m.w_qfa;
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) {
+    float pas = 0, act = 0;
+    if (!(m.disableflags & (1 << 5))) {
+      int j = ldi(it, m.i_dof_jntid + i);
+      int t = ldi(it, m.i_jnt_type + j);
+      float st = ldf(ft, m.f_jnt_stiffness + j);
+      if ((t == 2 || t == 3) && st != 0.f) {
+        int qa = ldi(it, m.i_jnt_qposadr + j);
+        pas -= st * (qpos[qa] - ldf(ft, m.f_qpos_spring + qa));
+      }
+      pas -= ldf(ft, m.f_dof_damping + i) * qvel[i];
+    }
+    if (!(m.disableflags & (1 << 10))) {
+      #pragma unroll 1
+      for (int a = 0; a < m.nu; a++) {
+        const int* ai = it + m.i_act + 6 * a;
+        if (ldi(ai, 0) != i) continue;
+        const float* af = ft + m.f_act + 11 * a;
+        float gear = ldf(af, 0);
+        float c = ctrl[a];
+        if (ldi(ai, 4) && !(m.disableflags & (1 << 7))) c = clampf(c, ldf(af, 7), ldf(af, 8));
+        float len = gear * qpos[ldi(ai, 1)], vel = gear * qvel[i];
+        float gain = ldf(af, 1) + (ldi(ai, 2) ? ldf(af, 2) * len + ldf(af, 3) * vel : 0.f);
+        float bs = ldi(ai, 3) ? ldf(af, 4) + ldf(af, 5) * len + ldf(af, 6) * vel : 0.f;
+        float force = gain * c + bs;
+        if (P.rand_gain) force *= P.rand_gain[P.env_uadr[E.env] + a];
+        if (ldi(ai, 5)) force = clampf(force, ldf(af, 9), ldf(af, 10));
+        act += gear * force;
+      }
+    }
+    qfa[i] = act;
+    qfs[i] = pas - bias[i] + act;
+  }
+  __syncwarp();
+}
+
+}  // namespace mjbdev

@@ -1,0 +1,66 @@
+// Device-side model descriptor shared by host and kernels.
+//
+// Every model constant the step needs lives in two flat HBM tables (ints and
+// floats) that stay L2-resident; a POD descriptor per model holds sizes and
+// offsets into them plus the per-env shared-memory workspace layout.  This
+// replaces the reference's string-baked GLSL constants (forward.hpp:84-106,
+// collision.hpp:505-515) so one kernel serves any model, and several models in
+// one launch.
+#pragma once
+
+#define MJB_CONTACT_FLOATS 16  // pos3 frame9 dist pair(bits) dim includemargin
+
+struct DevModelDesc {
+  // sizes
+  int nq, nv, nu, nbody, njnt, ngeom, npair, nlimit, nfloss, nlevel, nmesh;
+  int ncon_max, nefc_max, ntri;
+  int cone, disableflags, iterations, ls_iterations, implicit;
+  float timestep, gravity[3], tolerance, impratio, scale;  // scale = 1/(meaninertia*max(1,nv))
+
+  // int table offsets
+  int i_body_parentid, i_body_rootid, i_body_jntadr, i_body_jntnum, i_body_dofadr, i_body_dofnum, i_body_subtreesize;
+  int i_level_start, i_level_body, i_child_start, i_child_list;
+  int i_jnt_type, i_jnt_qposadr, i_jnt_dofadr;
+  int i_dof_bodyid, i_dof_jntid, i_dof_parentid;
+  int i_geom_type, i_geom_bodyid, i_geom_dataid;
+  int i_pair;    // 6 per pair: g1 g2 b1 b2 condim maxcon
+  int i_limit;   // 3 per limited joint: jnt dof qposadr
+  int i_floss;   // 1 per frictionloss dof: dof
+  int i_act;     // 6 per actuator: dof qposadr gaintype biastype ctrllimited forcelimited
+  int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
+  int i_mesh;    // 2 per mesh: vertadr vertnum
+
+  // float table offsets
+  int f_body_pos, f_body_quat, f_body_ipos, f_body_iquat, f_body_mass, f_body_inertia;
+  int f_jnt_pos, f_jnt_axis, f_jnt_stiffness, f_qpos0, f_qpos_spring;
+  int f_dof_armature, f_dof_damping, f_dof_damping_implicit, f_dof_invweight0;
+  int f_geom_pos, f_geom_quat, f_geom_size, f_geom_rbound;
+  int f_pair;    // 16 per pair: margin includemargin friction(5) solref(2) solimp(5) invw_t invw_r
+  int f_limit;   // 10 per limit: lo hi margin solref(2) solimp(5)
+  int f_floss;   // 8 per frictionloss dof: floss solref(2) solimp(5)
+  int f_act;     // 11 per actuator: gear gain(3) bias(3) ctrlrange(2) forcerange(2)
+  int f_mesh_vert;
+
+  // per-env shared-memory workspace (float offsets from the warp's base)
+  int ws_size;
+  int w_qpos, w_qvel, w_ctrl, w_x, w_xwarm;
+  int w_scom, w_cdof, w_M, w_qfs, w_qas, w_qfa, w_vec;   // w_vec: 8*nv solver vectors
+  int w_con, w_rowcon;
+  // phase region K (kinematics / dynamics), aliased by region S (solver)
+  int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;
+  int w_J, w_efc, w_H, w_active;
+};
+
+// efc row metadata stride (floats) in the workspace: aref D floss type y force q
+#define MJB_EFC_FIELDS 8
+enum { EFC_AREF = 0, EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y, EFC_FORCE, EFC_Q, EFC_CON };
+enum { ROW_FRICTION = 0, ROW_LIMIT = 1, ROW_PYRAMID = 2, ROW_FRICTIONLESS = 3 };
+
+// status bits (per env, OR over substeps)
+enum {
+  MJB_STATUS_BADSTATE = 1,
+  MJB_STATUS_BADQACC = 2,
+  MJB_STATUS_CONTACT_OVERFLOW = 4,
+  MJB_STATUS_EFC_OVERFLOW = 8,
+  MJB_STATUS_UNSUPPORTED_PAIR = 16,
+};

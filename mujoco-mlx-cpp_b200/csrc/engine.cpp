@@ -1,0 +1,692 @@
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
+cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
+cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
+                             float* qpos, float* qvel, float* warm, cudaStream_t s);
+
+namespace mjb {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+void DevBuf<T>::alloc(size_t count) {
+  release();
+  n = count;
+  if (count) {
+    check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    check(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+  }
+}
+template <class T>
+void DevBuf<T>::upload(const std::vector<T>& v, cudaStream_t s) {
+  if (n < v.size() || !p) alloc(std::max<size_t>(v.size(), 1));
+  if (!v.empty()) check(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+}
+template struct DevBuf<float>;
+template struct DevBuf<int>;
+template struct DevBuf<DevModelDesc>;
+template struct DevBuf<uint16_t>;
+template struct DevBuf<unsigned long long>;
+
+namespace {
+
+struct TableBuilder {
+  std::vector<int>& it;
+  std::vector<float>& ft;
+  int ai(const std::vector<int>& v) {
+    int o = (int)it.size();
+    it.insert(it.end(), v.begin(), v.end());
+    if (v.empty()) it.push_back(0);
+    return o;
+  }
+  int af(const std::vector<double>& v) {
+    int o = (int)ft.size();
+    for (double x : v) ft.push_back((float)x);
+    if (v.empty()) ft.push_back(0.f);
+    return o;
+  }
+};
+
+// Supported narrowphase type combinations (type-ordered).
+bool pair_supported(int t1, int t2) {
+  if (t1 == GEOM_PLANE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX || t2 == GEOM_ELLIPSOID || t2 == GEOM_CYLINDER || t2 == GEOM_MESH;
+  if (t1 == GEOM_SPHERE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
+  if (t1 == GEOM_CAPSULE) return t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
+  return false;
+}
+
+}  // namespace
+
+Engine::Engine(const std::vector<const Model*>& models, const std::vector<int>& counts, int solver_iterations, int domain_rand, const EngineConfig& cfg)
+    : models_(models), counts_(counts), cfg_(cfg) {
+  if (models.empty() || models.size() != counts.size()) throw std::runtime_error("engine: need one count per model");
+  for (int c : counts)
+    if (c <= 0) throw std::runtime_error("engine: env counts must be positive");
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaDeviceProp prop;
+  check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  if (prop.major < 10) throw std::runtime_error("engine: this build targets sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
+  sm_count_ = prop.multiProcessorCount;
+  check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  rand_on_ = domain_rand != 0;
+  build_tables(cfg, solver_iterations);
+  alloc_state();
+  choose_launch();
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  invalidate_graphs();
+  if (h_ctrl_pinned_) cudaFreeHost(h_ctrl_pinned_);
+  for (auto& kv : h_stage_) cudaFreeHost(kv.second);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
+  h_itab_.clear();
+  h_ftab_.clear();
+  layouts_.clear();
+  TableBuilder tb{h_itab_, h_ftab_};
+  ws_stride_ = 0;
+  nv_max_ = 0;
+  for (const Model* mp : models_) {
+    const Model& m = *mp;
+    for (auto& p : m.pairs) {
+      int t1 = m.geom_type[p.g1], t2 = m.geom_type[p.g2];
+      if (!pair_supported(t1, t2))
+        throw std::runtime_error("engine: collision pair of geom types " + std::to_string(t1) + "-" + std::to_string(t2) + " has no collider in this build");
+    }
+    for (auto& p : m.pairs)
+      if (p.condim != 1 && p.condim != 3 && p.condim != 4 && p.condim != 6) throw std::runtime_error("engine: condim must be 1, 3, 4 or 6");
+    if (m.cone != CONE_PYRAMIDAL) throw std::runtime_error("engine: the elliptic cone is not supported by this build");
+    for (int j = 0; j < m.njnt; j++)
+      if (m.jnt_limited[j] && m.jnt_type[j] == JNT_BALL) throw std::runtime_error("engine: limited ball joints are not supported");
+    for (double g : m.body_gravcomp)
+      if (g != 0) throw std::runtime_error("engine: gravcomp is not supported");
+    DevModelDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.nq = m.nq; d.nv = m.nv; d.nu = m.nu; d.nbody = m.nbody; d.njnt = m.njnt; d.ngeom = m.ngeom;
+    d.npair = (int)m.pairs.size(); d.nmesh = m.nmesh;
+    d.cone = m.cone; d.disableflags = m.disableflags;
+    d.iterations = cfg.max_iter > 0 ? cfg.max_iter : (solver_iterations > 0 ? solver_iterations : m.iterations);
+    d.ls_iterations = m.ls_iterations;
+    d.timestep = (float)m.timestep;
+    for (int k = 0; k < 3; k++) d.gravity[k] = (float)m.gravity[k];
+    d.tolerance = (float)(cfg.tolerance > 0 ? cfg.tolerance : m.tolerance);
+    d.impratio = (float)m.impratio;
+    d.scale = (float)(1.0 / (m.meaninertia * std::max(1, m.nv)));
+    // levels (BFS by depth) and children
+    int maxd = 0;
+    for (int b = 0; b < m.nbody; b++) maxd = std::max(maxd, m.body_depth[b]);
+    std::vector<int> level_start(maxd + 2, 0), level_body;
+    for (int l = 0; l <= maxd; l++) {
+      level_start[l] = (int)level_body.size();
+      for (int b = 0; b < m.nbody; b++)
+        if (m.body_depth[b] == l) level_body.push_back(b);
+    }
+    level_start[maxd + 1] = (int)level_body.size();
+    d.nlevel = maxd + 1;
+    std::vector<int> child_start(m.nbody + 1, 0), child_list;
+    for (int b = 0; b < m.nbody; b++) {
+      child_start[b] = (int)child_list.size();
+      for (int c = 1; c < m.nbody; c++)
+        if (m.body_parentid[c] == b) child_list.push_back(c);
+    }
+    child_start[m.nbody] = (int)child_list.size();
+    d.i_body_parentid = tb.ai(m.body_parentid);
+    d.i_body_rootid = tb.ai(m.body_rootid);
+    d.i_body_jntadr = tb.ai(m.body_jntadr);
+    d.i_body_jntnum = tb.ai(m.body_jntnum);
+    d.i_body_dofadr = tb.ai(m.body_dofadr);
+    d.i_body_dofnum = tb.ai(m.body_dofnum);
+    d.i_body_subtreesize = tb.ai(m.body_subtreesize);
+    d.i_level_start = tb.ai(level_start);
+    d.i_level_body = tb.ai(level_body);
+    d.i_child_start = tb.ai(child_start);
+    d.i_child_list = tb.ai(child_list);
+    d.i_jnt_type = tb.ai(m.jnt_type);
+    d.i_jnt_qposadr = tb.ai(m.jnt_qposadr);
+    d.i_jnt_dofadr = tb.ai(m.jnt_dofadr);
+    d.i_dof_bodyid = tb.ai(m.dof_bodyid);
+    d.i_dof_jntid = tb.ai(m.dof_jntid);
+    d.i_dof_parentid = tb.ai(m.dof_parentid);
+    d.i_geom_type = tb.ai(m.geom_type);
+    d.i_geom_bodyid = tb.ai(m.geom_bodyid);
+    d.i_geom_dataid = tb.ai(m.geom_dataid);
+    std::vector<int> pi;
+    std::vector<double> pf;
+    for (auto& p : m.pairs) {
+      pi.insert(pi.end(), {p.g1, p.g2, p.b1, p.b2, p.condim, pair_max_contacts(m.geom_type[p.g1], m.geom_type[p.g2])});
+      pf.insert(pf.end(), {p.margin, p.margin - p.gap});
+      pf.insert(pf.end(), p.friction, p.friction + 5);
+      pf.insert(pf.end(), p.solref, p.solref + 2);
+      pf.insert(pf.end(), p.solimp, p.solimp + 5);
+      pf.insert(pf.end(), {p.invw_t, p.invw_r});
+    }
+    d.i_pair = tb.ai(pi);
+    d.f_pair = tb.af(pf);
+    std::vector<int> li;
+    std::vector<double> lf;
+    for (int j = 0; j < m.njnt; j++) {
+      if (!m.jnt_limited[j] || (m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE)) continue;
+      li.insert(li.end(), {j, m.jnt_dofadr[j], m.jnt_qposadr[j]});
+      lf.insert(lf.end(), {m.jnt_range[2 * j], m.jnt_range[2 * j + 1], m.jnt_margin[j], m.jnt_solref[2 * j], m.jnt_solref[2 * j + 1]});
+      lf.insert(lf.end(), &m.jnt_solimp[5 * j], &m.jnt_solimp[5 * j] + 5);
+    }
+    d.nlimit = (int)li.size() / 3;
+    d.i_limit = tb.ai(li);
+    d.f_limit = tb.af(lf);
+    std::vector<int> fi;
+    std::vector<double> ff;
+    for (int i = 0; i < m.nv; i++) {
+      if (m.dof_frictionloss[i] <= 0) continue;
+      fi.push_back(i);
+      ff.insert(ff.end(), {m.dof_frictionloss[i], m.dof_solref[2 * i], m.dof_solref[2 * i + 1]});
+      ff.insert(ff.end(), &m.dof_solimp[5 * i], &m.dof_solimp[5 * i] + 5);
+    }
+    d.nfloss = (int)fi.size();
+    d.i_floss = tb.ai(fi);
+    d.f_floss = tb.af(ff);
+    std::vector<int> ai;
+    std::vector<double> af;
+    for (int a = 0; a < m.nu; a++) {
+      int j = m.actuator_trnid[a];
+      ai.insert(ai.end(), {m.jnt_dofadr[j], m.jnt_qposadr[j], m.actuator_gaintype[a], m.actuator_biastype[a], m.actuator_ctrllimited[a], m.actuator_forcelimited[a]});
+      af.push_back(m.actuator_gear[a]);
+      af.insert(af.end(), &m.actuator_gainprm[3 * a], &m.actuator_gainprm[3 * a] + 3);
+      af.insert(af.end(), &m.actuator_biasprm[3 * a], &m.actuator_biasprm[3 * a] + 3);
+      af.insert(af.end(), {m.actuator_ctrlrange[2 * a], m.actuator_ctrlrange[2 * a + 1], m.actuator_forcerange[2 * a], m.actuator_forcerange[2 * a + 1]});
+    }
+    d.i_act = tb.ai(ai);
+    d.f_act = tb.af(af);
+    std::vector<int> tri;
+    for (int i = 0; i < m.nv; i++)
+      for (int j = 0; j <= i; j++) tri.push_back((i << 16) | j);
+    d.ntri = (int)tri.size();
+    d.i_tri = tb.ai(tri);
+    std::vector<int> mi;
+    for (int k = 0; k < m.nmesh; k++) mi.insert(mi.end(), {m.mesh_vertadr[k], m.mesh_vertnum[k]});
+    d.i_mesh = tb.ai(mi);
+    d.f_mesh_vert = tb.af(m.mesh_vert);
+    d.f_body_pos = tb.af(m.body_pos);
+    d.f_body_quat = tb.af(m.body_quat);
+    d.f_body_ipos = tb.af(m.body_ipos);
+    d.f_body_iquat = tb.af(m.body_iquat);
+    d.f_body_mass = tb.af(m.body_mass);
+    d.f_body_inertia = tb.af(m.body_inertia);
+    d.f_jnt_pos = tb.af(m.jnt_pos);
+    d.f_jnt_axis = tb.af(m.jnt_axis);
+    d.f_jnt_stiffness = tb.af(m.jnt_stiffness);
+    d.f_qpos0 = tb.af(m.qpos0);
+    d.f_qpos_spring = tb.af(m.qpos_spring);
+    d.f_dof_armature = tb.af(m.dof_armature);
+    d.f_dof_damping = tb.af(m.dof_damping);
+    d.f_dof_invweight0 = tb.af(m.dof_invweight0);
+    d.f_geom_pos = tb.af(m.geom_pos);
+    d.f_geom_quat = tb.af(m.geom_quat);
+    d.f_geom_size = tb.af(m.geom_size);
+    d.f_geom_rbound = tb.af(m.geom_rbound);
+    // implicit damping (Euler with eulerdamp, or the implicit integrators)
+    std::vector<double> damp(m.dof_damping);
+    if (m.integrator == 2 || m.integrator == 3) {
+      for (int a = 0; a < m.nu; a++) {
+        if (!m.actuator_biastype[a]) continue;
+        double gv = m.actuator_gaintype[a] ? m.actuator_gainprm[3 * a + 2] : 0;
+        double bv = m.actuator_biasprm[3 * a + 2];
+        if (gv != 0 || bv == 0) continue;
+        double g = m.actuator_gear[a];
+        damp[m.jnt_dofadr[m.actuator_trnid[a]]] += -bv * g * g;
+      }
+    } else if (m.disableflags & DSBL_EULERDAMP) {
+      std::fill(damp.begin(), damp.end(), 0.0);
+    }
+    d.implicit = 0;
+    for (double x : damp)
+      if (x != 0) d.implicit = 1;
+    d.f_dof_damping_implicit = tb.af(damp);
+    // contact / row capacity
+    int ncb = std::max(1, m.max_contacts_bound);
+    d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 32);
+    int rows_per_con = 1;
+    for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : 2 * (p.condim - 1));
+    int rows_bound = d.nfloss + 2 * d.nlimit + rows_per_con * d.ncon_max;
+    d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 96));
+    // workspace layout
+    int nv = m.nv, nb = m.nbody, nj = std::max(1, m.njnt), ng = std::max(1, m.ngeom), nu = std::max(1, m.nu);
+    int off = 0;
+    auto take = [&](int n) { int o = off; off += (n + 3) & ~3; return o; };
+    d.w_qpos = take(m.nq); d.w_qvel = take(nv); d.w_ctrl = take(nu); d.w_x = take(nv); d.w_xwarm = take(nv);
+    d.w_scom = take(3 * nb); d.w_cdof = take(6 * nv); d.w_M = take(nv * nv); d.w_qfs = take(nv); d.w_qas = take(nv); d.w_qfa = take(nv);
+    d.w_vec = take(8 * nv); d.w_con = take(MJB_CONTACT_FLOATS * d.ncon_max); d.w_rowcon = 0;
+    int kbase = off;
+    d.w_xpos = take(3 * nb); d.w_xquat = take(4 * nb); d.w_xmat = take(9 * nb); d.w_xipos = take(3 * nb);
+    d.w_xanchor = take(3 * nj); d.w_xaxis = take(3 * nj); d.w_gxpos = take(3 * ng); d.w_gxmat = take(9 * ng);
+    d.w_cinert = take(10 * nb); d.w_crb = take(10 * nb); d.w_cvel = take(6 * nb); d.w_cdofdot = take(6 * nv);
+    d.w_cacc = take(6 * nb); d.w_tmp = take(4 * nb);
+    int kend = off;
+    off = kbase;
+    d.w_J = take(d.nefc_max * nv); d.w_efc = take(MJB_EFC_FIELDS * d.nefc_max); d.w_H = take(nv * nv); d.w_active = take(d.nefc_max);
+    int send = off;
+    d.ws_size = std::max(kend, send);
+    ws_stride_ = std::max(ws_stride_, d.ws_size);
+    nv_max_ = std::max(nv_max_, nv);
+    ModelLayout L;
+    L.desc = d;
+    L.nq = m.nq; L.nv = m.nv; L.nu = m.nu; L.nbody = m.nbody;
+    layouts_.push_back(L);
+  }
+  desc_words_ = (int)(sizeof(DevModelDesc) / 4);
+  std::vector<DevModelDesc> descs;
+  for (auto& L : layouts_) descs.push_back(L.desc);
+  d_models_.alloc(descs.size());
+  check(cudaMemcpy(d_models_.p, descs.data(), descs.size() * sizeof(DevModelDesc), cudaMemcpyHostToDevice), "upload models");
+  d_itab_.alloc(h_itab_.size());
+  check(cudaMemcpy(d_itab_.p, h_itab_.data(), h_itab_.size() * 4, cudaMemcpyHostToDevice), "upload itab");
+  d_ftab_.alloc(h_ftab_.size());
+  check(cudaMemcpy(d_ftab_.p, h_ftab_.data(), h_ftab_.size() * 4, cudaMemcpyHostToDevice), "upload ftab");
+}
+
+void Engine::alloc_state() {
+  B_ = 0;
+  for (int c : counts_) B_ += c;
+  h_model_.assign(B_, 0);
+  h_qadr_.assign(B_, 0);
+  h_vadr_.assign(B_, 0);
+  h_uadr_.assign(B_, 0);
+  h_badr_.assign(B_, 0);
+  int e = 0, q = 0, v = 0, u = 0, b = 0;
+  for (size_t mi = 0; mi < models_.size(); mi++)
+    for (int k = 0; k < counts_[mi]; k++, e++) {
+      const Model& m = *models_[mi];
+      h_model_[e] = (int)mi;
+      h_qadr_[e] = q; h_vadr_[e] = v; h_uadr_[e] = u; h_badr_[e] = b;
+      q += m.nq; v += m.nv; u += std::max(m.nu, 0); b += m.nbody;
+    }
+  tot_q_ = q; tot_v_ = v; tot_u_ = u; tot_b_ = b;
+  d_model_.upload(h_model_, stream_);
+  d_qadr_.upload(h_qadr_, stream_);
+  d_vadr_.upload(h_vadr_, stream_);
+  d_uadr_.upload(h_uadr_, stream_);
+  d_badr_.upload(h_badr_, stream_);
+  std::vector<float> q0(q);
+  for (int i = 0; i < B_; i++) {
+    const Model& m = *models_[h_model_[i]];
+    for (int k = 0; k < m.nq; k++) q0[h_qadr_[i] + k] = (float)m.qpos0[k];
+  }
+  qpos0_.upload(q0, stream_);
+  qpos_.upload(q0, stream_);
+  qvel_.alloc(std::max(v, 1));
+  ctrl_.alloc(std::max(u, 1));
+  warm_.alloc(std::max(v, 1));
+  pred_.alloc(std::max(v, 1));
+  for (auto* buf : {&status_, &niter_sum_, &niter_max_, &ncon_, &nefc_, &choice_}) buf->alloc(B_);
+  counter_.alloc(1);
+  rec_xpos_.alloc(3 * b); rec_xquat_.alloc(4 * b); rec_scom_.alloc(3 * b); rec_cinert_.alloc(10 * b); rec_cvel_.alloc(6 * b);
+  rec_qfa_.alloc(std::max(v, 1)); rec_cfrc_.alloc(6 * b); rec_qacc_.alloc(std::max(v, 1));
+  check(cudaMallocHost(&h_ctrl_pinned_, sizeof(float) * std::max(u, 1)), "cudaMallocHost");
+  if (rand_on_) {
+    h_rand_mass_.assign(b, 1.f);
+    h_rand_fric_.assign(B_, 1.f);
+    h_rand_gain_.assign(std::max(u, 1), 1.f);
+    rand_mass_.upload(h_rand_mass_, stream_);
+    rand_fric_.upload(h_rand_fric_, stream_);
+    rand_gain_.upload(h_rand_gain_, stream_);
+  }
+  check(cudaStreamSynchronize(stream_), "init sync");
+}
+
+void Engine::choose_launch() {
+  lockstep_ = cfg_.lockstep ? 1 : 0;
+  const int per_warp = (desc_words_ + ws_stride_) * 4;
+  if (cfg_.warps_per_block > 0) warps_ = cfg_.warps_per_block;
+  else if (lockstep_) warps_ = std::max(1, std::min(16, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs per SM
+  else warps_ = 4;
+  smem_ = warps_ * (desc_words_ + ws_stride_) * 4;
+  if (smem_ > 227 * 1024) {
+    warps_ = std::max(1, (227 * 1024) / ((desc_words_ + ws_stride_) * 4));
+    smem_ = warps_ * (desc_words_ + ws_stride_) * 4;
+  }
+  if (smem_ > 227 * 1024) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
+  int bps = 0;
+  check(mjb_occupancy(warps_, smem_, &bps), "occupancy");
+  if (bps < 1) throw std::runtime_error("engine: kernel cannot be resident with this configuration");
+  if (cfg_.blocks_per_sm > 0) bps = std::min(bps, cfg_.blocks_per_sm);
+  persistent_ = lockstep_ ? 1 : (cfg_.persistent < 0 ? 1 : cfg_.persistent);
+  if (persistent_) grid_ = std::min(sm_count_ * bps, (B_ + warps_ - 1) / warps_);
+  else grid_ = (B_ + warps_ - 1) / warps_;
+  grid_ = std::max(grid_, 1);
+}
+
+void Engine::configure(const EngineConfig& cfg) {
+  bool rebuild = cfg.ncon_max != cfg_.ncon_max || cfg.nefc_max != cfg_.nefc_max || cfg.tolerance != cfg_.tolerance || cfg.max_iter != cfg_.max_iter;
+  cfg_ = cfg;
+  sync();
+  if (rebuild) build_tables(cfg_, 0);
+  choose_launch();
+  invalidate_graphs();
+}
+
+void Engine::launch_shape(int* grid, int* warps, int* smem, int* persistent) const {
+  if (grid) *grid = grid_;
+  if (warps) *warps = warps_;
+  if (smem) *smem = smem_;
+  if (persistent) *persistent = persistent_;
+}
+
+StepParams Engine::params(int n, bool record) {
+  StepParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.models = d_models_.p;
+  P.itab = d_itab_.p;
+  P.ftab = d_ftab_.p;
+  P.num_envs = B_;
+  P.env_model = d_model_.p;
+  P.env_qadr = d_qadr_.p;
+  P.env_vadr = d_vadr_.p;
+  P.env_uadr = d_uadr_.p;
+  P.env_badr = d_badr_.p;
+  P.qpos = qpos_.p;
+  P.qvel = qvel_.p;
+  P.ctrl = ctrl_.p;
+  P.qacc_warm = warm_.p;
+  P.qacc_pred = use_pred_ ? pred_.p : nullptr;
+  P.nsub = n;
+  P.max_iter = 0;
+  P.work_counter = (persistent_ && !lockstep_) ? counter_.p : nullptr;
+  P.lockstep = lockstep_;
+  P.stage_cycles = timing_ ? stage_cycles_.p : nullptr;
+  P.ws_stride = ws_stride_;
+  P.desc_words = desc_words_;
+  P.status = status_.p;
+  P.niter_sum = niter_sum_.p;
+  P.niter_max = niter_max_.p;
+  P.ncon_out = ncon_.p;
+  P.nefc_out = nefc_.p;
+  P.warm_choice = choice_.p;
+  if (record) {
+    P.rec_xpos = rec_xpos_.p;
+    P.rec_xquat = rec_xquat_.p;
+    P.rec_scom = rec_scom_.p;
+    P.rec_cinert = rec_cinert_.p;
+    P.rec_cvel = rec_cvel_.p;
+    P.rec_qfrc_actuator = rec_qfa_.p;
+    P.rec_cfrc_ext = rec_cfrc_.p;
+    P.rec_qacc = rec_qacc_.p;
+    if (dbg_ncon_ > 0) {
+      P.dbg_contacts = dbg_con_.p;
+      P.dbg_ncon_max = dbg_ncon_;
+      P.dbg_efc = dbg_efc_.p;
+      P.dbg_nefc_max = dbg_nefc_;
+      P.dbg_vec = dbg_vec_.p;
+      P.dbg_nv_max = nv_max_;
+    }
+  }
+  if (rand_on_) {
+    P.rand_mass = rand_mass_.p;
+    P.rand_friction = rand_fric_.p;
+    P.rand_gain = rand_gain_.p;
+  }
+  P.features = feat_.p;
+  P.feat_stride = feat_stride_;
+  return P;
+}
+
+void Engine::invalidate_graphs() {
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+  graphs_.clear();
+}
+
+void Engine::launch(int n, bool record) {
+  if (n <= 0) return;
+  StepParams P = params(n, record);
+  auto body = [&]() {
+    if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
+    check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+  };
+  if (!cfg_.use_graph) {
+    body();
+    return;
+  }
+  auto key = std::make_pair(n, record ? 1 : 0);
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    cudaGraph_t g;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    body();
+    check(cudaStreamEndCapture(stream_, &g), "end capture");
+    cudaGraphExec_t ge;
+    check(cudaGraphInstantiate(&ge, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    it = graphs_.emplace(key, ge).first;
+  }
+  check(cudaGraphLaunch(it->second, stream_), "graph launch");
+}
+
+void Engine::step(const float* ctrl_host, int n) {
+  if (tot_u_ > 0) {
+    if (ctrl_host) {
+      // stage through pinned memory so the copy is a true async DMA
+      check(cudaStreamSynchronize(stream_), "ctrl staging sync");
+      std::memcpy(h_ctrl_pinned_, ctrl_host, sizeof(float) * tot_u_);
+      check(cudaMemcpyAsync(ctrl_.p, h_ctrl_pinned_, sizeof(float) * tot_u_, cudaMemcpyHostToDevice, stream_), "ctrl upload");
+    } else {
+      check(cudaMemsetAsync(ctrl_.p, 0, sizeof(float) * tot_u_, stream_), "ctrl zero");
+    }
+  }
+  launch(n, cfg_.record != 0);
+}
+
+void Engine::step_device(int n) { launch(n, cfg_.record != 0); }
+
+void Engine::sync() { check(cudaStreamSynchronize(stream_), "stream sync"); }
+
+void Engine::get_state(float* qpos, float* qvel) {
+  if (qpos) check(cudaMemcpyAsync(qpos, qpos_.p, sizeof(float) * tot_q_, cudaMemcpyDeviceToHost, stream_), "get qpos");
+  if (qvel) check(cudaMemcpyAsync(qvel, qvel_.p, sizeof(float) * tot_v_, cudaMemcpyDeviceToHost, stream_), "get qvel");
+  sync();
+}
+
+void Engine::set_state(const float* qpos, const float* qvel) {
+  sync();
+  if (qpos) check(cudaMemcpy(qpos_.p, qpos, sizeof(float) * tot_q_, cudaMemcpyHostToDevice), "set qpos");
+  if (qvel) check(cudaMemcpy(qvel_.p, qvel, sizeof(float) * tot_v_, cudaMemcpyHostToDevice), "set qvel");
+}
+
+void Engine::set_env_state(int env, const float* qpos, const float* qvel) {
+  if (env < 0 || env >= B_) return;
+  const Model& m = *models_[h_model_[env]];
+  sync();
+  if (qpos) check(cudaMemcpy(qpos_.p + h_qadr_[env], qpos, sizeof(float) * m.nq, cudaMemcpyHostToDevice), "set env qpos");
+  if (qvel) check(cudaMemcpy(qvel_.p + h_vadr_[env], qvel, sizeof(float) * m.nv, cudaMemcpyHostToDevice), "set env qvel");
+}
+
+void Engine::reset(const int* mask) {
+  if (!mask) return;
+  DevBuf<int> dm;
+  std::vector<int> hm(mask, mask + B_);
+  dm.upload(hm, stream_);
+  check(mjb_launch_reset(d_models_.p, d_model_.p, d_qadr_.p, d_vadr_.p, d_ftab_.p, dm.p, B_, qpos_.p, qvel_.p, warm_.p, stream_), "reset kernel");
+  sync();
+}
+
+const float* Engine::get_host(const char* what, int* n) {
+  std::string w(what);
+  float* src = nullptr;
+  size_t cnt = 0;
+  if (w == "qpos") { src = qpos_.p; cnt = tot_q_; }
+  else if (w == "qvel") { src = qvel_.p; cnt = tot_v_; }
+  else if (w == "xpos") { src = rec_xpos_.p; cnt = 3 * tot_b_; }
+  else if (w == "xquat") { src = rec_xquat_.p; cnt = 4 * tot_b_; }
+  else if (w == "subtree_com") { src = rec_scom_.p; cnt = 3 * tot_b_; }
+  else if (w == "cinert") { src = rec_cinert_.p; cnt = 10 * tot_b_; }
+  else if (w == "cvel") { src = rec_cvel_.p; cnt = 6 * tot_b_; }
+  else if (w == "qfrc_actuator") { src = rec_qfa_.p; cnt = tot_v_; }
+  else if (w == "cfrc_ext") { src = rec_cfrc_.p; cnt = 6 * tot_b_; }
+  else if (w == "qacc") { src = rec_qacc_.p; cnt = tot_v_; }
+  else return nullptr;
+  auto it = h_stage_.find(w);
+  if (it == h_stage_.end()) {
+    float* h = nullptr;
+    check(cudaMallocHost(&h, sizeof(float) * std::max<size_t>(cnt, 1)), "cudaMallocHost");
+    it = h_stage_.emplace(w, h).first;
+    h_stage_n_[w] = cnt;
+  }
+  if (cnt) check(cudaMemcpyAsync(it->second, src, sizeof(float) * cnt, cudaMemcpyDeviceToHost, stream_), "getter copy");
+  sync();
+  if (n) *n = (int)cnt;
+  return it->second;
+}
+
+void Engine::stats(int* status, int* niter_sum, int* niter_max, int* ncon, int* nefc, int* choice) {
+  auto cp = [&](int* dst, DevBuf<int>& src) {
+    if (dst) check(cudaMemcpyAsync(dst, src.p, sizeof(int) * B_, cudaMemcpyDeviceToHost, stream_), "stats copy");
+  };
+  cp(status, status_);
+  cp(niter_sum, niter_sum_);
+  cp(niter_max, niter_max_);
+  cp(ncon, ncon_);
+  cp(nefc, nefc_);
+  cp(choice, choice_);
+  sync();
+}
+
+void Engine::set_debug(int ncon_max, int nefc_max) {
+  sync();
+  dbg_ncon_ = std::max(0, ncon_max);
+  dbg_nefc_ = std::max(0, nefc_max);
+  if (dbg_ncon_ > 0) {
+    dbg_con_.alloc((size_t)B_ * dbg_ncon_ * MJB_CONTACT_FLOATS);
+    dbg_efc_.alloc((size_t)B_ * std::max(1, dbg_nefc_) * 4);
+    dbg_vec_.alloc((size_t)B_ * 4 * nv_max_);
+  }
+  invalidate_graphs();
+}
+
+void Engine::get_debug(float* contacts, float* efc, float* vec) {
+  if (dbg_ncon_ <= 0) return;
+  if (contacts) check(cudaMemcpyAsync(contacts, dbg_con_.p, sizeof(float) * dbg_con_.n, cudaMemcpyDeviceToHost, stream_), "dbg copy");
+  if (efc) check(cudaMemcpyAsync(efc, dbg_efc_.p, sizeof(float) * dbg_efc_.n, cudaMemcpyDeviceToHost, stream_), "dbg copy");
+  if (vec) check(cudaMemcpyAsync(vec, dbg_vec_.p, sizeof(float) * dbg_vec_.n, cudaMemcpyDeviceToHost, stream_), "dbg copy");
+  sync();
+}
+
+int Engine::set_env_params(const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale) {
+  if (!rand_on_ || n < 0) return -1;
+  if (!env_idx && n != B_) return -1;
+  for (int i = 0; i < n; i++)
+    if (env_idx && (env_idx[i] < 0 || env_idx[i] >= B_)) return -2;
+  if (com_delta) {
+    for (int i = 0; i < n; i++) {
+      int e = env_idx ? env_idx[i] : i;
+      int nb = models_[h_model_[e]]->nbody;
+      for (int k = 0; k < 3 * nb; k++)
+        if (com_delta[(size_t)i * 3 * nb + k] != 0.f) return -1;  // COM offsets are not supported by this build
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    int e = env_idx ? env_idx[i] : i;
+    const Model& m = *models_[h_model_[e]];
+    if (mass_scale)
+      for (int b = 0; b < m.nbody; b++) h_rand_mass_[h_badr_[e] + b] = mass_scale[(size_t)i * m.nbody + b];
+    if (friction_scale) h_rand_fric_[e] = friction_scale[i];
+    if (gain_scale)
+      for (int a = 0; a < m.nu; a++) h_rand_gain_[h_uadr_[e] + a] = gain_scale[(size_t)i * m.nu + a];
+  }
+  sync();
+  rand_mass_.upload(h_rand_mass_, stream_);
+  rand_fric_.upload(h_rand_fric_, stream_);
+  rand_gain_.upload(h_rand_gain_, stream_);
+  sync();
+  return 0;
+}
+
+void Engine::stage_timing(int enable, unsigned long long* out8) {
+  sync();
+  if (out8) {
+    if (timing_) check(cudaMemcpy(out8, stage_cycles_.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stage cycles");
+    else std::memset(out8, 0, 8 * sizeof(unsigned long long));
+  }
+  if (enable >= 0) {
+    bool on = enable != 0;
+    if (on) {
+      if (!stage_cycles_.p) stage_cycles_.alloc(8);
+      check(cudaMemset(stage_cycles_.p, 0, 8 * sizeof(unsigned long long)), "stage cycles reset");
+    }
+    if (on != timing_) invalidate_graphs();
+    timing_ = on;
+  }
+}
+
+void Engine::set_features(int stride) {
+  sync();
+  feat_stride_ = stride;
+  if (stride > 0) feat_.alloc((size_t)B_ * stride);
+  else feat_.release();
+  invalidate_graphs();
+}
+
+}  // namespace mjb
+
+namespace mjb {
+
+// Packed read-back row: [qpos, qvel, |F| of each selected body (force part of
+// cfrc_ext), sum qfrc_actuator^2 over the dof range, sum |qfrc_actuator|]
+// (reference: mjmlx_batched_set_pack_spec / get_pack, src/batched.cpp:1675-1727).
+int Engine::pack_spec(const int* body_ids, int nsel, int dof_lo, int ndof) {
+  if (!uniform() || nsel < 0 || ndof < 0) return -1;
+  const Model& m = *models_[0];
+  if (nsel > 0 && !body_ids) return -1;
+  for (int i = 0; i < nsel; i++)
+    if (body_ids[i] < 0 || body_ids[i] >= m.nbody) return -1;
+  if (dof_lo < 0 || dof_lo + ndof > m.nv) return -1;
+  pack_bodies_.assign(body_ids, body_ids + nsel);
+  pack_dof_lo_ = dof_lo;
+  pack_ndof_ = ndof;
+  pack_stride_ = m.nq + m.nv + nsel + 2;
+  return pack_stride_;
+}
+
+int Engine::get_pack(float* out) {
+  if (pack_stride_ < 0) return -1;
+  const Model& m = *models_[0];
+  std::vector<float> qp(tot_q_), qv(tot_v_);
+  get_state(qp.data(), qv.data());
+  int n = 0;
+  const float* cf = get_host("cfrc_ext", &n);
+  std::vector<float> cfrc(cf, cf + n);
+  const float* qa = get_host("qfrc_actuator", &n);
+  for (int e = 0; e < B_; e++) {
+    float* row = out + (size_t)e * pack_stride_;
+    std::memcpy(row, &qp[(size_t)e * m.nq], sizeof(float) * m.nq);
+    std::memcpy(row + m.nq, &qv[(size_t)e * m.nv], sizeof(float) * m.nv);
+    for (size_t k = 0; k < pack_bodies_.size(); k++) {
+      const float* f = &cfrc[((size_t)e * m.nbody + pack_bodies_[k]) * 6 + 3];
+      row[m.nq + m.nv + k] = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    }
+    float s2 = 0, s1 = 0;
+    for (int d = pack_dof_lo_; d < pack_dof_lo_ + pack_ndof_; d++) {
+      float v = qa[(size_t)e * m.nv + d];
+      s2 += v * v;
+      s1 += std::fabs(v);
+    }
+    row[m.nq + m.nv + pack_bodies_.size()] = s2;
+    row[m.nq + m.nv + pack_bodies_.size() + 1] = s1;
+  }
+  return 0;
+}
+
+int Engine::raycast(const float*, const float*, int, int, const unsigned char*, int, float*, int*) {
+  throw std::runtime_error("raycast is not available in this build yet");
+}
+
+}  // namespace mjb

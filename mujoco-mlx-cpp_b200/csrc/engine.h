@@ -1,0 +1,172 @@
+// Host runtime of the batched step: device model tables, HBM state buffers,
+// launch configuration, CUDA graphs, getters.  Replaces the reference's
+// BatchedSim + make_batched_step pipeline (src/batched.cpp:891-1247,
+// src/internal.h:520-612) with explicit CUDA buffers and one fused launch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "devmodel.h"
+#include "model.h"
+#include "step_params.h"
+
+namespace mjb {
+
+struct EngineConfig {
+  int warps_per_block = 0;   // 0: autotuned / default
+  int persistent = -1;       // -1 auto, 0 static env mapping, 1 persistent work queue
+  int blocks_per_sm = 0;     // persistent grid: 0 = occupancy limit
+  int ncon_max = 0;          // 0 = auto per model
+  int nefc_max = 0;          // 0 = auto per model
+  int use_graph = 1;
+  int record = 1;            // write derived quantities (xpos, cvel, ...) on the last substep
+  int warmstart = 0;         // 0 previous-step (MuJoCo), 1 learned prediction + fallback
+  double tolerance = -1;     // > 0 overrides the model tolerance
+  int max_iter = 0;          // > 0 overrides the model / config iteration count
+  int lockstep = 1;          // warps of a CTA run the stages together (instruction-cache locality)
+};
+
+class CudaError : public std::runtime_error {
+ public:
+  using std::runtime_error::runtime_error;
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count);
+  void upload(const std::vector<T>& v, cudaStream_t s);
+};
+
+struct ModelLayout {
+  DevModelDesc desc;
+  int nq, nv, nu, nbody;
+};
+
+class Engine {
+ public:
+  Engine(const std::vector<const Model*>& models, const std::vector<int>& counts, int solver_iterations, int domain_rand, const EngineConfig& cfg);
+  ~Engine();
+
+  int num_envs() const { return B_; }
+  int nmodels() const { return (int)models_.size(); }
+  const Model& model(int i) const { return *models_[i]; }
+  int total_q() const { return tot_q_; }
+  int total_v() const { return tot_v_; }
+  int total_u() const { return tot_u_; }
+  int total_b() const { return tot_b_; }
+  bool uniform() const { return models_.size() == 1; }
+
+  void step(const float* ctrl_host, int n);    // host ctrl, async
+  void step_device(int n);                      // ctrl already on device
+  void sync();
+  cudaStream_t stream() const { return stream_; }
+
+  void get_state(float* qpos, float* qvel);
+  void set_state(const float* qpos, const float* qvel);
+  void set_env_state(int env, const float* qpos, const float* qvel);
+  void reset(const int* mask);
+  const float* get_host(const char* what, int* n);  // staging copies of recorded quantities
+
+  // per-env stats of the last launch
+  void stats(int* status, int* niter_sum, int* niter_max, int* ncon, int* nefc, int* choice);
+  void set_debug(int ncon_max, int nefc_max);
+  void get_debug(float* contacts, float* efc, float* vec);
+  int dbg_ncon_max() const { return dbg_ncon_; }
+  int dbg_nefc_max() const { return dbg_nefc_; }
+  int dbg_nv_max() const { return nv_max_; }
+
+  // domain randomisation
+  int set_env_params(const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale);
+  bool domain_rand() const { return rand_on_; }
+
+  // learned warm start
+  float* qacc_pred_device() { return pred_.p; }
+  void set_prediction_enabled(bool on) { use_pred_ = on; invalidate_graphs(); }
+  uint16_t* features_device() { return feat_.p; }
+  void set_features(int stride);
+
+  void configure(const EngineConfig& cfg);
+  const EngineConfig& config() const { return cfg_; }
+  void launch_shape(int* grid, int* warps, int* smem_bytes, int* persistent) const;
+  int lockstep() const { return lockstep_; }
+  void stage_timing(int enable, unsigned long long* out8);
+  std::vector<int> env_qadr() const { return h_qadr_; }
+  std::vector<int> env_vadr() const { return h_vadr_; }
+  std::vector<int> env_uadr() const { return h_uadr_; }
+
+  float* d_qpos() { return qpos_.p; }
+  float* d_qvel() { return qvel_.p; }
+  float* d_ctrl() { return ctrl_.p; }
+  float* d_qacc_warm() { return warm_.p; }
+
+  int pack_spec(const int* body_ids, int nsel, int dof_lo, int ndof);
+  int get_pack(float* out);
+  int raycast(const float* pnt, const float* vec, int nray, int bodyexclude, const unsigned char* geomgroup, int flg_static, float* dist, int* geomid);
+
+ private:
+  void build_tables(const EngineConfig& cfg, int solver_iterations);
+  void alloc_state();
+  void choose_launch();
+  void launch(int n, bool record);
+  void invalidate_graphs();
+  StepParams params(int n, bool record);
+
+  std::vector<const Model*> models_;
+  std::vector<int> counts_;
+  int B_ = 0, tot_q_ = 0, tot_v_ = 0, tot_u_ = 0, tot_b_ = 0, nv_max_ = 0;
+  EngineConfig cfg_;
+  bool rand_on_ = false;
+  bool use_pred_ = false;
+  cudaStream_t stream_ = nullptr;
+
+  std::vector<ModelLayout> layouts_;
+  std::vector<int> h_itab_;
+  std::vector<float> h_ftab_;
+  std::vector<int> h_model_, h_qadr_, h_vadr_, h_uadr_, h_badr_;
+  DevBuf<DevModelDesc> d_models_;
+  DevBuf<int> d_itab_, d_model_, d_qadr_, d_vadr_, d_uadr_, d_badr_;
+  DevBuf<float> d_ftab_;
+
+  DevBuf<float> qpos_, qvel_, ctrl_, warm_, pred_, qpos0_;
+  DevBuf<int> status_, niter_sum_, niter_max_, ncon_, nefc_, choice_, counter_;
+  DevBuf<float> rec_xpos_, rec_xquat_, rec_scom_, rec_cinert_, rec_cvel_, rec_qfa_, rec_cfrc_, rec_qacc_;
+  DevBuf<float> dbg_con_, dbg_efc_, dbg_vec_;
+  int dbg_ncon_ = 0, dbg_nefc_ = 0;
+  DevBuf<float> rand_mass_, rand_fric_, rand_gain_;
+  std::vector<float> h_rand_mass_, h_rand_fric_, h_rand_gain_;
+  DevBuf<uint16_t> feat_;
+  DevBuf<unsigned long long> stage_cycles_;
+  bool timing_ = false;
+  int feat_stride_ = 0;
+
+  float* h_ctrl_pinned_ = nullptr;
+  std::map<std::string, float*> h_stage_;
+  std::map<std::string, size_t> h_stage_n_;
+
+  int ws_stride_ = 0, desc_words_ = 0, warps_ = 4, grid_ = 1, smem_ = 0, persistent_ = 0, lockstep_ = 0, sm_count_ = 148;
+
+  std::map<std::pair<int, int>, cudaGraphExec_t> graphs_;
+
+  // packed read-back
+  std::vector<int> pack_bodies_;
+  int pack_dof_lo_ = 0, pack_ndof_ = 0, pack_stride_ = -1;
+  DevBuf<int> d_pack_bodies_;
+  DevBuf<float> d_pack_;
+};
+
+void check(cudaError_t e, const char* what);
+
+}  // namespace mjb

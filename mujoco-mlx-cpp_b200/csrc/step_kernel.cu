@@ -1,0 +1,392 @@
+// Fused physics-step kernel for sm_100a: one warp per environment, nsub
+// substeps per launch, every intermediate in the warp's shared-memory
+// workspace.  HBM traffic per env-substep is the state record only (qpos,
+// qvel, ctrl, warm-start qacc in; qpos, qvel, qacc out) -- the reference runs
+// six separate dispatches per substep that round-trip kinematics, mass
+// matrix, contacts and solver scratch through device memory
+// (src/batched.cpp:980-1228).
+#include <cuda_runtime.h>
+
+#include "dev_solver.cuh"
+#include "step_params.h"
+
+using namespace mjbdev;
+
+namespace {
+
+__device__ __forceinline__ bool badval(float v) { return !(fabsf(v) <= 1e10f); }
+
+__device__ __noinline__ void reset_env(Env& E) {
+  const DevModelDesc& m = *E.md;
+  float* ws = E.ws;
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nq; i += 32) ws[m.w_qpos + i] = ldf(E.ft, m.f_qpos0 + i);
+  #pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) {
+    ws[m.w_qvel + i] = 0;
+    ws[m.w_xwarm + i] = 0;
+    ws[m.w_x + i] = 0;
+  }
+  __syncwarp();
+}
+
+// contact wrench per body in com-based coordinates (torque about the
+// subtree COM of the body's root, force), accumulated by lane 0
+__device__ __noinline__ void record_cfrc(Env& E, const StepParams& P, int ncon, int nefc, float* out) {
+  const DevModelDesc& m = *E.md;
+  const float* efc = E.ws + m.w_efc;
+  const int ne = m.nefc_max;
+  const float* con = E.ws + m.w_con;
+  const float* scom = E.ws + m.w_scom;
+  #pragma unroll 1
+  for (int k = E.lane; k < 6 * m.nbody; k += 32) out[k] = 0;
+  __syncwarp();
+  if (E.lane == 0) {
+    int r = 0;
+    while (r < nefc) {
+      int c = (int)efc[EFC_CON * ne + r];
+      if (c < 0) { r++; continue; }
+      const float* cr = con + MJB_CONTACT_FLOATS * c;
+      int dim = (int)cr[14];
+      int nr = dim == 1 ? 1 : 2 * (dim - 1);
+      int p = (int)cr[13];
+      const float* pf = E.ft + m.f_pair + 16 * p;
+      float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
+      float fn = 0, ft[5] = {0, 0, 0, 0, 0};
+      #pragma unroll 1
+      for (int q = 0; q < nr; q++) fn += efc[EFC_FORCE * ne + r + q];
+      for (int d = 0; d + 1 < dim; d++)
+        ft[d] = ldf(pf, 2 + d) * fs * (efc[EFC_FORCE * ne + r + 2 * d] - efc[EFC_FORCE * ne + r + 2 * d + 1]);
+      const float* n = cr + 3;
+      const float* t1 = cr + 6;
+      const float* t2 = cr + 9;
+      float F[3], T[3];
+      for (int k = 0; k < 3; k++) {
+        F[k] = fn * n[k] + ft[0] * t1[k] + ft[1] * t2[k];
+        T[k] = ft[2] * n[k] + ft[3] * t1[k] + ft[4] * t2[k];
+      }
+      int b1 = ldi(E.it, m.i_pair + 6 * p + 2), b2 = ldi(E.it, m.i_pair + 6 * p + 3);
+      for (int side = 0; side < 2; side++) {
+        int b = side == 0 ? b2 : b1;
+        float sg = side == 0 ? 1.f : -1.f;
+        int root = ldi(E.it, m.i_body_rootid + b);
+        float off[3] = {cr[0] - scom[3 * root], cr[1] - scom[3 * root + 1], cr[2] - scom[3 * root + 2]}, tq[3];
+        cross3(off, F, tq);
+        for (int k = 0; k < 3; k++) {
+          out[6 * b + k] += sg * (tq[k] + T[k]);
+          out[6 * b + 3 + k] += sg * F[k];
+        }
+      }
+      r += nr;
+    }
+  }
+  __syncwarp();
+}
+
+}  // namespace
+
+extern __shared__ float mjb_smem[];
+
+namespace {
+
+__device__ __noinline__ void record_debug(Env& E, const StepParams& P, int ncon, int nefc, const float* qfc) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  const int lane = E.lane, nv = m.nv, env = E.env;
+  float* dc = P.dbg_contacts + (size_t)env * P.dbg_ncon_max * MJB_CONTACT_FLOATS;
+  int nc = ncon < P.dbg_ncon_max ? ncon : P.dbg_ncon_max;
+#pragma unroll 1
+  for (int k = lane; k < nc * MJB_CONTACT_FLOATS; k += 32) dc[k] = ws[m.w_con + k];
+  float* de = P.dbg_efc + (size_t)env * P.dbg_nefc_max * 4;
+  int ne = nefc < P.dbg_nefc_max ? nefc : P.dbg_nefc_max;
+#pragma unroll 1
+  for (int r = lane; r < ne; r += 32) {
+    EfcRef e{const_cast<float*>(ws) + m.w_efc + r, m.nefc_max};
+    de[4 * r] = e[EFC_TYPE];
+    de[4 * r + 1] = e[EFC_FORCE];
+    de[4 * r + 2] = e[EFC_D];
+    de[4 * r + 3] = e[EFC_AREF];
+  }
+  float* dv = P.dbg_vec + (size_t)env * 4 * P.dbg_nv_max;
+#pragma unroll 1
+  for (int k = lane; k < nv; k += 32) {
+    dv[k] = ws[m.w_qas + k];
+    dv[P.dbg_nv_max + k] = ws[m.w_qfs + k];
+    dv[2 * P.dbg_nv_max + k] = ws[m.w_x + k];
+    dv[3 * P.dbg_nv_max + k] = qfc[k];
+  }
+  __syncwarp();
+}
+
+__device__ __noinline__ void record_kin(Env& E, const StepParams& P, int badr) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  const int lane = E.lane;
+#pragma unroll 1
+  for (int k = lane; k < 3 * m.nbody; k += 32) {
+    P.rec_xpos[3 * badr + k] = ws[m.w_xpos + k];
+    P.rec_scom[3 * badr + k] = ws[m.w_scom + k];
+  }
+#pragma unroll 1
+  for (int k = lane; k < 4 * m.nbody; k += 32) P.rec_xquat[4 * badr + k] = ws[m.w_xquat + k];
+#pragma unroll 1
+  for (int k = lane; k < 10 * m.nbody; k += 32) P.rec_cinert[10 * badr + k] = ws[m.w_cinert + k];
+}
+
+__device__ __noinline__ void record_dyn(Env& E, const StepParams& P, int badr, int vadr) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  const int lane = E.lane;
+#pragma unroll 1
+  for (int k = lane; k < 6 * m.nbody; k += 32) P.rec_cvel[6 * badr + k] = ws[m.w_cvel + k];
+#pragma unroll 1
+  for (int k = lane; k < m.nv; k += 32) P.rec_qfrc_actuator[vadr + k] = ws[m.w_qfa + k];
+}
+
+// unconstrained acceleration qacc_smooth = M^-1 qfrc_smooth
+__device__ __noinline__ void d_qacc_smooth(Env& E) {
+  const DevModelDesc& m = *E.md;
+  float* ws = E.ws;
+  const int nv = m.nv, lane = E.lane;
+  float* H = ws + m.w_H;
+#pragma unroll 1
+  for (int k = lane; k < nv * nv; k += 32) H[k] = ws[m.w_M + k];
+#pragma unroll 1
+  for (int k = lane; k < nv; k += 32) ws[m.w_qas + k] = ws[m.w_qfs + k];
+  __syncwarp();
+  d_chol(H, nv, lane);
+  d_chol_solve(H, nv, ws + m.w_qas, lane);
+}
+
+// bad-acceleration check, implicit-damping solve, warm-start save, integration.
+// Returns false if the env was reset.
+__device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
+  const DevModelDesc& m = *E.md;
+  float* ws = E.ws;
+  const int nv = m.nv, lane = E.lane;
+  const float* x = ws + m.w_x;
+  bool badacc = false;
+#pragma unroll 1
+  for (int i = lane; i < nv; i += 32) badacc |= badval(x[i]);
+  if (__any_sync(FULL_MASK, badacc)) {
+    E.status |= MJB_STATUS_BADQACC;
+    reset_env(E);
+    return false;
+  }
+  const float* a = x;
+  if (m.implicit) {
+    float* H = ws + m.w_H;
+#pragma unroll 1
+    for (int k = lane; k < nv * nv; k += 32) {
+      int i = k / nv, j = k - i * nv;
+      H[k] = ws[m.w_M + k] + (i == j ? m.timestep * ldf(E.ft, m.f_dof_damping_implicit + i) : 0.f);
+    }
+#pragma unroll 1
+    for (int k = lane; k < nv; k += 32) acc[k] = ws[m.w_qfs + k] + qfc[k];
+    __syncwarp();
+    d_chol(H, nv, lane);
+    d_chol_solve(H, nv, acc, lane);
+    a = acc;
+  }
+#pragma unroll 1
+  for (int k = lane; k < nv; k += 32) ws[m.w_xwarm + k] = x[k];
+  __syncwarp();
+  d_integrate(E, a);
+  return true;
+}
+
+__device__ __noinline__ void check_state(Env& E) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  bool bad = false;
+#pragma unroll 1
+  for (int i = E.lane; i < m.nq; i += 32) bad |= badval(ws[m.w_qpos + i]);
+#pragma unroll 1
+  for (int i = E.lane; i < m.nv; i += 32) bad |= badval(ws[m.w_qvel + i]);
+  if (__any_sync(FULL_MASK, bad)) {
+    E.status |= MJB_STATUS_BADSTATE;
+    reset_env(E);
+  }
+}
+
+}  // namespace
+
+// Two execution modes share the stage functions:
+//  * independent warps (P.lockstep == 0): each warp takes envs from the
+//    persistent queue and runs all stages on its own;
+//  * block lockstep (P.lockstep == 1): the warps of a CTA process a group of
+//    envs together and meet at a barrier after every stage, so all warps of
+//    the CTA execute the same stage code at the same time (instruction-cache
+//    locality); envs whose Newton solve ends early wait at the barrier.
+__global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int W = blockDim.x >> 5;
+  const bool lockstep = P.lockstep != 0;
+  int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
+  float* ws = mjb_smem + W * P.desc_words + warp * P.ws_stride;
+  // optional per-stage timing: thread 0 of each CTA accumulates the clock
+  // between consecutive stage barriers
+  const bool timing = lockstep && P.stage_cycles != nullptr && threadIdx.x == 0;
+  unsigned long long tstage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long tlast = timing ? clock64() : 0;
+  int stage_id = 0;
+#define STAGE_SYNC()                                  \
+  do {                                                \
+    if (lockstep) __syncthreads();                    \
+    if (timing) {                                     \
+      long long t_ = clock64();                       \
+      tstage[stage_id & 7] += (unsigned long long)(t_ - tlast); \
+      tlast = t_;                                     \
+    }                                                 \
+    stage_id++;                                       \
+  } while (0)
+
+  int group = blockIdx.x;
+  int env = blockIdx.x * W + warp;
+  if (!lockstep && P.work_counter) {
+    int e = 0;
+    if (lane == 0) e = atomicAdd(P.work_counter, 1);
+    env = __shfl_sync(FULL_MASK, e, 0);
+  }
+  for (;;) {
+    if (lockstep) {
+      if (group * W >= P.num_envs) break;
+      env = group * W + warp;
+    } else if (env >= P.num_envs) {
+      break;
+    }
+    const bool valid = env < P.num_envs;
+    Env E;
+    E.it = P.itab;
+    E.ft = P.ftab;
+    E.ws = ws;
+    E.lane = lane;
+    E.env = env;
+    E.status = 0;
+    E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+    int qadr = 0, vadr = 0, badr = 0, nv = 0;
+    if (valid) {
+      const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
+#pragma unroll 1
+      for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
+      __syncwarp();
+      const DevModelDesc& m = *E.md;
+      nv = m.nv;
+      qadr = P.env_qadr[env];
+      vadr = P.env_vadr[env];
+      badr = P.env_badr[env];
+      const int uadr = P.env_uadr[env];
+#pragma unroll 1
+      for (int i = lane; i < m.nq; i += 32) ws[m.w_qpos + i] = P.qpos[qadr + i];
+#pragma unroll 1
+      for (int i = lane; i < nv; i += 32) {
+        ws[m.w_qvel + i] = P.qvel[vadr + i];
+        ws[m.w_xwarm + i] = P.qacc_warm[vadr + i];
+      }
+#pragma unroll 1
+      for (int i = lane; i < m.nu; i += 32) ws[m.w_ctrl + i] = P.ctrl[uadr + i];
+      __syncwarp();
+    }
+    const int max_iter = valid ? (P.max_iter > 0 ? P.max_iter : E.md->iterations) : 0;
+    int nsum = 0, nmax = 0, ncon = 0, nefc = 0, choice = 0;
+    float* vec = valid ? ws + E.md->w_vec : ws;
+    float* qfc = vec + 5 * nv;
+    float* acc = vec + 6 * nv;
+    float* bias = vec + 7 * nv;
+#pragma unroll 1
+    for (int s = 0; s < P.nsub; s++) {
+      const bool last = s == P.nsub - 1;
+      stage_id = 0;
+      if (valid) {
+        check_state(E);
+        d_kinematics(E);
+      }
+      STAGE_SYNC();
+      if (valid) ncon = d_collide(E);
+      STAGE_SYNC();
+      if (valid) {
+        d_com(E, P);
+        if (last && P.rec_xpos) record_kin(E, P, badr);
+        d_crb(E);
+      }
+      STAGE_SYNC();
+      if (valid) {
+        d_rne(E, bias);
+        d_forces(E, P, bias);
+        if (last && P.rec_xpos) record_dyn(E, P, badr, vadr);
+      }
+      STAGE_SYNC();
+      if (valid) d_qacc_smooth(E);
+      STAGE_SYNC();
+      if (valid) nefc = d_constraints(E, P, ncon);
+      STAGE_SYNC();
+      if (valid) {
+        const float* xpred = P.qacc_pred ? P.qacc_pred + vadr : nullptr;
+        int it = d_newton(E, P, nefc, max_iter, xpred, choice);
+        nsum += it;
+        nmax = it > nmax ? it : nmax;
+      }
+      STAGE_SYNC();
+      if (valid) {
+        d_jtf(E, nefc, qfc);
+        if (last && P.dbg_contacts) record_debug(E, P, ncon, nefc, qfc);
+        if (last && P.rec_cfrc_ext) record_cfrc(E, P, ncon, nefc, P.rec_cfrc_ext + 6 * badr);
+        if (last && P.rec_qacc) {
+#pragma unroll 1
+          for (int k = lane; k < nv; k += 32) P.rec_qacc[vadr + k] = ws[E.md->w_x + k];
+        }
+        d_finish(E, qfc, acc);
+      }
+      STAGE_SYNC();
+    }
+    if (valid) {
+      const DevModelDesc& m = *E.md;
+#pragma unroll 1
+      for (int i = lane; i < m.nq; i += 32) P.qpos[qadr + i] = ws[m.w_qpos + i];
+#pragma unroll 1
+      for (int i = lane; i < nv; i += 32) {
+        P.qvel[vadr + i] = ws[m.w_qvel + i];
+        P.qacc_warm[vadr + i] = ws[m.w_xwarm + i];
+      }
+      if (lane == 0) {
+        if (P.status) P.status[env] = E.status;
+        if (P.niter_sum) P.niter_sum[env] = nsum;
+        if (P.niter_max) P.niter_max[env] = nmax;
+        if (P.ncon_out) P.ncon_out[env] = ncon;
+        if (P.nefc_out) P.nefc_out[env] = nefc;
+        if (P.warm_choice) P.warm_choice[env] = choice;
+      }
+      __syncwarp();
+    }
+    if (lockstep) {
+      group += gridDim.x;
+      __syncthreads();
+    } else if (P.work_counter) {
+      int e = 0;
+      if (lane == 0) e = atomicAdd(P.work_counter, 1);
+      env = __shfl_sync(FULL_MASK, e, 0);
+    } else {
+      env += gridDim.x * W;
+    }
+  }
+  if (timing)
+    for (int k = 0; k < 8; k++) atomicAdd(P.stage_cycles + k, tstage[k]);
+#undef STAGE_SYNC
+}
+
+cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
+  static size_t configured = 0;
+  if (smem_bytes > configured) {
+    cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    configured = smem_bytes;
+  }
+  mjb_step_kernel<<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel, warps_per_block * 32, smem_bytes);
+}

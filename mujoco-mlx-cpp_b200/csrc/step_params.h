@@ -1,0 +1,70 @@
+// Launch parameters of the fused physics-step kernel (POD, host and device).
+#pragma once
+#include <stdint.h>
+
+#include "devmodel.h"
+
+struct StepParams {
+  // model tables
+  const DevModelDesc* models;
+  const int* itab;
+  const float* ftab;
+
+  // batch layout: per-env model id and offsets into the state arrays
+  int num_envs;
+  const int* env_model;
+  const int* env_qadr;   // into qpos
+  const int* env_vadr;   // into qvel / qacc_warm / qacc_pred
+  const int* env_uadr;   // into ctrl / rand_gain
+  const int* env_badr;   // into body-indexed outputs and rand_mass
+
+  // state (env-major records, HBM-resident)
+  float* qpos;
+  float* qvel;
+  const float* ctrl;
+  float* qacc_warm;
+  const float* qacc_pred;   // predicted warm start (nullable)
+
+  int nsub;                 // substeps per launch (same ctrl)
+  int max_iter;             // <= 0: model default
+  int* work_counter;        // persistent scheduling queue head (nullable = static env mapping)
+  int lockstep;             // 1: the warps of a CTA run each stage together (barrier between stages)
+  unsigned long long* stage_cycles;  // nullable: per-stage SM clock totals (lockstep mode, 8 stages)
+  int ws_stride;            // floats of shared workspace per warp
+  int desc_words;           // 32-bit words of DevModelDesc copied into shared memory
+
+  // per-env statistics of this launch
+  int* status;
+  int* niter_sum;
+  int* niter_max;
+  int* ncon_out;
+  int* nefc_out;
+  int* warm_choice;
+
+  // values recorded on the last substep (nullable)
+  float* rec_xpos;
+  float* rec_xquat;
+  float* rec_scom;
+  float* rec_cinert;
+  float* rec_cvel;
+  float* rec_qfrc_actuator;
+  float* rec_cfrc_ext;
+  float* rec_qacc;
+
+  // parity/debug outputs on the last substep (nullable)
+  float* dbg_contacts;      // [B][dbg_ncon_max][MJB_CONTACT_FLOATS]
+  int dbg_ncon_max;
+  float* dbg_efc;           // [B][dbg_nefc_max][4]: type, force, D, aref
+  int dbg_nefc_max;
+  float* dbg_vec;           // [B][4*dbg_nv_max]: qacc_smooth, qfrc_smooth, qacc, qfrc_constraint
+  int dbg_nv_max;
+
+  // per-env randomisation (nullable)
+  const float* rand_mass;      // [badr + body]
+  const float* rand_friction;  // [env]
+  const float* rand_gain;      // [uadr + actuator]
+
+  // learned warm start: feature rows written after each substep (nullable)
+  uint16_t* features;          // bf16 [B][feat_stride]
+  int feat_stride;
+};

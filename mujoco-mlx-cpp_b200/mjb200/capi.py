@@ -26,6 +26,12 @@ class MjmlxBatchedConfig(C.Structure):
                 ("solver_iterations", C.c_int), ("domain_rand", C.c_int)]
 
 
+class MjbEngineConfig(C.Structure):
+    _fields_ = [("warps_per_block", C.c_int), ("persistent", C.c_int), ("blocks_per_sm", C.c_int), ("ncon_max", C.c_int),
+                ("nefc_max", C.c_int), ("use_graph", C.c_int), ("record", C.c_int), ("warmstart", C.c_int),
+                ("tolerance", C.c_double), ("max_iter", C.c_int), ("lockstep", C.c_int)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(f"{LIB_PATH} is missing: run mujoco-mlx-cpp_b200/build.py (no fallback exists)")
@@ -41,7 +47,37 @@ def _load():
         "mjmlx_model_opt_timestep": (C.c_float, [C.c_void_p]),
         "mjmlx_name2id": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p]),
         "mjb200_model_dump": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+        "mjmlx_batched_create": (C.c_void_p, [C.c_void_p, C.POINTER(MjmlxBatchedConfig)]),
+        "mjmlx_batched_free": (None, [C.c_void_p]),
+        "mjmlx_batched_step": (None, [C.c_void_p, _f32p]),
+        "mjmlx_batched_step_n": (None, [C.c_void_p, _f32p, C.c_int]),
+        "mjmlx_batched_reset": (None, [C.c_void_p, _i32p]),
+        "mjmlx_batched_get_state": (None, [C.c_void_p, _f32p, _f32p, _i32p, _i32p]),
+        "mjmlx_batched_set_state": (None, [C.c_void_p, _f32p, _f32p]),
+        "mjmlx_batched_set_env_qpos": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
+        "mjmlx_batched_set_env_qvel": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
+        "mjmlx_batched_set_env_params": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p, _f32p, _f32p, _f32p]),
+        "mjmlx_batched_set_pack_spec": (C.c_int, [C.c_void_p, _i32p, C.c_int, C.c_int, C.c_int]),
+        "mjmlx_batched_get_pack": (C.c_int, [C.c_void_p, _f32p]),
+        "mjmlx_batched_raycast": (C.c_int, [C.c_void_p, _f32p, _f32p, C.c_int, C.c_int, C.POINTER(C.c_ubyte), C.c_int, _f32p, _i32p]),
+        "mjmlx_batched_eval_state": (None, [C.c_void_p]),
+        "mjb200_default_engine_config": (MjbEngineConfig, []),
+        "mjb200_batched_create_multi": (C.c_void_p, [C.POINTER(C.c_void_p), _i32p, C.c_int, C.POINTER(MjmlxBatchedConfig), C.POINTER(MjbEngineConfig)]),
+        "mjb200_batched_configure": (C.c_int, [C.c_void_p, C.POINTER(MjbEngineConfig)]),
+        "mjb200_batched_get_config": (C.c_int, [C.c_void_p, C.POINTER(MjbEngineConfig)]),
+        "mjb200_batched_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
+        "mjb200_batched_step_device": (C.c_int, [C.c_void_p, C.c_int]),
+        "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+        "mjb200_batched_stream": (C.c_void_p, [C.c_void_p]),
+        "mjb200_batched_launch_shape": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p]),
+        "mjb200_batched_stats": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
+        "mjb200_batched_get_qacc": (_f32p, [C.c_void_p, _i32p]),
+        "mjb200_batched_set_debug": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+        "mjb200_batched_stage_timing": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)]),
+        "mjb200_batched_get_debug": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
     }
+    for g in ("qpos", "qvel", "xpos", "xquat", "subtree_com", "cinert", "cvel", "qfrc_actuator", "cfrc_ext"):
+        sig[f"mjmlx_batched_get_{g}"] = (_f32p, [C.c_void_p, _i32p])
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype = res
@@ -112,5 +148,151 @@ def load_model(path: str) -> Model:
     return Model(lib.mjmlx_load_model(path.encode()))
 
 
-class BatchedSim:  # filled in by engine bindings below
-    pass
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(_f32p)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_i32p)
+
+
+def engine_config(**kw) -> MjbEngineConfig:
+    c = lib.mjb200_default_engine_config()
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class BatchedSim:
+    """Batched simulation on the CUDA engine (mirrors the reference's Python
+    BatchedSim: step(ctrl, n), state(), set_state())."""
+
+    def __init__(self, models, counts=None, solver_iterations: int = 0, domain_rand: int = 0, integrator: int = 0, **engine_kw):
+        if isinstance(models, Model):
+            models = [models]
+            counts = [counts if counts is not None else 1]
+        self.models = list(models)
+        self.counts = list(counts)
+        cfg = MjmlxBatchedConfig(int(sum(self.counts)), integrator, 1, solver_iterations, domain_rand)
+        ecfg = engine_config(**engine_kw)
+        arr = (C.c_void_p * len(self.models))(*[m.handle.value for m in self.models])
+        cnt = np.ascontiguousarray(self.counts, np.int32)
+        h = lib.mjb200_batched_create_multi(arr, _ip(cnt), len(self.models), C.byref(cfg), C.byref(ecfg))
+        if not h:
+            raise RuntimeError("batched create failed: " + last_error())
+        self.handle = C.c_void_p(h)
+        n, tq, tv, tu = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        lib.mjb200_batched_layout(self.handle, C.byref(n), C.byref(tq), C.byref(tv), C.byref(tu), None, None, None)
+        self.num_envs, self.total_q, self.total_v, self.total_u = n.value, tq.value, tv.value, tu.value
+        self.qadr = np.zeros(self.num_envs, np.int32)
+        self.vadr = np.zeros(self.num_envs, np.int32)
+        self.uadr = np.zeros(self.num_envs, np.int32)
+        lib.mjb200_batched_layout(self.handle, None, None, None, None, _ip(self.qadr), _ip(self.vadr), _ip(self.uadr))
+        self.uniform = len(self.models) == 1
+
+    def close(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.mjmlx_batched_free(h)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- stepping
+    def step(self, ctrl=None, n: int = 1):
+        c = None if ctrl is None else np.ascontiguousarray(ctrl, np.float32).reshape(-1)
+        if c is not None and c.size != self.total_u:
+            raise ValueError(f"ctrl must have {self.total_u} values")
+        lib.mjmlx_batched_step_n(self.handle, _fp(c), n)
+
+    def step_device(self, n: int = 1):
+        if lib.mjb200_batched_step_device(self.handle, n) != 0:
+            raise RuntimeError(last_error())
+
+    def sync(self):
+        lib.mjmlx_batched_eval_state(self.handle)
+
+    # ---- state
+    def state(self):
+        qpos = np.zeros(self.total_q, np.float32)
+        qvel = np.zeros(self.total_v, np.float32)
+        lib.mjmlx_batched_get_state(self.handle, _fp(qpos), _fp(qvel), None, None)
+        if self.uniform:
+            return qpos.reshape(self.num_envs, -1), qvel.reshape(self.num_envs, -1)
+        return qpos, qvel
+
+    def set_state(self, qpos=None, qvel=None):
+        qp = None if qpos is None else np.ascontiguousarray(qpos, np.float32).reshape(-1)
+        qv = None if qvel is None else np.ascontiguousarray(qvel, np.float32).reshape(-1)
+        lib.mjmlx_batched_set_state(self.handle, _fp(qp), _fp(qv))
+
+    def reset(self, mask):
+        m = np.ascontiguousarray(mask, np.int32)
+        lib.mjmlx_batched_reset(self.handle, _ip(m))
+
+    def get(self, name: str):
+        n = C.c_int()
+        if name == "qacc":
+            p = lib.mjb200_batched_get_qacc(self.handle, C.byref(n))
+        else:
+            p = getattr(lib, f"mjmlx_batched_get_{name}")(self.handle, C.byref(n))
+        if not p:
+            raise RuntimeError(f"get {name} failed: " + last_error())
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def stats(self):
+        B = self.num_envs
+        out = {k: np.zeros(B, np.int32) for k in ("status", "niter_sum", "niter_max", "ncon", "nefc", "warm_choice")}
+        lib.mjb200_batched_stats(self.handle, *[_ip(out[k]) for k in ("status", "niter_sum", "niter_max", "ncon", "nefc", "warm_choice")])
+        return out
+
+    def set_env_params(self, env_idx=None, mass_scale=None, friction_scale=None, gain_scale=None):
+        n = self.num_envs if env_idx is None else len(env_idx)
+        ei = None if env_idx is None else np.ascontiguousarray(env_idx, np.int32)
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1)
+        ms, fs, gs = conv(mass_scale), conv(friction_scale), conv(gain_scale)
+        return lib.mjmlx_batched_set_env_params(self.handle, _ip(ei), n, _fp(ms), None, _fp(fs), _fp(gs))
+
+    # ---- debug capture
+    def set_debug(self, ncon_max: int = 32, nefc_max: int = 128):
+        self.dbg = (ncon_max, nefc_max)
+        lib.mjb200_batched_set_debug(self.handle, ncon_max, nefc_max)
+
+    def get_debug(self):
+        nc, ne = self.dbg
+        B = self.num_envs
+        nvmax = max(m.nv for m in self.models)
+        con = np.zeros((B, nc, 16), np.float32)
+        efc = np.zeros((B, ne, 4), np.float32)
+        vec = np.zeros((B, 4, nvmax), np.float32)
+        lib.mjb200_batched_get_debug(self.handle, _fp(con), _fp(efc), _fp(vec))
+        return con, efc, vec
+
+    def configure(self, **kw):
+        c = MjbEngineConfig()
+        lib.mjb200_batched_get_config(self.handle, C.byref(c))
+        for k, v in kw.items():
+            setattr(c, k, v)
+        if lib.mjb200_batched_configure(self.handle, C.byref(c)) != 0:
+            raise RuntimeError(last_error())
+
+    STAGES = ("kinematics", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "newton", "integrate")
+
+    def stage_timing(self, enable: int = -1):
+        out = (C.c_ulonglong * 8)()
+        lib.mjb200_batched_stage_timing(self.handle, enable, out)
+        return dict(zip(self.STAGES, [int(x) for x in out]))
+
+    def launch_shape(self):
+        g, w, s, p = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        lib.mjb200_batched_launch_shape(self.handle, C.byref(g), C.byref(w), C.byref(s), C.byref(p))
+        return dict(grid=g.value, warps_per_block=w.value, smem_bytes=s.value, persistent=p.value)
+
+    def device_state(self):
+        ptrs = [C.c_void_p() for _ in range(4)]
+        lib.mjb200_batched_device_state(self.handle, *[C.byref(p) for p in ptrs])
+        return [p.value for p in ptrs]
+
+    def stream(self):
+        return lib.mjb200_batched_stream(self.handle)

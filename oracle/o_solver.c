@@ -56,11 +56,12 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
   int nv = m->nv;
   d->nefc = 0;
   d->nefc_dropped = 0;
+  int stop = 0;  /* set when a row group does not fit: it and every later group are dropped */
   if (m->disableflags & 1) return;
   if (!(m->disableflags & (1 << 2))) {
     for (int i = 0; i < nv; i++) {
       if (m->dof_frictionloss[i] <= 0) continue;
-      if (d->nefc + 1 > d->nefc_max) { d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+      if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
       double k, b, imp;
       impedance(m, &m->dof_solref[2 * i], &m->dof_solimp[5 * i], 0, &k, &b, &imp);
       int r = add_row(d, nv, T_FRICTION);
@@ -80,7 +81,7 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
         double dist = side == 0 ? d->qpos[qa] - m->jnt_range[2 * j] : m->jnt_range[2 * j + 1] - d->qpos[qa];
         double margin = m->jnt_margin[j];
         if (!(dist < margin)) continue;
-        if (d->nefc + 1 > d->nefc_max) { d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+        if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
         double k, b, imp, pos = dist - margin;
         impedance(m, &m->jnt_solref[2 * j], &m->jnt_solimp[5 * j], pos, &k, &b, &imp);
         int r = add_row(d, nv, T_LIMIT);
@@ -106,7 +107,7 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
     const double* pr = &m->pair_real[16 * pair];
     int dim = pi[4];
     int nrow = dim == 1 ? 1 : 2 * (dim - 1);
-    if (d->nefc + nrow > d->nefc_max) { d->nefc_dropped += nrow; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+    if (stop || d->nefc + nrow > d->nefc_max) { stop = 1; d->nefc_dropped += nrow; d->status |= ORACLE_EFC_OVERFLOW; continue; }
     double fs = (rnd ? rnd->friction_scale : 1.0);
     double mu[5];
     for (int k = 0; k < 5; k++) mu[k] = pr[2 + k] * fs;
@@ -206,24 +207,24 @@ typedef struct {
   const int* type;
 } Prob;
 
-/* total cost at x; fills y (jar), force, Ma, grad */
-static double eval_point(const Prob* P, const double* x, double* y, double* force, double* Ma, double* grad) {
+/* total cost at x with d = x - qacc_smooth: 0.5 d'Md + sum of row costs;
+ * fills y (jar), force, Md = M d, grad = Md - J'force */
+static double eval_point(const Prob* P, const double* x, double* y, double* force, double* Md, double* grad) {
   int nv = P->nv;
   double cost = 0;
   for (int i = 0; i < nv; i++) {
     double s = 0;
-    for (int j = 0; j < nv; j++) s += P->M[i * nv + j] * x[j];
-    Ma[i] = s;
+    for (int j = 0; j < nv; j++) s += P->M[i * nv + j] * (x[j] - P->qacc_smooth[j]);
+    Md[i] = s;
   }
-  /* Gauss term 0.5 (x - a0)' M (x - a0) = 0.5 x'Mx - x' f + 0.5 a0' f */
-  for (int i = 0; i < nv; i++) cost += 0.5 * x[i] * Ma[i] - x[i] * P->qfrc_smooth[i] + 0.5 * P->qacc_smooth[i] * P->qfrc_smooth[i];
+  for (int i = 0; i < nv; i++) cost += 0.5 * (x[i] - P->qacc_smooth[i]) * Md[i];
   for (int r = 0; r < P->nefc; r++) {
     y[r] = rowdot(&P->J[r * nv], x, nv) - P->aref[r];
     force[r] = row_force(P->type[r], P->D[r], P->floss[r], y[r]);
     cost += row_cost(P->type[r], P->D[r], P->floss[r], y[r]);
   }
   for (int i = 0; i < nv; i++) {
-    double s = Ma[i] - P->qfrc_smooth[i];
+    double s = Md[i];
     for (int r = 0; r < P->nefc; r++) s -= P->J[r * nv + i] * force[r];
     grad[i] = s;
   }
@@ -327,7 +328,7 @@ void oracle_solve(const OModel* m, OData* d, int max_iter) {
         for (int j = 0; j < nv; j++) s += d->M[i * nv + j] * p[j];
         Mp[i] = s;
         A += p[i] * s;
-        B += p[i] * (Ma[i] - d->qfrc_smooth[i]);
+        B += p[i] * Ma[i];
       }
       for (int r = 0; r < ne; r++) q[r] = rowdot(&d->efc_J[r * nv], p, nv);
       double dcost;

@@ -63,10 +63,11 @@ CONTACT_STRIDE = 20
 
 
 def _load():
-    import sys
-    sys.path.insert(0, HERE)
-    from build import build  # noqa: E402
-    path = build()
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mjb_oracle_build", os.path.join(HERE, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    path = mod.build()
     lib = C.CDLL(path)
     for fn in ("oracle_kinematics", "oracle_collide"):
         getattr(lib, fn).argtypes = [C.POINTER(OModel), C.POINTER(OData)]

