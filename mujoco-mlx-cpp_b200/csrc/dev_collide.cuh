@@ -205,6 +205,13 @@ __device__ __forceinline__ int c_capsule_box(const float* c, const float* R, con
   float r0[3] = {a0[0] - bc[0], a0[1] - bc[1], a0[2] - bc[2]}, r1[3] = {a1[0] - bc[0], a1[1] - bc[1], a1[2] - bc[2]}, l0[3], l1[3];
   mulmatT(BR, r0, l0);
   mulmatT(BR, r1, l1);
+  // exact cull: the segment's bounding box (box frame) separated from the box
+  // inflated by radius + margin means every axis point is farther than that
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float ext = bh[k] + sz[0] + margin;
+    if (fminf(l0[k], l1[k]) > ext || fmaxf(l0[k], l1[k]) < -ext) return 0;
+  }
   const float g = 0.6180339887498949f;
   float lo = 0, hi = 1;
   float x1 = hi - g * (hi - lo), x2 = lo + g * (hi - lo), p[3];

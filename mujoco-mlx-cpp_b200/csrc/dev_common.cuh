@@ -91,6 +91,38 @@ struct EfcRef {
   __device__ __forceinline__ float& operator[](int f) const { return base[f * ne]; }
 };
 
+// Dot products with four independent accumulators (instruction-level
+// parallelism instead of one long dependent FMA chain).
+__device__ __forceinline__ float dot_c(const float* a, const float* b, int n) {
+  float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int k = 0;
+#pragma unroll 1
+  for (; k + 3 < n; k += 4) {
+    s0 += a[k] * b[k];
+    s1 += a[k + 1] * b[k + 1];
+    s2 += a[k + 2] * b[k + 2];
+    s3 += a[k + 3] * b[k + 3];
+  }
+#pragma unroll 1
+  for (; k < n; k++) s0 += a[k] * b[k];
+  return (s0 + s1) + (s2 + s3);
+}
+// sum_k a[k * stride] * b[k]
+__device__ __forceinline__ float dot_s(const float* a, int stride, const float* b, int n) {
+  float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  int k = 0;
+#pragma unroll 1
+  for (; k + 3 < n; k += 4) {
+    s0 += a[k * stride] * b[k];
+    s1 += a[(k + 1) * stride] * b[k + 1];
+    s2 += a[(k + 2) * stride] * b[k + 2];
+    s3 += a[(k + 3) * stride] * b[k + 3];
+  }
+#pragma unroll 1
+  for (; k < n; k++) s0 += a[k * stride] * b[k];
+  return (s0 + s1) + (s2 + s3);
+}
+
 // read-only model table access (L1/L2 cached, tables are shared by every env)
 __device__ __forceinline__ int ldi(const int* t, int i) { return __ldg(t + i); }
 __device__ __forceinline__ float ldf(const float* t, int i) { return __ldg(t + i); }

@@ -13,47 +13,74 @@
 
 namespace mjbdev {
 
-// Cholesky of the n x n matrix A (row-major, in place, lower triangle = L).
-__device__ __noinline__ void d_chol(float* A, int n, int lane) {
-  #pragma unroll 1
-  for (int j = 0; j < n; j++) {
-    float s = A[j * n + j];
-    #pragma unroll 1
-    for (int k = 0; k < j; k++) s -= A[j * n + k] * A[j * n + k];
-    float d = sqrtf(fmaxf(s, 1e-30f));
+// Cholesky of the n x n SPD matrix A (row-major, lower triangle used, in
+// place: L below the diagonal, L_jj on it); idiag[j] = 1 / L_jj.
+// Right-looking: after column k is scaled, each lane updates its own rows of
+// the trailing block with independent FMAs (no long dependency chains).
+__device__ __noinline__ void d_chol(float* A, int n, int lane, float* idiag) {
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    float d = sqrtf(fmaxf(A[k * n + k], 1e-30f));
     float id = 1.f / d;
     __syncwarp();
-    #pragma unroll 1
-    for (int i = j + 1 + lane; i < n; i += 32) {
-      float t = A[i * n + j];
-      #pragma unroll 1
-      for (int k = 0; k < j; k++) t -= A[i * n + k] * A[j * n + k];
-      A[i * n + j] = t * id;
+#pragma unroll 1
+    for (int i = k + 1 + lane; i < n; i += 32) A[i * n + k] *= id;
+    if (lane == 0) {
+      A[k * n + k] = d;
+      idiag[k] = id;
     }
-    if (lane == 0) A[j * n + j] = d;
+    __syncwarp();
+#pragma unroll 1
+    for (int i = k + 1 + lane; i < n; i += 32) {
+      float* ri = A + i * n;
+      const float lik = ri[k];
+      int j = k + 1;
+#pragma unroll 1
+      for (; j + 3 <= i; j += 4) {
+        float l0 = A[j * n + k], l1 = A[(j + 1) * n + k], l2 = A[(j + 2) * n + k], l3 = A[(j + 3) * n + k];
+        ri[j] -= lik * l0;
+        ri[j + 1] -= lik * l1;
+        ri[j + 2] -= lik * l2;
+        ri[j + 3] -= lik * l3;
+      }
+#pragma unroll 1
+      for (; j <= i; j++) ri[j] -= lik * A[j * n + k];
+    }
     __syncwarp();
   }
 }
 
-// x := (L L')^-1 x
-__device__ __noinline__ void d_chol_solve(const float* L, int n, float* x, int lane) {
-  #pragma unroll 1
+// x := (L L')^-1 x.  The running vector lives in registers (element i on lane
+// i; a second slot covers n up to 64) and each solved entry is broadcast with a
+// shuffle, so the substitution needs no shared-memory round trip per step.
+__device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, int n, float* x, int lane) {
+  float x0 = lane < n ? x[lane] : 0.f;
+  float x1 = lane + 32 < n ? x[lane + 32] : 0.f;
+#pragma unroll 1
   for (int k = 0; k < n; k++) {
-    float xk = x[k] / L[k * n + k];
-    __syncwarp();
-    #pragma unroll 1
-    for (int i = k + 1 + lane; i < n; i += 32) x[i] -= L[i * n + k] * xk;
-    if (lane == 0) x[k] = xk;
-    __syncwarp();
+    float v = k < 32 ? __shfl_sync(FULL_MASK, x0, k) : __shfl_sync(FULL_MASK, x1, k - 32);
+    float xk = v * idiag[k];
+    if (lane == (k & 31)) {
+      if (k < 32) x0 = xk;
+      else x1 = xk;
+    }
+    if (lane > k && lane < n) x0 -= L[lane * n + k] * xk;
+    if (lane + 32 > k && lane + 32 < n) x1 -= L[(lane + 32) * n + k] * xk;
   }
+#pragma unroll 1
   for (int k = n - 1; k >= 0; k--) {
-    float xk = x[k] / L[k * n + k];
-    __syncwarp();
-    #pragma unroll 1
-    for (int i = lane; i < k; i += 32) x[i] -= L[k * n + i] * xk;
-    if (lane == 0) x[k] = xk;
-    __syncwarp();
+    float v = k < 32 ? __shfl_sync(FULL_MASK, x0, k) : __shfl_sync(FULL_MASK, x1, k - 32);
+    float xk = v * idiag[k];
+    if (lane == (k & 31)) {
+      if (k < 32) x0 = xk;
+      else x1 = xk;
+    }
+    if (lane < k && lane < n) x0 -= L[k * n + lane] * xk;
+    if (lane + 32 < k && lane + 32 < n) x1 -= L[k * n + lane + 32] * xk;
   }
+  if (lane < n) x[lane] = x0;
+  if (lane + 32 < n) x[lane + 32] = x1;
+  __syncwarp();
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
@@ -265,9 +292,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
     // reference acceleration: aref = -b J v - k imp pos
     #pragma unroll 1
     for (int r = row0 + E.lane; r < nefc; r += 32) {
-      float jv = 0;
-      #pragma unroll 1
-      for (int c = 0; c < nv; c++) jv += J[r * nv + c] * qvel[c];
+      float jv = dot_c(J + r * nv, qvel, nv);
       EfcRef e{efc + r, ne};
       e[EFC_AREF] = -e[EFC_AREF] * jv - e[EFC_Y];
     }
@@ -306,28 +331,20 @@ __device__ __forceinline__ float row_cost_delta(int type, float D, float fl, flo
 __device__ __noinline__ float d_cost(Env& E, int nefc, const float* x, float* tmp) {
   const DevModelDesc& m = *E.md;
   const int nv = m.nv, ne = m.nefc_max, lane = E.lane;
-  const float* __restrict__ M = E.ws + m.w_M;
-  const float* __restrict__ qas = E.ws + m.w_qas;
-  const float* __restrict__ J = E.ws + m.w_J;
-  float* efc = E.ws + m.w_efc;
-  #pragma unroll 1
+  const float* M = E.ws + m.w_M;
+  const float* qas = E.ws + m.w_qas;
+  const float* J = E.ws + m.w_J;
+  const float* efc = E.ws + m.w_efc;
+#pragma unroll 1
   for (int i = lane; i < nv; i += 32) tmp[i] = x[i] - qas[i];
   __syncwarp();
   float c = 0;
-  #pragma unroll 1
-  for (int i = lane; i < nv; i += 32) {
-    float s = 0;
-    #pragma unroll 1
-    for (int j = 0; j < nv; j++) s += M[i * nv + j] * tmp[j];
-    c += 0.5f * tmp[i] * s;
-  }
-  #pragma unroll 1
+#pragma unroll 1
+  for (int i = lane; i < nv; i += 32) c += 0.5f * tmp[i] * dot_c(M + i * nv, tmp, nv);
+#pragma unroll 1
   for (int r = lane; r < nefc; r += 32) {
-    const EfcRef e{efc + r, ne};
-    float y = -e[EFC_AREF];
-    #pragma unroll 1
-    for (int j = 0; j < nv; j++) y += J[r * nv + j] * x[j];
-    c += row_cost((int)e[EFC_TYPE], e[EFC_D], e[EFC_FLOSS], y);
+    float y = dot_c(J + r * nv, x, nv) - efc[EFC_AREF * ne + r];
+    c += row_cost((int)efc[EFC_TYPE * ne + r], efc[EFC_D * ne + r], efc[EFC_FLOSS * ne + r], y);
   }
   __syncwarp();
   return warp_sum(c);
@@ -337,11 +354,9 @@ __device__ __noinline__ float d_cost(Env& E, int nefc, const float* x, float* tm
 // (||Md||^2 + ||J'force||^2) that sets the FP32 round-off floor of g.
 __device__ __forceinline__ float grad_update(const float* J, const float* force, const float* Md, float* grad, int nv, int nefc, int lane, float& terms) {
   float gn = 0, tn = 0;
-  #pragma unroll 1
+#pragma unroll 1
   for (int i = lane; i < nv; i += 32) {
-    float f = 0;
-    #pragma unroll 1
-    for (int r = 0; r < nefc; r++) f += J[r * nv + i] * force[r];
+    float f = dot_s(J + i, nv, force, nefc);
     float g = Md[i] - f;
     grad[i] = g;
     gn += g * g;
@@ -352,7 +367,7 @@ __device__ __forceinline__ float grad_update(const float* J, const float* force,
 }
 
 // Newton solve from the warm start; x (w_x) holds the result.  Returns the
-// iteration count.  vec: Md, grad, p, Mp, tmp (5 nv).
+// iteration count.  vec: Md, grad, p, Mp, tmp, -, -, -, idiag.
 // The Hessian factor is rebuilt only when the set of rows in their quadratic
 // zone changed since the last factorisation.  Termination: improvement or
 // gradient below tolerance * meaninertia * nv, where the gradient test also
@@ -363,15 +378,16 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   const DevModelDesc& m = *E.md;
   const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations, i_tri = m.i_tri;
   float* ws = E.ws;
-  const float* __restrict__ M = ws + m.w_M;
-  const float* __restrict__ qas = ws + m.w_qas;
-  const float* __restrict__ J = ws + m.w_J;
+  const float* M = ws + m.w_M;
+  const float* qas = ws + m.w_qas;
+  const float* J = ws + m.w_J;
   float* efc = ws + m.w_efc;
   float* H = ws + m.w_H;
   float* x = ws + m.w_x;
+  int* act_list = reinterpret_cast<int*>(ws + m.w_active);
   const float* xw = ws + m.w_xwarm;
   float* vec = ws + m.w_vec;
-  float *Md = vec, *grad = vec + nv, *p = vec + 2 * nv, *Mp = vec + 3 * nv, *tmp = vec + 4 * nv;
+  float *Md = vec, *grad = vec + nv, *p = vec + 2 * nv, *Mp = vec + 3 * nv, *tmp = vec + 4 * nv, *idiag = vec + 8 * nv;
   float* eY = efc + EFC_Y * ne;
   float* eF = efc + EFC_FORCE * ne;
   float* eQ = efc + EFC_Q * ne;
@@ -384,9 +400,7 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
 
   // warm start: lowest cost of smooth / previous / predicted
   choice = 0;
-  #pragma unroll 1
-  for (int i = lane; i < nv; i += 32) x[i] = qas[i];
-  __syncwarp();
+  const float* src = qas;
   if (!(m.disableflags & (1 << 8)) && nefc > 0) {
     float best = d_cost(E, nefc, qas, tmp);
     float cw = d_cost(E, nefc, xw, tmp);
@@ -395,32 +409,20 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
       float cp = d_cost(E, nefc, xpred, tmp);
       if (cp <= best) { best = cp; choice = 2; }
     }
-    const float* src = choice == 1 ? xw : choice == 2 ? xpred : qas;
-    #pragma unroll 1
-    for (int i = lane; i < nv; i += 32) x[i] = src[i];
-    __syncwarp();
-  } else if (!(m.disableflags & (1 << 8)) && xpred) {
-    choice = 2;
-    #pragma unroll 1
-    for (int i = lane; i < nv; i += 32) x[i] = qas[i];
-    __syncwarp();
+    src = choice == 1 ? xw : choice == 2 ? xpred : qas;
   }
-  // state at x: d = x - a0, Md, y, force, grad
-  #pragma unroll 1
-  for (int i = lane; i < nv; i += 32) tmp[i] = x[i] - qas[i];
-  __syncwarp();
-  #pragma unroll 1
+#pragma unroll 1
   for (int i = lane; i < nv; i += 32) {
-    float s = 0;
-    #pragma unroll 1
-    for (int j = 0; j < nv; j++) s += M[i * nv + j] * tmp[j];
-    Md[i] = s;
+    x[i] = src[i];
+    tmp[i] = src[i] - qas[i];
   }
-  #pragma unroll 1
+  __syncwarp();
+  // state at x: d = x - a0, Md, y, force, grad
+#pragma unroll 1
+  for (int i = lane; i < nv; i += 32) Md[i] = dot_c(M + i * nv, tmp, nv);
+#pragma unroll 1
   for (int r = lane; r < nefc; r += 32) {
-    float y = -eA[r];
-    #pragma unroll 1
-    for (int j = 0; j < nv; j++) y += J[r * nv + j] * x[j];
+    float y = dot_c(J + r * nv, x, nv) - eA[r];
     eY[r] = y;
     eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
   }
@@ -431,64 +433,72 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   const float eps_floor = 16.f * 1.1920929e-7f;
   if (nefc == 0 || scale * sqrtf(gn) < tol || gn <= eps_floor * eps_floor * terms) return 0;
   const int ntri = nv * (nv + 1) / 2;
-  const int nwords = (nefc + 31) >> 5;
-  unsigned act_prev[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};  // impossible pattern: forces the first build
-  bool have_factor = false;
+  int nact_prev = -1;
   int niter = 0;
-  #pragma unroll 1
+#pragma unroll 1
   for (int iter = 0; iter < max_iter; iter++) {
-    // active (quadratic-zone) pattern of the rows; nefc <= 128 uses the fast path
-    bool same = have_factor && nefc <= 128;
-    unsigned act[4] = {0, 0, 0, 0};
-    #pragma unroll 1
-    for (int w = 0; w < nwords && w < 4; w++) {
-      int r = 32 * w + lane;
+    // compact list of rows in their quadratic zone (order preserved)
+    int nact = 0;
+    bool changed = false;
+#pragma unroll 1
+    for (int base = 0; base < nefc; base += 32) {
+      int r = base + lane;
       bool q = r < nefc && row_quad((int)eT[r], eD[r], eL[r], eY[r]);
-      act[w] = __ballot_sync(FULL_MASK, q);
-      if (act[w] != act_prev[w]) same = false;
+      unsigned b = __ballot_sync(FULL_MASK, q);
+      int pos = nact + __popc(b & ((1u << lane) - 1u));
+      if (q) {
+        if (nact_prev < 0 || pos >= nact_prev || act_list[pos] != r) changed = true;
+      }
+      nact += __popc(b);
+      changed = __any_sync(FULL_MASK, changed);
+      __syncwarp();
+      if (q) act_list[pos] = r;
     }
-    if (nefc > 128) same = false;
-    if (!same) {
-      #pragma unroll 1
+    if (nact != nact_prev) changed = true;
+    __syncwarp();
+    if (changed) {
+      // H = M + sum over quadratic rows of D J'J: lower-triangle entries in parallel
+#pragma unroll 1
       for (int t = lane; t < ntri; t += 32) {
         int packed = ldi(it, i_tri + t);
         int i = packed >> 16, j = packed & 0xffff;
-        float s = M[i * nv + j];
-        #pragma unroll 1
-        for (int r = 0; r < nefc; r++) {
-          bool q = nefc <= 128 ? ((act[r >> 5] >> (r & 31)) & 1u) : row_quad((int)eT[r], eD[r], eL[r], eY[r]);
-          if (q) s += eD[r] * J[r * nv + i] * J[r * nv + j];
+        float s0 = M[i * nv + j], s1 = 0, s2 = 0, s3 = 0;
+        int a = 0;
+#pragma unroll 1
+        for (; a + 3 < nact; a += 4) {
+          int r0 = act_list[a], r1 = act_list[a + 1], r2 = act_list[a + 2], r3 = act_list[a + 3];
+          s0 += eD[r0] * J[r0 * nv + i] * J[r0 * nv + j];
+          s1 += eD[r1] * J[r1 * nv + i] * J[r1 * nv + j];
+          s2 += eD[r2] * J[r2 * nv + i] * J[r2 * nv + j];
+          s3 += eD[r3] * J[r3 * nv + i] * J[r3 * nv + j];
         }
-        H[i * nv + j] = s;
+#pragma unroll 1
+        for (; a < nact; a++) {
+          int r0 = act_list[a];
+          s0 += eD[r0] * J[r0 * nv + i] * J[r0 * nv + j];
+        }
+        H[i * nv + j] = (s0 + s1) + (s2 + s3);
       }
       __syncwarp();
-      d_chol(H, nv, lane);
-      for (int w = 0; w < 4; w++) act_prev[w] = act[w];
-      have_factor = true;
+      d_chol(H, nv, lane, idiag);
+      nact_prev = nact;
     }
-    #pragma unroll 1
+#pragma unroll 1
     for (int i = lane; i < nv; i += 32) p[i] = -grad[i];
     __syncwarp();
-    d_chol_solve(H, nv, p, lane);
+    d_chol_solve(H, idiag, nv, p, lane);
     // line-search coefficients A = p'Mp, B = p'Md, q = J p
     float A = 0, B = 0, gp = 0;
-    #pragma unroll 1
+#pragma unroll 1
     for (int i = lane; i < nv; i += 32) {
-      float s = 0;
-      #pragma unroll 1
-      for (int j = 0; j < nv; j++) s += M[i * nv + j] * p[j];
+      float s = dot_c(M + i * nv, p, nv);
       Mp[i] = s;
       A += p[i] * s;
       B += p[i] * Md[i];
       gp += grad[i] * p[i];
     }
-    #pragma unroll 1
-    for (int r = lane; r < nefc; r += 32) {
-      float s = 0;
-      #pragma unroll 1
-      for (int j = 0; j < nv; j++) s += J[r * nv + j] * p[j];
-      eQ[r] = s;
-    }
+#pragma unroll 1
+    for (int r = lane; r < nefc; r += 32) eQ[r] = dot_c(J + r * nv, p, nv);
     A = warp_sum(A);
     B = warp_sum(B);
     gp = warp_sum(gp);
@@ -498,7 +508,7 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     float d0, h0;
     {
       float g1 = 0, g2 = 0;
-      #pragma unroll 1
+#pragma unroll 1
       for (int r = lane; r < nefc; r += 32) {
         int ty = (int)eT[r];
         float q = eQ[r], y = eY[r], D = eD[r], fl = eL[r];
@@ -513,10 +523,10 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     if (d0 < 0.f) {
       float lo = 0, dlo = d0, hi = -1, dhi = 0;
       float a = -d0 / h0;
-      #pragma unroll 1
+#pragma unroll 1
       for (int it2 = 0; it2 < ls_iter; it2++) {
         float g1 = 0, g2 = 0;
-        #pragma unroll 1
+#pragma unroll 1
         for (int r = lane; r < nefc; r += 32) {
           int ty = (int)eT[r];
           float q = eQ[r], y = eY[r] + a * q, D = eD[r], fl = eL[r];
@@ -540,16 +550,16 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     if (alpha == 0.f) break;
     // cost change along the step (accurate for small steps)
     float dc = 0;
-    #pragma unroll 1
+#pragma unroll 1
     for (int r = lane; r < nefc; r += 32) dc += row_cost_delta((int)eT[r], eD[r], eL[r], eY[r], alpha * eQ[r]);
     dc = warp_sum(dc) + 0.5f * alpha * alpha * A + alpha * B;
     // update x, Md, y, force, grad
-    #pragma unroll 1
+#pragma unroll 1
     for (int i = lane; i < nv; i += 32) {
       x[i] += alpha * p[i];
       Md[i] += alpha * Mp[i];
     }
-    #pragma unroll 1
+#pragma unroll 1
     for (int r = lane; r < nefc; r += 32) {
       float y = eY[r] + alpha * eQ[r];
       eY[r] = y;
@@ -570,13 +580,8 @@ __device__ __noinline__ void d_jtf(Env& E, int nefc, float* out) {
   const int nv = m.nv, ne = m.nefc_max;
   const float* J = E.ws + m.w_J;
   const float* eF = E.ws + m.w_efc + EFC_FORCE * ne;
-  #pragma unroll 1
-  for (int i = E.lane; i < nv; i += 32) {
-    float s = 0;
-    #pragma unroll 1
-    for (int r = 0; r < nefc; r++) s += J[r * nv + i] * eF[r];
-    out[i] = s;
-  }
+#pragma unroll 1
+  for (int i = E.lane; i < nv; i += 32) out[i] = dot_s(J + i, nv, eF, nefc);
   __syncwarp();
 }
 

@@ -111,6 +111,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     if (m.cone != CONE_PYRAMIDAL) throw std::runtime_error("engine: the elliptic cone is not supported by this build");
     for (int j = 0; j < m.njnt; j++)
       if (m.jnt_limited[j] && m.jnt_type[j] == JNT_BALL) throw std::runtime_error("engine: limited ball joints are not supported");
+    if (m.nv > 64) throw std::runtime_error("engine: models with more than 64 dofs are not supported by this build");
     for (double g : m.body_gravcomp)
       if (g != 0) throw std::runtime_error("engine: gravcomp is not supported");
     DevModelDesc d;
@@ -256,18 +257,18 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.f_dof_damping_implicit = tb.af(damp);
     // contact / row capacity
     int ncb = std::max(1, m.max_contacts_bound);
-    d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 32);
+    d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 24);
     int rows_per_con = 1;
     for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : 2 * (p.condim - 1));
     int rows_bound = d.nfloss + 2 * d.nlimit + rows_per_con * d.ncon_max;
-    d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 96));
+    d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 64));
     // workspace layout
     int nv = m.nv, nb = m.nbody, nj = std::max(1, m.njnt), ng = std::max(1, m.ngeom), nu = std::max(1, m.nu);
     int off = 0;
     auto take = [&](int n) { int o = off; off += (n + 3) & ~3; return o; };
     d.w_qpos = take(m.nq); d.w_qvel = take(nv); d.w_ctrl = take(nu); d.w_x = take(nv); d.w_xwarm = take(nv);
     d.w_scom = take(3 * nb); d.w_cdof = take(6 * nv); d.w_M = take(nv * nv); d.w_qfs = take(nv); d.w_qas = take(nv); d.w_qfa = take(nv);
-    d.w_vec = take(8 * nv); d.w_con = take(MJB_CONTACT_FLOATS * d.ncon_max); d.w_rowcon = 0;
+    d.w_vec = take(9 * nv); d.w_con = take(MJB_CONTACT_FLOATS * d.ncon_max); d.w_rowcon = 0;
     int kbase = off;
     d.w_xpos = take(3 * nb); d.w_xquat = take(4 * nb); d.w_xmat = take(9 * nb); d.w_xipos = take(3 * nb);
     d.w_xanchor = take(3 * nj); d.w_xaxis = take(3 * nj); d.w_gxpos = take(3 * ng); d.w_gxmat = take(9 * ng);
@@ -349,7 +350,7 @@ void Engine::choose_launch() {
   lockstep_ = cfg_.lockstep ? 1 : 0;
   const int per_warp = (desc_words_ + ws_stride_) * 4;
   if (cfg_.warps_per_block > 0) warps_ = cfg_.warps_per_block;
-  else if (lockstep_) warps_ = std::max(1, std::min(16, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs per SM
+  else if (lockstep_) warps_ = std::max(1, std::min(8, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs of up to 8 warps per SM
   else warps_ = 4;
   smem_ = warps_ * (desc_words_ + ws_stride_) * 4;
   if (smem_ > 227 * 1024) {
@@ -613,14 +614,14 @@ int Engine::set_env_params(const int* env_idx, int n, const float* mass_scale, c
 void Engine::stage_timing(int enable, unsigned long long* out8) {
   sync();
   if (out8) {
-    if (timing_) check(cudaMemcpy(out8, stage_cycles_.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stage cycles");
+    if (timing_) check(cudaMemcpy(out8, stage_cycles_.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stage cycles");
     else std::memset(out8, 0, 8 * sizeof(unsigned long long));
   }
   if (enable >= 0) {
     bool on = enable != 0;
     if (on) {
-      if (!stage_cycles_.p) stage_cycles_.alloc(8);
-      check(cudaMemset(stage_cycles_.p, 0, 8 * sizeof(unsigned long long)), "stage cycles reset");
+      if (!stage_cycles_.p) stage_cycles_.alloc(16);
+      check(cudaMemset(stage_cycles_.p, 0, 16 * sizeof(unsigned long long)), "stage cycles reset");
     }
     if (on != timing_) invalidate_graphs();
     timing_ = on;

@@ -154,8 +154,9 @@ __device__ __noinline__ void d_qacc_smooth(Env& E) {
 #pragma unroll 1
   for (int k = lane; k < nv; k += 32) ws[m.w_qas + k] = ws[m.w_qfs + k];
   __syncwarp();
-  d_chol(H, nv, lane);
-  d_chol_solve(H, nv, ws + m.w_qas, lane);
+  float* idiag = ws + m.w_vec + 8 * nv;
+  d_chol(H, nv, lane, idiag);
+  d_chol_solve(H, idiag, nv, ws + m.w_qas, lane);
 }
 
 // bad-acceleration check, implicit-damping solve, warm-start save, integration.
@@ -184,8 +185,9 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
 #pragma unroll 1
     for (int k = lane; k < nv; k += 32) acc[k] = ws[m.w_qfs + k] + qfc[k];
     __syncwarp();
-    d_chol(H, nv, lane);
-    d_chol_solve(H, nv, acc, lane);
+    float* idiag = ws + m.w_vec + 8 * nv;
+    d_chol(H, nv, lane, idiag);
+    d_chol_solve(H, idiag, nv, acc, lane);
     a = acc;
   }
 #pragma unroll 1
@@ -232,7 +234,10 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
   int stage_id = 0;
 #define STAGE_SYNC()                                  \
   do {                                                \
-    if (lockstep) __syncthreads();                    \
+    if (lockstep) {                                   \
+      __syncwarp();                                   \
+      __syncthreads();                                \
+    }                                                 \
     if (timing) {                                     \
       long long t_ = clock64();                       \
       tstage[stage_id & 7] += (unsigned long long)(t_ - tlast); \
@@ -326,7 +331,9 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
         nsum += it;
         nmax = it > nmax ? it : nmax;
       }
-      STAGE_SYNC();
+      // no barrier here: warps whose Newton solve ends early go on through
+      // integration and the next substep's kinematics while the slowest
+      // solves of the CTA finish (the next barrier follows kinematics)
       if (valid) {
         d_jtf(E, nefc, qfc);
         if (last && P.dbg_contacts) record_debug(E, P, ncon, nefc, qfc);
@@ -337,7 +344,6 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
         }
         d_finish(E, qfc, acc);
       }
-      STAGE_SYNC();
     }
     if (valid) {
       const DevModelDesc& m = *E.md;

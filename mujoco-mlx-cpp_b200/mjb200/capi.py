@@ -277,10 +277,10 @@ class BatchedSim:
         if lib.mjb200_batched_configure(self.handle, C.byref(c)) != 0:
             raise RuntimeError(last_error())
 
-    STAGES = ("kinematics", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "newton", "integrate")
+    STAGES = ("kinematics", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "newton_finish_kin", "x7", "x8", "x9", "x10", "x11", "x12", "x13", "x14", "x15")
 
     def stage_timing(self, enable: int = -1):
-        out = (C.c_ulonglong * 8)()
+        out = (C.c_ulonglong * 16)()
         lib.mjb200_batched_stage_timing(self.handle, enable, out)
         return dict(zip(self.STAGES, [int(x) for x in out]))
 

@@ -234,6 +234,13 @@ static int capsule_box(const double* c, const double* R, const double* sz, const
   double r0[3] = {a0[0] - bc[0], a0[1] - bc[1], a0[2] - bc[2]}, r1[3] = {a1[0] - bc[0], a1[1] - bc[1], a1[2] - bc[2]}, l0[3], l1[3];
   o_mulmatT(BR, r0, l0);
   o_mulmatT(BR, r1, l1);
+  /* exact cull: segment bounding box (box frame) outside the box inflated by
+     radius + margin */
+  for (int k = 0; k < 3; k++) {
+    double ext = bh[k] + sz[0] + margin;
+    double lo = l0[k] < l1[k] ? l0[k] : l1[k], hi = l0[k] < l1[k] ? l1[k] : l0[k];
+    if (lo > ext || hi < -ext) return 0;
+  }
   /* golden-section search of the convex signed distance along the axis */
   const double g = 0.6180339887498949;
   double lo = 0, hi = 1;
