@@ -63,6 +63,9 @@ MJMLX_API int mjb200_batched_layout(const MjmlxBatchedSim* sim, int* num_envs, i
 
 /* n physics steps with the controls already in device memory (no host copy). */
 MJMLX_API int mjb200_batched_step_device(MjmlxBatchedSim* sim, int n);
+/* n physics steps with controls read from device memory ctrl_dev[total_u]
+ * (copied on the sim's stream, device to device); n = 0 only copies. */
+MJMLX_API int mjb200_batched_step_device_ctrl(MjmlxBatchedSim* sim, const float* ctrl_dev, int n);
 /* Device pointers of the HBM-resident state (float, env-major records). */
 MJMLX_API int mjb200_batched_device_state(MjmlxBatchedSim* sim, float** qpos, float** qvel, float** ctrl, float** qacc_warmstart);
 /* The CUDA stream (cudaStream_t) every launch of the sim is ordered on. */

@@ -244,6 +244,11 @@ MJMLX_API int mjb200_batched_step_device(MjmlxBatchedSim* sim, int n) {
   return guard("mjb200_batched_step_device", [&]() { sim->engine->step_device(n); return 0; }, -1);
 }
 
+MJMLX_API int mjb200_batched_step_device_ctrl(MjmlxBatchedSim* sim, const float* ctrl_dev, int n) {
+  if (!sim || n < 0) return -1;
+  return guard("mjb200_batched_step_device_ctrl", [&]() { sim->engine->step_device_ctrl(ctrl_dev, n); return 0; }, -1);
+}
+
 MJMLX_API int mjb200_batched_device_state(MjmlxBatchedSim* sim, float** qpos, float** qvel, float** ctrl, float** qacc) {
   if (!sim) return -1;
   Engine& e = *sim->engine;

@@ -489,6 +489,11 @@ void Engine::step(const float* ctrl_host, int n) {
 
 void Engine::step_device(int n) { launch(n, cfg_.record != 0); }
 
+void Engine::step_device_ctrl(const float* dctrl, int n) {
+  if (tot_u_ > 0 && dctrl) check(cudaMemcpyAsync(ctrl_.p, dctrl, sizeof(float) * tot_u_, cudaMemcpyDeviceToDevice, stream_), "ctrl device copy");
+  launch(n, cfg_.record != 0);
+}
+
 void Engine::sync() { check(cudaStreamSynchronize(stream_), "stream sync"); }
 
 void Engine::get_state(float* qpos, float* qvel) {

@@ -71,6 +71,7 @@ class Engine {
 
   void step(const float* ctrl_host, int n);    // host ctrl, async
   void step_device(int n);                      // ctrl already on device
+  void step_device_ctrl(const float* dctrl, int n);  // ctrl copied from another device buffer
   void sync();
   cudaStream_t stream() const { return stream_; }
 

@@ -67,6 +67,7 @@ def _load():
         "mjb200_batched_get_config": (C.c_int, [C.c_void_p, C.POINTER(MjbEngineConfig)]),
         "mjb200_batched_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "mjb200_batched_step_device": (C.c_int, [C.c_void_p, C.c_int]),
+        "mjb200_batched_step_device_ctrl": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         "mjb200_batched_stream": (C.c_void_p, [C.c_void_p]),
         "mjb200_batched_launch_shape": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p]),
@@ -208,6 +209,10 @@ class BatchedSim:
 
     def step_device(self, n: int = 1):
         if lib.mjb200_batched_step_device(self.handle, n) != 0:
+            raise RuntimeError(last_error())
+
+    def step_device_ctrl(self, ctrl_ptr: int, n: int = 1):
+        if lib.mjb200_batched_step_device_ctrl(self.handle, C.c_void_p(ctrl_ptr), n) != 0:
             raise RuntimeError(last_error())
 
     def sync(self):
