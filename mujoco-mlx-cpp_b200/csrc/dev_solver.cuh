@@ -83,6 +83,48 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
   __syncwarp();
 }
 
+// A = M + sum over the listed rows r of D_r J_r' J_r + dscale * diag(ddiag),
+// built in shared memory from the lower-triangle entry table (entries spread
+// over the lanes), then factored by the right-looking shared-memory Cholesky
+// into the row-major lower triangle of L with idiag = 1 / L_jj.
+__device__ __noinline__ void d_factor_smem(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
+                                           int n, int lane, const int* it, int i_tri, float* L, float* idiag) {
+  const int ntri = n * (n + 1) / 2;
+#pragma unroll 1
+  for (int t = lane; t < ntri; t += 32) {
+    int packed = ldi(it, i_tri + t);
+    int i = packed >> 16, j = packed & 0xffff;
+    float s0 = M[i * n + j], s1 = 0, s2 = 0, s3 = 0;
+    if (i == j && ddiag) s0 += dscale * ldf(ddiag, i);
+    int a = 0;
+#pragma unroll 1
+    for (; a + 3 < nact; a += 4) {
+      int r0 = act[a], r1 = act[a + 1], r2 = act[a + 2], r3 = act[a + 3];
+      s0 += eD[r0] * J[r0 * n + i] * J[r0 * n + j];
+      s1 += eD[r1] * J[r1 * n + i] * J[r1 * n + j];
+      s2 += eD[r2] * J[r2 * n + i] * J[r2 * n + j];
+      s3 += eD[r3] * J[r3 * n + i] * J[r3 * n + j];
+    }
+#pragma unroll 1
+    for (; a < nact; a++) {
+      int r0 = act[a];
+      s0 += eD[r0] * J[r0 * n + i] * J[r0 * n + j];
+    }
+    L[i * n + j] = (s0 + s1) + (s2 + s3);
+  }
+  __syncwarp();
+  d_chol(L, n, lane, idiag);
+}
+
+__device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const float* ddiag, float dscale, float* L, float* idiag) {
+  const DevModelDesc& m = *E.md;
+  const int nv = m.nv;
+  const float* M = E.ws + m.w_M;
+  const float* J = E.ws + m.w_J;
+  const float* eD = E.ws + m.w_efc + EFC_D * m.nefc_max;
+  d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag);
+}
+
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
   float tc = sr0, dr = sr1;
   if (!(m.disableflags & (1 << 11)) && tc > 0 && tc < 2 * m.timestep) tc = 2 * m.timestep;
@@ -376,7 +418,7 @@ __device__ __forceinline__ float grad_update(const float* J, const float* force,
 __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int max_iter, const float* xpred, int& choice) {
   (void)P;
   const DevModelDesc& m = *E.md;
-  const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations, i_tri = m.i_tri;
+  const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations;
   float* ws = E.ws;
   const float* M = ws + m.w_M;
   const float* qas = ws + m.w_qas;
@@ -396,7 +438,6 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   const float* eL = efc + EFC_FLOSS * ne;
   const float* eT = efc + EFC_TYPE * ne;
   const float scale = m.scale, tol = m.tolerance;
-  const int* it = E.it;
 
   // warm start: lowest cost of smooth / previous / predicted
   choice = 0;
@@ -432,7 +473,6 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   __syncwarp();
   const float eps_floor = 16.f * 1.1920929e-7f;
   if (nefc == 0 || scale * sqrtf(gn) < tol || gn <= eps_floor * eps_floor * terms) return 0;
-  const int ntri = nv * (nv + 1) / 2;
   int nact_prev = -1;
   int niter = 0;
 #pragma unroll 1
@@ -457,30 +497,7 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     if (nact != nact_prev) changed = true;
     __syncwarp();
     if (changed) {
-      // H = M + sum over quadratic rows of D J'J: lower-triangle entries in parallel
-#pragma unroll 1
-      for (int t = lane; t < ntri; t += 32) {
-        int packed = ldi(it, i_tri + t);
-        int i = packed >> 16, j = packed & 0xffff;
-        float s0 = M[i * nv + j], s1 = 0, s2 = 0, s3 = 0;
-        int a = 0;
-#pragma unroll 1
-        for (; a + 3 < nact; a += 4) {
-          int r0 = act_list[a], r1 = act_list[a + 1], r2 = act_list[a + 2], r3 = act_list[a + 3];
-          s0 += eD[r0] * J[r0 * nv + i] * J[r0 * nv + j];
-          s1 += eD[r1] * J[r1 * nv + i] * J[r1 * nv + j];
-          s2 += eD[r2] * J[r2 * nv + i] * J[r2 * nv + j];
-          s3 += eD[r3] * J[r3 * nv + i] * J[r3 * nv + j];
-        }
-#pragma unroll 1
-        for (; a < nact; a++) {
-          int r0 = act_list[a];
-          s0 += eD[r0] * J[r0 * nv + i] * J[r0 * nv + j];
-        }
-        H[i * nv + j] = (s0 + s1) + (s2 + s3);
-      }
-      __syncwarp();
-      d_chol(H, nv, lane, idiag);
+      d_factor(E, act_list, nact, nullptr, 0.f, H, idiag);
       nact_prev = nact;
     }
 #pragma unroll 1

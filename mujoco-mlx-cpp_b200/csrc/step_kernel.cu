@@ -150,12 +150,10 @@ __device__ __noinline__ void d_qacc_smooth(Env& E) {
   const int nv = m.nv, lane = E.lane;
   float* H = ws + m.w_H;
 #pragma unroll 1
-  for (int k = lane; k < nv * nv; k += 32) H[k] = ws[m.w_M + k];
-#pragma unroll 1
   for (int k = lane; k < nv; k += 32) ws[m.w_qas + k] = ws[m.w_qfs + k];
   __syncwarp();
   float* idiag = ws + m.w_vec + 8 * nv;
-  d_chol(H, nv, lane, idiag);
+  d_factor(E, nullptr, 0, nullptr, 0.f, H, idiag);
   d_chol_solve(H, idiag, nv, ws + m.w_qas, lane);
 }
 
@@ -178,15 +176,10 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
   if (m.implicit) {
     float* H = ws + m.w_H;
 #pragma unroll 1
-    for (int k = lane; k < nv * nv; k += 32) {
-      int i = k / nv, j = k - i * nv;
-      H[k] = ws[m.w_M + k] + (i == j ? m.timestep * ldf(E.ft, m.f_dof_damping_implicit + i) : 0.f);
-    }
-#pragma unroll 1
     for (int k = lane; k < nv; k += 32) acc[k] = ws[m.w_qfs + k] + qfc[k];
     __syncwarp();
     float* idiag = ws + m.w_vec + 8 * nv;
-    d_chol(H, nv, lane, idiag);
+    d_factor(E, nullptr, 0, E.ft + m.f_dof_damping_implicit, m.timestep, H, idiag);
     d_chol_solve(H, idiag, nv, acc, lane);
     a = acc;
   }

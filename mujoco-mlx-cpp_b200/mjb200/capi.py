@@ -7,7 +7,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "libmjb200.so")
+LIB_PATH = os.environ.get("MJB200_LIB") or os.path.join(os.path.dirname(_HERE), "libmjb200.so")
 
 _f32p = C.POINTER(C.c_float)
 _i32p = C.POINTER(C.c_int)
