@@ -66,6 +66,30 @@ MJMLX_API int mjb200_batched_step_device(MjmlxBatchedSim* sim, int n);
 /* n physics steps with controls read from device memory ctrl_dev[total_u]
  * (copied on the sim's stream, device to device); n = 0 only copies. */
 MJMLX_API int mjb200_batched_step_device_ctrl(MjmlxBatchedSim* sim, const float* ctrl_dev, int n);
+/* Allocation-free step.  No counterpart in the reference.
+ *
+ * For callers that must not have the library allocate device memory while
+ * they step: code recording the step into a CUDA graph by stream capture,
+ * programs that reserve their whole device memory budget up front, real-time
+ * control loops that cannot wait on an allocator.  Runs n physics steps of
+ * the sim's model(s) on state held in the caller's device buffers, laid out
+ * like the sim's own (mjb200_batched_layout offsets): qpos[total_q],
+ * qvel[total_v], ctrl[total_u] (may be NULL when total_u == 0) and
+ * qacc_warmstart[total_v] (zeros for a cold start), all updated in place.
+ * The launch is ordered on `stream` (cudaStream_t; NULL = legacy default
+ * stream).  Per-env statistics of the call are not kept (mjb200_batched_stats
+ * still reports the sim's own last step).
+ *
+ * Scratch comes from a fixed area inside the library, sized for at most
+ * 65536 envs; a larger sim is rejected (return -2, mjb200_last_error says
+ * why).  Make the first call on each device before any stream capture: it
+ * looks up the scratch address once for that device.  The scratch is shared
+ * by every sim on a device, so calls whose kernels may overlap in time race;
+ * order them on one stream.
+ *
+ * Returns 0 on success, -1 bad arguments, -2 too many envs, -3 CUDA error. */
+MJMLX_API int mjb200_batched_step_noalloc(MjmlxBatchedSim* sim, float* qpos, float* qvel, const float* ctrl, float* qacc_warmstart, int n,
+                                          void* stream);
 /* Device pointers of the HBM-resident state (float, env-major records). */
 MJMLX_API int mjb200_batched_device_state(MjmlxBatchedSim* sim, float** qpos, float** qvel, float** ctrl, float** qacc_warmstart);
 /* The CUDA stream (cudaStream_t) every launch of the sim is ordered on. */

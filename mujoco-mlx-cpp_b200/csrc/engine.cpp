@@ -442,6 +442,41 @@ StepParams Engine::params(int n, bool record) {
   return P;
 }
 
+StepParams Engine::external_params(float* qpos, float* qvel, const float* ctrl, float* qacc_warm, int n, int* work_counter, int* stats6) const {
+  StepParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.models = d_models_.p;
+  P.itab = d_itab_.p;
+  P.ftab = d_ftab_.p;
+  P.num_envs = B_;
+  P.env_model = d_model_.p;
+  P.env_qadr = d_qadr_.p;
+  P.env_vadr = d_vadr_.p;
+  P.env_uadr = d_uadr_.p;
+  P.env_badr = d_badr_.p;
+  P.qpos = qpos;
+  P.qvel = qvel;
+  P.ctrl = ctrl;
+  P.qacc_warm = qacc_warm;
+  P.nsub = n;
+  P.work_counter = work_counter;
+  P.lockstep = 0;
+  P.ws_stride = ws_stride_;
+  P.desc_words = desc_words_;
+  P.status = stats6;
+  P.niter_sum = stats6 + B_;
+  P.niter_max = stats6 + 2 * B_;
+  P.ncon_out = stats6 + 3 * B_;
+  P.nefc_out = stats6 + 4 * B_;
+  P.warm_choice = stats6 + 5 * B_;
+  if (rand_on_) {
+    P.rand_mass = rand_mass_.p;
+    P.rand_friction = rand_fric_.p;
+    P.rand_gain = rand_gain_.p;
+  }
+  return P;
+}
+
 void Engine::invalidate_graphs() {
   for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
   graphs_.clear();

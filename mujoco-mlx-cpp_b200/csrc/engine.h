@@ -113,6 +113,14 @@ class Engine {
   float* d_ctrl() { return ctrl_.p; }
   float* d_qacc_warm() { return warm_.p; }
 
+  // Launch parameters that read and write caller-owned buffers (state in the
+  // sim's layout, work-queue head, six per-env statistics arrays of num_envs
+  // ints each) instead of the engine's own; used by the allocation-free entry.
+  StepParams external_params(float* qpos, float* qvel, const float* ctrl, float* qacc_warm, int n, int* work_counter, int* stats6) const;
+  int desc_words() const { return desc_words_; }
+  int ws_stride() const { return ws_stride_; }
+  int sm_count() const { return sm_count_; }
+
   int pack_spec(const int* body_ids, int nsel, int dof_lo, int ndof);
   int get_pack(float* out);
   int raycast(const float* pnt, const float* vec, int nray, int bodyexclude, const unsigned char* geomgroup, int flg_static, float* dist, int* geomid);

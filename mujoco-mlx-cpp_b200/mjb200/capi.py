@@ -68,6 +68,7 @@ def _load():
         "mjb200_batched_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "mjb200_batched_step_device": (C.c_int, [C.c_void_p, C.c_int]),
         "mjb200_batched_step_device_ctrl": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+        "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         "mjb200_batched_stream": (C.c_void_p, [C.c_void_p]),
         "mjb200_batched_launch_shape": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p]),
@@ -214,6 +215,12 @@ class BatchedSim:
     def step_device_ctrl(self, ctrl_ptr: int, n: int = 1):
         if lib.mjb200_batched_step_device_ctrl(self.handle, C.c_void_p(ctrl_ptr), n) != 0:
             raise RuntimeError(last_error())
+
+    def step_noalloc(self, qpos_ptr: int, qvel_ptr: int, ctrl_ptr: int, warm_ptr: int, n: int = 1, stream: int | None = None) -> int:
+        """Allocation-free step on caller-owned device buffers; returns the C
+        status (0 ok, -1 bad arguments, -2 too many envs, -3 CUDA error)."""
+        return lib.mjb200_batched_step_noalloc(self.handle, C.c_void_p(qpos_ptr), C.c_void_p(qvel_ptr), C.c_void_p(ctrl_ptr),
+                                               C.c_void_p(warm_ptr), n, C.c_void_p(stream))
 
     def sync(self):
         lib.mjmlx_batched_eval_state(self.handle)
