@@ -200,15 +200,17 @@ def run_ours(args, world, rank, local):
     import torch
 
     import mjb200
+    from mjb200 import replicas
 
     torch.cuda.set_device(local)
     B = args.envs
     K, W = args.steps, args.warmup
     m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
     sim = mjb200.BatchedSim(m, B, record=0)
-    q0, v0 = mjb200.models.quadruped_initial_state_fast(B, seed=1000 + 7919 * rank)
+    seed_state, seed_ctrl = replicas.rank_seeds(rank)
+    q0, v0 = mjb200.models.quadruped_initial_state_fast(B, seed=seed_state)
     nu = m.nu
-    ctrl_all = np.stack([mjb200.models.quadruped_controls_fast(B, s, seed=2000 + 7919 * rank) for s in range(K + W)]).astype(np.float32)
+    ctrl_all = np.stack([mjb200.models.quadruped_controls_fast(B, s, seed=seed_ctrl) for s in range(K + W)]).astype(np.float32)
     ctrl_dev = torch.from_numpy(ctrl_all).cuda()
     stride = B * nu
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -247,10 +249,7 @@ def run_ours(args, world, rank, local):
     niter_mean = float(st["niter_sum"].mean() / SUBSTEPS)
     niter_p99 = float(np.percentile(st["niter_max"], 99))
     total_s = sum(step_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([total_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = replicas.reduce_over_ranks(total_s, "max", device="cuda")
     value = world * B * K / total_s
 
     # ---- e2e: public C ABI with host buffers
@@ -269,10 +268,7 @@ def run_ours(args, world, rank, local):
         sim.step(host_ctrl[W + k], SUBSTEPS)
         qp, qv = sim.state()
         e2e_s += time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.reduce_over_ranks(e2e_s, "max", device="cuda")
     e2e_value = world * B * K / e2e_s
     h2d = B * nu * 4
     d2h = B * (m.nq + m.nv) * 4

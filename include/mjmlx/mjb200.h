@@ -107,11 +107,6 @@ MJMLX_API int mjb200_batched_stats(MjmlxBatchedSim* sim, int* status, int* niter
 /* Solver acceleration qacc of the last substep, float[total_v]. */
 MJMLX_API const float* mjb200_batched_get_qacc(MjmlxBatchedSim* sim, int* n_out);
 
-/* Capture contacts / constraint rows / solver vectors of the last substep.
- * set_debug(ncon_max, nefc_max) enables capture (0 disables); get_debug fills
- * contacts[num_envs*ncon_max*16] (pos3 frame9 dist pair dim includemargin),
- * efc[num_envs*nefc_max*4] (type force D aref), vec[num_envs*4*nv_max]
- * (qacc_smooth, qfrc_smooth, qacc, qfrc_constraint); returns nv_max. */
 /* Per-stage SM clock totals of the lockstep step kernel (8 stages: state check
  * + kinematics, collision, COM + CRB, RNE + forces, unconstrained solve,
  * constraint build, Newton, integration).  enable 1 starts (and zeroes) the
@@ -119,6 +114,11 @@ MJMLX_API const float* mjb200_batched_get_qacc(MjmlxBatchedSim* sim, int* n_out)
  * totals accumulated so far.  Returns 0 / -1. */
 MJMLX_API int mjb200_batched_stage_timing(MjmlxBatchedSim* sim, int enable, unsigned long long* cycles8);
 
+/* Capture contacts / constraint rows / solver vectors of the last substep.
+ * set_debug(ncon_max, nefc_max) enables capture (0 disables); get_debug fills
+ * contacts[num_envs*ncon_max*16] (pos3 frame9 dist pair dim includemargin),
+ * efc[num_envs*nefc_max*4] (type force D aref), vec[num_envs*4*nv_max]
+ * (qacc_smooth, qfrc_smooth, qacc, qfrc_constraint); returns nv_max. */
 MJMLX_API int mjb200_batched_set_debug(MjmlxBatchedSim* sim, int ncon_max, int nefc_max);
 MJMLX_API int mjb200_batched_get_debug(MjmlxBatchedSim* sim, float* contacts, float* efc, float* vec);
 

@@ -1,0 +1,212 @@
+"""Known answers and structural rules that pin the FP64 oracle (CPU only).
+
+MuJoCo C is not installed here and the reference ships no golden vectors for
+this path, so the oracle is pinned by closed-form mechanics (free fall, a
+pendulum, rigid-body mass matrices, exp-map rotation), by the reference's own
+structural rules (condim 3 pyramidal contacts give 4 rows each,
+tests/test_friction_condim3.cpp:88-101 of the reference) and by the
+optimality conditions of the Gauss-principle problem the Newton solver
+minimises (solver.hpp:592-854 of the reference).
+"""
+import numpy as np
+import pytest
+
+import mjb200
+import oracle
+
+G = 9.81
+H = 0.005
+
+
+def env_from_xml(xml, ncon_max=64, nefc_max=256):
+    m = mjb200.load_model_from_string(xml)
+    om = oracle.OracleModel(m.dump())
+    return om, oracle.OracleEnv(om, ncon_max, nefc_max)
+
+
+def wrap(body, option='<option timestep="0.005"/>', extra=""):
+    return f"<mujoco>{option}{extra}<worldbody>{body}</worldbody></mujoco>"
+
+
+PLANE = '<geom type="plane" size="5 5 0.1"/>'
+
+
+def test_free_fall_closed_form():
+    om, env = env_from_xml(wrap(PLANE + '<body pos="0 0 1"><freejoint/><geom type="sphere" size="0.1" mass="2"/></body>'))
+    for n in range(1, 11):
+        env.step()
+        # semi-implicit Euler: v_n = -g h n, z_n = 1 - g h^2 n (n + 1) / 2
+        assert env.a["qvel"][2] == pytest.approx(-G * H * n, rel=1e-12)
+        assert env.a["qpos"][2] == pytest.approx(1 - G * H * H * n * (n + 1) / 2, rel=1e-12)
+        assert env.d.ncon == 0 and env.d.nefc == 0 and env.d.status == 0
+    np.testing.assert_allclose(env.a["qpos"][3:], [1, 0, 0, 0], atol=1e-15)
+
+
+@pytest.mark.parametrize("theta", [0.3, -1.1, 2.0])
+def test_pendulum_acceleration(theta):
+    L, m, r = 0.7, 1.5, 0.02
+    om, env = env_from_xml(wrap(f'<body><joint type="hinge" axis="0 1 0"/><geom type="sphere" pos="0 0 {-L}" size="{r}" mass="{m}"/></body>'))
+    env.a["qpos"][0] = theta
+    env.step()
+    inertia = m * L * L + 0.4 * m * r * r
+    want = -m * G * L * np.sin(theta) / inertia
+    assert env.a["qacc_smooth"][0] == pytest.approx(want, rel=1e-10)
+    assert env.a["M"][0] == pytest.approx(inertia, rel=1e-10)
+
+
+def test_free_box_mass_matrix_and_invweights():
+    m_, hx, hy, hz = 3.0, 0.1, 0.2, 0.3
+    xml = wrap(f'<body pos="0 0 2" quat="0.9 0.1 0.3 0.2"><freejoint/><geom type="box" size="{hx} {hy} {hz}" mass="{m_}"/></body>')
+    model = mjb200.load_model_from_string(xml)
+    d = model.dump()
+    om = oracle.OracleModel(d)
+    env = oracle.OracleEnv(om)
+    env.step()
+    I = m_ / 3 * np.array([hy * hy + hz * hz, hx * hx + hz * hz, hx * hx + hy * hy])
+    M = env.a["M"].reshape(6, 6)
+    # translational dofs in the world frame, rotational dofs in the body frame
+    np.testing.assert_allclose(M, np.diag([m_, m_, m_, *I]), atol=1e-12)
+    np.testing.assert_allclose(d["dof_invweight0"], [1 / m_] * 3 + [np.mean(1 / I)] * 3, rtol=1e-10)
+    np.testing.assert_allclose(d["body_invweight0"][2:4], [1 / m_, np.mean(1 / I)], rtol=1e-10)
+    assert d["opt_real"][7] == pytest.approx((3 * m_ + I.sum()) / 6, rel=1e-12)  # meaninertia
+
+
+def test_exp_map_rotation():
+    om, env = env_from_xml(wrap('<body pos="0 0 3"><freejoint/><geom type="sphere" size="0.1" mass="1"/></body>'))
+    w = np.array([0.4, -1.0, 2.0])
+    env.a["qvel"][3:] = w
+    env.step()
+    ang = np.linalg.norm(w) * H
+    ax = w / np.linalg.norm(w)
+    np.testing.assert_allclose(env.a["qpos"][3:], [np.cos(ang / 2), *(np.sin(ang / 2) * ax)], atol=1e-14)
+    np.testing.assert_allclose(env.a["qvel"][3:], w, atol=1e-14)  # isotropic body: no gyroscopic torque
+
+
+def test_sphere_plane_contact_frame_and_rows():
+    om, env = env_from_xml(wrap(PLANE + '<body pos="0 0 0.099"><freejoint/><geom type="sphere" size="0.1" mass="2"/></body>'))
+    env.step()
+    assert env.d.ncon == 1 and env.d.nefc == 4
+    c = env.contacts()[0]
+    assert c[12] == pytest.approx(-0.001, abs=1e-12)            # distance
+    frame = c[3:12].reshape(3, 3)
+    np.testing.assert_allclose(frame[0], [0, 0, 1], atol=1e-15)  # normal from the plane (geom 1) to the sphere
+    np.testing.assert_allclose(frame @ frame.T, np.eye(3), atol=1e-14)
+    np.testing.assert_allclose(c[0:3], [0, 0, -0.0005], atol=1e-12)  # midpoint of the penetration
+    assert list(env.efc()["type"]) == [2, 2, 2, 2]
+
+
+@pytest.mark.parametrize("geom,ncon", [
+    ('<geom type="box" size="0.2 0.1 0.05" mass="1"/>', 4),
+    ('<geom type="capsule" fromto="-0.2 0 0 0.2 0 0" size="0.05" mass="1"/>', 2),
+    ('<geom type="sphere" size="0.05" mass="1"/>', 1),
+])
+def test_plane_multi_contact_counts(geom, ncon):
+    om, env = env_from_xml(wrap(PLANE + f'<body pos="0 0 0.049"><freejoint/>{geom}</body>'))
+    env.step()
+    assert env.d.ncon == ncon
+    assert env.d.nefc == 4 * ncon
+
+
+def test_resting_sphere_supports_its_weight():
+    m_ = 2.0
+    om, env = env_from_xml(wrap(PLANE + f'<body pos="0 0 0.1"><freejoint/><geom type="sphere" size="0.1" mass="{m_}"/></body>'))
+    for _ in range(600):
+        env.step()
+    assert env.d.ncon == 1
+    assert abs(env.a["qvel"]).max() < 1e-6
+    # the pyramid rows' forces sum to the normal force
+    assert env.efc()["force"].sum() == pytest.approx(m_ * G, rel=1e-4)
+    assert -2e-3 < env.a["qpos"][2] - 0.1 < 0
+
+
+def test_joint_limit_and_frictionloss_rows():
+    xml = wrap('<body><joint type="hinge" axis="0 1 0" range="-0.5 0.5" limited="true" frictionloss="0.1"/>'
+               '<geom type="capsule" fromto="0 0 0 0 0 -0.5" size="0.02" mass="1"/></body>')
+    om, env = env_from_xml(xml)
+    env.a["qpos"][0] = 0.0
+    env.step()
+    assert list(env.efc()["type"]) == [0]                       # frictionloss row only
+    env.a["qpos"][0] = 0.6
+    env.a["qvel"][0] = 0.0
+    env.step()
+    t = list(env.efc()["type"])
+    assert t == [0, 1]                                            # frictionloss before the limit row
+    assert env.efc()["force"][1] > 0                               # the limit pushes back
+
+
+def test_contact_overflow_keeps_first_contacts():
+    om, env = env_from_xml(wrap(PLANE + '<body pos="0 0 0.049"><freejoint/><geom type="box" size="0.2 0.1 0.05" mass="1"/></body>'),
+                           ncon_max=2)
+    env.step()
+    assert env.d.ncon == 2 and env.d.status & 4
+    assert env.d.nefc == 8
+
+
+def test_bad_state_resets_to_qpos0():
+    om, env = env_from_xml(wrap('<body pos="0 0 1"><freejoint/><geom type="sphere" size="0.1" mass="1"/></body>'))
+    env.a["qvel"][1] = np.nan
+    env.step()
+    assert env.d.status & 1
+    assert np.isfinite(env.a["qpos"]).all() and np.isfinite(env.a["qvel"]).all()
+
+
+def _gauss_residual(om, env):
+    """Optimality of the Newton solution for pyramid/limit rows: with
+    r = J qacc - aref and f = -D min(r, 0), M (qacc - qacc_smooth) = J^T f."""
+    nv = om.nv
+    M = env.a["M"].reshape(nv, nv)
+    e = env.efc()
+    r = e["J"] @ env.a["qacc"] - e["aref"]
+    f = -e["D"] * np.minimum(r, 0.0)
+    lhs = M @ (env.a["qacc"] - env.a["qacc_smooth"])
+    rhs = e["J"].T @ f
+    return np.linalg.norm(lhs - rhs) / max(np.linalg.norm(M @ env.a["qacc_smooth"]), 1.0), f, e["force"]
+
+
+def test_newton_solution_is_gauss_optimal_quadruped(quad_model):
+    om = oracle.OracleModel(quad_model.dump())
+    qpos, qvel = mjb200.models.quadruped_initial_state(24)
+    ob = oracle.OracleBatch(om, 24)
+    ob.set_state(qpos, qvel)
+    checked = 0
+    for s in range(40):
+        ob.set_ctrl(mjb200.models.quadruped_controls(24, s // 4))
+        ob.step(1, nthread=4)
+        if s % 10 == 9:
+            for env in ob.envs:
+                assert env.d.status == 0
+                types = env.efc()["type"]
+                # condim 3 pyramidal: 4 rows per contact
+                assert (types == 2).sum() == 4 * env.d.ncon
+                assert set(types.tolist()) <= {1, 2}
+                res, f, force = _gauss_residual(om, env)
+                assert res < 1e-6
+                np.testing.assert_allclose(force, f, atol=1e-6 * max(1.0, np.abs(f).max(initial=0.0)))
+                checked += 1
+    assert checked == 96
+
+
+def test_quadruped_mass_matrix_spd(quad_model):
+    om = oracle.OracleModel(quad_model.dump())
+    qpos, qvel = mjb200.models.quadruped_initial_state(8)
+    for e in range(8):
+        env = oracle.OracleEnv(om)
+        env.a["qpos"][:] = qpos[e]
+        env.a["qvel"][:] = qvel[e]
+        env.step()
+        M = env.a["M"].reshape(om.nv, om.nv)
+        np.testing.assert_allclose(M, M.T, atol=1e-12)
+        assert np.linalg.eigvalsh(M).min() > 0
+
+
+def test_batch_threads_deterministic(quad_model):
+    om = oracle.OracleModel(quad_model.dump())
+    qpos, qvel = mjb200.models.quadruped_initial_state(16)
+    out = []
+    for nthread in (1, 4):
+        ob = oracle.OracleBatch(om, 16)
+        ob.set_state(qpos, qvel)
+        ob.set_ctrl(mjb200.models.quadruped_controls(16, 0))
+        ob.step(8, nthread=nthread)
+        out.append(ob.state())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
