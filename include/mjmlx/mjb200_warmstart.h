@@ -1,0 +1,84 @@
+/*
+ * mjb200 learned Newton warm start.  No counterpart in the reference, whose
+ * Newton solver starts from qacc = 0 (src/compat/mkx_kernels/solver.hpp:592).
+ *
+ * A 3 x 256 GELU MLP maps the state an env reaches at the end of a substep
+ * (qpos without the free root's x, y; qvel; the converged qacc; normal and
+ * distance of up to 16 contacts) plus the controls of the next substep to the
+ * change of the converged acceleration over that substep.  Attached to a sim,
+ * its prediction is a third warm-start candidate of the Newton solver next to
+ * qacc_smooth and the previous qacc; the solver keeps the lowest Gauss cost
+ * and iterates to the same tolerance as without it.
+ *
+ * All arrays named *_dev are device pointers (float, row-major).  Functions
+ * return 0 on success and -1 on error (message in mjb200_last_error), unless
+ * stated otherwise.
+ */
+#ifndef MJB200_WARMSTART_H
+#define MJB200_WARMSTART_H
+
+#include "mjb200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct MjbWarmStart MjbWarmStart;
+
+/* Network for in_raw inputs and nout outputs (the model's nv).  in_raw for a
+ * sim is mjb200_warmstart_input_width(sim).  NULL on failure. */
+MJMLX_API MjbWarmStart* mjb200_warmstart_create(int in_raw, int nout, unsigned long long seed);
+MJMLX_API void mjb200_warmstart_free(MjbWarmStart* net);
+
+/* Input width (features + controls) the sim's learned warm start expects, or -1. */
+MJMLX_API int mjb200_warmstart_input_width(const MjmlxBatchedSim* sim);
+
+/* Sizes: input width, padded input width, hidden width, output width, padded
+ * output width, total parameter count.  Any pointer may be NULL. */
+MJMLX_API int mjb200_warmstart_dims(const MjbWarmStart* net, int* in_raw, int* in_pad, int* hidden, int* nout, int* out_pad, int* nparams);
+
+/* FP32 parameters in the order W0[hidden][in_pad], b0[hidden], W1[hidden][hidden],
+ * b1, W2[hidden][hidden], b2, W3[out_pad][hidden], b3[out_pad] (host arrays). */
+MJMLX_API int mjb200_warmstart_get_params(const MjbWarmStart* net, float* params);
+MJMLX_API int mjb200_warmstart_set_params(MjbWarmStart* net, const float* params);
+
+/* Input / target normalisation (host arrays of in_raw and nout floats). */
+MJMLX_API int mjb200_warmstart_set_normalization(MjbWarmStart* net, const float* in_mean, const float* in_std, const float* out_mean, const float* out_std);
+MJMLX_API int mjb200_warmstart_get_normalization(const MjbWarmStart* net, float* in_mean, float* in_std, float* out_mean, float* out_std);
+/* Mean and standard deviation of training data xraw_dev[n][in_raw], traw_dev[n][nout]. */
+MJMLX_API int mjb200_warmstart_fit_normalization(MjbWarmStart* net, const float* xraw_dev, const float* traw_dev, int n);
+
+/* Network output y_dev[n][nout] (normalised target units) for raw inputs. */
+MJMLX_API int mjb200_warmstart_forward(MjbWarmStart* net, const float* xraw_dev, int n, float* y_dev);
+/* Loss and gradient of one batch of n rows (n a multiple of 64): loss = mean
+ * over rows and outputs of the squared error in normalised units; grads
+ * (host, parameter layout) may be NULL. */
+MJMLX_API int mjb200_warmstart_gradients(MjbWarmStart* net, const float* xraw_dev, const float* traw_dev, int n, float* grads, float* loss);
+/* Adam training, batch a multiple of 64, cosine-decayed learning rate;
+ * epoch_loss (host, epochs floats) may be NULL.  Returns the number of
+ * optimiser steps, or -1. */
+MJMLX_API int mjb200_warmstart_train(MjbWarmStart* net, const float* xraw_dev, const float* traw_dev, int n, int epochs, int batch, float lr,
+                                     unsigned long long seed, float* epoch_loss);
+
+/* Training data from a plain rollout of the sim (learned warm start off):
+ * ctrl_dev holds nctrl control sets of total_u floats, each applied for
+ * substeps_per_ctrl substeps; every substep after the first writes num_envs
+ * rows xraw_dev[.][in_raw] and traw_dev[.][nv] while max_rows allows.
+ * Returns the number of rows written, or -1. */
+MJMLX_API int mjb200_batched_warmstart_collect(MjmlxBatchedSim* sim, const float* ctrl_dev, int nctrl, int substeps_per_ctrl, float* xraw_dev,
+                                               float* traw_dev, int max_rows);
+/* Attaches a net to the sim (NULL detaches).  The net must outlive the
+ * attachment and serves one sim batch size. */
+MJMLX_API int mjb200_batched_set_warmstart(MjmlxBatchedSim* sim, MjbWarmStart* net);
+
+/* C[M][N] (float, device) = A[M][K] * B[N][K]^T with bf16 device operands, on
+ * the tcgen05 GEMM the network uses.  K a multiple of 64; N 64, 128, 192 or a
+ * multiple of 256.  stream: cudaStream_t (NULL = legacy default).  Returns
+ * 0, -1 bad arguments, -3 CUDA error. */
+MJMLX_API int mjb200_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MJB200_WARMSTART_H */

@@ -25,3 +25,15 @@ cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, c
   mjb_reset_kernel<<<grid, warps * 32, 0, s>>>(models, env_model, qadr, vadr, ftab, mask, B, qpos, qvel, warm);
   return cudaGetLastError();
 }
+
+// out = a - b elementwise (training targets of the learned warm start).
+__global__ void mjb_sub_kernel(int n, const float* a, const float* b, float* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] - b[i];
+}
+
+cudaError_t mjb_sub(int n, const float* a, const float* b, float* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  mjb_sub_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, a, b, out);
+  return cudaGetLastError();
+}

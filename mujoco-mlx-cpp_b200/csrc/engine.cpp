@@ -1,13 +1,16 @@
 #include "engine.h"
+#include "warmstart.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
 cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
+cudaError_t mjb_sub(int n, const float* a, const float* b, float* out, cudaStream_t s);
 cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
                              float* qpos, float* qvel, float* warm, cudaStream_t s);
 
@@ -36,6 +39,7 @@ template struct DevBuf<int>;
 template struct DevBuf<DevModelDesc>;
 template struct DevBuf<uint16_t>;
 template struct DevBuf<unsigned long long>;
+template struct DevBuf<double>;
 
 namespace {
 
@@ -77,6 +81,7 @@ Engine::Engine(const std::vector<const Model*>& models, const std::vector<int>& 
   check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
   if (prop.major < 10) throw std::runtime_error("engine: this build targets sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
   sm_count_ = prop.multiProcessorCount;
+  if (const char* pz = std::getenv("MJB200_POISON_WORKSPACE")) poison_ = std::atoi(pz) != 0;
   check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   rand_on_ = domain_rand != 0;
   build_tables(cfg, solver_iterations);
@@ -400,7 +405,6 @@ StepParams Engine::params(int n, bool record) {
   P.qvel = qvel_.p;
   P.ctrl = ctrl_.p;
   P.qacc_warm = warm_.p;
-  P.qacc_pred = use_pred_ ? pred_.p : nullptr;
   P.nsub = n;
   P.max_iter = 0;
   P.work_counter = (persistent_ && !lockstep_) ? counter_.p : nullptr;
@@ -408,6 +412,7 @@ StepParams Engine::params(int n, bool record) {
   P.stage_cycles = timing_ ? stage_cycles_.p : nullptr;
   P.ws_stride = ws_stride_;
   P.desc_words = desc_words_;
+  P.poison_workspace = poison_;
   P.status = status_.p;
   P.niter_sum = niter_sum_.p;
   P.niter_max = niter_max_.p;
@@ -437,8 +442,6 @@ StepParams Engine::params(int n, bool record) {
     P.rand_friction = rand_fric_.p;
     P.rand_gain = rand_gain_.p;
   }
-  P.features = feat_.p;
-  P.feat_stride = feat_stride_;
   return P;
 }
 
@@ -482,8 +485,50 @@ void Engine::invalidate_graphs() {
   graphs_.clear();
 }
 
+void Engine::launch_learned(int n, bool record) {
+  const bool first_valid = feat_valid_;
+  const Model& m = *models_[0];
+  const int F = feature_count(), qskip = feature_qskip();
+  auto body = [&]() {
+    for (int s = 0; s < n; s++) {
+      const bool have = first_valid || s > 0;
+      if (have) net_->infer(feat_.p, feat_stride_, F, ctrl_.p, m.nu, warm_.p, pred_.p, B_, stream_);
+      StepParams P = params(1, record && s == n - 1);
+      P.qacc_pred = have ? pred_.p : nullptr;
+      P.features = feat_.p;
+      P.feat_stride = feat_stride_;
+      P.feat_qskip = qskip;
+      P.stats_accumulate = s > 0;
+      if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
+      check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+    }
+  };
+  feat_valid_ = true;
+  if (!cfg_.use_graph) {
+    body();
+    return;
+  }
+  auto key = std::make_pair(n, (record ? 1 : 0) | (first_valid ? 2 : 0) | 4);
+  auto it = graphs_.find(key);
+  if (it == graphs_.end()) {
+    cudaGraph_t g;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    body();
+    check(cudaStreamEndCapture(stream_, &g), "end capture");
+    cudaGraphExec_t ge;
+    check(cudaGraphInstantiate(&ge, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    it = graphs_.emplace(key, ge).first;
+  }
+  check(cudaGraphLaunch(it->second, stream_), "graph launch");
+}
+
 void Engine::launch(int n, bool record) {
   if (n <= 0) return;
+  if (net_) {
+    launch_learned(n, record);
+    return;
+  }
   StepParams P = params(n, record);
   auto body = [&]() {
     if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
@@ -539,12 +584,14 @@ void Engine::get_state(float* qpos, float* qvel) {
 
 void Engine::set_state(const float* qpos, const float* qvel) {
   sync();
+  feat_valid_ = false;
   if (qpos) check(cudaMemcpy(qpos_.p, qpos, sizeof(float) * tot_q_, cudaMemcpyHostToDevice), "set qpos");
   if (qvel) check(cudaMemcpy(qvel_.p, qvel, sizeof(float) * tot_v_, cudaMemcpyHostToDevice), "set qvel");
 }
 
 void Engine::set_env_state(int env, const float* qpos, const float* qvel) {
   if (env < 0 || env >= B_) return;
+  feat_valid_ = false;
   const Model& m = *models_[h_model_[env]];
   sync();
   if (qpos) check(cudaMemcpy(qpos_.p + h_qadr_[env], qpos, sizeof(float) * m.nq, cudaMemcpyHostToDevice), "set env qpos");
@@ -553,6 +600,7 @@ void Engine::set_env_state(int env, const float* qpos, const float* qvel) {
 
 void Engine::reset(const int* mask) {
   if (!mask) return;
+  feat_valid_ = false;
   DevBuf<int> dm;
   std::vector<int> hm(mask, mask + B_);
   dm.upload(hm, stream_);
@@ -668,12 +716,81 @@ void Engine::stage_timing(int enable, unsigned long long* out8) {
   }
 }
 
-void Engine::set_features(int stride) {
+int Engine::feature_qskip() const {
+  const Model& m = *models_[0];
+  return (m.njnt > 0 && m.jnt_type[0] == JNT_FREE && m.jnt_bodyid[0] == 1) ? 2 : 0;
+}
+
+int Engine::feature_count() const {
+  const Model& m = *models_[0];
+  return m.nq - feature_qskip() + 2 * m.nv + 4 * MJB_FEAT_CONTACTS;
+}
+
+void Engine::ensure_features() {
+  if (!uniform()) throw std::runtime_error("learned warm start: needs a single-model batch");
+  const int F = feature_count();
+  const int stride = (F + 3) & ~3;
+  if (feat_.p && feat_stride_ == stride) return;
   sync();
   feat_stride_ = stride;
-  if (stride > 0) feat_.alloc((size_t)B_ * stride);
-  else feat_.release();
+  feat_.alloc((size_t)B_ * stride);
+  feat_valid_ = false;
   invalidate_graphs();
+}
+
+void Engine::set_warmstart(WarmStartNet* net) {
+  sync();
+  if (net) {
+    ensure_features();
+    const Model& m = *models_[0];
+    if (net->in_raw() != feature_count() + m.nu || net->nout() != m.nv)
+      throw std::runtime_error("learned warm start: the net's input / output widths do not match this model");
+    net->prepare_inference(B_);
+  }
+  net_ = net;
+  invalidate_graphs();
+}
+
+int Engine::collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows) {
+  ensure_features();
+  const Model& m = *models_[0];
+  const int F = feature_count(), nu = m.nu, nv = m.nv, in_raw = F + nu;
+  tmp_prev_.alloc((size_t)B_ * nv);
+  WarmStartNet* saved = net_;
+  net_ = nullptr;
+  bool have = false;
+  int rows = 0;
+  for (int c = 0; c < nctrl; c++) {
+    if (nu > 0) check(cudaMemcpyAsync(ctrl_.p, ctrl_seq + (size_t)c * tot_u_, sizeof(float) * tot_u_, cudaMemcpyDeviceToDevice, stream_), "collect ctrl");
+    for (int s = 0; s < sub_per_ctrl; s++) {
+      const bool take = have && rows + B_ <= max_rows;
+      if (take) {
+        float* xr = xraw + (size_t)rows * in_raw;
+        check(cudaMemcpy2DAsync(xr, sizeof(float) * in_raw, feat_.p, sizeof(float) * feat_stride_, sizeof(float) * F, B_, cudaMemcpyDeviceToDevice,
+                                stream_),
+              "collect features");
+        if (nu > 0)
+          check(cudaMemcpy2DAsync(xr + F, sizeof(float) * in_raw, ctrl_.p, sizeof(float) * nu, sizeof(float) * nu, B_, cudaMemcpyDeviceToDevice, stream_),
+                "collect ctrl rows");
+        check(cudaMemcpyAsync(tmp_prev_.p, warm_.p, sizeof(float) * (size_t)B_ * nv, cudaMemcpyDeviceToDevice, stream_), "collect prev");
+      }
+      StepParams P = params(1, false);
+      P.features = feat_.p;
+      P.feat_stride = feat_stride_;
+      P.feat_qskip = feature_qskip();
+      if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
+      check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+      if (take) {
+        check(mjb_sub(B_ * nv, warm_.p, tmp_prev_.p, traw + (size_t)rows * nv, stream_), "collect target");
+        rows += B_;
+      }
+      have = true;
+    }
+  }
+  sync();
+  feat_valid_ = true;
+  net_ = saved;
+  return rows;
 }
 
 }  // namespace mjb

@@ -94,10 +94,23 @@ class Engine {
   bool domain_rand() const { return rand_on_; }
 
   // learned warm start
+  // Raw features per env written after each substep (qpos minus the leading
+  // free-joint x, y; qvel; converged qacc; 16 x contact normal and distance).
+  int feature_count() const;
+  int feature_qskip() const;
+  // Attaches a trained net (null detaches): every substep then first runs the
+  // net on the features of the previous substep and the current controls and
+  // offers its prediction to the Newton solver as a warm-start candidate.
+  void set_warmstart(class WarmStartNet* net);
+  class WarmStartNet* warmstart() const { return net_; }
+  // Plain rollout that records training pairs: for each substep after the
+  // first, xraw row = [features of the previous substep | controls] and traw
+  // row = converged qacc of the substep minus that of the previous one.
+  // ctrl_seq: nctrl device control sets of total_u floats, each held for
+  // sub_per_ctrl substeps.  Returns the number of rows written (<= max_rows).
+  int collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows);
+  const float* features_device() const { return feat_.p; }
   float* qacc_pred_device() { return pred_.p; }
-  void set_prediction_enabled(bool on) { use_pred_ = on; invalidate_graphs(); }
-  uint16_t* features_device() { return feat_.p; }
-  void set_features(int stride);
 
   void configure(const EngineConfig& cfg);
   const EngineConfig& config() const { return cfg_; }
@@ -130,6 +143,8 @@ class Engine {
   void alloc_state();
   void choose_launch();
   void launch(int n, bool record);
+  void launch_learned(int n, bool record);
+  void ensure_features();
   void invalidate_graphs();
   StepParams params(int n, bool record);
 
@@ -138,7 +153,6 @@ class Engine {
   int B_ = 0, tot_q_ = 0, tot_v_ = 0, tot_u_ = 0, tot_b_ = 0, nv_max_ = 0;
   EngineConfig cfg_;
   bool rand_on_ = false;
-  bool use_pred_ = false;
   cudaStream_t stream_ = nullptr;
 
   std::vector<ModelLayout> layouts_;
@@ -156,10 +170,13 @@ class Engine {
   int dbg_ncon_ = 0, dbg_nefc_ = 0;
   DevBuf<float> rand_mass_, rand_fric_, rand_gain_;
   std::vector<float> h_rand_mass_, h_rand_fric_, h_rand_gain_;
-  DevBuf<uint16_t> feat_;
+  DevBuf<float> feat_, tmp_prev_;
   DevBuf<unsigned long long> stage_cycles_;
   bool timing_ = false;
+  int poison_ = 0;   // MJB200_POISON_WORKSPACE=1 at creation: NaN-fill shared workspaces (test aid)
   int feat_stride_ = 0;
+  bool feat_valid_ = false;   // features of the last substep are in feat_ (cleared by state changes)
+  class WarmStartNet* net_ = nullptr;
 
   float* h_ctrl_pinned_ = nullptr;
   std::map<std::string, float*> h_stage_;

@@ -1,0 +1,501 @@
+// Learned warm start: BF16 tensor-core GEMMs (tcgen05 + TMEM, TMA operand
+// loads) with the epilogues the MLP's forward and backward passes need, plus
+// the small kernels around them (feature gather/normalise with transpose,
+// column sums, Adam, column statistics).
+//
+// GEMM shape: C[M x N] = A[M x K] * B[N x K]^T with A and B row-major and
+// K-contiguous ("TN"), M tiled by 128 rows per CTA, N <= 256 per CTA, K in
+// chunks of 64 (one 128-byte swizzle row per tile row).  Warp 0 lane 0 issues
+// TMA loads into a 3-stage ring, warp 1 lane 0 issues tcgen05.mma (M 128,
+// N = tile, K 16 per instruction) accumulating in TMEM, and all four warps
+// read their 32 TMEM lanes back for the fused epilogue.  Every mbarrier wait
+// is bounded by the global timer; a wait that gives up sets an abort flag
+// for the CTA and the caller's error word, and the CTA skips the epilogue,
+// releases its TMEM and returns.
+#include "mlp_kernels.cuh"
+
+#include <mutex>
+
+namespace mjb {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BK = 64;
+constexpr int STAGES = 3;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Waits for the phase with the given parity; false when the CTA aborted or
+// the time limit passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  const uint32_t addr = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+    if ((it & 63) == 0) {
+      unsigned long long t = global_ns();
+      if (it == 0) t0 = t;
+      else if (t - t0 > kWaitLimitNs) return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows of
+// 128 bytes, 8-row groups 1024 bytes apart (SBO), LBO unused (1), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
+        "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+__device__ __forceinline__ void store_row16(__nv_bfloat16* dst, const float* v) {
+  __align__(16) __nv_bfloat162 h[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+  const uint4* s = reinterpret_cast<const uint4*>(h);
+  d[0] = s[0];
+  d[1] = s[1];
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmArgs a) {
+  constexpr int A_BYTES = BM * BK * 2;
+  constexpr int B_BYTES = BN * BK * 2;
+  constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nk = a.K / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  int issued = 0;
+  if (warp == 0 && lane == 0) {
+    for (int kc = 0; kc < nk; kc++) {
+      const int s = kc % STAGES;
+      if (kc >= STAGES && !mbar_wait(&empty[s], ((kc / STAGES) - 1) & 1, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      uint8_t* sa = smem + s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      tma_load_2d(sa, &tmA, &full[s], kc * BK, m0);
+      tma_load_2d(sa + A_BYTES, &tmB, &full[s], kc * BK, n0);
+      issued = kc + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    for (int kc = 0; kc < nk; kc++) {
+      const int s = kc % STAGES;
+      if (!mbar_wait(&full[s], (kc / STAGES) & 1, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = smem_u32(smem + s * STAGE_BYTES);
+      const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+      for (int k = 0; k < BK / 16; k++) mma_bf16(tmem, sw128_desc(sa + 32 * k), sw128_desc(sb + 32 * k), IDESC, (kc | k) != 0);
+      mma_commit(&empty[s]);
+    }
+    mma_commit(done);
+  }
+  __syncwarp();
+  const bool ok = mbar_wait(done, 0, abort_flag) && !*abort_flag;
+  __syncwarp();
+  tc_fence_after();
+
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+    const bool rv = row < a.M;
+    const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+    float lsum = 0.f;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      float v[16];
+      tmem_ld16(tbase + c0, v);
+      const int col0 = n0 + c0;
+      if (col0 >= a.N) continue;  // warp-uniform
+      if (a.bias && a.mode != EPI_BWD_GELU) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] += a.bias[col0 + i];
+      }
+      // rows past M store nothing; the warp stays converged for the next
+      // tcgen05.ld (a .sync.aligned instruction)
+      if (rv) switch (a.mode) {
+        case EPI_F32: {
+          float4* d = reinterpret_cast<float4*>(a.out_f32 + (size_t)row * a.ldo + col0);
+#pragma unroll
+          for (int i = 0; i < 4; i++) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+          break;
+        }
+        case EPI_HIDDEN: {
+          if (a.pre) store_row16(a.pre + (size_t)row * a.ldo + col0, v);
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] = gelu(v[i]);
+          store_row16(a.out + (size_t)row * a.ldo + col0, v);
+          if (a.out_t) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) a.out_t[(size_t)(col0 + i) * a.ldt + row] = __float2bfloat16_rn(v[i]);
+          }
+          break;
+        }
+        case EPI_OUT_LOSS: {
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            const int col = col0 + i;
+            float d = 0.f;
+            if (col < a.nvalid) {
+              d = v[i] - a.target[(size_t)row * a.nvalid + col];
+              lsum += d * d;
+            }
+            v[i] = a.scale * d;
+          }
+          store_row16(a.out + (size_t)row * a.ldo + col0, v);
+          if (a.out_t) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) a.out_t[(size_t)(col0 + i) * a.ldt + row] = __float2bfloat16_rn(v[i]);
+          }
+          break;
+        }
+        case EPI_OUT_PRED: {
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            const int col = col0 + i;
+            if (col < a.nvalid) {
+              const size_t o = (size_t)row * a.nvalid + col;
+              a.pred[o] = a.prev[o] + a.omean[col] + a.ostd[col] * v[i];
+            }
+          }
+          break;
+        }
+        case EPI_BWD_GELU: {
+          const __nv_bfloat16* z = a.pre_in + (size_t)row * a.ldo + col0;
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] *= gelu_grad(__bfloat162float(z[i]));
+          store_row16(a.out + (size_t)row * a.ldo + col0, v);
+          if (a.out_t) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) a.out_t[(size_t)(col0 + i) * a.ldt + row] = __float2bfloat16_rn(v[i]);
+          }
+          break;
+        }
+        default:
+          break;
+      }
+      __syncwarp();
+    }
+    if (a.mode == EPI_OUT_LOSS && a.loss) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+      if (lane == 0) atomicAdd(a.loss, lsum);
+    }
+  } else if (threadIdx.x == 0) {
+    if (a.err) atomicExch(a.err, 1);
+    // let the TMA copies this thread issued land before the CTA's shared
+    // memory is released (each wait again bounded by the time limit)
+    volatile int no_abort = 0;
+    for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; kc++) mbar_wait(&full[kc % STAGES], (kc / STAGES) & 1, &no_abort);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+template <int BN>
+size_t gemm_smem_bytes() {
+  return 1024 + (size_t)STAGES * (BM * BK * 2 + BN * BK * 2) + 128;
+}
+
+template <int BN>
+cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmArgs& a, cudaStream_t s) {
+  const size_t smem = gemm_smem_bytes<BN>();
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [&] { attr_err = cudaFuncSetAttribute(gemm_tn_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
+  if (attr_err != cudaSuccess) return attr_err;
+  dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN);
+  gemm_tn_kernel<BN><<<grid, 128, smem, s>>>(tmA, tmB, a);
+  return cudaGetLastError();
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+}  // namespace
+
+bool make_tmap_bf16(CUtensorMap* map, const void* base, int rows, int cols, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn || !base || rows <= 0 || cols <= 0 || cols % BK != 0 || box_rows <= 0 || box_rows > 256) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t gemm_tn(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmArgs& a, cudaStream_t s) {
+  if (a.M <= 0 || a.K <= 0 || a.K % BK != 0 || a.N <= 0 || a.N % 16 != 0) return cudaErrorInvalidValue;
+  if (a.N == 64) return launch_gemm<64>(tmA, tmB, a, s);
+  if (a.N == 128) return launch_gemm<128>(tmA, tmB, a, s);
+  if (a.N == 192) return launch_gemm<192>(tmA, tmB, a, s);
+  if (a.N % 256 == 0) return launch_gemm<256>(tmA, tmB, a, s);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace mjb
+
+// ---------------------------------------------------------------- helpers
+
+namespace mjb {
+namespace {
+
+constexpr int GATHER_ROWS = 64;
+
+// One CTA normalises GATHER_ROWS rows into bf16: row r of the output takes
+// raw source row src_row (idx[r] or r) = [a (na floats) | b (nb floats)],
+// x_j = (raw_j - mean_j) * istd_j, zero past na + nb up to ld.  Writes the
+// row-major tile and, when xt is given, its transpose (xt[j * ldt + r]), both
+// coalesced through a shared-memory tile.  With targets: t[r][k] =
+// (traw[src][k] - tmean[k]) * tistd[k].
+__global__ void __launch_bounds__(256) gather_kernel(int rows, const int* idx, const float* a, int lda, int na, const float* b, int ldb, int nb,
+                                                     const float* mean, const float* istd, __nv_bfloat16* x, int ld, __nv_bfloat16* xt, int ldt,
+                                                     const float* traw, int nt, const float* tmean, const float* tistd, float* t) {
+  extern __shared__ __nv_bfloat16 tile[];  // [GATHER_ROWS][ld + 2]
+  const int r0 = blockIdx.x * GATHER_ROWS;
+  const int pitch = ld + 2;
+  for (int e = threadIdx.x; e < GATHER_ROWS * ld; e += blockDim.x) {
+    const int rr = e / ld, j = e % ld, r = r0 + rr;
+    float v = 0.f;
+    if (r < rows) {
+      const size_t src = idx ? (size_t)idx[r] : (size_t)r;
+      if (j < na) v = (a[src * lda + j] - mean[j]) * istd[j];
+      else if (j < na + nb) v = (b[src * ldb + (j - na)] - mean[j]) * istd[j];
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    tile[rr * pitch + j] = h;
+    if (r < rows) x[(size_t)r * ld + j] = h;
+  }
+  if (t) {
+    for (int e = threadIdx.x; e < GATHER_ROWS * nt; e += blockDim.x) {
+      const int rr = e / nt, k = e % nt, r = r0 + rr;
+      if (r >= rows) continue;
+      const size_t src = idx ? (size_t)idx[r] : (size_t)r;
+      t[(size_t)r * nt + k] = (traw[src * nt + k] - tmean[k]) * tistd[k];
+    }
+  }
+  if (!xt) return;
+  __syncthreads();
+  for (int e = threadIdx.x; e < GATHER_ROWS * ld; e += blockDim.x) {
+    const int j = e / GATHER_ROWS, rr = e % GATHER_ROWS, r = r0 + rr;
+    if (r < rows) xt[(size_t)j * ldt + r] = tile[rr * pitch + j];
+  }
+}
+
+// out[j] = sum_r g[j * ld + r] over r < n (one CTA per j).
+__global__ void __launch_bounds__(256) rowsum_kernel(const __nv_bfloat16* g, int ld, int n, float* out) {
+  const int j = blockIdx.x;
+  float s = 0.f;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) s += __bfloat162float(g[(size_t)j * ld + r]);
+  __shared__ float red[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    out[j] = t;
+  }
+}
+
+// Adam on n fp32 parameters; for a weight matrix [rows][cols] also writes the
+// bf16 copy w and its transpose wt (either may be null).
+__global__ void adam_kernel(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps, float bc1, float bc2,
+                            float wd, int rows, int cols, __nv_bfloat16* w, __nv_bfloat16* wt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  float pi = p[i] - lr * ((mi / bc1) / (sqrtf(vi / bc2) + eps) + wd * p[i]);
+  p[i] = pi;
+  if (w) w[i] = __float2bfloat16_rn(pi);
+  if (wt) {
+    const int r = i / cols, c = i % cols;
+    wt[(size_t)c * rows + r] = __float2bfloat16_rn(pi);
+  }
+  (void)rows;
+}
+
+// Column sums and sums of squares of x[n][c] (double accumulators).
+__global__ void __launch_bounds__(256) colstats_kernel(const float* x, int n, int c, int ld, double* sum, double* sq) {
+  for (int j = threadIdx.x; j < c; j += blockDim.x) {
+    double s = 0, q = 0;
+    for (int r = blockIdx.x; r < n; r += gridDim.x) {
+      const double v = x[(size_t)r * ld + j];
+      s += v;
+      q += v * v;
+    }
+    atomicAdd(sum + j, s);
+    atomicAdd(sq + j, q);
+  }
+}
+
+// w[i] = bf16(p[i]) and the transpose, for uploading initial weights.
+__global__ void cast_weights_kernel(int rows, int cols, const float* p, __nv_bfloat16* w, __nv_bfloat16* wt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  const __nv_bfloat16 h = __float2bfloat16_rn(p[i]);
+  w[i] = h;
+  if (wt) wt[(size_t)(i % cols) * rows + i / cols] = h;
+}
+
+}  // namespace
+
+cudaError_t gather_rows(int rows, const int* idx, const float* a, int lda, int na, const float* b, int ldb, int nb, const float* mean, const float* istd,
+                        __nv_bfloat16* x, int ld, __nv_bfloat16* xt, int ldt, const float* traw, int nt, const float* tmean, const float* tistd,
+                        float* t, cudaStream_t s) {
+  if (rows <= 0) return cudaSuccess;
+  const size_t smem = (size_t)GATHER_ROWS * (ld + 2) * sizeof(__nv_bfloat16);
+  static std::once_flag once;
+  std::call_once(once, [] { cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024); });
+  if (smem > 64 * 1024) return cudaErrorInvalidValue;
+  gather_kernel<<<(rows + GATHER_ROWS - 1) / GATHER_ROWS, 256, smem, s>>>(rows, idx, a, lda, na, b, ldb, nb, mean, istd, x, ld, xt, ldt, traw, nt,
+                                                                            tmean, tistd, t);
+  return cudaGetLastError();
+}
+
+cudaError_t rowsum_bf16(const __nv_bfloat16* g, int rows, int ld, int n, float* out, cudaStream_t s) {
+  rowsum_kernel<<<rows, 256, 0, s>>>(g, ld, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t adam_step(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps, int t, float wd, int rows, int cols,
+                      __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s) {
+  const float bc1 = 1.f - powf(b1, (float)t), bc2 = 1.f - powf(b2, (float)t);
+  adam_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, p, g, m, v, lr, b1, b2, eps, bc1, bc2, wd, rows, cols, w, wt);
+  return cudaGetLastError();
+}
+
+cudaError_t column_stats(const float* x, int n, int c, int ld, double* sum, double* sq, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(sum, 0, sizeof(double) * c, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sq, 0, sizeof(double) * c, s);
+  if (e != cudaSuccess) return e;
+  colstats_kernel<<<256, 256, 0, s>>>(x, n, c, ld, sum, sq);
+  return cudaGetLastError();
+}
+
+cudaError_t cast_weights(int rows, int cols, const float* p, __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s) {
+  cast_weights_kernel<<<(rows * cols + 255) / 256, 256, 0, s>>>(rows, cols, p, w, wt);
+  return cudaGetLastError();
+}
+
+}  // namespace mjb

@@ -1,0 +1,71 @@
+// Shared declarations of the learned warm-start kernels (BF16 tcgen05 GEMMs
+// with fused epilogues, feature gathers, reductions, Adam).
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mjb {
+
+// Epilogue of C[M x N] = A[M x K] * B[N x K]^T (both operands K-contiguous).
+enum GemmEpilogue : int {
+  EPI_F32 = 0,          // out_f32[row * ldo + col] = acc (+ bias when given)
+  EPI_HIDDEN = 1,       // z = acc + bias; pre = bf16(z) (optional); out = bf16(gelu(z)); out_t = transposed out (optional)
+  EPI_OUT_LOSS = 2,     // y = acc + bias; d = y - target (cols < nvalid); loss += sum d^2; out / out_t = bf16(scale * d)
+  EPI_OUT_PRED = 3,     // y = acc + bias; pred[row * nvalid + col] = prev[...] + omean[col] + ostd[col] * y   (cols < nvalid)
+  EPI_BWD_GELU = 4,     // dz = acc * gelu'(pre_in); out = bf16(dz); out_t = transposed (optional)
+};
+
+struct GemmArgs {
+  int M, N, K;          // N: columns computed (multiple of 16, <= 256 per CTA tile); K multiple of 64
+  int mode;
+  int ldo;              // leading dimension of out / out_f32 / pre / pre_in (elements)
+  int ldt;              // leading dimension of out_t (>= M)
+  int nvalid;           // EPI_OUT_*: number of real output columns
+  const float* bias;    // [N] or null
+  float* out_f32;
+  __nv_bfloat16* out;
+  __nv_bfloat16* out_t;
+  __nv_bfloat16* pre;
+  const __nv_bfloat16* pre_in;
+  const float* target;  // EPI_OUT_LOSS: [M][nvalid]
+  float* loss;          // EPI_OUT_LOSS: accumulated sum of squares
+  float scale;          // EPI_OUT_LOSS: gradient scale
+  const float* prev;    // EPI_OUT_PRED: [M][nvalid]
+  const float* omean;
+  const float* ostd;
+  float* pred;
+  int* err;             // set to a nonzero code when a bounded wait gives up
+};
+
+// Encodes a 2-D bf16 row-major [rows][cols] tensor map with a box of
+// {64, box_rows} and 128-byte swizzle (zero fill outside the tensor).
+bool make_tmap_bf16(CUtensorMap* map, const void* base, int rows, int cols, int box_rows);
+
+// Launches the tcgen05 GEMM for C[M x N] = A * B^T.  tmA: A [M][K] with box
+// rows 128; tmB: B [N][K] with box rows = the CTA's N tile (N <= 256 in one
+// tile, else 256-column tiles).
+cudaError_t gemm_tn(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmArgs& a, cudaStream_t s);
+
+}  // namespace mjb
+
+namespace mjb {
+
+// Normalising gather into bf16 rows (and optionally their transpose) plus
+// normalised targets; see gather_kernel.
+cudaError_t gather_rows(int rows, const int* idx, const float* a, int lda, int na, const float* b, int ldb, int nb, const float* mean, const float* istd,
+                        __nv_bfloat16* x, int ld, __nv_bfloat16* xt, int ldt, const float* traw, int nt, const float* tmean, const float* tistd,
+                        float* t, cudaStream_t s);
+// out[j] = sum over r < n of g[j * ld + r], j < rows.
+cudaError_t rowsum_bf16(const __nv_bfloat16* g, int rows, int ld, int n, float* out, cudaStream_t s);
+// One Adam step (bias-corrected, decoupled weight decay wd) on n parameters;
+// writes bf16 copies w ([rows][cols]) and wt (transpose) when given.
+cudaError_t adam_step(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps, int t, float wd, int rows, int cols,
+                      __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s);
+// Column sums / sums of squares of x[n][c] with row stride ld.
+cudaError_t column_stats(const float* x, int n, int c, int ld, double* sum, double* sq, cudaStream_t s);
+// bf16 copy of a fp32 weight matrix and its transpose.
+cudaError_t cast_weights(int rows, int cols, const float* p, __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s);
+
+}  // namespace mjb

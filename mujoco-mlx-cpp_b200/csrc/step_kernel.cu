@@ -190,6 +190,37 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
   return true;
 }
 
+// Feature row of the learned warm start, written after a substep: the state
+// the next substep starts from (qpos without the skipped leading
+// coordinates, qvel), the converged acceleration of this substep, and the
+// normal and distance of the first MJB_FEAT_CONTACTS contacts.
+__device__ __noinline__ void write_features(Env& E, const StepParams& P, int ncon) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  const int nv = m.nv, lane = E.lane;
+  float* f = P.features + (size_t)E.env * P.feat_stride;
+  const int nqf = m.nq - P.feat_qskip;
+#pragma unroll 1
+  for (int i = lane; i < nqf; i += 32) f[i] = ws[m.w_qpos + P.feat_qskip + i];
+  f += nqf;
+#pragma unroll 1
+  for (int i = lane; i < nv; i += 32) {
+    f[i] = ws[m.w_qvel + i];
+    f[nv + i] = ws[m.w_x + i];
+  }
+  f += 2 * nv;
+#pragma unroll 1
+  for (int k = lane; k < 4 * MJB_FEAT_CONTACTS; k += 32) {
+    const int c = k >> 2, q = k & 3;
+    float v = 0.f;
+    if (c < ncon) {
+      const float* con = ws + m.w_con + c * MJB_CONTACT_FLOATS;
+      v = q < 3 ? con[3 + q] : con[12];
+    }
+    f[k] = v;
+  }
+}
+
 __device__ __noinline__ void check_state(Env& E) {
   const DevModelDesc& m = *E.md;
   const float* ws = E.ws;
@@ -263,6 +294,13 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
     E.status = 0;
     E.md = reinterpret_cast<const DevModelDesc*>(dsm);
     int qadr = 0, vadr = 0, badr = 0, nv = 0;
+    if (P.poison_workspace) {
+      // test aid: any read of the workspace before it is written in this
+      // launch shows up as NaN (the state check then resets the env)
+#pragma unroll 1
+      for (int k = lane; k < P.ws_stride; k += 32) ws[k] = __int_as_float(0x7fc00000);
+      __syncwarp();
+    }
     if (valid) {
       const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
 #pragma unroll 1
@@ -336,6 +374,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
           for (int k = lane; k < nv; k += 32) P.rec_qacc[vadr + k] = ws[E.md->w_x + k];
         }
         d_finish(E, qfc, acc);
+        if (P.features) write_features(E, P, ncon);
       }
     }
     if (valid) {
@@ -349,8 +388,8 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       }
       if (lane == 0) {
         if (P.status) P.status[env] = E.status;
-        if (P.niter_sum) P.niter_sum[env] = nsum;
-        if (P.niter_max) P.niter_max[env] = nmax;
+        if (P.niter_sum) P.niter_sum[env] = P.stats_accumulate ? P.niter_sum[env] + nsum : nsum;
+        if (P.niter_max) P.niter_max[env] = P.stats_accumulate ? max(P.niter_max[env], nmax) : nmax;
         if (P.ncon_out) P.ncon_out[env] = ncon;
         if (P.nefc_out) P.nefc_out[env] = nefc;
         if (P.warm_choice) P.warm_choice[env] = choice;

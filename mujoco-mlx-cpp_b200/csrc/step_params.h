@@ -64,7 +64,14 @@ struct StepParams {
   const float* rand_friction;  // [env]
   const float* rand_gain;      // [uadr + actuator]
 
-  // learned warm start: feature rows written after each substep (nullable)
-  uint16_t* features;          // bf16 [B][feat_stride]
+  // learned warm start: feature rows written after each substep (nullable):
+  // qpos[feat_qskip:nq], qvel, converged qacc, then MJB_FEAT_CONTACTS x
+  // (contact normal, distance) in contact order, zero padded
+  float* features;             // [B][feat_stride]
   int feat_stride;
+  int feat_qskip;
+  int stats_accumulate;        // 1: add this launch's Newton iterations to niter_sum / max into niter_max
+  int poison_workspace;        // 1: fill each env's shared workspace with NaN before its first stage (test aid)
 };
+
+#define MJB_FEAT_CONTACTS 16

@@ -68,6 +68,21 @@ def _load():
         "mjb200_batched_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "mjb200_batched_step_device": (C.c_int, [C.c_void_p, C.c_int]),
         "mjb200_batched_step_device_ctrl": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+        "mjb200_warmstart_create": (C.c_void_p, [C.c_int, C.c_int, C.c_ulonglong]),
+        "mjb200_warmstart_free": (None, [C.c_void_p]),
+        "mjb200_warmstart_input_width": (C.c_int, [C.c_void_p]),
+        "mjb200_warmstart_dims": (C.c_int, [C.c_void_p] + [_i32p] * 6),
+        "mjb200_warmstart_get_params": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_warmstart_set_params": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_warmstart_set_normalization": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p, _f32p]),
+        "mjb200_warmstart_get_normalization": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p, _f32p]),
+        "mjb200_warmstart_fit_normalization": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+        "mjb200_warmstart_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+        "mjb200_warmstart_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, _f32p, _f32p]),
+        "mjb200_warmstart_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _f32p]),
+        "mjb200_batched_warmstart_collect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
+        "mjb200_batched_set_warmstart": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         "mjb200_batched_stream": (C.c_void_p, [C.c_void_p]),
@@ -165,6 +180,74 @@ def engine_config(**kw) -> MjbEngineConfig:
     return c
 
 
+class WarmStart:
+    """Learned Newton warm-start network (mjb200_warmstart.h).  Device arrays
+    are passed as integer device pointers (e.g. torch tensor data_ptr())."""
+
+    def __init__(self, in_raw: int, nout: int, seed: int = 0):
+        h = lib.mjb200_warmstart_create(in_raw, nout, seed)
+        if not h:
+            raise RuntimeError(last_error())
+        self.handle = C.c_void_p(h)
+        d = [C.c_int() for _ in range(6)]
+        lib.mjb200_warmstart_dims(self.handle, *[C.byref(x) for x in d])
+        self.in_raw, self.in_pad, self.hidden, self.nout, self.out_pad, self.nparams = [x.value for x in d]
+
+    def close(self):
+        h = getattr(self, "handle", None)
+        if h:
+            lib.mjb200_warmstart_free(h)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def _ok(self, rc):
+        if rc < 0:
+            raise RuntimeError(last_error())
+        return rc
+
+    def get_params(self):
+        p = np.zeros(self.nparams, np.float32)
+        self._ok(lib.mjb200_warmstart_get_params(self.handle, _fp(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        self._ok(lib.mjb200_warmstart_set_params(self.handle, _fp(p)))
+
+    def set_normalization(self, in_mean, in_std, out_mean, out_std):
+        a = [np.ascontiguousarray(x, np.float32) for x in (in_mean, in_std, out_mean, out_std)]
+        self._ok(lib.mjb200_warmstart_set_normalization(self.handle, *[_fp(x) for x in a]))
+
+    def get_normalization(self):
+        a = [np.zeros(self.in_raw, np.float32), np.zeros(self.in_raw, np.float32), np.zeros(self.nout, np.float32), np.zeros(self.nout, np.float32)]
+        self._ok(lib.mjb200_warmstart_get_normalization(self.handle, *[_fp(x) for x in a]))
+        return a
+
+    def fit_normalization(self, xraw_ptr: int, traw_ptr: int, n: int):
+        self._ok(lib.mjb200_warmstart_fit_normalization(self.handle, C.c_void_p(xraw_ptr), C.c_void_p(traw_ptr), n))
+
+    def forward(self, xraw_ptr: int, n: int, y_ptr: int):
+        self._ok(lib.mjb200_warmstart_forward(self.handle, C.c_void_p(xraw_ptr), n, C.c_void_p(y_ptr)))
+
+    def gradients(self, xraw_ptr: int, traw_ptr: int, n: int):
+        g = np.zeros(self.nparams, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._ok(lib.mjb200_warmstart_gradients(self.handle, C.c_void_p(xraw_ptr), C.c_void_p(traw_ptr), n, _fp(g), _fp(loss)))
+        return float(loss[0]), g
+
+    def train(self, xraw_ptr: int, traw_ptr: int, n: int, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0):
+        hist = np.zeros(max(epochs, 1), np.float32)
+        steps = self._ok(lib.mjb200_warmstart_train(self.handle, C.c_void_p(xraw_ptr), C.c_void_p(traw_ptr), n, epochs, batch, lr, seed, _fp(hist)))
+        return steps, hist
+
+
+def gemm_bf16(a_ptr: int, b_ptr: int, c_ptr: int, M: int, N: int, K: int, stream: int | None = None) -> int:
+    return lib.mjb200_gemm_bf16(C.c_void_p(a_ptr), C.c_void_p(b_ptr), C.c_void_p(c_ptr), M, N, K, C.c_void_p(stream))
+
+
 class BatchedSim:
     """Batched simulation on the CUDA engine (mirrors the reference's Python
     BatchedSim: step(ctrl, n), state(), set_state())."""
@@ -221,6 +304,22 @@ class BatchedSim:
         status (0 ok, -1 bad arguments, -2 too many envs, -3 CUDA error)."""
         return lib.mjb200_batched_step_noalloc(self.handle, C.c_void_p(qpos_ptr), C.c_void_p(qvel_ptr), C.c_void_p(ctrl_ptr),
                                                C.c_void_p(warm_ptr), n, C.c_void_p(stream))
+
+    # ---- learned warm start
+    def warmstart_input_width(self) -> int:
+        return lib.mjb200_warmstart_input_width(self.handle)
+
+    def warmstart_collect(self, ctrl_ptr: int, nctrl: int, substeps_per_ctrl: int, xraw_ptr: int, traw_ptr: int, max_rows: int) -> int:
+        rc = lib.mjb200_batched_warmstart_collect(self.handle, C.c_void_p(ctrl_ptr), nctrl, substeps_per_ctrl, C.c_void_p(xraw_ptr),
+                                                  C.c_void_p(traw_ptr), max_rows)
+        if rc < 0:
+            raise RuntimeError(last_error())
+        return rc
+
+    def set_warmstart(self, net):
+        self._warmstart = net
+        if lib.mjb200_batched_set_warmstart(self.handle, net.handle if net is not None else None) != 0:
+            raise RuntimeError(last_error())
 
     def sync(self):
         lib.mjmlx_batched_eval_state(self.handle)
