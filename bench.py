@@ -8,15 +8,22 @@ FP32, condim 3 pyramidal, self-collision on, Newton 16 iterations at
 tolerance 1e-8, seeded uniform random position targets resampled every control
 step.  Data are synthetic (seeded Philox), there is no dataset.
 
-  value   whole-job env-steps/s with the per-step controls already resident in
-          HBM (device-to-device copy into the sim, then the step kernel),
-          CUDA events on the sim's stream, L2 flushed (256 MB write) before
-          every timed step.
+  value   whole-job env-steps/s of the learned-warm-start engine with the
+          per-step controls already resident in HBM (device-to-device copy
+          into the sim, then per substep: feature gather + 4 tcgen05 GEMMs of
+          the MLP + the step kernel), CUDA events on the sim's stream, L2
+          flushed (256 MB write) before every timed step.  The net is trained
+          first, on the GPU, from plain rollouts with disjoint seeds
+          (--train-ctrl-steps x 4 substeps x envs pairs, --train-epochs).
+          solver.plain holds the same numbers for the plain solver
+          (previous-step warm start, one fused launch of 4 substeps), and
+          solver.learned / iteration_reduction the comparison at the same
+          tolerance.
   e2e     the same metric through the public C ABI with host buffers:
           mjmlx_batched_step_n(ctrl host array, 4) + mjmlx_batched_get_state
           (qpos, qvel to host) every step, wall clock.
-  roofline  the step kernel: algorithmic 488 B per env-substep (qpos, qvel,
-          ctrl, warm-start qacc read; qpos, qvel, qacc written) over the
+  roofline  the plain step kernel: algorithmic 488 B per env-substep (qpos,
+          qvel, ctrl, warm-start qacc read; qpos, qvel, qacc written) over the
           kernel's CUDA-event time, against the measured HBM copy peak.
   cpu_baseline  the FP64 CPU oracle (a port of the step; MuJoCo C is not on
           the machine) on all host threads, bounded sample, rank 0 at N = 1.
@@ -67,6 +74,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--envs", type=int, default=16384)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--train-ctrl-steps", type=int, default=32, help="control steps of the warm-start training rollouts")
+    ap.add_argument("--train-epochs", type=int, default=8)
     return ap.parse_args()
 
 
@@ -195,43 +204,53 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, world, rank, local):
+def train_warmstart(m, B, nctrl, epochs, seed=50000):
+    """Learned warm start for the bench: plain rollouts of B envs for nctrl
+    control steps (seeds disjoint from the timed workload) give
+    B * (4 * nctrl - 1) training pairs; the net trains on the GPU."""
     import numpy as np
     import torch
 
     import mjb200
-    from mjb200 import replicas
 
-    torch.cuda.set_device(local)
-    B = args.envs
-    K, W = args.steps, args.warmup
-    m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
+    t0 = time.perf_counter()
     sim = mjb200.BatchedSim(m, B, record=0)
-    seed_state, seed_ctrl = replicas.rank_seeds(rank)
-    q0, v0 = mjb200.models.quadruped_initial_state_fast(B, seed=seed_state)
-    nu = m.nu
-    ctrl_all = np.stack([mjb200.models.quadruped_controls_fast(B, s, seed=seed_ctrl) for s in range(K + W)]).astype(np.float32)
-    ctrl_dev = torch.from_numpy(ctrl_all).cuda()
-    stride = B * nu
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.ExternalStream(sim.stream())
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=seed)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    ctrl = torch.from_numpy(np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed + 1) for c in range(nctrl)]).astype(np.float32)).cuda()
+    width = sim.warmstart_input_width()
+    rows = B * (SUBSTEPS * nctrl - 1)
+    xraw = torch.empty(rows, width, device="cuda")
+    traw = torch.empty(rows, m.nv, device="cuda")
+    torch.cuda.synchronize()
+    got = sim.warmstart_collect(ctrl.data_ptr(), nctrl, SUBSTEPS, xraw.data_ptr(), traw.data_ptr(), rows)
+    t1 = time.perf_counter()
+    net = mjb200.WarmStart(width, m.nv, seed=seed + 2)
+    net.fit_normalization(xraw.data_ptr(), traw.data_ptr(), got)
+    steps, hist = net.train(xraw.data_ptr(), traw.data_ptr(), got, epochs=epochs, batch=4096, lr=1e-3, seed=seed + 3)
+    t2 = time.perf_counter()
+    sim.close()
+    del xraw, traw, ctrl
+    torch.cuda.empty_cache()
+    return net, {"pairs": got, "epochs": epochs, "batch": 4096, "optimizer_steps": steps, "loss_first_epoch": float(hist[0]),
+                 "loss_last_epoch": float(hist[-1]), "collect_s": round(t1 - t0, 3), "train_s": round(t2 - t1, 3),
+                 "network": "MLP %d -> 256 -> 256 -> 256 -> %d, GELU, bf16 tcgen05 GEMMs, fp32 accumulate / Adam" % (width, m.nv)}
 
-    def reset_state():
-        sim.set_state(q0.astype(np.float32), v0.astype(np.float32))
 
-    # ---- value: inputs resident in HBM
-    reset_state()
+def time_device(sim, ctrl_dev, stride, K, W, flush, stream, world):
+    """K timed env-steps with controls resident in HBM; returns per-step
+    times (ms, control copy + physics) and the physics-only times."""
+    import torch
+
     base = ctrl_dev.data_ptr()
     for w in range(W):
         sim.step_device_ctrl(base + 4 * w * stride, SUBSTEPS)
     sim.sync()
-    sampler = ClockSampler(torch.cuda.current_device())
-    sampler.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    niter_mean, niter_p99, ncon_mean = [], [], []
+    iters, imax = [], []
     with torch.cuda.stream(stream):
         for k in range(K):
             flush.zero_()
@@ -242,19 +261,13 @@ def run_ours(args, world, rank, local):
             sim.step_device(SUBSTEPS)
             c.record(stream)
     torch.cuda.synchronize()
-    clocks = sampler.stop()
-    step_ms = [a.elapsed_time(c) for a, b, c in ev]
-    kern_ms = [b.elapsed_time(c) for a, b, c in ev]
     st = sim.stats()
-    niter_mean = float(st["niter_sum"].mean() / SUBSTEPS)
-    niter_p99 = float(np.percentile(st["niter_max"], 99))
-    total_s = sum(step_ms) / 1e3
-    total_s = replicas.reduce_over_ranks(total_s, "max", device="cuda")
-    value = world * B * K / total_s
+    return [a.elapsed_time(c) for a, b, c in ev], [b.elapsed_time(c) for a, b, c in ev], st
 
-    # ---- e2e: public C ABI with host buffers
-    reset_state()
-    host_ctrl = [np.ascontiguousarray(ctrl_all[s]) for s in range(K + W)]
+
+def time_e2e(sim, host_ctrl, K, W, flush, world):
+    import torch
+
     for w in range(W):
         sim.step(host_ctrl[w], SUBSTEPS)
         sim.state()
@@ -266,32 +279,78 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sim.step(host_ctrl[W + k], SUBSTEPS)
-        qp, qv = sim.state()
+        sim.state()
         e2e_s += time.perf_counter() - t0
-    e2e_s = replicas.reduce_over_ranks(e2e_s, "max", device="cuda")
-    e2e_value = world * B * K / e2e_s
+    return e2e_s
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import mjb200
+    from mjb200 import replicas
+
+    torch.cuda.set_device(local)
+    B = args.envs
+    K, W = args.steps, args.warmup
+    m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    net, train_info = train_warmstart(m, B, args.train_ctrl_steps, args.train_epochs)
+    seed_state, seed_ctrl = replicas.rank_seeds(rank)
+    q0, v0 = mjb200.models.quadruped_initial_state_fast(B, seed=seed_state)
+    nu = m.nu
+    ctrl_all = np.stack([mjb200.models.quadruped_controls_fast(B, s, seed=seed_ctrl) for s in range(K + W)]).astype(np.float32)
+    ctrl_dev = torch.from_numpy(ctrl_all).cuda()
+    host_ctrl = [np.ascontiguousarray(ctrl_all[s]) for s in range(K + W)]
+    stride = B * nu
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    res = {}
+    for mode in ("plain", "learned"):
+        sim = mjb200.BatchedSim(m, B, record=0)
+        if mode == "learned":
+            sim.set_warmstart(net)
+        stream = torch.cuda.ExternalStream(sim.stream())
+        sim.set_state(q0.astype(np.float32), v0.astype(np.float32))
+        step_ms, kern_ms, st = time_device(sim, ctrl_dev, stride, K, W, flush, stream, world)
+        total_s = replicas.reduce_over_ranks(sum(step_ms) / 1e3, "max", device="cuda")
+        sim.set_state(q0.astype(np.float32), v0.astype(np.float32))
+        e2e_s = replicas.reduce_over_ranks(time_e2e(sim, host_ctrl, K, W, flush, world), "max", device="cuda")
+        # iteration statistics of the last timed env-step (per env: mean over
+        # its 4 substeps; p99 over envs of the per-substep maximum)
+        res[mode] = {"value": world * B * K / total_s, "ms_per_step": 1e3 * total_s / K, "kernel_ms": statistics.mean(kern_ms),
+                     "e2e": world * B * K / e2e_s, "newton_iter_mean": float(st["niter_sum"].mean() / SUBSTEPS),
+                     "newton_iter_p99": float(np.percentile(st["niter_max"], 99)),
+                     "predicted_warmstart_share": float(np.mean(st["warm_choice"] == 2)), "launch": sim.launch_shape()}
+        sim.close()
+    clocks = sampler.stop()
     h2d = B * nu * 4
     d2h = B * (m.nq + m.nv) * 4
 
-    # ---- roofline of the step kernel
-    kern_s = statistics.mean(kern_ms) / 1e3
+    # roofline of the step kernel (plain path: one fused launch of 4 substeps per env-step)
+    kern_s = res["plain"]["kernel_ms"] / 1e3
     alg_bytes = BYTES_PER_ENV_SUBSTEP * SUBSTEPS * B
     achieved = alg_bytes / kern_s / 1e9
     peak, peak_kind = peaks()
     tr = profile_traffic_per_env_launch()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tr * B) if tr is not None else None, "kernel": "mjb_step_kernel", "kernel_ms": statistics.mean(kern_ms),
+                "traffic": (tr * B) if tr is not None else None, "kernel": "mjb_step_kernel", "kernel_ms": res["plain"]["kernel_ms"],
                 "algorithmic_bytes_per_launch": alg_bytes}
 
     if rank != 0:
         return
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": 1e3 * total_s / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+    L, P = res["learned"], res["plain"]
+    line = {"metric": METRIC, "value": L["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": L["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(B),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": roofline, "gpu_launches": K,
-            "solver": {"warmstart": "previous-step (plain)", "newton_iter_mean": niter_mean, "newton_iter_p99": niter_p99,
-                       "launch": sim.launch_shape()},
+            "e2e": {"value": L["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roofline,
+            "gpu_launches": K * SUBSTEPS * 6,
+            "solver": {"value_is": "learned warm start (previous-step and qacc_smooth candidates kept as fallback), same tolerance 1e-8",
+                       "learned": L, "plain": P, "learned_over_plain": L["value"] / P["value"],
+                       "iteration_reduction": 1.0 - L["newton_iter_mean"] / max(P["newton_iter_mean"], 1e-9), "training": train_info},
             "clocks": clocks}
     if world == 1:
         line["cpu_baseline"] = cpu_reference(B, args.cpu_seconds)

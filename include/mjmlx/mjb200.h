@@ -66,6 +66,18 @@ MJMLX_API int mjb200_batched_step_device(MjmlxBatchedSim* sim, int n);
 /* n physics steps with controls read from device memory ctrl_dev[total_u]
  * (copied on the sim's stream, device to device); n = 0 only copies. */
 MJMLX_API int mjb200_batched_step_device_ctrl(MjmlxBatchedSim* sim, const float* ctrl_dev, int n);
+/* n physics steps with controls already in device memory, where the first
+ * step offers qacc_dev[total_v] (device, the sim's layout) to the Newton
+ * solver as an extra warm-start candidate, kept when its Gauss cost is lowest
+ * (e.g. a model-predictive controller's guess).  The solver still iterates to
+ * its tolerance.  No counterpart in the reference. */
+MJMLX_API int mjb200_batched_step_warmstart(MjmlxBatchedSim* sim, const float* qacc_dev, int n);
+/* The previous-step acceleration qacc[total_v] the solver warm-starts from
+ * (host arrays); with get/set_state it checkpoints the whole solver state so
+ * a resumed run repeats the original bit for bit.  No counterpart in the
+ * reference (its solver starts from zero). */
+MJMLX_API int mjb200_batched_get_qacc_warmstart(MjmlxBatchedSim* sim, float* qacc);
+MJMLX_API int mjb200_batched_set_qacc_warmstart(MjmlxBatchedSim* sim, const float* qacc);
 /* Allocation-free step.  No counterpart in the reference.
  *
  * For callers that must not have the library allocate device memory while

@@ -249,6 +249,30 @@ MJMLX_API int mjb200_batched_step_device_ctrl(MjmlxBatchedSim* sim, const float*
   return guard("mjb200_batched_step_device_ctrl", [&]() { sim->engine->step_device_ctrl(ctrl_dev, n); return 0; }, -1);
 }
 
+MJMLX_API int mjb200_batched_step_warmstart(MjmlxBatchedSim* sim, const float* qacc_dev, int n) {
+  if (!sim || !sim->engine || !qacc_dev || n < 0) {
+    set_error("mjb200_batched_step_warmstart: bad arguments");
+    return -1;
+  }
+  try {
+    sim->engine->step_with_warmstart(qacc_dev, n);
+    return 0;
+  } catch (const std::exception& e) {
+    set_error(std::string("mjb200_batched_step_warmstart: ") + e.what());
+    return -3;
+  }
+}
+
+MJMLX_API int mjb200_batched_get_qacc_warmstart(MjmlxBatchedSim* sim, float* qacc) {
+  if (!sim || !sim->engine || !qacc) return -1;
+  return guard("mjb200_batched_get_qacc_warmstart", [&]() { sim->engine->get_qacc_warmstart(qacc); return 0; }, -1);
+}
+
+MJMLX_API int mjb200_batched_set_qacc_warmstart(MjmlxBatchedSim* sim, const float* qacc) {
+  if (!sim || !sim->engine || !qacc) return -1;
+  return guard("mjb200_batched_set_qacc_warmstart", [&]() { sim->engine->set_qacc_warmstart(qacc); return 0; }, -1);
+}
+
 MJMLX_API int mjb200_batched_device_state(MjmlxBatchedSim* sim, float** qpos, float** qvel, float** ctrl, float** qacc) {
   if (!sim) return -1;
   Engine& e = *sim->engine;

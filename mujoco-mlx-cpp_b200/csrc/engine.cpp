@@ -569,6 +569,27 @@ void Engine::step(const float* ctrl_host, int n) {
 
 void Engine::step_device(int n) { launch(n, cfg_.record != 0); }
 
+void Engine::get_qacc_warmstart(float* out) {
+  check(cudaMemcpyAsync(out, warm_.p, sizeof(float) * tot_v_, cudaMemcpyDeviceToHost, stream_), "get warm start");
+  sync();
+}
+
+void Engine::set_qacc_warmstart(const float* in) {
+  sync();
+  check(cudaMemcpy(warm_.p, in, sizeof(float) * tot_v_, cudaMemcpyHostToDevice), "set warm start");
+}
+
+void Engine::step_with_warmstart(const float* qacc, int n) {
+  if (n <= 0) return;
+  check(cudaMemcpyAsync(pred_.p, qacc, sizeof(float) * tot_v_, cudaMemcpyDeviceToDevice, stream_), "warm start copy");
+  StepParams P = params(1, cfg_.record != 0 && n == 1);
+  P.qacc_pred = pred_.p;
+  if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
+  check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+  feat_valid_ = false;
+  if (n > 1) launch(n - 1, cfg_.record != 0);
+}
+
 void Engine::step_device_ctrl(const float* dctrl, int n) {
   if (tot_u_ > 0 && dctrl) check(cudaMemcpyAsync(ctrl_.p, dctrl, sizeof(float) * tot_u_, cudaMemcpyDeviceToDevice, stream_), "ctrl device copy");
   launch(n, cfg_.record != 0);

@@ -109,6 +109,13 @@ class Engine {
   // ctrl_seq: nctrl device control sets of total_u floats, each held for
   // sub_per_ctrl substeps.  Returns the number of rows written (<= max_rows).
   int collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows);
+  // n substeps; the first offers qacc[total_v] (device) to the Newton
+  // solver as an extra warm-start candidate (kept when its cost is lowest).
+  void step_with_warmstart(const float* qacc, int n);
+  // Host copies of the previous-step acceleration the solver warm-starts
+  // from (checkpoint / resume of the full solver state).
+  void get_qacc_warmstart(float* out);
+  void set_qacc_warmstart(const float* in);
   const float* features_device() const { return feat_.p; }
   float* qacc_pred_device() { return pred_.p; }
 

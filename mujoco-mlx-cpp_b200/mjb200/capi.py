@@ -83,6 +83,9 @@ def _load():
         "mjb200_batched_warmstart_collect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_set_warmstart": (C.c_int, [C.c_void_p, C.c_void_p]),
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+        "mjb200_batched_get_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_batched_step_warmstart": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
         "mjb200_batched_stream": (C.c_void_p, [C.c_void_p]),
@@ -304,6 +307,21 @@ class BatchedSim:
         status (0 ok, -1 bad arguments, -2 too many envs, -3 CUDA error)."""
         return lib.mjb200_batched_step_noalloc(self.handle, C.c_void_p(qpos_ptr), C.c_void_p(qvel_ptr), C.c_void_p(ctrl_ptr),
                                                C.c_void_p(warm_ptr), n, C.c_void_p(stream))
+
+    def qacc_warmstart(self):
+        out = np.zeros(self.total_v, np.float32)
+        if lib.mjb200_batched_get_qacc_warmstart(self.handle, _fp(out)) != 0:
+            raise RuntimeError(last_error())
+        return out
+
+    def set_qacc_warmstart(self, qacc):
+        a = np.ascontiguousarray(qacc, np.float32).reshape(-1)
+        if a.size != self.total_v or lib.mjb200_batched_set_qacc_warmstart(self.handle, _fp(a)) != 0:
+            raise RuntimeError("set_qacc_warmstart: " + last_error())
+
+    def step_warmstart(self, qacc_ptr: int, n: int = 1):
+        if lib.mjb200_batched_step_warmstart(self.handle, C.c_void_p(qacc_ptr), n) != 0:
+            raise RuntimeError(last_error())
 
     # ---- learned warm start
     def warmstart_input_width(self) -> int:

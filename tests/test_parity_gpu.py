@@ -206,3 +206,40 @@ def test_poisoned_workspace_changes_nothing(quad_model):
         res.append(r.stdout.split())
     assert res[0][0] == "0" and res[1][0] == "0"
     assert res[0][1] == res[1][1]
+
+
+def test_checkpoint_resume_bitwise(quad_model):
+    """qpos, qvel and the solver's warm-start qacc checkpoint the whole step
+    state: a resumed sim repeats the original run bit for bit; a caller
+    warm-start equal to the converged solution needs (almost) no iterations."""
+    B = 512
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=61)
+    ctrls = [mjb200.models.quadruped_controls_fast(B, c, seed=62).astype(np.float32) for c in range(16)]
+    a = mjb200.BatchedSim(quad_model, B)
+    a.set_state(q.astype(np.float32), v.astype(np.float32))
+    for c in ctrls[:8]:
+        a.step(c, 4)
+    qp, qv = a.state()
+    warm = a.qacc_warmstart()
+    b = mjb200.BatchedSim(quad_model, B)
+    b.set_state(qp, qv)
+    b.set_qacc_warmstart(warm)
+    for c in ctrls[8:]:
+        a.step(c, 4)
+        b.step(c, 4)
+    assert all(np.array_equal(x, y) for x, y in zip(a.state(), b.state()))
+    # perfect caller warm start: the converged solution of the same step
+    import torch
+
+    b.set_state(qp, qv)
+    b.set_qacc_warmstart(warm)
+    b.step(ctrls[8], 1)
+    it_plain = b.stats()["niter_sum"].mean()
+    sol = torch.from_numpy(b.qacc_warmstart()).cuda()
+    b.set_state(qp, qv)
+    b.set_qacc_warmstart(warm)
+    torch.cuda.synchronize()
+    b.step_warmstart(sol.data_ptr(), 1)
+    st = b.stats()
+    assert st["niter_sum"].mean() < 0.5 * it_plain
+    assert np.mean(st["warm_choice"] == 2) > 0.5
