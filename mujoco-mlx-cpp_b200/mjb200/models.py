@@ -126,3 +126,182 @@ def quadruped_initial_state_fast(num_envs: int, seed: int = 1000):
             lo, hi = QUAD_RANGES[j]
             qpos[:, 7 + 3 * leg + j] = np.clip(QUAD_NOMINAL[j] + off[:, 3 * leg + j], lo, hi)
     return qpos, np.zeros((num_envs, 18))
+
+
+# ---------------------------------------------------------------- humanoid
+
+HUMANOID_JOINTS = (
+    # name, axis, range (rad)
+    ("abdomen_y", "0 1 0", (-1.0, 0.5)),
+    ("right_hip_x", "1 0 0", (-0.5, 0.1)), ("right_hip_z", "0 0 1", (-1.0, 0.6)), ("right_hip_y", "0 1 0", (-1.8, 0.35)),
+    ("right_knee", "0 -1 0", (-2.6, -0.03)), ("right_ankle_y", "0 1 0", (-0.8, 0.8)),
+    ("left_hip_x", "-1 0 0", (-0.5, 0.1)), ("left_hip_z", "0 0 -1", (-1.0, 0.6)), ("left_hip_y", "0 1 0", (-1.8, 0.35)),
+    ("left_knee", "0 -1 0", (-2.6, -0.03)), ("left_ankle_y", "0 1 0", (-0.8, 0.8)),
+    ("right_shoulder1", "2 1 1", (-1.5, 1.0)), ("right_shoulder2", "0 -1 1", (-1.5, 1.0)), ("right_elbow", "0 -1 1", (-1.5, 0.9)),
+    ("left_shoulder1", "2 -1 1", (-1.0, 1.5)), ("left_shoulder2", "0 1 1", (-1.0, 1.5)), ("left_elbow", "0 -1 -1", (-1.5, 0.9)),
+)
+
+
+def humanoid_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.005) -> str:
+    """21-DoF-class capsule humanoid: free-joint torso and 17 hinges (1 spine,
+    2 x 5 legs, 2 x 3 arms), capsule radii 0.04-0.06 m, sphere head,
+    position actuators on every hinge, self-collision on (parent/child pairs
+    filtered).  nq 24, nv 23, nu 17."""
+    J = {n: (a, r) for n, a, r in HUMANOID_JOINTS}
+
+    def joint(n, pos="0 0 0"):
+        a, (lo, hi) = J[n]
+        return f'<joint name="{n}" type="hinge" pos="{pos}" axis="{a}" range="{lo} {hi}" armature="0.02" damping="0.5"/>'
+
+    def leg(side, sy):
+        s = side
+        return f"""
+          <body name="{s}_thigh" pos="0 {0.1*sy:.3f} -0.04">
+            {joint(s+"_hip_x")}{joint(s+"_hip_z")}{joint(s+"_hip_y")}
+            <geom name="{s}_thigh_g" type="capsule" fromto="0 0 0 0 {0.01*sy:.3f} -0.34" size="0.06"/>
+            <body name="{s}_shin" pos="0 {0.01*sy:.3f} -0.403">
+              {joint(s+"_knee", "0 0 .02")}
+              <geom name="{s}_shin_g" type="capsule" fromto="0 0 0 0 0 -0.3" size="0.05"/>
+              <body name="{s}_foot" pos="0 0 -0.39">
+                {joint(s+"_ankle_y", "0 0 0.08")}
+                <geom name="{s}_foot_g" type="capsule" fromto="-0.07 0 0.04 0.14 0 0.04" size="0.04"/>
+              </body>
+            </body>
+          </body>"""
+
+    def arm(side, sy):
+        s = side
+        return f"""
+      <body name="{s}_upper_arm" pos="0 {0.17*sy:.3f} 0.06">
+        {joint(s+"_shoulder1")}{joint(s+"_shoulder2")}
+        <geom name="{s}_uarm_g" type="capsule" fromto="0 0 0 .16 {0.16*sy:.3f} -.16" size="0.04"/>
+        <body name="{s}_lower_arm" pos=".18 {0.18*sy:.3f} -.18">
+          {joint(s+"_elbow")}
+          <geom name="{s}_larm_g" type="capsule" fromto="0.01 {0.01*sy:.3f} 0.01 .17 {0.17*sy:.3f} .17" size="0.04"/>
+        </body>
+      </body>"""
+
+    acts = []
+    for n, _, (lo, hi) in HUMANOID_JOINTS:
+        kp = 40 if ("shoulder" in n or "elbow" in n) else 100
+        acts.append(f'    <position name="{n}_act" joint="{n}" kp="{kp}" kv="2" ctrlrange="{lo} {hi}"/>')
+    return f"""<mujoco model="humanoid21">
+  <compiler angle="radian"/>
+  <option timestep="{timestep}" iterations="{iterations}" tolerance="{tolerance}" cone="pyramidal" integrator="Euler"/>
+  <default><geom condim="3" density="1000" friction="0.9 0.005 0.0001"/></default>
+  <worldbody>
+    <geom name="floor" type="plane" size="0 0 1" friction="1 0.005 0.0001"/>
+    <body name="torso" pos="0 0 1.3">
+      <freejoint name="root"/>
+      <geom name="torso_g" type="capsule" fromto="0 -.07 0 0 .07 0" size="0.06"/>
+      <geom name="head" type="sphere" pos="0 0 .19" size=".09"/>
+      <geom name="uwaist" type="capsule" fromto="-.01 -.06 -.12 -.01 .06 -.12" size="0.05"/>
+      <body name="lower_waist" pos="-.01 0 -.26">
+        <geom name="lwaist" type="capsule" fromto="0 -.06 0 0 .06 0" size="0.05"/>
+        {joint("abdomen_y", "0 0 .065")}
+        <body name="pelvis" pos="0 0 -.165">
+          <geom name="butt" type="capsule" fromto="-.02 -.07 0 -.02 .07 0" size="0.06"/>{leg("right", -1)}{leg("left", 1)}
+        </body>
+      </body>{arm("right", -1)}{arm("left", 1)}
+    </body>
+  </worldbody>
+  <actuator>
+{chr(10).join(acts)}
+  </actuator>
+</mujoco>
+"""
+
+
+# ---------------------------------------------------------------- arm + box
+
+ARM_RANGES = ((-2.9, 2.9), (-1.7, 1.7), (-2.9, 2.9), (-3.0, -0.1), (-2.9, 2.9), (-0.1, 3.7), (-2.9, 2.9))
+ARM_FINGER_RANGE = (0.0, 0.04)
+
+
+def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.005) -> str:
+    """7-hinge arm on a table with a two-finger gripper (box palm, slide
+    fingers) and a free box on the table.  The table top is the plane z = 0;
+    the arm does not collide with itself; the fingers are capsules and the
+    palm box does not touch the object (box-box and cylinder-box contacts are
+    not in this build's narrowphase).  nq 7 + 2 + 7 = 16, nv 15, nu 9."""
+    axes = ("0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1")
+    links = []
+    depth = 0
+    for i, (ax, (lo, hi)) in enumerate(zip(axes, ARM_RANGES)):
+        length = 0.16 if i % 2 == 0 else 0.14
+        links.append(f"""
+{'  ' * (i + 3)}<body name="link{i+1}" pos="0 0 {0.1 if i == 0 else prev_len:.3f}">
+{'  ' * (i + 4)}<joint name="j{i+1}" type="hinge" axis="{ax}" range="{lo} {hi}" armature="0.05" damping="1"/>
+{'  ' * (i + 4)}<geom name="link{i+1}_g" type="capsule" fromto="0 0 0 0 0 {length}" size="0.045" mass="{1.5 - 0.15*i:.2f}" contype="2" conaffinity="1"/>""")
+        prev_len = length
+        depth += 1
+    hand = f"""
+{'  ' * 10}<body name="hand" pos="0 0 {prev_len:.3f}">
+{'  ' * 11}<geom name="palm" type="box" size="0.04 0.06 0.015" pos="0 0 0.015" mass="0.4" contype="4" conaffinity="0"/>
+{'  ' * 11}<body name="finger_l" pos="0 0.02 0.03">
+{'  ' * 12}<joint name="finger_l_j" type="slide" axis="0 1 0" range="{ARM_FINGER_RANGE[0]} {ARM_FINGER_RANGE[1]}" armature="0.01" damping="2"/>
+{'  ' * 12}<geom name="finger_l_g" type="capsule" fromto="0 0 0 0 0 0.07" size="0.012" mass="0.05" contype="2" conaffinity="1"/>
+{'  ' * 11}</body>
+{'  ' * 11}<body name="finger_r" pos="0 -0.02 0.03">
+{'  ' * 12}<joint name="finger_r_j" type="slide" axis="0 -1 0" range="{ARM_FINGER_RANGE[0]} {ARM_FINGER_RANGE[1]}" armature="0.01" damping="2"/>
+{'  ' * 12}<geom name="finger_r_g" type="capsule" fromto="0 0 0 0 0 0.07" size="0.012" mass="0.05" contype="2" conaffinity="1"/>
+{'  ' * 11}</body>
+{'  ' * 10}</body>"""
+    closes = "".join(f"\n{'  ' * (i + 3)}</body>" for i in reversed(range(7)))
+    acts = [f'    <position name="j{i+1}_act" joint="j{i+1}" kp="80" kv="4" ctrlrange="{lo} {hi}"/>' for i, (lo, hi) in enumerate(ARM_RANGES)]
+    acts += [f'    <position name="{f}_act" joint="{f}_j" kp="40" kv="1" ctrlrange="{ARM_FINGER_RANGE[0]} {ARM_FINGER_RANGE[1]}"/>'
+             for f in ("finger_l", "finger_r")]
+    return f"""<mujoco model="arm7_gripper_box">
+  <compiler angle="radian"/>
+  <option timestep="{timestep}" iterations="{iterations}" tolerance="{tolerance}" cone="pyramidal" integrator="Euler"/>
+  <default><geom condim="3" friction="1 0.005 0.0001"/></default>
+  <worldbody>
+    <geom name="table" type="plane" size="0 0 1"/>
+    <body name="base" pos="0 0 0">
+      <geom name="base_g" type="box" size="0.08 0.08 0.05" pos="0 0 0.05" mass="5" contype="2" conaffinity="0"/>{''.join(links)}{hand}{closes}
+    </body>
+    <body name="object" pos="0.45 0 0.03">
+      <freejoint name="object_root"/>
+      <geom name="object_g" type="box" size="0.03 0.03 0.03" mass="0.2"/>
+    </body>
+  </worldbody>
+  <actuator>
+{chr(10).join(acts)}
+  </actuator>
+</mujoco>
+"""
+
+
+def joint_ranges(model) -> np.ndarray:
+    """Ranges [nu, 2] of the joints the model's actuators drive (position targets)."""
+    d = model.dump()
+    trn = d["actuator_trnid"]
+    rng = d["jnt_range"].reshape(-1, 2)
+    return rng[trn]
+
+
+def random_state(model, num_envs: int, seed: int, height=None, noise: float = 0.1):
+    """qpos0 plus N(0, noise) on hinge/slide joints (clipped to their ranges),
+    an optional root height range for a free root, zero velocity."""
+    d = model.dump()
+    g = np.random.Generator(np.random.Philox(key=seed))
+    q0 = d["qpos0"].astype(np.float64)
+    qpos = np.tile(q0, (num_envs, 1))
+    jt, qa, lim = d["jnt_type"], d["jnt_qposadr"], d["jnt_limited"]
+    rng = d["jnt_range"].reshape(-1, 2)
+    for j in range(len(jt)):
+        if jt[j] in (2, 3):
+            a = qa[j]
+            lo, hi = rng[j] if lim[j] else (-np.inf, np.inf)
+            centre = 0.0 if lo <= 0.0 <= hi else 0.5 * (lo + hi)
+            qpos[:, a] = np.clip(centre + g.normal(0.0, noise, size=num_envs), lo, hi)
+    if height is not None and len(jt) and jt[0] == 0:
+        qpos[:, 2] = g.uniform(height[0], height[1], size=num_envs)
+    return qpos, np.zeros((num_envs, model.nv))
+
+
+def random_controls(model, num_envs: int, step: int, seed: int):
+    """Position targets U[joint range] for control step `step`."""
+    r = joint_ranges(model)
+    g = np.random.Generator(np.random.Philox(key=seed, counter=step))
+    return r[:, 0] + (r[:, 1] - r[:, 0]) * g.random((num_envs, len(r)))

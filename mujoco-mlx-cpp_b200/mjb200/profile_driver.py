@@ -1,0 +1,118 @@
+"""Small fixed workloads for profiling the engine's kernels under a profiler
+(e.g. ncu with -k / -c), one process, one GPU.
+
+    python -m mjb200.profile_driver step    --envs 4096 --ctrl 3
+    python -m mjb200.profile_driver learned --envs 4096 --ctrl 3
+    python -m mjb200.profile_driver gemm    --rows 16384
+    python -m mjb200.profile_driver sensitivity --envs 4096
+
+`step`: the quadruped workload (4 substeps per control step, seeded random
+position targets) on the plain solver; `learned`: the same after a short
+warm-start training (collect + 2 epochs) with the net attached; `gemm`: the
+MLP's forward GEMM shapes (rows x 192 -> 256 -> 256 -> 256 -> 64) and one
+weight-gradient shape (256 x 256, K = 4096), each launched `--repeat` times;
+`sensitivity`: Newton iterations of one substep from warm starts at known
+distances from the converged solution x* (x* + eps (previous - x*)), which
+bounds what any predicted warm start can save.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+
+def _quick_warmstart(mjb200, torch, m, B, nctrl=8, epochs=2, seed=50000):
+    """Warm-start net trained briefly on plain rollouts of the same model."""
+    col = mjb200.BatchedSim(m, B, record=0)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=seed)
+    col.set_state(q.astype(np.float32), v.astype(np.float32))
+    ctrl = torch.from_numpy(np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed + 1) for c in range(nctrl)]).astype(np.float32)).cuda()
+    width = col.warmstart_input_width()
+    rows = B * (4 * nctrl - 1)
+    x = torch.empty(rows, width, device="cuda")
+    t = torch.empty(rows, m.nv, device="cuda")
+    torch.cuda.synchronize()
+    n = col.warmstart_collect(ctrl.data_ptr(), nctrl, 4, x.data_ptr(), t.data_ptr(), rows)
+    net = mjb200.WarmStart(width, m.nv, seed=seed + 2)
+    net.fit_normalization(x.data_ptr(), t.data_ptr(), n)
+    net.train(x.data_ptr(), t.data_ptr(), n, epochs=epochs, batch=4096, lr=1e-3, seed=seed + 3)
+    col.close()
+    return net
+
+
+def _sensitivity(mjb200, m, B):
+    nv = m.nv
+    sim = mjb200.BatchedSim(m, B, record=0)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=31)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    for c in range(10):
+        sim.step(mjb200.models.quadruped_controls_fast(B, c, seed=32).astype(np.float32), 4)
+    ctrl = mjb200.models.quadruped_controls_fast(B, 10, seed=32).astype(np.float32)
+    sim.step(ctrl, 3)
+    sq, sv = sim.state()
+    prev = sim.qacc_warmstart().reshape(B, nv)
+
+    def run(cand):
+        sim.set_state(sq, sv)
+        sim.set_qacc_warmstart(cand.astype(np.float32))
+        sim.step(ctrl, 1)
+        st = sim.stats()
+        return st["niter_sum"].copy(), st["nefc"].copy(), sim.qacc_warmstart().reshape(B, nv)
+
+    it0, nefc, xs = run(prev)
+    print("envs %d, with contacts %d" % (B, int((nefc > 0).sum())))
+    print("warm start                      mean iterations")
+    print("previous qacc                   %.3f" % it0.mean())
+    for eps in (0.0, 1e-3, 1e-2, 3e-2, 0.1, 0.3, 0.6):
+        it, _, _ = run(xs + eps * (prev - xs))
+        print("x* + %-5g (prev - x*)         %.3f" % (eps, it.mean()))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["step", "learned", "gemm", "sensitivity"])
+    ap.add_argument("--envs", type=int, default=4096)
+    ap.add_argument("--ctrl", type=int, default=3, help="control steps (4 substeps each)")
+    ap.add_argument("--rows", type=int, default=16384)
+    ap.add_argument("--repeat", type=int, default=3)
+    a = ap.parse_args(argv)
+
+    import torch
+
+    import mjb200
+
+    if a.what == "gemm":
+        g = torch.Generator().manual_seed(0)
+        shapes = [(a.rows, 256, 192), (a.rows, 256, 256), (a.rows, 64, 256), (256, 256, 4096)]
+        for M, N, K in shapes:
+            A = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+            B = torch.randn(N, K, generator=g).to(torch.bfloat16).cuda()
+            C = torch.empty(M, N, device="cuda")
+            torch.cuda.synchronize()
+            for _ in range(a.repeat):
+                if mjb200.gemm_bf16(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K) != 0:
+                    raise RuntimeError(mjb200.capi.last_error())
+            torch.cuda.synchronize()
+        print("gemm done")
+        return
+
+    m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
+    B = a.envs
+    if a.what == "sensitivity":
+        _sensitivity(mjb200, m, B)
+        return
+    sim = mjb200.BatchedSim(m, B, record=0)
+    if a.what == "learned":
+        net = _quick_warmstart(mjb200, torch, m, B)
+        sim.set_warmstart(net)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=1000)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    for c in range(a.ctrl):
+        sim.step(mjb200.models.quadruped_controls_fast(B, c, seed=2000).astype(np.float32), 4)
+    sim.sync()
+    print("step done", sim.stats()["niter_sum"].mean() / 4.0)
+
+
+if __name__ == "__main__":
+    main()
