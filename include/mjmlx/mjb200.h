@@ -55,6 +55,13 @@ MJMLX_API MjmlxBatchedSim* mjb200_batched_create_multi(const MjmlxModel* const* 
                                                        const MjmlxBatchedConfig* config, const MjbEngineConfig* ecfg);
 MJMLX_API int mjb200_batched_configure(MjmlxBatchedSim* sim, const MjbEngineConfig* ecfg);
 MJMLX_API int mjb200_batched_get_config(const MjmlxBatchedSim* sim, MjbEngineConfig* out);
+/* Launch-shape autotuner: times envs-per-CTA 2/4/8/16 with lockstep CTAs and
+ * with the independent-warp work queue, reps launches of nsub substeps each,
+ * from the sim's current state (restored before every candidate and at the
+ * end), and keeps the fastest.  Per candidate i (at most max_candidates):
+ * warps[i], lockstep[i], ms[i] (mean per launch, -1 if it cannot launch);
+ * any array may be NULL.  Returns the number of candidates, or -1. */
+MJMLX_API int mjb200_batched_autotune(MjmlxBatchedSim* sim, int nsub, int reps, int max_candidates, int* warps, int* lockstep, float* ms);
 
 /* Record layout: num_envs, sum of nq / nv / nu over envs, and the per-env
  * offsets (arrays of num_envs, each may be NULL). */

@@ -223,6 +223,19 @@ MJMLX_API int mjb200_batched_get_config(const MjmlxBatchedSim* sim, MjbEngineCon
   return 0;
 }
 
+MJMLX_API int mjb200_batched_autotune(MjmlxBatchedSim* sim, int nsub, int reps, int max_candidates, int* warps, int* lockstep, float* ms) {
+  if (!sim || !sim->engine || nsub <= 0 || reps <= 0) return -1;
+  return guard("mjb200_batched_autotune", [&]() {
+    auto res = sim->engine->autotune(nsub, reps);
+    for (int i = 0; i < (int)res.size() && i < max_candidates; i++) {
+      if (warps) warps[i] = res[i].warps_per_block;
+      if (lockstep) lockstep[i] = res[i].lockstep;
+      if (ms) ms[i] = res[i].ms;
+    }
+    return (int)res.size();
+  }, -1);
+}
+
 MJMLX_API int mjb200_batched_layout(const MjmlxBatchedSim* sim, int* num_envs, int* total_q, int* total_v, int* total_u, int* qadr, int* vadr, int* uadr) {
   if (!sim) return -1;
   Engine& e = *sim->engine;

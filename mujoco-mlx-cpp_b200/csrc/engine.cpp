@@ -382,6 +382,78 @@ void Engine::configure(const EngineConfig& cfg) {
   invalidate_graphs();
 }
 
+std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
+  if (nsub <= 0 || reps <= 0) throw std::runtime_error("autotune: nsub and reps must be positive");
+  sync();
+  DevBuf<float> sq, sv, sw;
+  sq.alloc(tot_q_);
+  sv.alloc(tot_v_);
+  sw.alloc(tot_v_);
+  auto copy = [&](float* dst, const float* src, size_t n) { check(cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream_), "autotune copy"); };
+  copy(sq.p, qpos_.p, tot_q_);
+  copy(sv.p, qvel_.p, tot_v_);
+  copy(sw.p, warm_.p, tot_v_);
+  auto restore = [&]() {
+    copy(qpos_.p, sq.p, tot_q_);
+    copy(qvel_.p, sv.p, tot_v_);
+    copy(warm_.p, sw.p, tot_v_);
+  };
+  const EngineConfig orig = cfg_;
+  const int per_warp = (desc_words_ + ws_stride_) * 4;
+  std::vector<TuneCandidate> out;
+  cudaEvent_t e0, e1;
+  check(cudaEventCreate(&e0), "event");
+  check(cudaEventCreate(&e1), "event");
+  const bool feat_valid = feat_valid_;
+  for (int lock : {1, 0}) {
+    for (int w : {2, 4, 8, 16}) {
+      TuneCandidate c{w, lock, 0, -1.f};
+      if (w * per_warp > 227 * 1024) {
+        out.push_back(c);
+        continue;
+      }
+      EngineConfig cfg = orig;
+      cfg.warps_per_block = w;
+      cfg.lockstep = lock;
+      cfg.persistent = 1;
+      cfg.blocks_per_sm = 0;
+      try {
+        configure(cfg);
+      } catch (const std::exception&) {
+        out.push_back(c);
+        continue;
+      }
+      restore();
+      launch(nsub, false);  // warm-up (and graph capture)
+      restore();
+      check(cudaEventRecord(e0, stream_), "event");
+      for (int r = 0; r < reps; r++) launch(nsub, false);
+      check(cudaEventRecord(e1, stream_), "event");
+      check(cudaEventSynchronize(e1), "event sync");
+      float ms = 0;
+      check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+      c.ms = ms / reps;
+      out.push_back(c);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const TuneCandidate* best = nullptr;
+  for (auto& c : out)
+    if (c.ms >= 0 && (!best || c.ms < best->ms)) best = &c;
+  EngineConfig cfg = orig;
+  if (best) {
+    cfg.warps_per_block = best->warps_per_block;
+    cfg.lockstep = best->lockstep;
+    cfg.persistent = 1;
+  }
+  configure(cfg);
+  restore();
+  sync();
+  feat_valid_ = feat_valid;
+  return out;
+}
+
 void Engine::launch_shape(int* grid, int* warps, int* smem, int* persistent) const {
   if (grid) *grid = grid_;
   if (warps) *warps = warps_;

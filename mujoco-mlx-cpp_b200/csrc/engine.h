@@ -120,6 +120,16 @@ class Engine {
   float* qacc_pred_device() { return pred_.p; }
 
   void configure(const EngineConfig& cfg);
+  // Launch-shape autotuner: times each candidate (envs per CTA 2/4/8/16,
+  // lockstep CTAs or the independent-warp work queue) on `reps` launches of
+  // `nsub` substeps from the sim's current state, restoring the state before
+  // every candidate and at the end, then keeps the fastest.  Results do not
+  // depend on the launch shape (the same stage code runs per env).
+  struct TuneCandidate {
+    int warps_per_block, lockstep, blocks_per_sm;
+    float ms;  // mean per launch; < 0 when the shape cannot launch
+  };
+  std::vector<TuneCandidate> autotune(int nsub, int reps);
   const EngineConfig& config() const { return cfg_; }
   void launch_shape(int* grid, int* warps, int* smem_bytes, int* persistent) const;
   int lockstep() const { return lockstep_; }

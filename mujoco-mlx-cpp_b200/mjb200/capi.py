@@ -85,6 +85,7 @@ def _load():
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "mjb200_batched_get_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_batched_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p]),
         "mjb200_batched_step_warmstart": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
@@ -318,6 +319,17 @@ class BatchedSim:
         a = np.ascontiguousarray(qacc, np.float32).reshape(-1)
         if a.size != self.total_v or lib.mjb200_batched_set_qacc_warmstart(self.handle, _fp(a)) != 0:
             raise RuntimeError("set_qacc_warmstart: " + last_error())
+
+    def autotune(self, nsub: int = 4, reps: int = 3):
+        """Times the launch-shape candidates and keeps the fastest; returns
+        [(warps_per_block, lockstep, ms per launch)]."""
+        w = np.zeros(16, np.int32)
+        l = np.zeros(16, np.int32)
+        t = np.zeros(16, np.float32)
+        n = lib.mjb200_batched_autotune(self.handle, nsub, reps, 16, _ip(w), _ip(l), _fp(t))
+        if n < 0:
+            raise RuntimeError(last_error())
+        return [(int(w[i]), int(l[i]), float(t[i])) for i in range(n)]
 
     def step_warmstart(self, qacc_ptr: int, n: int = 1):
         if lib.mjb200_batched_step_warmstart(self.handle, C.c_void_p(qacc_ptr), n) != 0:
