@@ -71,6 +71,14 @@ MJMLX_API int mjb200_batched_warmstart_collect(MjmlxBatchedSim* sim, const float
  * attachment and serves one sim batch size. */
 MJMLX_API int mjb200_batched_set_warmstart(MjmlxBatchedSim* sim, MjbWarmStart* net);
 
+/* Prediction for B envs from device arrays feat_dev[B][fstride] (first nfeat
+ * used), ctrl_dev[B][nu] and the previous qacc prev_dev[B][nout]:
+ * pred_dev = prev + mean + std * net(...).  fused = 1 runs the single fused
+ * kernel the sims use, 0 the gather kernel plus four GEMM launches (same
+ * arithmetic).  Runs on the legacy default stream and waits for it. */
+MJMLX_API int mjb200_warmstart_predict(MjbWarmStart* net, const float* feat_dev, int fstride, int nfeat, const float* ctrl_dev, int nu,
+                                       const float* prev_dev, float* pred_dev, int B, int fused);
+
 /* C[M][N] (float, device) = A[M][K] * B[N][K]^T with bf16 device operands, on
  * the tcgen05 GEMM the network uses.  K a multiple of 64; N 64, 128, 192 or a
  * multiple of 256.  stream: cudaStream_t (NULL = legacy default).  Returns

@@ -139,6 +139,17 @@ MJMLX_API int mjb200_batched_set_warmstart(MjmlxBatchedSim* sim, MjbWarmStart* w
   });
 }
 
+MJMLX_API int mjb200_warmstart_predict(MjbWarmStart* w, const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev,
+                                       float* pred, int B, int fused) {
+  if (!w || !feat || !prev || !pred || B <= 0 || (nu > 0 && !ctrl)) return -1;
+  return guarded("mjb200_warmstart_predict", [&] {
+    w->net->infer(feat, fstride, nfeat, ctrl, nu, prev, pred, B, nullptr, fused != 0);
+    mjb::check(cudaStreamSynchronize(nullptr), "predict sync");
+    if (w->net->error_word()) throw std::runtime_error("a bounded wait in an inference kernel timed out");
+    return 0;
+  });
+}
+
 MJMLX_API int mjb200_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, void* stream) {
   if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0 || K % 64 != 0) {
     set_error("mjb200_gemm_bf16: bad arguments");

@@ -499,3 +499,206 @@ cudaError_t cast_weights(int rows, int cols, const float* p, __nv_bfloat16* w, _
 }
 
 }  // namespace mjb
+
+// ------------------------------------------------------- fused inference
+
+namespace mjb {
+namespace {
+
+constexpr int INF_ACT_BYTES = 128 * 256 * 2;     // 128 rows x up to 256 bf16, 4 K-chunks of 16 KB
+constexpr int INF_STAGE_BYTES = 256 * 64 * 2;    // one 64-wide K-chunk of up to 256 weight rows
+constexpr int INF_STAGES = 2;
+
+// Byte offset of element (row r, column j) in the chunked, 128-byte
+// swizzled K-major operand layout (chunk = 64 columns x 128 rows).
+__device__ __forceinline__ uint32_t act_off(int r, int j) {
+  const int c = j >> 6, jj = j & 63;
+  return (uint32_t)(c * 16384 + r * 128 + ((((jj >> 3) ^ (r & 7)) & 7) << 4) + (jj & 7) * 2);
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w) : "memory");
+}
+
+// One CTA computes the warm-start prediction of 128 envs: gather and
+// normalise [features | controls] into bf16 (shared memory, UMMA operand
+// layout), then for each layer: stream the weight K-chunks through a 2-stage
+// TMA ring, tcgen05.mma into TMEM, and write bias + GELU activations back
+// over the operand buffer; the output layer writes prev + mean + std * y.
+__global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const __grid_constant__ CUtensorMap w0, const __grid_constant__ CUtensorMap w1,
+                                                           const __grid_constant__ CUtensorMap w2, const __grid_constant__ CUtensorMap w3,
+                                                           InferArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* act = smem;
+  uint8_t* ring = smem + INF_ACT_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + INF_STAGES * INF_STAGE_BYTES);
+  uint64_t* empty = full + INF_STAGES;
+  uint64_t* done = empty + INF_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const CUtensorMap* maps[4] = {&w0, &w1, &w2, &w3};
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * 128;
+  const uint32_t act_s = smem_u32(act);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < INF_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(256u) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // gather + normalise: warp w fills rows 32w .. 32w+31; lane handles the
+  // columns lane + 32k; 4 rows per pass keep up to 32 independent loads per
+  // lane in flight (the gather is latency bound otherwise)
+  {
+    const int kmax = a.in_pad >> 5, nin = a.nfeat + a.nu;
+    float mu[8], is[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int j = lane + 32 * k;
+      mu[k] = (k < kmax && j < nin) ? a.mean[j] : 0.f;
+      is[k] = (k < kmax && j < nin) ? a.istd[j] : 0.f;
+    }
+#pragma unroll 1
+    for (int rr = 0; rr < 32; rr += 4) {
+      float v[4][8];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int env = m0 + warp * 32 + rr + q;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int j = lane + 32 * k;
+          float x = 0.f;
+          if (k < kmax && env < a.B) {
+            if (j < a.nfeat) x = __ldg(a.feat + (size_t)env * a.fstride + j);
+            else if (j < nin) x = __ldg(a.ctrl + (size_t)env * a.nu + (j - a.nfeat));
+          }
+          v[q][k] = x;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = warp * 32 + rr + q;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          if (k < kmax) {
+            const int j = lane + 32 * k;
+            *reinterpret_cast<__nv_bfloat16*>(act + act_off(r, j)) = __float2bfloat16_rn((v[q][k] - mu[k]) * is[k]);
+          }
+        }
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  int g = 0;  // K-chunk counter over all layers (ring stage and phase)
+  bool ok = true;
+#pragma unroll 1
+  for (int l = 0; l < 4 && ok; l++) {
+    const int N = a.rows[l], K = a.cols[l], nk = K / 64;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    if (warp == 0 && lane == 0) {
+      for (int c = 0; c < nk; c++) {
+        const int gc = g + c, s = gc % INF_STAGES;
+        if (gc >= INF_STAGES && !mbar_wait(&empty[s], ((gc / INF_STAGES) - 1) & 1, abort_flag)) {
+          *abort_flag = 1;
+          break;
+        }
+        mbar_expect_tx(&full[s], (uint32_t)(N * 128));
+        tma_load_2d(ring + s * INF_STAGE_BYTES, maps[l], &full[s], c * 64, 0);
+      }
+    } else if (warp == 1 && lane == 0) {
+      for (int c = 0; c < nk; c++) {
+        const int gc = g + c, s = gc % INF_STAGES;
+        if (!mbar_wait(&full[s], (gc / INF_STAGES) & 1, abort_flag)) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = act_s + c * 16384;
+        const uint32_t sb = smem_u32(ring + s * INF_STAGE_BYTES);
+#pragma unroll
+        for (int k = 0; k < 4; k++) mma_bf16(tmem, sw128_desc(sa + 32 * k), sw128_desc(sb + 32 * k), idesc, (c | k) != 0);
+        mma_commit(&empty[s]);
+      }
+      mma_commit(done);
+    }
+    g += nk;
+    __syncwarp();
+    ok = mbar_wait(done, l & 1, abort_flag) && !*abort_flag;
+    __syncwarp();
+    tc_fence_after();
+    if (!ok) break;
+    // epilogue: TMEM lanes of this warp = its 32 rows
+    const int r = warp * 32 + lane, env = m0 + r;
+    const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+    const float* bias = a.bias[l];
+#pragma unroll 1
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      float v[16];
+      tmem_ld16(tbase + c0, v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) v[i] += bias[c0 + i];
+      if (l < 3) {
+        __align__(16) __nv_bfloat162 h[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) h[i] = __floats2bfloat162_rn(gelu(v[2 * i]), gelu(v[2 * i + 1]));
+        const uint4* hv = reinterpret_cast<const uint4*>(h);
+        st_shared_v4(act_s + act_off(r, c0), hv[0]);
+        st_shared_v4(act_s + act_off(r, c0 + 8), hv[1]);
+      } else if (env < a.B) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int k = c0 + i;
+          if (k < a.nout) {
+            const size_t o = (size_t)env * a.nout + k;
+            a.pred[o] = a.prev[o] + a.omean[k] + a.ostd[k] * v[i];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (!ok && threadIdx.x == 0 && a.err) atomicExch(a.err, 2);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
+  }
+}
+
+}  // namespace
+
+cudaError_t mlp_infer(const CUtensorMap* wmaps, const InferArgs& a, cudaStream_t s) {
+  if (a.B <= 0) return cudaSuccess;
+  if (a.in_pad > 256 || a.in_pad % 64 != 0) return cudaErrorInvalidValue;
+  for (int l = 0; l < 4; l++)
+    if (a.rows[l] > 256 || a.rows[l] % 16 != 0 || a.cols[l] % 64 != 0 || a.cols[l] > 256) return cudaErrorInvalidValue;
+  const size_t smem = 1024 + INF_ACT_BYTES + INF_STAGES * INF_STAGE_BYTES + 128;
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [&] { attr_err = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
+  if (attr_err != cudaSuccess) return attr_err;
+  mlp_infer_kernel<<<(a.B + 127) / 128, 128, smem, s>>>(wmaps[0], wmaps[1], wmaps[2], wmaps[3], a);
+  return cudaGetLastError();
+}
+
+}  // namespace mjb

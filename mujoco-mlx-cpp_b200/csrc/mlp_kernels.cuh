@@ -68,4 +68,26 @@ cudaError_t column_stats(const float* x, int n, int c, int ld, double* sum, doub
 // bf16 copy of a fp32 weight matrix and its transpose.
 cudaError_t cast_weights(int rows, int cols, const float* p, __nv_bfloat16* w, __nv_bfloat16* wt, cudaStream_t s);
 
+// Fused warm-start inference (gather + normalise + 4 layers + prediction).
+struct InferArgs {
+  int B;                  // envs (rows)
+  const float* feat;      // [B][fstride], first nfeat used
+  int fstride, nfeat;
+  const float* ctrl;      // [B][nu]
+  int nu;
+  int in_pad;             // padded input width (multiple of 64, <= 256)
+  const float* mean;      // [nfeat + nu]
+  const float* istd;
+  int rows[4], cols[4];   // layer shapes (weights [rows][cols]); cols[0] = in_pad
+  const float* bias[4];
+  int nout;
+  const float* prev;      // [B][nout]
+  const float* omean;
+  const float* ostd;
+  float* pred;            // [B][nout]
+  int* err;
+};
+// wmaps: tensor maps of the 4 bf16 weight matrices, box {64, rows[l]}.
+cudaError_t mlp_infer(const CUtensorMap* wmaps, const InferArgs& a, cudaStream_t s);
+
 }  // namespace mjb

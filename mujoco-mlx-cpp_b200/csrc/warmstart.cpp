@@ -382,9 +382,35 @@ void WarmStartNet::prepare_inference(int B) {
   inf_B_ = B;
 }
 
-void WarmStartNet::infer(const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev, float* pred, int B, cudaStream_t s) {
+void WarmStartNet::infer(const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev, float* pred, int B, cudaStream_t s,
+                         bool fused) {
   if (nfeat + nu != in_raw_) throw std::runtime_error("warm start: features + controls do not match the network input width");
   prepare_inference(B);
+  if (fused) {
+    InferArgs a{};
+    a.B = B;
+    a.feat = feat;
+    a.fstride = fstride;
+    a.nfeat = nfeat;
+    a.ctrl = ctrl;
+    a.nu = nu;
+    a.in_pad = in_pad_;
+    a.mean = in_mean_.p;
+    a.istd = in_istd_.p;
+    for (int l = 0; l < kLayers; l++) {
+      a.rows[l] = rows_[l];
+      a.cols[l] = cols_[l];
+      a.bias[l] = Bias(l);
+    }
+    a.nout = nout_;
+    a.prev = prev;
+    a.omean = out_mean_.p;
+    a.ostd = out_std_.p;
+    a.pred = pred;
+    a.err = err_.p;
+    check(mlp_infer(m_w_, a, s), "warm start fused inference");
+    return;
+  }
   check(gather_rows(B, nullptr, feat, fstride, nfeat, ctrl, nu, nu, in_mean_.p, in_istd_.p, bf(xi_), in_pad_, nullptr, 0, nullptr, 0, nullptr, nullptr,
                     nullptr, s),
         "gather");

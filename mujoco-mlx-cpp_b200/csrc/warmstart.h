@@ -58,7 +58,10 @@ class WarmStartNet {
   // Inference for a sim: features feat[B][fstride] (first nfeat used) and
   // controls ctrl[B][nu] form the raw input; pred[B][nout] = prev + mean +
   // std * y.  Runs on stream s (capturable: buffers are fixed per B).
-  void infer(const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev, float* pred, int B, cudaStream_t s);
+  // fused: one kernel (gather + 4 layers + prediction); otherwise the gather
+  // kernel and 4 GEMM launches.  Both compute the same arithmetic.
+  void infer(const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev, float* pred, int B, cudaStream_t s,
+             bool fused = true);
   // Allocates the inference buffers for batches of B envs (separate from the
   // training buffers, so captured inference graphs stay valid while the net
   // trains); a net serves one inference batch size.

@@ -82,6 +82,7 @@ def _load():
         "mjb200_warmstart_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _f32p]),
         "mjb200_batched_warmstart_collect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_set_warmstart": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "mjb200_warmstart_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "mjb200_batched_get_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
@@ -241,6 +242,10 @@ class WarmStart:
         loss = np.zeros(1, np.float32)
         self._ok(lib.mjb200_warmstart_gradients(self.handle, C.c_void_p(xraw_ptr), C.c_void_p(traw_ptr), n, _fp(g), _fp(loss)))
         return float(loss[0]), g
+
+    def predict(self, feat_ptr: int, fstride: int, nfeat: int, ctrl_ptr: int, nu: int, prev_ptr: int, pred_ptr: int, B: int, fused: bool = True):
+        self._ok(lib.mjb200_warmstart_predict(self.handle, C.c_void_p(feat_ptr), fstride, nfeat, C.c_void_p(ctrl_ptr), nu, C.c_void_p(prev_ptr),
+                                              C.c_void_p(pred_ptr), B, 1 if fused else 0))
 
     def train(self, xraw_ptr: int, traw_ptr: int, n: int, epochs: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0):
         hist = np.zeros(max(epochs, 1), np.float32)

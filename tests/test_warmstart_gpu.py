@@ -200,3 +200,25 @@ def test_learned_path_single_step_parity(quad_model, trained_quad_net):
     errs = np.array(errs)
     assert np.median(errs) <= 1e-4 and errs.max() <= 2e-3, (np.median(errs), errs.max())
     assert np.mean(st["warm_choice"] == 2) > 0.2
+
+
+@pytest.mark.parametrize("B", [128, 1000, 16384])
+def test_fused_inference_matches_unfused(B):
+    """The fused inference kernel (gather + 4 layers in one launch) against
+    the gather kernel + 4 GEMMs: same bf16 rounding points, FP32 sums in a
+    different order, so agreement to 1e-3 of the prediction's scale."""
+    net, p, xraw, traw, (im, is_, om, os_) = _net_and_data(256, seed=9, out_scale=10.0)
+    rng = np.random.default_rng(10)
+    nfeat, nu = 117, 12
+    feat = torch.from_numpy((rng.normal(size=(B, 120)) * 2).astype(np.float32)).cuda()
+    ctrl = torch.from_numpy(rng.normal(size=(B, nu)).astype(np.float32)).cuda()
+    prev = torch.from_numpy(rng.normal(size=(B, 18)).astype(np.float32)).cuda()
+    outs = []
+    for fused in (True, False):
+        pred = torch.full((B, 18), float("nan"), device="cuda")
+        torch.cuda.synchronize()
+        net.predict(feat.data_ptr(), 120, nfeat, ctrl.data_ptr(), nu, prev.data_ptr(), pred.data_ptr(), B, fused)
+        outs.append(pred.cpu().numpy())
+    assert np.isfinite(outs[0]).all()
+    scale = np.abs(outs[1] - prev.cpu().numpy()).max()
+    assert np.abs(outs[0] - outs[1]).max() <= 1e-3 * scale + 1e-6, np.abs(outs[0] - outs[1]).max() / scale
