@@ -210,3 +210,18 @@ def test_batch_threads_deterministic(quad_model):
         ob.step(8, nthread=nthread)
         out.append(ob.state())
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("condim,rows", [(1, 1), (3, 4), (4, 6), (6, 10)])
+def test_rows_per_contact_by_condim(condim, rows):
+    """The reference's legacy structural rule (tests/test_friction_condim3.cpp,
+    tests/test_friction_condim46.cpp): pyramidal contacts give 2 (condim - 1)
+    rows, frictionless contacts 1."""
+    xml = wrap(PLANE.replace('size="5 5 0.1"', f'size="5 5 0.1" condim="{condim}"') +
+               f'<body pos="0 0 0.049"><freejoint/><geom type="box" size="0.2 0.1 0.05" mass="1" condim="{condim}"/></body>')
+    om, env = env_from_xml(xml)
+    env.step()
+    assert env.d.ncon == 4
+    assert env.d.nefc == 4 * rows
+    res, f, force = _gauss_residual(om, env)
+    assert res < 1e-6

@@ -243,3 +243,32 @@ def test_checkpoint_resume_bitwise(quad_model):
     st = b.stats()
     assert st["niter_sum"].mean() < 0.5 * it_plain
     assert np.mean(st["warm_choice"] == 2) > 0.5
+
+
+@pytest.mark.parametrize("condim", [1, 4, 6])
+def test_condim_single_step_parity(condim):
+    """Pyramidal contacts with condim 1 (frictionless), 4 (torsional) and 6
+    (rolling): 2 (condim - 1) rows per contact (1 for condim 1), and the
+    single-step qacc against the oracle within the quadruped tolerances."""
+    model = mjb200.load_model_from_string(mjb200.models.quadruped_xml(condim=condim))
+    om = oracle.OracleModel(model.dump())
+    B = 48
+    states = visited_states(om, nsteps=(30, 90), B=B)
+    sim = mjb200.BatchedSim(model, B, ncon_max=48, nefc_max=320)
+    rows_per = 1 if condim == 1 else 2 * (condim - 1)
+    for qp, qv, ctrl in states:
+        g = gpu_step_from(sim, qp, qv, ctrl, 48, 320)
+        o = oracle_step_from(om, qp.astype(np.float64), qv.astype(np.float64), ctrl.astype(np.float64), ncon_max=48, nefc_max=320)
+        errs = []
+        for e in range(B):
+            st = g["stats"]
+            assert st["status"][e] == 0
+            ok, nb = contact_sets_match(g["con"][e], o[e]["contacts"], st["ncon"][e])
+            assert ok
+            if nb == 0:
+                assert st["nefc"][e] == o[e]["nefc"]
+                nlim = int((o[e]["efc"]["type"] == 1).sum())
+                assert o[e]["nefc"] == rows_per * o[e]["ncon"] + nlim
+                errs.append(rel_err(g["vec"][e, 2, : om.nv], o[e]["qacc"]))
+        errs = np.array(errs)
+        assert np.median(errs) <= 1e-4 and errs.max() <= 2e-3, (condim, np.median(errs), errs.max())
