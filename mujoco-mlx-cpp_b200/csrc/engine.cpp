@@ -11,6 +11,9 @@
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
 cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
 cudaError_t mjb_sub(int n, const float* a, const float* b, float* out, cudaStream_t s);
+cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
+cudaError_t mjb_launch_ray(int B, int nray, const int* env_model, const int* geom_base, const int* geom_count, const float* ginfo, const float* gpose,
+                           int ng_max, const float* pnt, const float* vec, float* dist, int* geomid, cudaStream_t s);
 cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
                              float* qpos, float* qvel, float* warm, cudaStream_t s);
 
@@ -936,8 +939,54 @@ int Engine::get_pack(float* out) {
   return 0;
 }
 
-int Engine::raycast(const float*, const float*, int, int, const unsigned char*, int, float*, int*) {
-  throw std::runtime_error("raycast is not available in this build yet");
+int Engine::raycast(const float* pnt, const float* vec, int nray, int bodyexclude, const unsigned char* geomgroup, int flg_static, float* dist,
+                    int* geomid) {
+  if (nray <= 0 || !pnt || !vec || !dist || !geomid) return -1;
+  const size_t total = (size_t)B_ * nray;
+  // per-model geom table {type, size, include}; include applies the call's
+  // body / group / static filters and the supported types
+  std::vector<int> base(models_.size()), cnt(models_.size());
+  std::vector<float> ginfo;
+  int ng_max = 0;
+  for (size_t mi = 0; mi < models_.size(); mi++) {
+    const Model& m = *models_[mi];
+    base[mi] = (int)(ginfo.size() / 5);
+    cnt[mi] = m.ngeom;
+    ng_max = std::max(ng_max, m.ngeom);
+    for (int g = 0; g < m.ngeom; g++) {
+      const int type = m.geom_type[g], body = m.geom_bodyid[g], group = m.geom_group[g];
+      const bool group_ok = !geomgroup || (group >= 0 && group < 6 && geomgroup[group]);
+      const bool static_ok = flg_static || m.body_weldid[body] != 0;
+      const bool supported = type == GEOM_PLANE || type == GEOM_SPHERE || type == GEOM_CAPSULE || type == GEOM_ELLIPSOID || type == GEOM_CYLINDER ||
+                             type == GEOM_BOX;
+      const bool inc = body != bodyexclude && group_ok && static_ok && supported;
+      ginfo.insert(ginfo.end(), {(float)type, (float)m.geom_size[3 * g], (float)m.geom_size[3 * g + 1], (float)m.geom_size[3 * g + 2], inc ? 1.f : 0.f});
+    }
+  }
+  if (ng_max == 0) {
+    std::fill(dist, dist + total, -1.f);
+    std::fill(geomid, geomid + total, -1);
+    return 0;
+  }
+  DevBuf<float> d_ginfo, d_rays, d_pose, d_dist;
+  DevBuf<int> d_base, d_cnt, d_gid;
+  d_ginfo.upload(ginfo, stream_);
+  d_base.upload(base, stream_);
+  d_cnt.upload(cnt, stream_);
+  d_rays.alloc(total * 6);
+  check(cudaMemcpyAsync(d_rays.p, pnt, sizeof(float) * total * 3, cudaMemcpyHostToDevice, stream_), "ray points");
+  check(cudaMemcpyAsync(d_rays.p + total * 3, vec, sizeof(float) * total * 3, cudaMemcpyHostToDevice, stream_), "ray vectors");
+  d_pose.alloc((size_t)B_ * ng_max * 12);
+  d_dist.alloc(total);
+  d_gid.alloc(total);
+  StepParams P = params(1, false);
+  check(mjb_launch_geom_pose(P, d_pose.p, ng_max, warps_, smem_, stream_), "geom pose kernel");
+  check(mjb_launch_ray(B_, nray, d_model_.p, d_base.p, d_cnt.p, d_ginfo.p, d_pose.p, ng_max, d_rays.p, d_rays.p + total * 3, d_dist.p, d_gid.p, stream_),
+        "ray kernel");
+  check(cudaMemcpyAsync(dist, d_dist.p, sizeof(float) * total, cudaMemcpyDeviceToHost, stream_), "ray dist");
+  check(cudaMemcpyAsync(geomid, d_gid.p, sizeof(int) * total, cudaMemcpyDeviceToHost, stream_), "ray geom");
+  sync();
+  return 0;
 }
 
 }  // namespace mjb

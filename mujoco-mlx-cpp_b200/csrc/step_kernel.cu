@@ -412,6 +412,53 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
 #undef STAGE_SYNC
 }
 
+// Geom poses of every env at its current qpos (kinematics only), for ray
+// casting: gpose[env][g][12] = world position (3), rotation matrix (9, row
+// major).  One warp per env; the workspace layout is the step kernel's.
+__global__ void __launch_bounds__(256) mjb_geom_pose_kernel(StepParams P, float* gpose, int ng_max) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
+  int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
+  float* ws = mjb_smem + W * P.desc_words + warp * P.ws_stride;
+  const int env = blockIdx.x * W + warp;
+  if (env >= P.num_envs) return;
+  const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
+#pragma unroll 1
+  for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
+  __syncwarp();
+  Env E;
+  E.it = P.itab;
+  E.ft = P.ftab;
+  E.ws = ws;
+  E.lane = lane;
+  E.env = env;
+  E.status = 0;
+  E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+  const DevModelDesc& m = *E.md;
+  const int qadr = P.env_qadr[env];
+#pragma unroll 1
+  for (int i = lane; i < m.nq; i += 32) ws[m.w_qpos + i] = P.qpos[qadr + i];
+  __syncwarp();
+  d_kinematics(E);
+  float* out = gpose + (size_t)env * ng_max * 12;
+#pragma unroll 1
+  for (int k = lane; k < m.ngeom * 12; k += 32) {
+    const int g = k / 12, q = k % 12;
+    out[k] = q < 3 ? ws[m.w_gxpos + 3 * g + q] : ws[m.w_gxmat + 9 * g + (q - 3)];
+  }
+}
+
+cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
+  static size_t configured = 0;
+  if (smem_bytes > configured) {
+    cudaError_t e = cudaFuncSetAttribute(mjb_geom_pose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    configured = smem_bytes;
+  }
+  const int grid = (P.num_envs + warps_per_block - 1) / warps_per_block;
+  mjb_geom_pose_kernel<<<grid, warps_per_block * 32, smem_bytes, stream>>>(P, gpose, ng_max);
+  return cudaGetLastError();
+}
+
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
   static size_t configured = 0;
   if (smem_bytes > configured) {

@@ -340,6 +340,21 @@ class BatchedSim:
         if lib.mjb200_batched_step_warmstart(self.handle, C.c_void_p(qacc_ptr), n) != 0:
             raise RuntimeError(last_error())
 
+    def raycast(self, pnt, vec, bodyexclude: int = -1, geomgroup=None, flg_static: int = 1):
+        """Rays pnt/vec [num_envs, nray, 3] (world frame, per env) against each
+        env's geoms at its current qpos: (dist [num_envs, nray], geom id)."""
+        p = np.ascontiguousarray(pnt, np.float32)
+        v = np.ascontiguousarray(vec, np.float32)
+        nray = p.shape[1]
+        dist = np.zeros((self.num_envs, nray), np.float32)
+        gid = np.zeros((self.num_envs, nray), np.int32)
+        gg = None if geomgroup is None else np.ascontiguousarray(geomgroup, np.uint8)
+        rc = lib.mjmlx_batched_raycast(self.handle, _fp(p), _fp(v), nray, bodyexclude,
+                                       None if gg is None else gg.ctypes.data_as(C.POINTER(C.c_ubyte)), flg_static, _fp(dist), _ip(gid))
+        if rc != 0:
+            raise RuntimeError("raycast: " + last_error())
+        return dist, gid
+
     # ---- learned warm start
     def warmstart_input_width(self) -> int:
         return lib.mjb200_warmstart_input_width(self.handle)

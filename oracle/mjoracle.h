@@ -101,6 +101,10 @@ void oracle_integrate(const OModel* m, OData* d);
  * uses the model's iteration count */
 void oracle_step(const OModel* m, OData* d, const ORand* r, int max_iter);
 
+/* nearest ray hit t (pnt + t vec) among the geoms with include[g] != 0 at
+ * the poses of the last oracle_kinematics call; -1 and geomid -1 when none */
+double oracle_ray(const OModel* m, const OData* d, const double* pnt, const double* vec, const int* include, int* geomid);
+
 /* step B envs (state arrays env-major) over nthread host threads; each env
  * uses its own OData built from the per-env pointer tables */
 void oracle_step_batch(const OModel* m, OData* const* d, int B, int nsub, int max_iter, int nthread);

@@ -76,6 +76,8 @@ def _load():
     lib.oracle_solve.argtypes = [C.POINTER(OModel), C.POINTER(OData), C.c_int]
     lib.oracle_integrate.argtypes = [C.POINTER(OModel), C.POINTER(OData)]
     lib.oracle_step.argtypes = [C.POINTER(OModel), C.POINTER(OData), C.POINTER(ORand), C.c_int]
+    lib.oracle_ray.restype = C.c_double
+    lib.oracle_ray.argtypes = [C.POINTER(OModel), C.POINTER(OData), _dp, _dp, _ip, _ip]
     lib.oracle_step_batch.argtypes = [C.POINTER(OModel), C.POINTER(C.POINTER(OData)), C.c_int, C.c_int, C.c_int, C.c_int]
     return lib
 
@@ -141,6 +143,18 @@ class OracleEnv:
         d.qacc_predicted = None
         self.d = d
         self._pred = None
+
+    def ray(self, pnt, vec, include):
+        """Nearest hit (t, geom id) at the poses of the last kinematics pass."""
+        p = np.ascontiguousarray(pnt, np.float64)
+        v = np.ascontiguousarray(vec, np.float64)
+        inc = np.ascontiguousarray(include, np.int32)
+        g = C.c_int(-1)
+        t = lib.oracle_ray(C.byref(self.om.c), C.byref(self.d), _ptr(p, "f"), _ptr(v, "f"), _ptr(inc, "i"), C.byref(g))
+        return t, g.value
+
+    def kinematics(self):
+        lib.oracle_kinematics(C.byref(self.om.c), C.byref(self.d))
 
     def set_predicted(self, qacc):
         if qacc is None:

@@ -225,3 +225,29 @@ def test_rows_per_contact_by_condim(condim, rows):
     assert env.d.nefc == 4 * rows
     res, f, force = _gauss_residual(om, env)
     assert res < 1e-6
+
+
+def test_ray_known_answers():
+    """Closed-form ray hits: plane from above only, sphere, box from outside
+    and inside, capsule cap, cylinder disc, body exclusion."""
+    xml = wrap(PLANE + '<body pos="0 0 1"><freejoint/><geom type="sphere" size="0.2"/></body>'
+                       '<body pos="2 0 1"><geom type="box" size="0.1 0.2 0.3"/></body>'
+                       '<body pos="0 2 1"><geom type="capsule" size="0.1 0.3"/></body>'
+                       '<body pos="0 -2 1"><geom type="cylinder" size="0.1 0.3"/></body>')
+    om, env = env_from_xml(xml)
+    env.kinematics()
+    inc = np.ones(om.ngeom, np.int32)
+    t, g = env.ray([0, 0, 3], [0, 0, -1], inc)
+    assert (t, g) == (pytest.approx(1.8), 1)                 # sphere top at z = 1.2
+    t, g = env.ray([5, 5, 1], [0, 0, -2], inc)
+    assert (t, g) == (pytest.approx(0.5), 0)                 # plane, t in units of vec
+    assert env.ray([5, 5, -1], [0, 0, 1], inc) == (-1, -1)   # plane not hit from below
+    t, g = env.ray([2, 0, 1], [1, 0, 0], inc)
+    assert (t, g) == (pytest.approx(0.1), 2)                 # box exit from inside
+    t, g = env.ray([0, 2, 3], [0, 0, -1], inc)
+    assert (t, g) == (pytest.approx(3 - 1.4), 3)             # capsule cap top at z = 1.4
+    t, g = env.ray([0, -2, 3], [0, 0, -1], inc)
+    assert (t, g) == (pytest.approx(3 - 1.3), 4)             # cylinder disc at z = 1.3
+    inc[1] = 0
+    t, g = env.ray([0, 0, 3], [0, 0, -1], inc)
+    assert g == 0 and t == pytest.approx(3.0)               # sphere excluded: the plane
