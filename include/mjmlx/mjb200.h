@@ -126,6 +126,13 @@ MJMLX_API int mjb200_batched_stats(MjmlxBatchedSim* sim, int* status, int* niter
 /* Solver acceleration qacc of the last substep, float[total_v]. */
 MJMLX_API const float* mjb200_batched_get_qacc(MjmlxBatchedSim* sim, int* n_out);
 
+/* Packed read-back without a host copy: runs the pack kernel for the spec
+ * set by mjmlx_batched_set_pack_spec on the sim's stream and returns its
+ * device buffer (num_envs x stride floats, owned by the sim, valid until the
+ * next pack or free).  Order reads after it on the sim's stream.  No
+ * counterpart in the reference (its get_pack copies to the host).  0 / -1. */
+MJMLX_API int mjb200_batched_pack_device(MjmlxBatchedSim* sim, float** pack_dev);
+
 /* Per-stage SM clock totals of the lockstep step kernel (8 stages: state check
  * + kinematics, collision, COM + CRB, RNE + forces, unconstrained solve,
  * constraint build, Newton, integration).  enable 1 starts (and zeroes) the

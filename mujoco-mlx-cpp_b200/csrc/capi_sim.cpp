@@ -223,6 +223,11 @@ MJMLX_API int mjb200_batched_get_config(const MjmlxBatchedSim* sim, MjbEngineCon
   return 0;
 }
 
+MJMLX_API int mjb200_batched_pack_device(MjmlxBatchedSim* sim, float** pack_dev) {
+  if (!sim || !sim->engine || !pack_dev) return -1;
+  return guard("mjb200_batched_pack_device", [&]() { return sim->engine->pack_device(pack_dev); }, -1);
+}
+
 MJMLX_API int mjb200_batched_autotune(MjmlxBatchedSim* sim, int nsub, int reps, int max_candidates, int* warps, int* lockstep, float* ms) {
   if (!sim || !sim->engine || nsub <= 0 || reps <= 0) return -1;
   return guard("mjb200_batched_autotune", [&]() {

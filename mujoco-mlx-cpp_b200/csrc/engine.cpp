@@ -11,6 +11,8 @@
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
 cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
 cudaError_t mjb_sub(int n, const float* a, const float* b, float* out, cudaStream_t s);
+cudaError_t mjb_launch_pack(int B, int nq, int nv, int nbody, const float* qpos, const float* qvel, const float* cfrc, const float* qfa, const int* bodies,
+                            int nsel, int dof_lo, int ndof, int stride, float* out, cudaStream_t s);
 cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
 cudaError_t mjb_launch_ray(int B, int nray, const int* env_model, const int* geom_base, const int* geom_count, const float* ginfo, const float* gpose,
                            int ng_max, const float* pnt, const float* vec, float* dist, int* geomid, cudaStream_t s);
@@ -910,32 +912,27 @@ int Engine::pack_spec(const int* body_ids, int nsel, int dof_lo, int ndof) {
   return pack_stride_;
 }
 
-int Engine::get_pack(float* out) {
+int Engine::pack_device(float** out_dev) {
   if (pack_stride_ < 0) return -1;
+  if (!cfg_.record) throw std::runtime_error("get_pack needs the recorded cfrc_ext / qfrc_actuator (engine config record = 1)");
   const Model& m = *models_[0];
-  std::vector<float> qp(tot_q_), qv(tot_v_);
-  get_state(qp.data(), qv.data());
-  int n = 0;
-  const float* cf = get_host("cfrc_ext", &n);
-  std::vector<float> cfrc(cf, cf + n);
-  const float* qa = get_host("qfrc_actuator", &n);
-  for (int e = 0; e < B_; e++) {
-    float* row = out + (size_t)e * pack_stride_;
-    std::memcpy(row, &qp[(size_t)e * m.nq], sizeof(float) * m.nq);
-    std::memcpy(row + m.nq, &qv[(size_t)e * m.nv], sizeof(float) * m.nv);
-    for (size_t k = 0; k < pack_bodies_.size(); k++) {
-      const float* f = &cfrc[((size_t)e * m.nbody + pack_bodies_[k]) * 6 + 3];
-      row[m.nq + m.nv + k] = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
-    }
-    float s2 = 0, s1 = 0;
-    for (int d = pack_dof_lo_; d < pack_dof_lo_ + pack_ndof_; d++) {
-      float v = qa[(size_t)e * m.nv + d];
-      s2 += v * v;
-      s1 += std::fabs(v);
-    }
-    row[m.nq + m.nv + pack_bodies_.size()] = s2;
-    row[m.nq + m.nv + pack_bodies_.size() + 1] = s1;
-  }
+  const size_t need = (size_t)B_ * pack_stride_;
+  if (d_pack_.n < need) d_pack_.alloc(need);
+  std::vector<int> bodies(pack_bodies_.begin(), pack_bodies_.end());
+  if (bodies.empty()) bodies.push_back(0);
+  d_pack_bodies_.upload(bodies, stream_);
+  check(mjb_launch_pack(B_, m.nq, m.nv, m.nbody, qpos_.p, qvel_.p, rec_cfrc_.p, rec_qfa_.p, d_pack_bodies_.p, (int)pack_bodies_.size(), pack_dof_lo_,
+                        pack_ndof_, pack_stride_, d_pack_.p, stream_),
+        "pack kernel");
+  if (out_dev) *out_dev = d_pack_.p;
+  return 0;
+}
+
+int Engine::get_pack(float* out) {
+  float* dev = nullptr;
+  if (pack_device(&dev) != 0) return -1;
+  check(cudaMemcpyAsync(out, dev, sizeof(float) * (size_t)B_ * pack_stride_, cudaMemcpyDeviceToHost, stream_), "pack copy");
+  sync();
   return 0;
 }
 

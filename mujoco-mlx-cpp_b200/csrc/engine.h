@@ -153,6 +153,9 @@ class Engine {
 
   int pack_spec(const int* body_ids, int nsel, int dof_lo, int ndof);
   int get_pack(float* out);
+  // Runs the pack kernel on the sim's stream and returns the device buffer
+  // (num_envs x stride floats, valid until the next pack call).
+  int pack_device(float** out_dev);
   int raycast(const float* pnt, const float* vec, int nray, int bodyexclude, const unsigned char* geomgroup, int flg_static, float* dist, int* geomid);
 
  private:

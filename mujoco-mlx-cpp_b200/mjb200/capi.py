@@ -86,6 +86,7 @@ def _load():
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "mjb200_batched_get_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
+        "mjb200_batched_pack_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
         "mjb200_batched_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p]),
         "mjb200_batched_step_warmstart": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
@@ -339,6 +340,28 @@ class BatchedSim:
     def step_warmstart(self, qacc_ptr: int, n: int = 1):
         if lib.mjb200_batched_step_warmstart(self.handle, C.c_void_p(qacc_ptr), n) != 0:
             raise RuntimeError(last_error())
+
+    # ---- packed read-back
+    def set_pack_spec(self, body_ids, dof_lo: int, ndof: int) -> int:
+        b = np.ascontiguousarray(body_ids, np.int32)
+        stride = lib.mjmlx_batched_set_pack_spec(self.handle, _ip(b), len(b), dof_lo, ndof)
+        if stride < 0:
+            raise RuntimeError("set_pack_spec: " + last_error())
+        self.pack_stride = stride
+        return stride
+
+    def get_pack(self):
+        out = np.zeros((self.num_envs, self.pack_stride), np.float32)
+        if lib.mjmlx_batched_get_pack(self.handle, _fp(out)) != 0:
+            raise RuntimeError("get_pack: " + last_error())
+        return out
+
+    def pack_device(self) -> int:
+        """Device pointer of the packed rows (num_envs x stride floats)."""
+        p = C.c_void_p()
+        if lib.mjb200_batched_pack_device(self.handle, C.byref(p)) != 0:
+            raise RuntimeError("pack_device: " + last_error())
+        return p.value
 
     def raycast(self, pnt, vec, bodyexclude: int = -1, geomgroup=None, flg_static: int = 1):
         """Rays pnt/vec [num_envs, nray, 3] (world frame, per env) against each

@@ -272,3 +272,37 @@ def test_condim_single_step_parity(condim):
                 errs.append(rel_err(g["vec"][e, 2, : om.nv], o[e]["qacc"]))
         errs = np.array(errs)
         assert np.median(errs) <= 1e-4 and errs.max() <= 2e-3, (condim, np.median(errs), errs.max())
+
+
+def test_packed_readback_device_and_host(quad_model):
+    """Packed rows (reference: mjmlx_batched_get_pack) assembled by the pack
+    kernel equal the same quantities read back separately, and the device
+    buffer (no host copy) holds the same rows."""
+    B = 256
+    sim = mjb200.BatchedSim(quad_model, B)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=71)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    for c in range(10):
+        sim.step(mjb200.models.quadruped_controls_fast(B, c, seed=72).astype(np.float32), 4)
+    feet = [4, 7, 10, 13]
+    stride = sim.set_pack_spec(feet, 6, 12)
+    assert stride == 19 + 18 + 4 + 2
+    packed = sim.get_pack()
+    qp, qv = sim.state()
+    cf = sim.get("cfrc_ext").reshape(B, -1, 6)
+    qa = sim.get("qfrc_actuator").reshape(B, -1)
+    want = np.concatenate([qp, qv, np.linalg.norm(cf[:, feet, 3:], axis=2), (qa[:, 6:18] ** 2).sum(1, keepdims=True),
+                           np.abs(qa[:, 6:18]).sum(1, keepdims=True)], axis=1)
+    np.testing.assert_allclose(packed, want, rtol=1e-5, atol=1e-5)
+    assert (packed[:, 37:41] > 0).any()          # some feet carry load
+    ptr = sim.pack_device()
+    sim.sync()
+    assert ptr != 0
+    try:
+        from cuda.bindings import runtime as rt
+    except ImportError:  # older cuda-python layout
+        from cuda import cudart as rt
+    host = np.zeros((B, stride), np.float32)
+    err, = rt.cudaMemcpy(host.ctypes.data, ptr, host.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert int(err) == 0
+    np.testing.assert_array_equal(host, packed)
