@@ -15,9 +15,11 @@ namespace mjbdev {
 
 // Cholesky of the n x n SPD matrix A (row-major, lower triangle used, in
 // place: L below the diagonal, L_jj on it); idiag[j] = 1 / L_jj.
-// Right-looking: after column k is scaled, each lane updates its own rows of
-// the trailing block with independent FMAs (no long dependency chains).
-__device__ __noinline__ void d_chol(float* A, int n, int lane, float* idiag) {
+// Right-looking: after column k is scaled, the m(m+1)/2 entries of the
+// trailing lower triangle (m = n - k - 1) are spread evenly over the lanes,
+// so every lane does about m^2 / 64 independent updates per step instead of
+// the lane owning the last row doing m of them in sequence.
+__device__ __noinline__ void d_chol_smem(float* A, int n, int lane, float* idiag) {
 #pragma unroll 1
   for (int k = 0; k < n; k++) {
     float d = sqrtf(fmaxf(A[k * n + k], 1e-30f));
@@ -30,24 +32,72 @@ __device__ __noinline__ void d_chol(float* A, int n, int lane, float* idiag) {
       idiag[k] = id;
     }
     __syncwarp();
-#pragma unroll 1
-    for (int i = k + 1 + lane; i < n; i += 32) {
-      float* ri = A + i * n;
-      const float lik = ri[k];
-      int j = k + 1;
-#pragma unroll 1
-      for (; j + 3 <= i; j += 4) {
-        float l0 = A[j * n + k], l1 = A[(j + 1) * n + k], l2 = A[(j + 2) * n + k], l3 = A[(j + 3) * n + k];
-        ri[j] -= lik * l0;
-        ri[j + 1] -= lik * l1;
-        ri[j + 2] -= lik * l2;
-        ri[j + 3] -= lik * l3;
-      }
-#pragma unroll 1
-      for (; j <= i; j++) ri[j] -= lik * A[j * n + k];
+    const int m = n - k - 1, T = m * (m + 1) / 2, k1 = k + 1;
+#pragma unroll 2
+    for (int t = lane; t < T; t += 32) {
+      // entry t of the trailing lower triangle in row-major order: row r with
+      // r (r + 1) / 2 <= t < (r + 1) (r + 2) / 2, column t - r (r + 1) / 2
+      int r = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+      if ((r + 1) * (r + 2) / 2 <= t) r++;
+      else if (r * (r + 1) / 2 > t) r--;
+      const int c = t - r * (r + 1) / 2;
+      const int i = k1 + r, j = k1 + c;
+      A[i * n + j] -= A[i * n + k] * A[j * n + k];
     }
     __syncwarp();
   }
+}
+
+// Cholesky for n <= 32 with the pivot column in registers: lane i holds
+// A[i][k] of the current column k, the pivot comes from lane k by shuffle,
+// each l_jk is broadcast by shuffle to the rows below it, and lane i keeps
+// its updated A[i][k+1] in a register for the next step.  Same arithmetic in
+// the same order as d_chol_smem (bitwise identical factors), with the pivot
+// and column round trips through shared memory and two warp barriers per
+// step removed.
+__device__ __noinline__ void d_chol_reg(float* A, int n, int lane, float* idiag) {
+  const bool own = lane < n;
+  float c = own ? A[lane * n] : 0.f;
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    const float akk = __shfl_sync(FULL_MASK, c, k);
+    const float d = sqrtf(fmaxf(akk, 1e-30f)), id = 1.f / d;
+    const bool below = own && lane > k;
+    const float l = below ? c * id : 0.f;
+    if (lane == k) {
+      A[k * n + k] = d;
+      idiag[k] = id;
+    }
+    if (below) A[lane * n + k] = l;
+    float nc = below ? A[lane * n + k + 1] : 0.f;
+    const float l1 = __shfl_sync(FULL_MASK, l, (k + 1) & 31);
+    if (below) nc -= l * l1;
+    int j = k + 2;
+#pragma unroll 1
+    for (; j + 3 < n; j += 4) {
+      const float a0 = __shfl_sync(FULL_MASK, l, j), a1 = __shfl_sync(FULL_MASK, l, j + 1);
+      const float a2 = __shfl_sync(FULL_MASK, l, j + 2), a3 = __shfl_sync(FULL_MASK, l, j + 3);
+      if (own) {
+        float* r = A + lane * n;
+        if (lane >= j) r[j] -= l * a0;
+        if (lane >= j + 1) r[j + 1] -= l * a1;
+        if (lane >= j + 2) r[j + 2] -= l * a2;
+        if (lane >= j + 3) r[j + 3] -= l * a3;
+      }
+    }
+#pragma unroll 1
+    for (; j < n; j++) {
+      const float a0 = __shfl_sync(FULL_MASK, l, j);
+      if (own && lane >= j) A[lane * n + j] -= l * a0;
+    }
+    c = nc;
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void d_chol(float* A, int n, int lane, float* idiag) {
+  if (n <= 32) d_chol_reg(A, n, lane, idiag);
+  else d_chol_smem(A, n, lane, idiag);
 }
 
 // x := (L L')^-1 x.  The running vector lives in registers (element i on lane
