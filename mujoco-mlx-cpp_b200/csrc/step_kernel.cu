@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
 // Geom poses of every env at its current qpos (kinematics only), for ray
 // casting: gpose[env][g][12] = world position (3), rotation matrix (9, row
 // major).  One warp per env; the workspace layout is the step kernel's.
-__global__ void __launch_bounds__(256) mjb_geom_pose_kernel(StepParams P, float* gpose, int ng_max) {
+__global__ void __launch_bounds__(512) mjb_geom_pose_kernel(StepParams P, float* gpose, int ng_max) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
   int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
   float* ws = mjb_smem + W * P.desc_words + warp * P.ws_stride;

@@ -106,3 +106,19 @@ def test_raycast_mixed_models_match_oracle():
             e += 1
         o += m.nq * n
     assert hits > B * nray // 4
+
+
+def test_raycast_with_16_warp_ctas(quad_model):
+    """The geom-pose pass runs with the sim's launch shape, including the
+    largest lockstep CTA (16 warps)."""
+    B = 48
+    sim = mjb200.BatchedSim(quad_model, B, warps_per_block=16)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=57)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    rng = np.random.default_rng(3)
+    pnt, vec = _rays(q, 8, rng)
+    dist, gid = sim.raycast(pnt, vec)
+    ref = mjb200.BatchedSim(quad_model, B)
+    ref.set_state(q.astype(np.float32), v.astype(np.float32))
+    d2, g2 = ref.raycast(pnt, vec)
+    assert np.array_equal(gid, g2) and np.array_equal(dist, d2)
