@@ -305,3 +305,49 @@ def random_controls(model, num_envs: int, step: int, seed: int):
     r = joint_ranges(model)
     g = np.random.Generator(np.random.Philox(key=seed, counter=step))
     return r[:, 0] + (r[:, 1] - r[:, 0]) * g.random((num_envs, len(r)))
+
+
+# ---------------------------------------------------------------- hinge chains
+
+CHAIN_LINK = 0.1
+
+
+def chain_xml(n: int, cfg: str, iterations: int = 50) -> str:
+    """Pendulum chain of n hinge links (alternating y / x axes, capsules of
+    0.1 m, joint damping 0.02) for robustness sweeps over the dof count, in
+    the spirit of the reference's tests/test_robustness.cpp.  cfg:
+    "free" (no collision pairs), "limit" (joint limits +-0.35 rad), "floss"
+    (frictionloss 0.05), "contact" (floor touched when the first joint swings
+    1.2 rad), "all" (limits, frictionloss and contact)."""
+    H = n * CHAIN_LINK + 0.05
+    touch = H - n * CHAIN_LINK * math.cos(1.2) - 0.004
+    floor_z = touch if cfg in ("contact", "all") else -50.0
+    floor_col = ' contype="0" conaffinity="0"' if cfg == "free" else ""
+    jattr = ""
+    if cfg in ("limit", "all"):
+        jattr += ' limited="true" range="-0.35 0.35"'
+    if cfg in ("floss", "all"):
+        jattr += ' frictionloss="0.05"'
+    gcol = ' contype="0" conaffinity="0"' if cfg == "free" else ' contype="1" conaffinity="1"'
+    body = []
+    for i in range(n):
+        axis = "1 0 0" if i % 2 else "0 1 0"
+        z = H if i == 0 else -CHAIN_LINK
+        body.append(f'<body pos="0 0 {z:.4f}"><joint name="j{i}" type="hinge" axis="{axis}" damping="0.02"{jattr}/>'
+                    f'<geom type="capsule" fromto="0 0 0 0 0 {-CHAIN_LINK}" size="0.02" density="500"{gcol}/>')
+    return (f'<mujoco model="chain{n}_{cfg}"><compiler angle="radian"/>'
+            f'<option timestep="0.002" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            f'<worldbody><geom type="plane" size="5 5 0.1" pos="0 0 {floor_z:.4f}"{floor_col}/>'
+            + "".join(body) + "</body>" * n + "</worldbody></mujoco>")
+
+
+def chain_state(n: int, cfg: str, num_envs: int, seed: int):
+    """Random joint angles N(0, 0.5) (beyond the limits for some envs), the
+    first joint swung by 1.2 rad for contact configurations, random joint
+    velocities N(0, 0.5)."""
+    g = np.random.Generator(np.random.Philox(key=seed))
+    q = g.normal(0.0, 0.5, size=(num_envs, n))
+    if cfg in ("contact", "all"):
+        q[:, 0] += 1.2
+    v = g.normal(0.0, 0.5, size=(num_envs, n))
+    return q, v
