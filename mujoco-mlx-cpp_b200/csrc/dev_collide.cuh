@@ -257,6 +257,151 @@ __device__ __forceinline__ void c_make_frame(const float n_in[3], float* frame) 
   for (int k = 0; k < 3; k++) { frame[k] = n[k]; frame[3 + k] = t1[k]; frame[6 + k] = t2[k]; }
 }
 
+// Box-box by separating axes (the 15 face / edge-cross axes), as in the
+// oracle: face axes are kept unless an edge axis penetrates less by more
+// than 5 % (and 1e-5 of the box scale).  Face case: the incident face is
+// clipped against the side planes of the reference face; points below the
+// reference face plus the margin become contacts (midpoint between the point
+// and its projection), at most 4, chosen as the extremes along the reference
+// face's diagonals.  Edge case: one contact at the closest points of the two
+// supporting edges.  Normal from box 1 to box 2.
+__device__ __forceinline__ float box_radius(const float (*ax)[3], const float* h, const float* L) {
+  return h[0] * fabsf(dot3(ax[0], L)) + h[1] * fabsf(dot3(ax[1], L)) + h[2] * fabsf(dot3(ax[2], L));
+}
+
+__device__ __noinline__ int c_box_box(const float* c1, const float* R1, const float* h1, const float* c2, const float* R2, const float* h2, float margin,
+                                      DCon* out) {
+  float A[3][3], B[3][3], T[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      A[k][r] = R1[3 * r + k];
+      B[k][r] = R2[3 * r + k];
+    }
+    T[k] = c2[k] - c1[k];
+  }
+  float best_face = -1e30f, best_edge = -1e30f, Le[3] = {0.f, 0.f, 0.f};
+  int face = -1, ei = -1, ej = -1;
+#pragma unroll 1
+  for (int i = 0; i < 6; i++) {
+    const float* L = i < 3 ? A[i] : B[i - 3];
+    const float dd = fabsf(dot3(T, L)) - box_radius(A, h1, L) - box_radius(B, h2, L);
+    if (dd > margin) return 0;
+    if (dd > best_face) { best_face = dd; face = i; }
+  }
+#pragma unroll 1
+  for (int i = 0; i < 3; i++) {
+#pragma unroll 1
+    for (int j = 0; j < 3; j++) {
+      float L[3];
+      cross3(A[i], B[j], L);
+      const float len = norm3(L);
+      if (len < 1e-6f) continue;
+      for (int k = 0; k < 3; k++) L[k] /= len;
+      const float dd = fabsf(dot3(T, L)) - box_radius(A, h1, L) - box_radius(B, h2, L);
+      if (dd > margin) return 0;
+      if (dd > best_edge) { best_edge = dd; ei = i; ej = j; for (int k = 0; k < 3; k++) Le[k] = L[k]; }
+    }
+  }
+  const float scale = h1[0] + h1[1] + h1[2] + h2[0] + h2[1] + h2[2];
+  if (ei >= 0 && best_edge - best_face > 0.05f * fabsf(best_face) + 1e-5f * scale) {
+    float L[3] = {Le[0], Le[1], Le[2]};
+    if (dot3(T, L) < 0.f) for (int k = 0; k < 3; k++) L[k] = -L[k];
+    float ca[3] = {c1[0], c1[1], c1[2]}, cb[3] = {c2[0], c2[1], c2[2]}, a0[3], a1[3], b0[3], b1[3], xa[3], xb[3];
+    for (int m = 0; m < 3; m++) {
+      if (m != ei) { const float sg = dot3(A[m], L) >= 0.f ? 1.f : -1.f; for (int k = 0; k < 3; k++) ca[k] += sg * h1[m] * A[m][k]; }
+      if (m != ej) { const float sg = dot3(B[m], L) >= 0.f ? 1.f : -1.f; for (int k = 0; k < 3; k++) cb[k] -= sg * h2[m] * B[m][k]; }
+    }
+    for (int k = 0; k < 3; k++) {
+      a0[k] = ca[k] - h1[ei] * A[ei][k]; a1[k] = ca[k] + h1[ei] * A[ei][k];
+      b0[k] = cb[k] - h2[ej] * B[ej][k]; b1[k] = cb[k] + h2[ej] * B[ej][k];
+    }
+    c_segment_segment(a0, a1, b0, b1, xa, xb);
+    for (int k = 0; k < 3; k++) { out->pos[k] = 0.5f * (xa[k] + xb[k]); out->n[k] = L[k]; }
+    out->dist = best_edge;
+    return 1;
+  }
+  const bool refA = face < 3;
+  const int ax = face % 3;
+  const float (*Rf)[3] = refA ? A : B;
+  const float (*Ri)[3] = refA ? B : A;
+  const float *cf = refA ? c1 : c2, *ci = refA ? c2 : c1, *hf = refA ? h1 : h2, *hi = refA ? h2 : h1;
+  const float Tri[3] = {ci[0] - cf[0], ci[1] - cf[1], ci[2] - cf[2]};
+  const float sn = dot3(Tri, Rf[ax]) >= 0.f ? 1.f : -1.f;
+  const float n[3] = {sn * Rf[ax][0], sn * Rf[ax][1], sn * Rf[ax][2]};
+  int kf = 0;
+  float bestk = -1.f;
+  for (int k = 0; k < 3; k++) { const float a = fabsf(dot3(Ri[k], n)); if (a > bestk) { bestk = a; kf = k; } }
+  const float s = dot3(Ri[kf], n) > 0.f ? -1.f : 1.f;
+  const int k1 = (kf + 1) % 3, k2 = (kf + 2) % 3;
+  float poly[8][3], tmp[8][3];
+  int np = 4;
+  const float sg1[4] = {1.f, -1.f, -1.f, 1.f}, sg2[4] = {1.f, 1.f, -1.f, -1.f};
+  for (int v = 0; v < 4; v++)
+    for (int k = 0; k < 3; k++) poly[v][k] = ci[k] + s * hi[kf] * Ri[kf][k] + sg1[v] * hi[k1] * Ri[k1][k] + sg2[v] * hi[k2] * Ri[k2][k];
+  const int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
+#pragma unroll 1
+  for (int pl = 0; pl < 4 && np > 0; pl++) {
+    const float* dir = pl < 2 ? Rf[a1] : Rf[a2];
+    const float sgn = (pl % 2) ? -1.f : 1.f, ext = pl < 2 ? hf[a1] : hf[a2];
+    int nt = 0;
+#pragma unroll 1
+    for (int v = 0; v < np; v++) {
+      const float* P = poly[v];
+      const float* Q = poly[(v + 1) % np];
+      const float dp = sgn * ((P[0] - cf[0]) * dir[0] + (P[1] - cf[1]) * dir[1] + (P[2] - cf[2]) * dir[2]) - ext;
+      const float dq = sgn * ((Q[0] - cf[0]) * dir[0] + (Q[1] - cf[1]) * dir[1] + (Q[2] - cf[2]) * dir[2]) - ext;
+      if (dp <= 0.f && nt < 8) { for (int k = 0; k < 3; k++) tmp[nt][k] = P[k]; nt++; }
+      if ((dp <= 0.f) != (dq <= 0.f) && nt < 8) {
+        const float t = dp / (dp - dq);
+        for (int k = 0; k < 3; k++) tmp[nt][k] = P[k] + t * (Q[k] - P[k]);
+        nt++;
+      }
+    }
+    np = nt;
+    for (int v = 0; v < np; v++)
+      for (int k = 0; k < 3; k++) poly[v][k] = tmp[v][k];
+  }
+  const float refc[3] = {cf[0] + hf[ax] * n[0], cf[1] + hf[ax] * n[1], cf[2] + hf[ax] * n[2]};
+  float dep[8], uu[8], vv[8];
+  int idx[8], nc = 0;
+  for (int v = 0; v < np; v++) {
+    const float dd = (poly[v][0] - refc[0]) * n[0] + (poly[v][1] - refc[1]) * n[1] + (poly[v][2] - refc[2]) * n[2];
+    if (!(dd < margin)) continue;
+    dep[nc] = dd;
+    uu[nc] = (poly[v][0] - cf[0]) * Rf[a1][0] + (poly[v][1] - cf[1]) * Rf[a1][1] + (poly[v][2] - cf[2]) * Rf[a1][2];
+    vv[nc] = (poly[v][0] - cf[0]) * Rf[a2][0] + (poly[v][1] - cf[1]) * Rf[a2][1] + (poly[v][2] - cf[2]) * Rf[a2][2];
+    idx[nc] = v;
+    nc++;
+  }
+  int sel[4], ns = 0;
+  if (nc <= 4) {
+    for (int v = 0; v < nc; v++) sel[ns++] = v;
+  } else {
+    const float du[4] = {1.f, 1.f, -1.f, -1.f}, dv[4] = {1.f, -1.f, 1.f, -1.f};
+    for (int q = 0; q < 4; q++) {
+      int bi = 0;
+      for (int v = 1; v < nc; v++)
+        if (du[q] * uu[v] + dv[q] * vv[v] > du[q] * uu[bi] + dv[q] * vv[bi]) bi = v;
+      bool dup = false;
+      for (int t = 0; t < ns; t++) dup |= sel[t] == bi;
+      if (!dup) sel[ns++] = bi;
+    }
+  }
+  const float nrm = refA ? 1.f : -1.f;
+  for (int t = 0; t < ns; t++) {
+    const int v = idx[sel[t]];
+    const float dd = dep[sel[t]];
+    for (int k = 0; k < 3; k++) {
+      out[t].pos[k] = poly[v][k] - 0.5f * dd * n[k];
+      out[t].n[k] = nrm * n[k];
+    }
+    out[t].dist = dd;
+  }
+  return ns;
+}
+
 // Narrowphase of one pair; returns the number of contacts (<= 4), or -1 for a
 // type combination without a collider.
 __device__ __noinline__ int c_collide_pair(int t1, int t2, const float* c1, const float* R1, const float* s1, float rb1, const float* c2, const float* R2,
@@ -291,6 +436,7 @@ __device__ __noinline__ int c_collide_pair(int t1, int t2, const float* c1, cons
   }
   if (t1 == 2 && t2 == 6) return c_sphere_box(c1, s1[0], c2, R2, s2, margin, cs);
   if (t1 == 3 && t2 == 6) return c_capsule_box(c1, R1, s1, c2, R2, s2, margin, cs);
+  if (t1 == 6 && t2 == 6) return c_box_box(c1, R1, s1, c2, R2, s2, margin, cs);
   return -1;
 }
 

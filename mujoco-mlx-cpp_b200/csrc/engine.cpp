@@ -70,6 +70,7 @@ bool pair_supported(int t1, int t2) {
   if (t1 == GEOM_PLANE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX || t2 == GEOM_ELLIPSOID || t2 == GEOM_CYLINDER || t2 == GEOM_MESH;
   if (t1 == GEOM_SPHERE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
   if (t1 == GEOM_CAPSULE) return t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
+  if (t1 == GEOM_BOX) return t2 == GEOM_BOX;
   return false;
 }
 

@@ -1253,6 +1253,7 @@ int pair_max_contacts(int t1, int t2) {
     if (t2 == GEOM_BOX) return 4;
     return 1;
   }
+  if (t1 == GEOM_BOX && t2 == GEOM_BOX) return 4;
   return 1;
 }
 

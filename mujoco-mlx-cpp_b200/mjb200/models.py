@@ -221,9 +221,9 @@ ARM_FINGER_RANGE = (0.0, 0.04)
 def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.005) -> str:
     """7-hinge arm on a table with a two-finger gripper (box palm, slide
     fingers) and a free box on the table.  The table top is the plane z = 0;
-    the arm does not collide with itself; the fingers are capsules and the
-    palm box does not touch the object (box-box and cylinder-box contacts are
-    not in this build's narrowphase).  nq 7 + 2 + 7 = 16, nv 15, nu 9."""
+    the arm does not collide with itself; the palm box touches the object
+    (box-box); the fingers are capsules (cylinder-box contacts are not in this
+    build's narrowphase).  nq 7 + 2 + 7 = 16, nv 15, nu 9."""
     axes = ("0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1")
     links = []
     depth = 0
@@ -237,7 +237,7 @@ def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.0
         depth += 1
     hand = f"""
 {'  ' * 10}<body name="hand" pos="0 0 {prev_len:.3f}">
-{'  ' * 11}<geom name="palm" type="box" size="0.04 0.06 0.015" pos="0 0 0.015" mass="0.4" contype="4" conaffinity="0"/>
+{'  ' * 11}<geom name="palm" type="box" size="0.04 0.06 0.015" pos="0 0 0.015" mass="0.4" contype="2" conaffinity="1"/>
 {'  ' * 11}<body name="finger_l" pos="0 0.02 0.03">
 {'  ' * 12}<joint name="finger_l_j" type="slide" axis="0 1 0" range="{ARM_FINGER_RANGE[0]} {ARM_FINGER_RANGE[1]}" armature="0.01" damping="2"/>
 {'  ' * 12}<geom name="finger_l_g" type="capsule" fromto="0 0 0 0 0 0.07" size="0.012" mass="0.05" contype="2" conaffinity="1"/>
@@ -351,3 +351,43 @@ def chain_state(n: int, cfg: str, num_envs: int, seed: int):
         q[:, 0] += 1.2
     v = g.normal(0.0, 0.5, size=(num_envs, n))
     return q, v
+
+
+# ---------------------------------------------------------------- box pile
+
+def box_pile_xml(nbox: int = 4, seed: int = 0, iterations: int = 30) -> str:
+    """nbox free boxes (half sizes U[0.04, 0.12], masses U[0.2, 1.0] kg)
+    stacked loosely above a plane, for box-box / box-plane contacts."""
+    g = np.random.Generator(np.random.Philox(key=seed))
+    bodies = []
+    z = 0.0
+    for i in range(nbox):
+        h = g.uniform(0.04, 0.12, size=3)
+        z += h[2] + 0.01
+        x, y = g.uniform(-0.05, 0.05, size=2)
+        bodies.append(f'<body name="box{i}" pos="{x:.4f} {y:.4f} {z:.4f}"><freejoint/>'
+                      f'<geom type="box" size="{h[0]:.4f} {h[1]:.4f} {h[2]:.4f}" mass="{g.uniform(0.2, 1.0):.3f}"/></body>')
+        z += h[2]
+    return (f'<mujoco model="box_pile{nbox}"><compiler angle="radian"/>'
+            f'<option timestep="0.005" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            '<default><geom condim="3" friction="0.8 0.005 0.0001"/></default>'
+            '<worldbody><geom name="floor" type="plane" size="0 0 1"/>' + "".join(bodies) + '</worldbody></mujoco>')
+
+
+def box_pile_state(model, num_envs: int, seed: int):
+    """qpos0 with each box's position jittered by U[-0.03, 0.03] m and its
+    orientation rotated by up to 0.4 rad about a random axis."""
+    d = model.dump()
+    g = np.random.Generator(np.random.Philox(key=seed))
+    q0 = d["qpos0"].astype(np.float64)
+    nb = model.nq // 7
+    qpos = np.tile(q0, (num_envs, 1))
+    for b in range(nb):
+        a = 7 * b
+        qpos[:, a:a + 3] += g.uniform(-0.03, 0.03, size=(num_envs, 3))
+        ax = g.normal(size=(num_envs, 3))
+        ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+        ang = g.uniform(0.0, 0.4, size=num_envs)
+        qpos[:, a + 3] = np.cos(ang / 2)
+        qpos[:, a + 4:a + 7] = ax * np.sin(ang / 2)[:, None]
+    return qpos, np.zeros((num_envs, model.nv))

@@ -7,7 +7,9 @@
  *   plane-sphere 1, plane-capsule 2 (end caps), plane-box <= 4 (deepest
  *   corners), plane-ellipsoid/cylinder/mesh 1 (support point),
  *   sphere-sphere 1, sphere-capsule 1, capsule-capsule 1 (closest segment
- *   points), sphere-box 1, capsule-box 1 (deepest axis point, convex search).
+ *   points), sphere-box 1, capsule-box 1 (deepest axis point, convex search),
+ *   box-box <= 4 (separating axes; clipped face contacts or one edge-edge
+ *   contact).
  * Contact normals point from geom1 to geom2; dist < 0 is penetration; the
  * contact position is the midpoint between the two surfaces.  The tangent
  * frame is built from the normal by projecting (0,1,0), or (0,0,1) when
@@ -271,6 +273,137 @@ static int capsule_box(const double* c, const double* R, const double* sz, const
   return sphere_box(s, sz[0], bc, BR, bh, margin, out);
 }
 
+/* Box-box by separating axes.  The 15 axes (3 + 3 face normals, 9 edge
+ * cross products) give the least-penetrating axis; a face axis is kept
+ * unless an edge axis penetrates less by more than 5 % (and 1e-5 of the box
+ * scale).  Face case: the incident face (the face of the other box most
+ * anti-parallel to the reference normal) is clipped against the side planes
+ * of the reference face; points below the reference face plus the margin
+ * become contacts at the midpoint between the point and its projection,
+ * reduced to at most 4 by taking the extremes along the reference face's
+ * diagonals.  Edge case: one contact at the closest points of the two
+ * supporting edges.  Normal from box 1 to box 2. */
+static double box_radius(const double (*ax)[3], const double* h, const double* L) {
+  return h[0] * fabs(o_dot3(ax[0], L)) + h[1] * fabs(o_dot3(ax[1], L)) + h[2] * fabs(o_dot3(ax[2], L));
+}
+
+static int box_box(const double* c1, const double* R1, const double* h1, const double* c2, const double* R2, const double* h2, double margin, Con* out) {
+  double A[3][3], B[3][3], T[3];
+  for (int k = 0; k < 3; k++)
+    for (int r = 0; r < 3; r++) { A[k][r] = R1[3 * r + k]; B[k][r] = R2[3 * r + k]; }
+  for (int k = 0; k < 3; k++) T[k] = c2[k] - c1[k];
+  double best_face = -1e300, best_edge = -1e300, Le[3] = {0, 0, 0};
+  int face = -1, ei = -1, ej = -1;
+  for (int i = 0; i < 6; i++) {
+    const double* L = i < 3 ? A[i] : B[i - 3];
+    double dd = fabs(o_dot3(T, L)) - box_radius((const double(*)[3])A, h1, L) - box_radius((const double(*)[3])B, h2, L);
+    if (dd > margin) return 0;
+    if (dd > best_face) { best_face = dd; face = i; }
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double L[3];
+      o_cross(A[i], B[j], L);
+      double len = o_norm3(L);
+      if (len < 1e-6) continue;
+      for (int k = 0; k < 3; k++) L[k] /= len;
+      double dd = fabs(o_dot3(T, L)) - box_radius((const double(*)[3])A, h1, L) - box_radius((const double(*)[3])B, h2, L);
+      if (dd > margin) return 0;
+      if (dd > best_edge) { best_edge = dd; ei = i; ej = j; for (int k = 0; k < 3; k++) Le[k] = L[k]; }
+    }
+  double scale = h1[0] + h1[1] + h1[2] + h2[0] + h2[1] + h2[2];
+  if (ei >= 0 && best_edge - best_face > 0.05 * fabs(best_face) + 1e-5 * scale) {
+    double L[3] = {Le[0], Le[1], Le[2]};
+    if (o_dot3(T, L) < 0) for (int k = 0; k < 3; k++) L[k] = -L[k];
+    double ca[3], cb[3], a0[3], a1[3], b0[3], b1[3], xa[3], xb[3];
+    for (int k = 0; k < 3; k++) { ca[k] = c1[k]; cb[k] = c2[k]; }
+    for (int m = 0; m < 3; m++) {
+      if (m != ei) { double sg = o_dot3(A[m], L) >= 0 ? 1 : -1; for (int k = 0; k < 3; k++) ca[k] += sg * h1[m] * A[m][k]; }
+      if (m != ej) { double sg = o_dot3(B[m], L) >= 0 ? 1 : -1; for (int k = 0; k < 3; k++) cb[k] -= sg * h2[m] * B[m][k]; }
+    }
+    for (int k = 0; k < 3; k++) {
+      a0[k] = ca[k] - h1[ei] * A[ei][k]; a1[k] = ca[k] + h1[ei] * A[ei][k];
+      b0[k] = cb[k] - h2[ej] * B[ej][k]; b1[k] = cb[k] + h2[ej] * B[ej][k];
+    }
+    segment_segment(a0, a1, b0, b1, xa, xb);
+    for (int k = 0; k < 3; k++) { out->pos[k] = 0.5 * (xa[k] + xb[k]); out->n[k] = L[k]; }
+    out->dist = best_edge;
+    return 1;
+  }
+  /* face case */
+  const int refA = face < 3, ax = face % 3;
+  const double (*Rf)[3] = refA ? (const double(*)[3])A : (const double(*)[3])B;
+  const double (*Ri)[3] = refA ? (const double(*)[3])B : (const double(*)[3])A;
+  const double *cf = refA ? c1 : c2, *ci = refA ? c2 : c1, *hf = refA ? h1 : h2, *hi = refA ? h2 : h1;
+  double Tri[3] = {ci[0] - cf[0], ci[1] - cf[1], ci[2] - cf[2]}, n[3];
+  double sn = o_dot3(Tri, Rf[ax]) >= 0 ? 1 : -1;
+  for (int k = 0; k < 3; k++) n[k] = sn * Rf[ax][k];
+  int kf = 0;
+  double bestk = -1;
+  for (int k = 0; k < 3; k++) { double a = fabs(o_dot3(Ri[k], n)); if (a > bestk) { bestk = a; kf = k; } }
+  double s = o_dot3(Ri[kf], n) > 0 ? -1 : 1;
+  int k1 = (kf + 1) % 3, k2 = (kf + 2) % 3;
+  double poly[16][3], tmp[16][3];
+  int np = 4;
+  const double sg1[4] = {1, -1, -1, 1}, sg2[4] = {1, 1, -1, -1};
+  for (int v = 0; v < 4; v++)
+    for (int k = 0; k < 3; k++) poly[v][k] = ci[k] + s * hi[kf] * Ri[kf][k] + sg1[v] * hi[k1] * Ri[k1][k] + sg2[v] * hi[k2] * Ri[k2][k];
+  const int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
+  /* clip against (p - cf).dir <= ext for dir in {u, -u, v, -v} */
+  for (int pl = 0; pl < 4 && np > 0; pl++) {
+    const double* dir = pl < 2 ? Rf[a1] : Rf[a2];
+    double sgn = (pl % 2) ? -1 : 1, ext = pl < 2 ? hf[a1] : hf[a2];
+    int nt = 0;
+    for (int v = 0; v < np; v++) {
+      const double* P = poly[v];
+      const double* Q = poly[(v + 1) % np];
+      double dp = sgn * ((P[0] - cf[0]) * dir[0] + (P[1] - cf[1]) * dir[1] + (P[2] - cf[2]) * dir[2]) - ext;
+      double dq = sgn * ((Q[0] - cf[0]) * dir[0] + (Q[1] - cf[1]) * dir[1] + (Q[2] - cf[2]) * dir[2]) - ext;
+      if (dp <= 0) { for (int k = 0; k < 3; k++) tmp[nt][k] = P[k]; nt++; }
+      if ((dp <= 0) != (dq <= 0)) {
+        double t = dp / (dp - dq);
+        for (int k = 0; k < 3; k++) tmp[nt][k] = P[k] + t * (Q[k] - P[k]);
+        nt++;
+      }
+    }
+    np = nt;
+    for (int v = 0; v < np; v++) for (int k = 0; k < 3; k++) poly[v][k] = tmp[v][k];
+  }
+  double refc[3];
+  for (int k = 0; k < 3; k++) refc[k] = cf[k] + hf[ax] * n[k];
+  double pts[16][3], dep[16], uu[16], vv[16];
+  int nc = 0;
+  for (int v = 0; v < np; v++) {
+    double dd = (poly[v][0] - refc[0]) * n[0] + (poly[v][1] - refc[1]) * n[1] + (poly[v][2] - refc[2]) * n[2];
+    if (!(dd < margin)) continue;
+    for (int k = 0; k < 3; k++) pts[nc][k] = poly[v][k] - 0.5 * dd * n[k];
+    dep[nc] = dd;
+    uu[nc] = (poly[v][0] - cf[0]) * Rf[a1][0] + (poly[v][1] - cf[1]) * Rf[a1][1] + (poly[v][2] - cf[2]) * Rf[a1][2];
+    vv[nc] = (poly[v][0] - cf[0]) * Rf[a2][0] + (poly[v][1] - cf[1]) * Rf[a2][1] + (poly[v][2] - cf[2]) * Rf[a2][2];
+    nc++;
+  }
+  int sel[4], ns = 0;
+  if (nc <= 4) {
+    for (int v = 0; v < nc; v++) sel[ns++] = v;
+  } else {
+    const double du[4] = {1, 1, -1, -1}, dv[4] = {1, -1, 1, -1};
+    for (int q = 0; q < 4; q++) {
+      int bi = 0;
+      for (int v = 1; v < nc; v++)
+        if (du[q] * uu[v] + dv[q] * vv[v] > du[q] * uu[bi] + dv[q] * vv[bi]) bi = v;
+      int dup = 0;
+      for (int t = 0; t < ns; t++) dup |= sel[t] == bi;
+      if (!dup) sel[ns++] = bi;
+    }
+  }
+  double nrm = refA ? 1 : -1;
+  for (int t = 0; t < ns; t++) {
+    for (int k = 0; k < 3; k++) { out[t].pos[k] = pts[sel[t]][k]; out[t].n[k] = nrm * n[k]; }
+    out[t].dist = dep[sel[t]];
+  }
+  return ns;
+}
+
 static int add_contacts(const OModel* m, OData* d, int pair, const Con* cs, int n) {
   const int* pi = &m->pair_int[6 * pair];
   const double* pr = &m->pair_real[16 * pair];
@@ -339,6 +472,7 @@ void oracle_collide(const OModel* m, OData* d) {
         n = sphere_sphere(x1, s1[0], x2, s2[0], margin, cs);
       } else if (t1 == 2 && t2 == 6) n = sphere_box(c1, s1[0], c2, R2, s2, margin, cs);
       else if (t1 == 3 && t2 == 6) n = capsule_box(c1, R1, s1, c2, R2, s2, margin, cs);
+      else if (t1 == 6 && t2 == 6) n = box_box(c1, R1, s1, c2, R2, s2, margin, cs);
       else { d->status |= ORACLE_UNSUPPORTED; continue; }
     }
     add_contacts(m, d, p, cs, n);

@@ -251,3 +251,62 @@ def test_ray_known_answers():
     inc[1] = 0
     t, g = env.ray([0, 0, 3], [0, 0, -1], inc)
     assert g == 0 and t == pytest.approx(3.0)               # sphere excluded: the plane
+
+
+def test_box_box_face_contact():
+    """A 0.2 x 0.1 x 0.1 (half sizes) box sunk 1 mm into a larger static box:
+    4 contacts at the small box's bottom corners, normal +z (geom 1 -> 2)."""
+    xml = wrap('<geom type="box" size="0.5 0.5 0.1" pos="0 0 0.1"/>'
+               '<body pos="0.05 -0.03 0.299"><freejoint/><geom type="box" size="0.2 0.1 0.1" mass="1"/></body>')
+    om, env = env_from_xml(xml)
+    env.step()
+    cons = env.contacts()
+    assert env.d.ncon == 4
+    for c in cons:
+        assert c[12] == pytest.approx(-0.001, abs=1e-9)
+        np.testing.assert_allclose(c[3:6], [0, 0, 1], atol=1e-12)
+        assert c[2] == pytest.approx(0.2 - 0.0005, abs=1e-9)
+    xy = sorted((round(c[0], 9), round(c[1], 9)) for c in cons)
+    assert xy == sorted([(round(0.05 + sx * 0.2, 9), round(-0.03 + sy * 0.1, 9)) for sx in (-1, 1) for sy in (-1, 1)])
+    assert env.d.nefc == 16
+
+
+def test_box_box_edge_contact_and_separation():
+    """Two boxes whose edges cross (rotated 45 deg about x and about y): one
+    edge-edge contact on the line between the centres; far apart: none."""
+    c, s = np.cos(np.pi / 8), np.sin(np.pi / 8)
+    h = 0.1 * np.sqrt(2)
+    gap = -0.002
+    xml = wrap(f'<geom type="box" size="0.1 0.1 0.1" quat="{c} {s} 0 0" pos="0 0 0"/>'
+               f'<body pos="0 0 {2 * h + gap}" quat="{c} 0 {s} 0"><freejoint/><geom type="box" size="0.1 0.1 0.1" mass="1"/></body>',
+               option='<option timestep="0.005" gravity="0 0 0"/>')
+    om, env = env_from_xml(xml)
+    env.step()
+    assert env.d.ncon == 1
+    con = env.contacts()[0]
+    assert con[12] == pytest.approx(gap, abs=1e-9)
+    np.testing.assert_allclose(con[3:6], [0, 0, 1], atol=1e-9)
+    np.testing.assert_allclose(con[0:3], [0, 0, h + gap / 2], atol=1e-9)
+    xml_far = xml.replace(f'pos="0 0 {2 * h + gap}"', 'pos="0 0 1"')
+    om, env = env_from_xml(xml_far)
+    env.step()
+    assert env.d.ncon == 0
+
+
+def test_box_stack_comes_to_rest():
+    m_ = 1.5
+    xml = wrap(PLANE + '<body pos="0 0 0.1"><freejoint/><geom type="box" size="0.3 0.3 0.1" mass="4"/></body>'
+                       f'<body pos="0.02 0.01 0.3"><freejoint/><geom type="box" size="0.15 0.1 0.1" mass="{m_}"/></body>')
+    om, env = env_from_xml(xml)
+    for _ in range(800):
+        env.step()
+    assert env.d.status == 0
+    assert abs(env.a["qvel"]).max() < 1e-4
+    types = env.efc()["type"]
+    # 4 floor contacts + 4 box-box contacts, all pyramidal
+    assert env.d.ncon == 8 and (types == 2).sum() == 32
+    cons = env.contacts()
+    bb = [i for i in range(8) if int(cons[i][14]) == 1 and int(cons[i][15]) == 2]
+    assert len(bb) == 4
+    rows = env.efc()["force"].reshape(-1, 4)
+    assert rows[bb].sum() == pytest.approx(m_ * G, rel=1e-3)
