@@ -103,6 +103,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def profile_issue_active():
+    """FP32 issue utilisation of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "mjb_step_kernel_quadruped.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("| smsp__issue_active |"):
+                    return float(line.split("|")[2].strip().split()[0]) / 100.0
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
 def profile_traffic_per_env_launch():
     """Per-env DRAM bytes of one step-kernel launch from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "mjb_step_kernel_quadruped.md")
@@ -337,7 +350,9 @@ def run_ours(args, world, rank, local):
     tr = profile_traffic_per_env_launch()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": (tr * B) if tr is not None else None, "kernel": "mjb_step_kernel", "kernel_ms": res["plain"]["kernel_ms"],
-                "algorithmic_bytes_per_launch": alg_bytes}
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "note": "latency / FP32-issue bound, not HBM bound: issue_active is the step kernel's measured issue utilisation (ncu)",
+                "issue_active": profile_issue_active()}
 
     if rank != 0:
         return
