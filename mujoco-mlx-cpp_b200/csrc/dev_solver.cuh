@@ -208,14 +208,50 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
   int nefc = 0;
   bool stop = false;
   if (m.disableflags & 1) return 0;
-  // --- frictionloss rows (static list)
-  if (!(m.disableflags & (1 << 2)) && m.nfloss > 0) {
-    int nf = m.nfloss;
-    if (nf > m.nefc_max) { nf = m.nefc_max; stop = true; }
+  // --- joint equality rows (static list): q1 - q1_0 = poly(q2 - q2_0)
+  // (reference: solver.hpp:259-289; bilateral rows, always in their
+  // quadratic zone)
+  if (!(m.disableflags & (1 << 1)) && m.neq > 0) {
+    int nq_ = m.neq;
+    if (nq_ > m.nefc_max) { nq_ = m.nefc_max; stop = true; }
     #pragma unroll 1
-    for (int r = E.lane; r < nf; r += 32) {
-      int dof = ldi(it, m.i_floss + r);
-      const float* f = ft + m.f_floss + 8 * r;
+    for (int r = E.lane; r < nq_; r += 32) {
+      const int d1 = ldi(it, m.i_eq + 4 * r), d2 = ldi(it, m.i_eq + 4 * r + 1);
+      const int qa1 = ldi(it, m.i_eq + 4 * r + 2), qa2 = ldi(it, m.i_eq + 4 * r + 3);
+      const float* f = ft + m.f_eq + 15 * r;
+      float poly = ldf(f, 2), dpoly = 0.f;
+      if (d2 >= 0) {
+        const float x = qpos[qa2] - ldf(f, 1);
+        poly = ldf(f, 2) + x * (ldf(f, 3) + x * (ldf(f, 4) + x * (ldf(f, 5) + x * ldf(f, 6))));
+        dpoly = ldf(f, 3) + x * (2.f * ldf(f, 4) + x * (3.f * ldf(f, 5) + x * 4.f * ldf(f, 6)));
+      }
+      const float pos = qpos[qa1] - ldf(f, 0) - poly;
+      const float vel = qvel[d1] - (d2 >= 0 ? dpoly * qvel[d2] : 0.f);
+      float si[5] = {ldf(f, 9), ldf(f, 10), ldf(f, 11), ldf(f, 12), ldf(f, 13)};
+      float k, b, imp;
+      impedance(m, ldf(f, 7), ldf(f, 8), si, pos, k, b, imp);
+      const float R = fmaxf((1.f - imp) / imp * ldf(f, 14), 1e-15f);
+      #pragma unroll 1
+      for (int c = 0; c < nv; c++) J[r * nv + c] = (c == d1 ? 1.f : 0.f) - (c == d2 ? dpoly : 0.f);
+      EfcRef e{efc + r, ne};
+      e[EFC_D] = 1.f / R;
+      e[EFC_AREF] = -b * vel - k * imp * pos;
+      e[EFC_FLOSS] = 0;
+      e[EFC_TYPE] = ROW_EQUALITY;
+      e[EFC_CON] = -1;
+    }
+    nefc = nq_;
+  }
+  // --- frictionloss rows (static list)
+  if (!stop && !(m.disableflags & (1 << 2)) && m.nfloss > 0) {
+    const int r0 = nefc;
+    int nf = m.nfloss;
+    if (r0 + nf > m.nefc_max) { nf = m.nefc_max - r0; stop = true; }
+    #pragma unroll 1
+    for (int q = E.lane; q < nf; q += 32) {
+      const int r = r0 + q;
+      int dof = ldi(it, m.i_floss + q);
+      const float* f = ft + m.f_floss + 8 * q;
       float si[5] = {ldf(f, 3), ldf(f, 4), ldf(f, 5), ldf(f, 6), ldf(f, 7)};
       float k, b, imp;
       impedance(m, ldf(f, 1), ldf(f, 2), si, 0.f, k, b, imp);
@@ -229,7 +265,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       e[EFC_TYPE] = ROW_FRICTION;
       e[EFC_CON] = -1;
     }
-    nefc = nf;
+    nefc = r0 + nf;
   }
   // --- joint limit rows (lower then upper side, joint order)
   if (!stop && !(m.disableflags & (1 << 3))) {
@@ -396,10 +432,12 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
 // ------------------------------------------------------------ Newton solver
 __device__ __forceinline__ bool row_quad(int type, float D, float fl, float y) {
   if (type == ROW_FRICTION) return fabsf(y) < fl / D;
+  if (type == ROW_EQUALITY) return true;
   return y < 0.f;
 }
 __device__ __forceinline__ float row_force(int type, float D, float fl, float y) {
   if (type == ROW_FRICTION) return clampf(-D * y, -fl, fl);
+  if (type == ROW_EQUALITY) return -D * y;
   return y < 0.f ? -D * y : 0.f;
 }
 __device__ __forceinline__ float row_cost(int type, float D, float fl, float y) {
@@ -408,6 +446,7 @@ __device__ __forceinline__ float row_cost(int type, float D, float fl, float y) 
     if (fabsf(y) < fl * R) return 0.5f * D * y * y;
     return fl * fabsf(y) - 0.5f * fl * fl * R;
   }
+  if (type == ROW_EQUALITY) return 0.5f * D * y * y;
   return y < 0.f ? 0.5f * D * y * y : 0.f;
 }
 __device__ __forceinline__ float row_cost_delta(int type, float D, float fl, float y, float dy) {

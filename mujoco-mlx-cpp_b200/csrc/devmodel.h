@@ -26,6 +26,7 @@ struct DevModelDesc {
   int i_pair;    // 6 per pair: g1 g2 b1 b2 condim maxcon
   int i_limit;   // 3 per limited joint: jnt dof qposadr
   int i_floss;   // 1 per frictionloss dof: dof
+  int neq, i_eq;  // joint equalities: 4 ints each (dof1, dof2 or -1, qposadr1, qposadr2)
   int i_act;     // 6 per actuator: dof qposadr gaintype biastype ctrllimited forcelimited
   int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
   int i_mesh;    // 2 per mesh: vertadr vertnum
@@ -38,6 +39,7 @@ struct DevModelDesc {
   int f_pair;    // 16 per pair: margin includemargin friction(5) solref(2) solimp(5) invw_t invw_r
   int f_limit;   // 10 per limit: lo hi margin solref(2) solimp(5)
   int f_floss;   // 8 per frictionloss dof: floss solref(2) solimp(5)
+  int f_eq;      // 15 per joint equality: qpos0 ref1, ref2, polycoef(5), solref(2), solimp(5), invweight
   int f_act;     // 11 per actuator: gear gain(3) bias(3) ctrlrange(2) forcerange(2)
   int f_mesh_vert;
 
@@ -54,7 +56,7 @@ struct DevModelDesc {
 // efc row metadata stride (floats) in the workspace: aref D floss type y force q
 #define MJB_EFC_FIELDS 8
 enum { EFC_AREF = 0, EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y, EFC_FORCE, EFC_Q, EFC_CON };
-enum { ROW_FRICTION = 0, ROW_LIMIT = 1, ROW_PYRAMID = 2, ROW_FRICTIONLESS = 3 };
+enum { ROW_FRICTION = 0, ROW_LIMIT = 1, ROW_PYRAMID = 2, ROW_FRICTIONLESS = 3, ROW_EQUALITY = 5 };
 
 // status bits (per env, OR over substeps)
 enum {

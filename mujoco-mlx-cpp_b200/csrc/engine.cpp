@@ -209,6 +209,27 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.nfloss = (int)fi.size();
     d.i_floss = tb.ai(fi);
     d.f_floss = tb.af(ff);
+    // joint equalities (reference: build_solver_equality_table, batched.cpp:413-455)
+    std::vector<int> qi;
+    std::vector<double> qf;
+    if (!(m.disableflags & DSBL_EQUALITY)) {
+      for (size_t e = 0; e < m.eq_type.size(); e++) {
+        if (!m.eq_active[e]) continue;
+        if (m.eq_type[e] != 2)
+          throw std::runtime_error("engine: connect / weld / tendon equality constraints are not supported (joint equalities are)");
+        const int j1 = m.eq_obj1[e], j2 = m.eq_obj2[e];
+        qi.insert(qi.end(), {m.jnt_dofadr[j1], j2 >= 0 ? m.jnt_dofadr[j2] : -1, m.jnt_qposadr[j1], j2 >= 0 ? m.jnt_qposadr[j2] : 0});
+        qf.push_back(m.qpos0[m.jnt_qposadr[j1]]);
+        qf.push_back(j2 >= 0 ? m.qpos0[m.jnt_qposadr[j2]] : 0.0);
+        qf.insert(qf.end(), &m.eq_data[5 * e], &m.eq_data[5 * e] + 5);
+        qf.insert(qf.end(), &m.eq_solref[2 * e], &m.eq_solref[2 * e] + 2);
+        qf.insert(qf.end(), &m.eq_solimp[5 * e], &m.eq_solimp[5 * e] + 5);
+        qf.push_back(m.eq_invweight[e]);
+      }
+    }
+    d.neq = (int)(qi.size() / 4);
+    d.i_eq = tb.ai(qi);
+    d.f_eq = tb.af(qf);
     std::vector<int> ai;
     std::vector<double> af;
     for (int a = 0; a < m.nu; a++) {
@@ -271,7 +292,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 24);
     int rows_per_con = 1;
     for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : 2 * (p.condim - 1));
-    int rows_bound = d.nfloss + 2 * d.nlimit + rows_per_con * d.ncon_max;
+    int rows_bound = d.neq + d.nfloss + 2 * d.nlimit + rows_per_con * d.ncon_max;
     d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 64));
     // workspace layout
     int nv = m.nv, nb = m.nbody, nj = std::max(1, m.njnt), ng = std::max(1, m.ngeom), nu = std::max(1, m.nu);

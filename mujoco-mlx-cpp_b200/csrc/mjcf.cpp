@@ -756,6 +756,44 @@ struct Compiler {
     }
   }
 
+  void parse_equality(const XmlNode& n) {
+    static const std::map<std::string, int> kinds = {{"connect", 0}, {"weld", 1}, {"joint", 2}, {"tendon", 3}};
+    for (auto& c : n.children) {
+      auto it = kinds.find(c.tag);
+      if (it == kinds.end()) fail("unsupported element <" + c.tag + "> inside <equality>");
+      std::string cls;
+      int o1 = -1, o2 = -1;
+      if (it->second == 2) {
+        auto j1 = c.attr("joint1"), j2 = c.attr("joint2");
+        if (!j1) fail("equality joint needs joint1");
+        o1 = joint_by_name(*j1);
+        if (j2) o2 = joint_by_name(*j2);
+        for (int j : {o1, o2})
+          if (j >= 0 && m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE) fail("equality joint couples hinge or slide joints only");
+      }
+      m.eq_type.push_back(it->second);
+      m.eq_obj1.push_back(o1);
+      m.eq_obj2.push_back(o2);
+      auto act = c.attr("active");
+      m.eq_active.push_back(!act || *act != "false");
+      auto pc = nums(c, "polycoef", cls, {0, 1, 0, 0, 0});
+      while (pc.size() < 5) pc.push_back(0);
+      auto sr = nums(c, "solref", cls, {0.02, 1});
+      auto si = nums(c, "solimp", cls, {0.9, 0.95, 0.001, 0.5, 2});
+      while (si.size() < 5) si.push_back(si.size() == 3 ? 0.5 : 2);
+      for (int k = 0; k < 5; k++) m.eq_data.push_back(pc[k]);
+      for (int k = 0; k < 2; k++) m.eq_solref.push_back(sr.at(k));
+      for (int k = 0; k < 5; k++) m.eq_solimp.push_back(si[k]);
+      m.eq_invweight.push_back(0);
+    }
+  }
+
+  int joint_by_name(const std::string& s) const {
+    for (int j = 0; j < m.njnt; j++)
+      if (m.jnt_name[j] == s) return j;
+    fail("unknown joint '" + s + "'");
+  }
+
   void parse_asset(const XmlNode& n) {
     for (auto& a : n.children) {
       if (a.tag != "mesh") fail("unsupported asset <" + a.tag + "> (only inline-vertex meshes are supported)");
@@ -879,6 +917,7 @@ struct Compiler {
     for (auto& c : root.children) {
       if (c.tag == "actuator") parse_actuator(c);
       else if (c.tag == "contact") parse_contact(c);
+      else if (c.tag == "equality") parse_equality(c);
       else if (c.tag == "compiler" || c.tag == "default" || c.tag == "asset" || c.tag == "option" || c.tag == "worldbody" || c.tag == "size" ||
                c.tag == "visual" || c.tag == "statistic" || c.tag == "keyframe")
         continue;
@@ -1324,6 +1363,13 @@ void finalize_model(Model& m, const LoadOptions& opt) {
   }
   if (m.qpos_spring.size() != (size_t)m.nq) m.qpos_spring = m.qpos0;
   compute_invweights(m);
+  // joint equality regulariser: sum of the coupled dofs' invweights
+  for (size_t e = 0; e < m.eq_type.size(); e++) {
+    if (m.eq_type[e] != 2) continue;
+    double w = m.dof_invweight0[m.jnt_dofadr[m.eq_obj1[e]]];
+    if (m.eq_obj2[e] >= 0) w += m.dof_invweight0[m.jnt_dofadr[m.eq_obj2[e]]];
+    m.eq_invweight[e] = w;
+  }
   build_pairs(m);
 }
 
@@ -1379,6 +1425,8 @@ std::string dump_model(const Model& m) {
   dd("actuator_gear", m.actuator_gear); dd("actuator_gainprm", m.actuator_gainprm); dd("actuator_biasprm", m.actuator_biasprm);
   dd("actuator_ctrlrange", m.actuator_ctrlrange); dd("actuator_forcerange", m.actuator_forcerange);
   di("exclude_body1", m.exclude_body1); di("exclude_body2", m.exclude_body2);
+  di("eq_type", m.eq_type); di("eq_obj1", m.eq_obj1); di("eq_obj2", m.eq_obj2); di("eq_active", m.eq_active);
+  dd("eq_data", m.eq_data); dd("eq_solref", m.eq_solref); dd("eq_solimp", m.eq_solimp); dd("eq_invweight", m.eq_invweight);
   std::vector<int> ep_i;
   std::vector<double> ep_f;
   for (auto& e : m.explicit_pairs) {

@@ -86,6 +86,11 @@ struct Model {
   };
   std::vector<ExplicitPair> explicit_pairs;
 
+  // <equality>: type 0 connect, 1 weld, 2 joint, 3 tendon (this build steps
+  // joint equalities: q1 - q1_0 = poly(q2 - q2_0), poly from 5 coefficients)
+  std::vector<int> eq_type, eq_obj1, eq_obj2, eq_active;
+  std::vector<double> eq_data, eq_solref, eq_solimp, eq_invweight;  // [5], [2], [5], [1] per equality
+
   // compiled collision candidates
   std::vector<Pair> pairs;
 

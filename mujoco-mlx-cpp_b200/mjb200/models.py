@@ -223,7 +223,8 @@ def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.0
     fingers) and a free box on the table.  The table top is the plane z = 0;
     the arm does not collide with itself; the palm box touches the object
     (box-box); the fingers are capsules (cylinder-box contacts are not in this
-    build's narrowphase).  nq 7 + 2 + 7 = 16, nv 15, nu 9."""
+    build's narrowphase); the right finger mimics the left through a joint
+    equality.  nq 7 + 2 + 7 = 16, nv 15, nu 9."""
     axes = ("0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1", "0 1 0", "0 0 1")
     links = []
     depth = 0
@@ -265,6 +266,9 @@ def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.0
       <geom name="object_g" type="box" size="0.03 0.03 0.03" mass="0.2"/>
     </body>
   </worldbody>
+  <equality>
+    <joint name="finger_mimic" joint1="finger_r_j" joint2="finger_l_j" polycoef="0 1 0 0 0"/>
+  </equality>
   <actuator>
 {chr(10).join(acts)}
   </actuator>
@@ -318,7 +322,8 @@ def chain_xml(n: int, cfg: str, iterations: int = 50) -> str:
     the spirit of the reference's tests/test_robustness.cpp.  cfg:
     "free" (no collision pairs), "limit" (joint limits +-0.35 rad), "floss"
     (frictionloss 0.05), "contact" (floor touched when the first joint swings
-    1.2 rad), "all" (limits, frictionloss and contact)."""
+    1.2 rad), "all" (limits, frictionloss and contact), "equality" (every
+    odd joint coupled to 0.5 x the previous joint by a joint equality)."""
     H = n * CHAIN_LINK + 0.05
     touch = H - n * CHAIN_LINK * math.cos(1.2) - 0.004
     floor_z = touch if cfg in ("contact", "all") else -50.0
@@ -335,10 +340,13 @@ def chain_xml(n: int, cfg: str, iterations: int = 50) -> str:
         z = H if i == 0 else -CHAIN_LINK
         body.append(f'<body pos="0 0 {z:.4f}"><joint name="j{i}" type="hinge" axis="{axis}" damping="0.02"{jattr}/>'
                     f'<geom type="capsule" fromto="0 0 0 0 0 {-CHAIN_LINK}" size="0.02" density="500"{gcol}/>')
+    eq = ""
+    if cfg == "equality":
+        eq = "<equality>" + "".join(f'<joint joint1="j{i}" joint2="j{i - 1}" polycoef="0 0.5 0 0 0"/>' for i in range(1, n, 2)) + "</equality>"
     return (f'<mujoco model="chain{n}_{cfg}"><compiler angle="radian"/>'
             f'<option timestep="0.002" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
             f'<worldbody><geom type="plane" size="5 5 0.1" pos="0 0 {floor_z:.4f}"{floor_col}/>'
-            + "".join(body) + "</body>" * n + "</worldbody></mujoco>")
+            + "".join(body) + "</body>" * n + "</worldbody>" + eq + "</mujoco>")
 
 
 def chain_state(n: int, cfg: str, num_envs: int, seed: int):

@@ -48,6 +48,10 @@ typedef struct OModel {
      pair_real[16*p] = margin gap friction(5) solref(2) solimp(5) invw_t invw_r */
   const int* pair_int;
   const double* pair_real;
+  /* equality constraints (type 2 = joint: q1 - q1_0 = poly(q2 - q2_0)) */
+  int neq;
+  const int *eq_type, *eq_obj1, *eq_obj2, *eq_active;
+  const double *eq_data, *eq_solref, *eq_solimp, *eq_invweight;
 } OModel;
 
 /* per-env randomisation (NULL pointers = identity) */
@@ -71,7 +75,7 @@ typedef struct OData {
   double *M, *qLD, *qfrc_bias, *qfrc_passive, *qfrc_actuator, *qfrc_smooth, *qacc_smooth;
   double *contact;              /* [ncon_max * ORACLE_CONTACT_STRIDE] */
   double *efc_J, *efc_aref, *efc_D, *efc_R, *efc_floss, *efc_force, *efc_jar;  /* [nefc_max(*nv)] */
-  int *efc_type;                /* 0 friction 1 limit 2 contact-pyramid 3 contact-frictionless 4 elliptic */
+  int *efc_type;                /* 0 friction 1 limit 2 contact-pyramid 3 contact-frictionless 5 equality */
   double *qacc, *qfrc_constraint, *cfrc_ext;
   double *work;                 /* >= 6*nv*nv + 16*nv + 8*nefc_max doubles */
   /* scalars */

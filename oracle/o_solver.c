@@ -19,7 +19,7 @@
 #include "mjoracle.h"
 #include "o_util.h"
 
-enum { T_FRICTION = 0, T_LIMIT = 1, T_PYRAMID = 2, T_FRICTIONLESS = 3 };
+enum { T_FRICTION = 0, T_LIMIT = 1, T_PYRAMID = 2, T_FRICTIONLESS = 3, T_EQUALITY = 5 };
 
 static void impedance(const OModel* m, const double* solref, const double* solimp, double pos, double* k, double* b, double* imp) {
   double tc = solref[0], dr = solref[1];
@@ -58,6 +58,36 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
   d->nefc_dropped = 0;
   int stop = 0;  /* set when a row group does not fit: it and every later group are dropped */
   if (m->disableflags & 1) return;
+  /* joint equalities first (reference: solver.hpp:259-289; bilateral) */
+  if (!(m->disableflags & (1 << 1))) {
+    for (int e = 0; e < m->neq; e++) {
+      if (!m->eq_active[e] || m->eq_type[e] != 2) continue;
+      if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+      int j1 = m->eq_obj1[e], j2 = m->eq_obj2[e];
+      int d1 = m->jnt_dofadr[j1], q1 = m->jnt_qposadr[j1];
+      const double* c = &m->eq_data[5 * e];
+      double poly = c[0], dpoly = 0;
+      int d2 = -1;
+      if (j2 >= 0) {
+        d2 = m->jnt_dofadr[j2];
+        int q2 = m->jnt_qposadr[j2];
+        double x = d->qpos[q2] - m->qpos0[q2];
+        poly = c[0] + x * (c[1] + x * (c[2] + x * (c[3] + x * c[4])));
+        dpoly = c[1] + x * (2 * c[2] + x * (3 * c[3] + x * 4 * c[4]));
+      }
+      double pos = d->qpos[q1] - m->qpos0[q1] - poly;
+      double vel = d->qvel[d1] - (d2 >= 0 ? dpoly * d->qvel[d2] : 0);
+      double k, b, imp;
+      impedance(m, &m->eq_solref[2 * e], &m->eq_solimp[5 * e], pos, &k, &b, &imp);
+      int r = add_row(d, nv, T_EQUALITY);
+      d->efc_J[r * nv + d1] = 1;
+      if (d2 >= 0) d->efc_J[r * nv + d2] -= dpoly;
+      double R = (1 - imp) / imp * m->eq_invweight[e];
+      d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+      d->efc_D[r] = 1 / d->efc_R[r];
+      d->efc_aref[r] = -b * vel - k * imp * pos;
+    }
+  }
   if (!(m->disableflags & (1 << 2))) {
     for (int i = 0; i < nv; i++) {
       if (m->dof_frictionloss[i] <= 0) continue;
@@ -179,6 +209,7 @@ static double row_cost(int type, double D, double fl, double y) {
     if (fabs(y) < fl * R) return 0.5 * D * y * y;
     return fl * fabs(y) - 0.5 * fl * fl * R;
   }
+  if (type == T_EQUALITY) return 0.5 * D * y * y;
   return y < 0 ? 0.5 * D * y * y : 0;
 }
 static double row_force(int type, double D, double fl, double y) {
@@ -186,10 +217,12 @@ static double row_force(int type, double D, double fl, double y) {
     double f = -D * y;
     return f > fl ? fl : f < -fl ? -fl : f;
   }
+  if (type == T_EQUALITY) return -D * y;
   return y < 0 ? -D * y : 0;
 }
 static int row_quadratic(int type, double D, double fl, double y) {
   if (type == T_FRICTION) return fabs(y) < fl / D;
+  if (type == T_EQUALITY) return 1;
   return y < 0;
 }
 /* s(y + dy) - s(y), written to keep precision when dy is small */

@@ -34,11 +34,16 @@ _MODEL_PTR = [
 ]
 
 
+_EQ_PTR = [("eq_type", "i"), ("eq_obj1", "i"), ("eq_obj2", "i"), ("eq_active", "i"),
+           ("eq_data", "f"), ("eq_solref", "f"), ("eq_solimp", "f"), ("eq_invweight", "f")]
+
+
 class OModel(C.Structure):
     _fields_ = ([(n, C.c_int) for n in _MODEL_INT] +
                 [("timestep", C.c_double), ("gravity", C.c_double * 3), ("tolerance", C.c_double), ("ls_tolerance", C.c_double),
                  ("impratio", C.c_double), ("meaninertia", C.c_double)] +
-                [(n, _ip if k == "i" else _dp) for n, k in _MODEL_PTR])
+                [(n, _ip if k == "i" else _dp) for n, k in _MODEL_PTR] +
+                [("neq", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _EQ_PTR])
 
 
 class ORand(C.Structure):
@@ -106,8 +111,9 @@ class OracleModel:
         m.timestep = orr[0]
         m.gravity[0], m.gravity[1], m.gravity[2] = orr[1:4]
         m.tolerance, m.ls_tolerance, m.impratio, m.meaninertia = orr[4:8]
-        for n, k in _MODEL_PTR:
-            a = dump[n]
+        m.neq = int(len(dump.get("eq_type", [])))
+        for n, k in _MODEL_PTR + _EQ_PTR:
+            a = dump[n] if n in dump else np.zeros(0)
             a = np.ascontiguousarray(a, dtype=np.int32 if k == "i" else np.float64)
             if a.size == 0:
                 a = np.zeros(1, a.dtype)

@@ -6,9 +6,10 @@ envs bit-identical.  Chains above 32 dofs use the shared-memory Cholesky and
 the second register slot of the triangular solves.
 
 Tolerance: contact sets and row counts equal; qacc relative error <= the
-larger of the fixed bounds (1e-4 median, 2e-3 max) and 4x the error of an
-FP32 Cholesky solve of the oracle's own mass matrix for the same state
-(numpy / LAPACK).  Long chains are ill conditioned (cond(M) ~ 1e5 at 33 dofs,
+larger of the fixed bounds (1e-4 median, 2e-3 max) and 8x the error of an
+FP32 Cholesky solve of the constrained Newton system at the oracle's solution
+for the same state (numpy / LAPACK); the factor covers the engine also
+forming M, J and the forces in FP32 along the chain.  Long chains are ill conditioned (cond(M) ~ 1e5 at 33 dofs,
 ~ 1e6 at 64), so FP32 arithmetic cannot reach 1e-4 there; the test asks the
 engine to be as accurate as FP32 allows."""
 import numpy as np
@@ -21,8 +22,10 @@ from parity import contact_sets_match, gpu_step_from, oracle_step_from, rel_err
 pytestmark = pytest.mark.gpu
 
 def _fp32_smooth_error(om, q, v, n):
-    """Relative error of an FP32 Cholesky solve of M qacc = qfrc_smooth with
-    the oracle's FP64 M and force for this state (the FP32 floor)."""
+    """Relative error of an FP32 Cholesky solve of the Newton system at the
+    oracle's solution (the FP32 floor for this state): with the oracle's
+    active set, (M + sum_active D_r J_r J_r') qacc = M qacc_smooth +
+    sum_active D_r J_r aref_r + sum_saturated J_r f_r."""
     import scipy.linalg as sl
 
     env = oracle.OracleEnv(om, 32, 256)
@@ -30,12 +33,24 @@ def _fp32_smooth_error(om, q, v, n):
     env.a["qvel"][:] = v
     env.step()
     M = env.a["M"].reshape(n, n)
-    x = env.a["qacc_smooth"]
-    x32 = sl.cho_solve(sl.cho_factor(M.astype(np.float32)), env.a["qfrc_smooth"].astype(np.float32))
+    x = env.a["qacc"]
+    e = env.efc()
+    fl = env.a["efc_floss"][: len(e["D"])]
+    H = M.copy()
+    rhs = M @ env.a["qacc_smooth"]
+    for r in range(len(e["D"])):
+        t, D, J, f = e["type"][r], e["D"][r], e["J"][r], e["force"][r]
+        active = t == 5 or (t in (1, 2, 3) and f > 0) or (t == 0 and abs(f) < fl[r] * (1 - 1e-9))
+        if active:
+            H += D * np.outer(J, J)
+            rhs += D * J * e["aref"][r]
+        elif t == 0:
+            rhs += J * f
+    x32 = sl.cho_solve(sl.cho_factor(H.astype(np.float32)), rhs.astype(np.float32))
     return float(np.linalg.norm(x32 - x) / max(np.linalg.norm(x), 1.0))
 
 
-CASES = [(n, cfg) for n in (2, 7, 18, 33, 64) for cfg in ("free", "limit", "floss", "contact", "all")]
+CASES = [(n, cfg) for n in (2, 7, 18, 33, 64) for cfg in ("free", "limit", "floss", "contact", "all", "equality")]
 
 
 @pytest.mark.parametrize("n,cfg", CASES)
@@ -68,8 +83,8 @@ def test_chain_parity_and_rollout(n, cfg):
                 errs.append(rel_err(g["vec"][e, 2, :n], o[e]["qacc"]))
                 fp32.append(_fp32_smooth_error(om, qs[e], vs[e], n))
         errs, fp32 = np.array(errs), np.array(fp32)
-        tol_med = max(1e-4, 4 * np.median(fp32))
-        tol_max = max(2e-3, 4 * fp32.max())
+        tol_med = max(1e-4, 8 * np.median(fp32))
+        tol_max = max(2e-3, 8 * fp32.max())
         assert np.median(errs) <= tol_med and errs.max() <= tol_max, (n, cfg, np.median(errs), errs.max(), tol_med, tol_max)
     # rollout: finite, identical envs identical; no resets up to 18 dofs.
     # Long chains with random joint velocities can reach |qacc| past the

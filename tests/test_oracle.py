@@ -157,7 +157,9 @@ def _gauss_residual(om, env):
     M = env.a["M"].reshape(nv, nv)
     e = env.efc()
     r = e["J"] @ env.a["qacc"] - e["aref"]
-    f = -e["D"] * np.minimum(r, 0.0)
+    fl = env.a["efc_floss"][: len(r)]
+    f = np.where(e["type"] == 5, -e["D"] * r, -e["D"] * np.minimum(r, 0.0))  # equality rows are bilateral
+    f = np.where(e["type"] == 0, np.clip(-e["D"] * r, -fl, fl), f)        # frictionloss rows saturate at +-floss
     lhs = M @ (env.a["qacc"] - env.a["qacc_smooth"])
     rhs = e["J"].T @ f
     return np.linalg.norm(lhs - rhs) / max(np.linalg.norm(M @ env.a["qacc_smooth"]), 1.0), f, e["force"]
@@ -310,3 +312,30 @@ def test_box_stack_comes_to_rest():
     assert len(bb) == 4
     rows = env.efc()["force"].reshape(-1, 4)
     assert rows[bb].sum() == pytest.approx(m_ * G, rel=1e-3)
+
+
+def test_joint_equality_couples_joints():
+    """Joint equality q_b - q_b0 = 0.5 (q_a - q_a0): one bilateral row ahead
+    of every other row, Gauss-optimal solutions, and the coupling held to
+    within the soft constraint's tracking error while the pendulum swings."""
+    xml = wrap('<body><joint name="a" type="hinge" axis="0 1 0" damping="0.2" frictionloss="0.01"/>'
+               '<geom type="capsule" fromto="0 0 0 0 0 -0.3" size="0.02" mass="1"/>'
+               '<body pos="0 0 -0.3"><joint name="b" type="hinge" axis="0 1 0" damping="0.2"/>'
+               '<geom type="capsule" fromto="0 0 0 0 0 -0.3" size="0.02" mass="1"/></body></body>',
+               extra="") .replace("</mujoco>", '<equality><joint joint1="b" joint2="a" polycoef="0 0.5 0 0 0"/></equality></mujoco>')
+    om, env = env_from_xml(xml)
+    env.a["qpos"][:] = [0.8, -0.3]
+    env.step()
+    t = env.efc()["type"]
+    assert list(t[:2]) == [5, 0]                     # equality row first, then frictionloss
+    res, f, force = _gauss_residual(om, env)
+    assert res < 1e-6
+    np.testing.assert_allclose(force[:1], f[:1], rtol=1e-9)
+    worst = 0.0
+    for i in range(1500):
+        env.step()
+        q = env.a["qpos"]
+        if i > 100:
+            worst = max(worst, abs(q[1] - 0.5 * q[0]))
+    assert worst < 0.02                              # soft-constraint tracking error while swinging
+    assert abs(env.a["qpos"][0]) > 1e-3              # it did swing
