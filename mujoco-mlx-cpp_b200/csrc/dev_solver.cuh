@@ -208,7 +208,8 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
   int nefc = 0;
   bool stop = false;
   if (m.disableflags & 1) return 0;
-  // --- joint equality rows (static list): q1 - q1_0 = poly(q2 - q2_0)
+  // --- joint / tendon equality rows (static list): x1 = poly(x2) with
+  // x = q - qpos0 for joints and length - length0 for fixed tendons
   // (reference: solver.hpp:259-289; bilateral rows, always in their
   // quadratic zone)
   if (!(m.disableflags & (1 << 1)) && m.neq > 0) {
@@ -216,23 +217,43 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
     if (nq_ > m.nefc_max) { nq_ = m.nefc_max; stop = true; }
     #pragma unroll 1
     for (int r = E.lane; r < nq_; r += 32) {
-      const int d1 = ldi(it, m.i_eq + 4 * r), d2 = ldi(it, m.i_eq + 4 * r + 1);
-      const int qa1 = ldi(it, m.i_eq + 4 * r + 2), qa2 = ldi(it, m.i_eq + 4 * r + 3);
+      const int* qi = it + m.i_eq + 5 * r;
+      const bool ten = ldi(qi, 0) == 1;
+      const int o1 = ldi(qi, 1), o2 = ldi(qi, 2);
       const float* f = ft + m.f_eq + 15 * r;
-      float poly = ldf(f, 2), dpoly = 0.f;
-      if (d2 >= 0) {
-        const float x = qpos[qa2] - ldf(f, 1);
-        poly = ldf(f, 2) + x * (ldf(f, 3) + x * (ldf(f, 4) + x * (ldf(f, 5) + x * ldf(f, 6))));
-        dpoly = ldf(f, 3) + x * (2.f * ldf(f, 4) + x * (3.f * ldf(f, 5) + x * 4.f * ldf(f, 6)));
+      float x1, v1, x2 = 0.f, v2 = 0.f;
+      if (ten) {
+        d_tendon_lv(m, it, ft, qpos, qvel, o1, x1, v1);
+        if (o2 >= 0) d_tendon_lv(m, it, ft, qpos, qvel, o2, x2, v2);
+      } else {
+        x1 = qpos[ldi(qi, 3)];
+        v1 = qvel[o1];
+        if (o2 >= 0) { x2 = qpos[ldi(qi, 4)]; v2 = qvel[o2]; }
       }
-      const float pos = qpos[qa1] - ldf(f, 0) - poly;
-      const float vel = qvel[d1] - (d2 >= 0 ? dpoly * qvel[d2] : 0.f);
+      x1 -= ldf(f, 0);
+      x2 -= ldf(f, 1);
+      float poly = ldf(f, 2), dpoly = 0.f;
+      if (o2 >= 0) {
+        poly = ldf(f, 2) + x2 * (ldf(f, 3) + x2 * (ldf(f, 4) + x2 * (ldf(f, 5) + x2 * ldf(f, 6))));
+        dpoly = ldf(f, 3) + x2 * (2.f * ldf(f, 4) + x2 * (3.f * ldf(f, 5) + x2 * 4.f * ldf(f, 6)));
+      }
+      const float pos = x1 - poly;
+      const float vel = v1 - dpoly * v2;
       float si[5] = {ldf(f, 9), ldf(f, 10), ldf(f, 11), ldf(f, 12), ldf(f, 13)};
       float k, b, imp;
       impedance(m, ldf(f, 7), ldf(f, 8), si, pos, k, b, imp);
       const float R = fmaxf((1.f - imp) / imp * ldf(f, 14), 1e-15f);
-      #pragma unroll 1
-      for (int c = 0; c < nv; c++) J[r * nv + c] = (c == d1 ? 1.f : 0.f) - (c == d2 ? dpoly : 0.f);
+      if (ten) {
+        d_tendon_row(m, it, ft, o1, 1.f, J + r * nv);
+        if (o2 >= 0) {
+          const int adr = ldi(it, m.i_ten + 3 * o2), num = ldi(it, m.i_ten + 3 * o2 + 1);
+          #pragma unroll 1
+          for (int w = adr; w < adr + num; w++) J[r * nv + ldi(it, m.i_wrap + 2 * w)] -= dpoly * ldf(ft, m.f_wrap + w);
+        }
+      } else {
+        #pragma unroll 1
+        for (int c = 0; c < nv; c++) J[r * nv + c] = (c == o1 ? 1.f : 0.f) - (c == o2 ? dpoly : 0.f);
+      }
       EfcRef e{efc + r, ne};
       e[EFC_D] = 1.f / R;
       e[EFC_AREF] = -b * vel - k * imp * pos;
@@ -262,6 +283,31 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       e[EFC_D] = 1.f / R;
       e[EFC_AREF] = -b * qvel[dof];
       e[EFC_FLOSS] = ldf(f, 0);
+      e[EFC_TYPE] = ROW_FRICTION;
+      e[EFC_CON] = -1;
+    }
+    nefc = r0 + nf;
+  }
+  // --- tendon frictionloss rows after the dof ones (reference: solver.hpp:320-342)
+  if (!stop && !(m.disableflags & (1 << 2)) && m.ntfloss > 0) {
+    const int r0 = nefc;
+    int nf = m.ntfloss;
+    if (r0 + nf > m.nefc_max) { nf = m.nefc_max - r0; stop = true; }
+    #pragma unroll 1
+    for (int q = E.lane; q < nf; q += 32) {
+      const int r = r0 + q;
+      const int t = ldi(it, m.i_tfloss + q);
+      const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
+      float si[5] = {ldf(tf, TEN_SIFRI), ldf(tf, TEN_SIFRI + 1), ldf(tf, TEN_SIFRI + 2), ldf(tf, TEN_SIFRI + 3), ldf(tf, TEN_SIFRI + 4)};
+      float k, b, imp, len, vel;
+      impedance(m, ldf(tf, TEN_SRFRI), ldf(tf, TEN_SRFRI + 1), si, 0.f, k, b, imp);
+      d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+      const float R = fmaxf((1.f - imp) / imp * ldf(tf, TEN_INVW), 1e-15f);
+      d_tendon_row(m, it, ft, t, 1.f, J + r * nv);
+      EfcRef e{efc + r, ne};
+      e[EFC_D] = 1.f / R;
+      e[EFC_AREF] = -b * vel;
+      e[EFC_FLOSS] = ldf(tf, TEN_FLOSS);
       e[EFC_TYPE] = ROW_FRICTION;
       e[EFC_CON] = -1;
     }
@@ -310,6 +356,47 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       }
       nefc += total;
       if (nefc > m.nefc_max) { nefc = m.nefc_max; stop = true; break; }
+    }
+    // --- tendon limit rows after the joint limits (reference: solver.hpp:370-395)
+    #pragma unroll 1
+    for (int base = 0; !stop && base < m.ntlimit; base += 32) {
+      const int li = base + E.lane;
+      int act[2] = {0, 0};
+      float dist[2] = {0, 0}, len = 0.f, vel = 0.f;
+      int t = 0;
+      if (li < m.ntlimit) {
+        t = ldi(it, m.i_tlimit + li);
+        const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
+        d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+        dist[0] = len - ldf(tf, TEN_LO);
+        dist[1] = ldf(tf, TEN_HI) - len;
+        act[0] = dist[0] < ldf(tf, TEN_MARGIN);
+        act[1] = dist[1] < ldf(tf, TEN_MARGIN);
+      }
+      const int cnt = act[0] + act[1];
+      const int incl = warp_incl_scan(cnt, E.lane);
+      const int total = __shfl_sync(FULL_MASK, incl, 31);
+      int r = nefc + incl - cnt;
+      for (int s = 0; s < 2; s++) {
+        if (!act[s]) continue;
+        if (r >= m.nefc_max) break;
+        const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
+        float si[5] = {ldf(tf, TEN_SILIM), ldf(tf, TEN_SILIM + 1), ldf(tf, TEN_SILIM + 2), ldf(tf, TEN_SILIM + 3), ldf(tf, TEN_SILIM + 4)};
+        float pos = dist[s] - ldf(tf, TEN_MARGIN), k, b, imp;
+        impedance(m, ldf(tf, TEN_SRLIM), ldf(tf, TEN_SRLIM + 1), si, pos, k, b, imp);
+        const float sg = s == 0 ? 1.f : -1.f;
+        d_tendon_row(m, it, ft, t, sg, J + r * nv);
+        const float R = fmaxf((1.f - imp) / imp * ldf(tf, TEN_INVW), 1e-15f);
+        EfcRef e{efc + r, ne};
+        e[EFC_D] = 1.f / R;
+        e[EFC_AREF] = -b * sg * vel - k * imp * pos;
+        e[EFC_FLOSS] = 0;
+        e[EFC_TYPE] = ROW_LIMIT;
+        e[EFC_CON] = -1;
+        r++;
+      }
+      nefc += total;
+      if (nefc > m.nefc_max) { nefc = m.nefc_max; stop = true; }
     }
   }
   // --- contact rows: offsets by scan, then per-contact impedance, then J by dof lanes

@@ -452,6 +452,41 @@ __device__ __noinline__ void d_rne(Env& E, float* bias) {
   __syncwarp();
 }
 
+// Fixed tendon t: length = sum coef * qpos and velocity = sum coef * qvel
+// over its wraps (reference: tendon.hpp emit_tendon_phase, fixed branch).
+__device__ __forceinline__ void d_tendon_lv(const DevModelDesc& m, const int* it, const float* ft, const float* qpos, const float* qvel, int t,
+                                            float& len, float& vel) {
+  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
+  float l = 0.f, v = 0.f;
+  #pragma unroll 1
+  for (int w = adr; w < adr + num; w++) {
+    const float c = ldf(ft, m.f_wrap + w);
+    l += c * qpos[ldi(it, m.i_wrap + 2 * w + 1)];
+    v += c * qvel[ldi(it, m.i_wrap + 2 * w)];
+  }
+  len = l;
+  vel = v;
+}
+
+// Component of tendon t's (constant) Jacobian on dof i.
+__device__ __forceinline__ float d_tendon_jac(const DevModelDesc& m, const int* it, const float* ft, int t, int i) {
+  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
+  float j = 0.f;
+  #pragma unroll 1
+  for (int w = adr; w < adr + num; w++)
+    if (ldi(it, m.i_wrap + 2 * w) == i) j += ldf(ft, m.f_wrap + w);
+  return j;
+}
+
+// row[0..nv) = sg * (Jacobian of tendon t), written by one lane.
+__device__ __forceinline__ void d_tendon_row(const DevModelDesc& m, const int* it, const float* ft, int t, float sg, float* row) {
+  #pragma unroll 1
+  for (int c = 0; c < m.nv; c++) row[c] = 0.f;
+  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
+  #pragma unroll 1
+  for (int w = adr; w < adr + num; w++) row[ldi(it, m.i_wrap + 2 * w)] += sg * ldf(ft, m.f_wrap + w);
+}
+
 // passive + actuation + smooth force
 __device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* bias) {
   const DevModelDesc& m = *E.md;
@@ -475,23 +510,52 @@ __device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* 
         pas -= st * (qpos[qa] - ldf(ft, m.f_qpos_spring + qa));
       }
       pas -= ldf(ft, m.f_dof_damping + i) * qvel[i];
+      // tendon spring with a dead band and damper, through J^T
+      // (reference: tendon.hpp:360-377)
+      #pragma unroll 1
+      for (int k = 0; k < m.npten; k++) {
+        const int t = ldi(it, m.i_pten + k);
+        const float jt = d_tendon_jac(m, it, ft, t, i);
+        if (jt == 0.f) continue;
+        const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
+        float len, vel;
+        d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+        const float kst = ldf(tf, TEN_STIFF), lo = ldf(tf, TEN_SPRLO), hi = ldf(tf, TEN_SPRHI);
+        float f = 0.f;
+        if (len > hi) f += kst * (hi - len);
+        else if (len < lo) f += kst * (lo - len);
+        f -= ldf(tf, TEN_DAMP) * vel;
+        pas += jt * f;
+      }
     }
     if (!(m.disableflags & (1 << 10))) {
       #pragma unroll 1
       for (int a = 0; a < m.nu; a++) {
-        const int* ai = it + m.i_act + 6 * a;
-        if (ldi(ai, 0) != i) continue;
+        const int* ai = it + m.i_act + 7 * a;
+        const int ten = ldi(ai, 6);
+        float moment = 1.f, len, vel;
+        if (ten >= 0) {
+          // tendon transmission: length / velocity / moment from the tendon
+          moment = d_tendon_jac(m, it, ft, ten, i);
+          if (moment == 0.f) continue;
+          d_tendon_lv(m, it, ft, qpos, qvel, ten, len, vel);
+        } else {
+          if (ldi(ai, 0) != i) continue;
+          len = qpos[ldi(ai, 1)];
+          vel = qvel[i];
+        }
         const float* af = ft + m.f_act + 11 * a;
         float gear = ldf(af, 0);
         float c = ctrl[a];
         if (ldi(ai, 4) && !(m.disableflags & (1 << 7))) c = clampf(c, ldf(af, 7), ldf(af, 8));
-        float len = gear * qpos[ldi(ai, 1)], vel = gear * qvel[i];
+        len *= gear;
+        vel *= gear;
         float gain = ldf(af, 1) + (ldi(ai, 2) ? ldf(af, 2) * len + ldf(af, 3) * vel : 0.f);
         float bs = ldi(ai, 3) ? ldf(af, 4) + ldf(af, 5) * len + ldf(af, 6) * vel : 0.f;
         float force = gain * c + bs;
         if (P.rand_gain) force *= P.rand_gain[P.env_uadr[E.env] + a];
         if (ldi(ai, 5)) force = clampf(force, ldf(af, 9), ldf(af, 10));
-        act += gear * force;
+        act += gear * moment * force;
       }
     }
     qfa[i] = act;

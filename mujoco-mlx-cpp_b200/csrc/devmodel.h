@@ -26,8 +26,13 @@ struct DevModelDesc {
   int i_pair;    // 6 per pair: g1 g2 b1 b2 condim maxcon
   int i_limit;   // 3 per limited joint: jnt dof qposadr
   int i_floss;   // 1 per frictionloss dof: dof
-  int neq, i_eq;  // joint equalities: 4 ints each (dof1, dof2 or -1, qposadr1, qposadr2)
-  int i_act;     // 6 per actuator: dof qposadr gaintype biastype ctrllimited forcelimited
+  int neq, i_eq;  // joint / tendon equalities: 5 ints each (kind 0 joint 1 tendon, obj1, obj2 or -1, qposadr1, qposadr2);
+                  // obj = dof for joints, tendon id for tendons
+  int i_act;     // 7 per actuator: dof qposadr gaintype biastype ctrllimited forcelimited tendon (-1 = joint transmission)
+  int ntendon, i_ten, i_wrap;  // fixed tendons: 3 ints each (wrapadr wrapnum limited); 2 per wrap (dof qposadr)
+  int ntfloss, i_tfloss;       // tendons with frictionloss (tendon ids)
+  int ntlimit, i_tlimit;       // limited tendons (tendon ids)
+  int npten, i_pten;           // tendons with stiffness or damping (tendon ids)
   int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
   int i_mesh;    // 2 per mesh: vertadr vertnum
 
@@ -41,6 +46,8 @@ struct DevModelDesc {
   int f_floss;   // 8 per frictionloss dof: floss solref(2) solimp(5)
   int f_eq;      // 15 per joint equality: qpos0 ref1, ref2, polycoef(5), solref(2), solimp(5), invweight
   int f_act;     // 11 per actuator: gear gain(3) bias(3) ctrlrange(2) forcerange(2)
+  int f_wrap;    // 1 per wrap: coef
+  int f_ten;     // MJB_TEN_FLOATS per tendon (layout below)
   int f_mesh_vert;
 
   // per-env shared-memory workspace (float offsets from the warp's base)
@@ -52,6 +59,13 @@ struct DevModelDesc {
   int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;
   int w_J, w_efc, w_H, w_active;
 };
+
+// per-tendon floats: range lo, hi, margin, frictionloss, stiffness, damping,
+// lengthspring lo, hi, solref_lim(2), solimp_lim(5), solref_fri(2),
+// solimp_fri(5), invweight0, length0
+#define MJB_TEN_FLOATS 24
+enum { TEN_LO = 0, TEN_HI, TEN_MARGIN, TEN_FLOSS, TEN_STIFF, TEN_DAMP, TEN_SPRLO, TEN_SPRHI, TEN_SRLIM, TEN_SILIM = 10, TEN_SRFRI = 15,
+       TEN_SIFRI = 17, TEN_INVW = 22, TEN_LEN0 = 23 };
 
 // efc row metadata stride (floats) in the workspace: aref D floss type y force q
 #define MJB_EFC_FIELDS 8

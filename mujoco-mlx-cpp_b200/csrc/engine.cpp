@@ -209,32 +209,73 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.nfloss = (int)fi.size();
     d.i_floss = tb.ai(fi);
     d.f_floss = tb.af(ff);
-    // joint equalities (reference: build_solver_equality_table, batched.cpp:413-455)
+    // fixed tendons (reference: build_tendon_host, batched.cpp:100-136, and
+    // the tendon limit / friction tables, batched.cpp:480-530)
+    std::vector<int> ti, wi, tfl, tlim, tpas;
+    std::vector<double> wf, tf;
+    for (int t = 0; t < m.ntendon; t++) {
+      ti.insert(ti.end(), {m.tendon_adr[t], m.tendon_num[t], m.tendon_limited[t]});
+      tf.insert(tf.end(), {m.tendon_range[2 * t], m.tendon_range[2 * t + 1], m.tendon_margin[t], m.tendon_frictionloss[t], m.tendon_stiffness[t],
+                           m.tendon_damping[t], m.tendon_lengthspring[2 * t], m.tendon_lengthspring[2 * t + 1]});
+      tf.insert(tf.end(), &m.tendon_solref_lim[2 * t], &m.tendon_solref_lim[2 * t] + 2);
+      tf.insert(tf.end(), &m.tendon_solimp_lim[5 * t], &m.tendon_solimp_lim[5 * t] + 5);
+      tf.insert(tf.end(), &m.tendon_solref_fri[2 * t], &m.tendon_solref_fri[2 * t] + 2);
+      tf.insert(tf.end(), &m.tendon_solimp_fri[5 * t], &m.tendon_solimp_fri[5 * t] + 5);
+      tf.insert(tf.end(), {m.tendon_invweight0[t], m.tendon_length0[t]});
+      if (m.tendon_frictionloss[t] > 0) tfl.push_back(t);
+      if (m.tendon_limited[t]) tlim.push_back(t);
+      if (m.tendon_stiffness[t] != 0 || m.tendon_damping[t] != 0) tpas.push_back(t);
+    }
+    for (size_t w = 0; w < m.wrap_joint.size(); w++) {
+      wi.insert(wi.end(), {m.jnt_dofadr[m.wrap_joint[w]], m.jnt_qposadr[m.wrap_joint[w]]});
+      wf.push_back(m.wrap_coef[w]);
+    }
+    d.ntendon = m.ntendon;
+    d.i_ten = tb.ai(ti);
+    d.i_wrap = tb.ai(wi);
+    d.f_wrap = tb.af(wf);
+    d.f_ten = tb.af(tf);
+    d.ntfloss = (int)tfl.size();
+    d.i_tfloss = tb.ai(tfl);
+    d.ntlimit = (int)tlim.size();
+    d.i_tlimit = tb.ai(tlim);
+    d.npten = (int)tpas.size();
+    d.i_pten = tb.ai(tpas);
+    // joint and tendon equalities (reference: build_solver_equality_table,
+    // batched.cpp:411-455; tendon ones measure length - tendon_length0)
     std::vector<int> qi;
     std::vector<double> qf;
     if (!(m.disableflags & DSBL_EQUALITY)) {
       for (size_t e = 0; e < m.eq_type.size(); e++) {
         if (!m.eq_active[e]) continue;
-        if (m.eq_type[e] != 2)
-          throw std::runtime_error("engine: connect / weld / tendon equality constraints are not supported (joint equalities are)");
-        const int j1 = m.eq_obj1[e], j2 = m.eq_obj2[e];
-        qi.insert(qi.end(), {m.jnt_dofadr[j1], j2 >= 0 ? m.jnt_dofadr[j2] : -1, m.jnt_qposadr[j1], j2 >= 0 ? m.jnt_qposadr[j2] : 0});
-        qf.push_back(m.qpos0[m.jnt_qposadr[j1]]);
-        qf.push_back(j2 >= 0 ? m.qpos0[m.jnt_qposadr[j2]] : 0.0);
+        if (m.eq_type[e] != 2 && m.eq_type[e] != 3)
+          throw std::runtime_error("engine: connect / weld equality constraints are not supported (joint and tendon equalities are)");
+        const int o1 = m.eq_obj1[e], o2 = m.eq_obj2[e];
+        if (m.eq_type[e] == 3) {
+          qi.insert(qi.end(), {1, o1, o2, 0, 0});
+          qf.push_back(m.tendon_length0[o1]);
+          qf.push_back(o2 >= 0 ? m.tendon_length0[o2] : 0.0);
+        } else {
+          qi.insert(qi.end(), {0, m.jnt_dofadr[o1], o2 >= 0 ? m.jnt_dofadr[o2] : -1, m.jnt_qposadr[o1], o2 >= 0 ? m.jnt_qposadr[o2] : 0});
+          qf.push_back(m.qpos0[m.jnt_qposadr[o1]]);
+          qf.push_back(o2 >= 0 ? m.qpos0[m.jnt_qposadr[o2]] : 0.0);
+        }
         qf.insert(qf.end(), &m.eq_data[5 * e], &m.eq_data[5 * e] + 5);
         qf.insert(qf.end(), &m.eq_solref[2 * e], &m.eq_solref[2 * e] + 2);
         qf.insert(qf.end(), &m.eq_solimp[5 * e], &m.eq_solimp[5 * e] + 5);
         qf.push_back(m.eq_invweight[e]);
       }
     }
-    d.neq = (int)(qi.size() / 4);
+    d.neq = (int)(qi.size() / 5);
     d.i_eq = tb.ai(qi);
     d.f_eq = tb.af(qf);
     std::vector<int> ai;
     std::vector<double> af;
     for (int a = 0; a < m.nu; a++) {
-      int j = m.actuator_trnid[a];
-      ai.insert(ai.end(), {m.jnt_dofadr[j], m.jnt_qposadr[j], m.actuator_gaintype[a], m.actuator_biastype[a], m.actuator_ctrllimited[a], m.actuator_forcelimited[a]});
+      const bool ten = m.actuator_trntype[a] == 3;
+      int j = ten ? 0 : m.actuator_trnid[a];
+      ai.insert(ai.end(), {ten ? -1 : m.jnt_dofadr[j], ten ? 0 : m.jnt_qposadr[j], m.actuator_gaintype[a], m.actuator_biastype[a],
+                           m.actuator_ctrllimited[a], m.actuator_forcelimited[a], ten ? m.actuator_trnid[a] : -1});
       af.push_back(m.actuator_gear[a]);
       af.insert(af.end(), &m.actuator_gainprm[3 * a], &m.actuator_gainprm[3 * a] + 3);
       af.insert(af.end(), &m.actuator_biasprm[3 * a], &m.actuator_biasprm[3 * a] + 3);
@@ -273,7 +314,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     std::vector<double> damp(m.dof_damping);
     if (m.integrator == 2 || m.integrator == 3) {
       for (int a = 0; a < m.nu; a++) {
-        if (!m.actuator_biastype[a]) continue;
+        if (!m.actuator_biastype[a] || m.actuator_trntype[a] != 0) continue;
         double gv = m.actuator_gaintype[a] ? m.actuator_gainprm[3 * a + 2] : 0;
         double bv = m.actuator_biasprm[3 * a + 2];
         if (gv != 0 || bv == 0) continue;
@@ -292,7 +333,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 24);
     int rows_per_con = 1;
     for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : 2 * (p.condim - 1));
-    int rows_bound = d.neq + d.nfloss + 2 * d.nlimit + rows_per_con * d.ncon_max;
+    int rows_bound = d.neq + d.nfloss + d.ntfloss + 2 * (d.nlimit + d.ntlimit) + rows_per_con * d.ncon_max;
     d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 64));
     // workspace layout
     int nv = m.nv, nb = m.nbody, nj = std::max(1, m.njnt), ng = std::max(1, m.ngeom), nu = std::max(1, m.nu);

@@ -666,15 +666,20 @@ struct Compiler {
       m.nu++;
       auto nm = a.attr("name");
       m.actuator_name.push_back(nm ? *nm : std::string());
-      std::string jn = get(a, "joint", cls);
-      if (jn.empty()) fail("actuator needs a joint transmission");
-      int jid = -1;
-      for (int j = 0; j < m.njnt; j++)
-        if (m.jnt_name[j] == jn) jid = j;
-      if (jid < 0) fail("actuator references unknown joint '" + jn + "'");
-      if (m.jnt_type[jid] != JNT_HINGE && m.jnt_type[jid] != JNT_SLIDE) fail("actuator transmission must be a hinge or slide joint");
-      m.actuator_trntype.push_back(0);
-      m.actuator_trnid.push_back(jid);
+      std::string jn = get(a, "joint", cls), tn = get(a, "tendon", cls);
+      if (jn.empty() == tn.empty()) fail("actuator needs exactly one transmission: joint= or tendon=");
+      if (!tn.empty()) {
+        m.actuator_trntype.push_back(3);
+        m.actuator_trnid.push_back(tendon_by_name(tn));
+      } else {
+        int jid = -1;
+        for (int j = 0; j < m.njnt; j++)
+          if (m.jnt_name[j] == jn) jid = j;
+        if (jid < 0) fail("actuator references unknown joint '" + jn + "'");
+        if (m.jnt_type[jid] != JNT_HINGE && m.jnt_type[jid] != JNT_SLIDE) fail("actuator transmission must be a hinge or slide joint");
+        m.actuator_trntype.push_back(0);
+        m.actuator_trnid.push_back(jid);
+      }
       auto gear = nums(a, "gear", cls, {1});
       m.actuator_gear.push_back(gear.at(0));
       double g[3] = {0, 0, 0}, bsp[3] = {0, 0, 0};
@@ -756,6 +761,57 @@ struct Compiler {
     }
   }
 
+  void parse_tendon(const XmlNode& n) {
+    for (auto& t : n.children) {
+      if (t.tag == "spatial") fail("spatial tendons are not supported by this build (fixed tendons are)");
+      if (t.tag != "fixed") fail("unsupported element <" + t.tag + "> inside <tendon>");
+      std::string cls;
+      auto nm = t.attr("name");
+      m.tendon_name.push_back(nm ? *nm : std::string());
+      m.tendon_adr.push_back((int)m.wrap_joint.size());
+      for (auto& w : t.children) {
+        if (w.tag != "joint") fail("fixed tendon elements must be <joint>");
+        auto jn = w.attr("joint");
+        if (!jn) fail("tendon joint needs joint=");
+        int j = joint_by_name(*jn);
+        if (m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE) fail("fixed tendons use hinge or slide joints");
+        m.wrap_joint.push_back(j);
+        m.wrap_coef.push_back(num(w, "coef", cls, 1));
+      }
+      m.tendon_num.push_back((int)m.wrap_joint.size() - m.tendon_adr.back());
+      auto rng = nums(t, "range", cls, {0, 0});
+      auto lim = t.attr("limited");
+      const bool auto_lim = !lim || *lim == "auto";
+      if (lim && !auto_lim && *lim != "true" && *lim != "false") fail("tendon limited= must be true, false or auto");
+      bool limited = auto_lim ? (rng.size() == 2 && rng[0] < rng[1]) : (*lim == "true");
+      m.tendon_limited.push_back(limited);
+      m.tendon_range.push_back(rng.at(0));
+      m.tendon_range.push_back(rng.at(1));
+      m.tendon_margin.push_back(num(t, "margin", cls, 0));
+      m.tendon_frictionloss.push_back(num(t, "frictionloss", cls, 0));
+      m.tendon_stiffness.push_back(num(t, "stiffness", cls, 0));
+      m.tendon_damping.push_back(num(t, "damping", cls, 0));
+      auto sl = nums(t, "springlength", cls, {-1, -1});
+      m.tendon_lengthspring.push_back(sl.at(0));
+      m.tendon_lengthspring.push_back(sl.size() > 1 ? sl[1] : sl[0]);
+      auto srl = nums(t, "solreflimit", cls, {0.02, 1});
+      auto sil = nums(t, "solimplimit", cls, {0.9, 0.95, 0.001, 0.5, 2});
+      auto srf = nums(t, "solreffriction", cls, {0.02, 1});
+      auto sif = nums(t, "solimpfriction", cls, {0.9, 0.95, 0.001, 0.5, 2});
+      while (sil.size() < 5) sil.push_back(sil.size() == 3 ? 0.5 : 2);
+      while (sif.size() < 5) sif.push_back(sif.size() == 3 ? 0.5 : 2);
+      for (int k = 0; k < 2; k++) { m.tendon_solref_lim.push_back(srl.at(k)); m.tendon_solref_fri.push_back(srf.at(k)); }
+      for (int k = 0; k < 5; k++) { m.tendon_solimp_lim.push_back(sil[k]); m.tendon_solimp_fri.push_back(sif[k]); }
+      m.ntendon++;
+    }
+  }
+
+  int tendon_by_name(const std::string& s) const {
+    for (int t = 0; t < m.ntendon; t++)
+      if (m.tendon_name[t] == s) return t;
+    fail("unknown tendon '" + s + "'");
+  }
+
   void parse_equality(const XmlNode& n) {
     static const std::map<std::string, int> kinds = {{"connect", 0}, {"weld", 1}, {"joint", 2}, {"tendon", 3}};
     for (auto& c : n.children) {
@@ -763,6 +819,12 @@ struct Compiler {
       if (it == kinds.end()) fail("unsupported element <" + c.tag + "> inside <equality>");
       std::string cls;
       int o1 = -1, o2 = -1;
+      if (it->second == 3) {
+        auto t1 = c.attr("tendon1"), t2 = c.attr("tendon2");
+        if (!t1) fail("equality tendon needs tendon1");
+        o1 = tendon_by_name(*t1);
+        if (t2) o2 = tendon_by_name(*t2);
+      }
       if (it->second == 2) {
         auto j1 = c.attr("joint1"), j2 = c.attr("joint2");
         if (!j1) fail("equality joint needs joint1");
@@ -914,11 +976,14 @@ struct Compiler {
         }
       }
     }
+    // tendons before the actuators and equalities that name them
+    for (auto& c : root.children)
+      if (c.tag == "tendon") parse_tendon(c);
     for (auto& c : root.children) {
       if (c.tag == "actuator") parse_actuator(c);
       else if (c.tag == "contact") parse_contact(c);
       else if (c.tag == "equality") parse_equality(c);
-      else if (c.tag == "compiler" || c.tag == "default" || c.tag == "asset" || c.tag == "option" || c.tag == "worldbody" || c.tag == "size" ||
+      else if (c.tag == "tendon" || c.tag == "compiler" || c.tag == "default" || c.tag == "asset" || c.tag == "option" || c.tag == "worldbody" || c.tag == "size" ||
                c.tag == "visual" || c.tag == "statistic" || c.tag == "keyframe")
         continue;
       else fail("unsupported top-level element <" + c.tag + ">");
@@ -1149,6 +1214,26 @@ void compute_invweights(Model& m) {
       m.dof_invweight0[a] = minv_diag[a];
     }
   }
+  // fixed tendons: rest length and invweight J M^-1 J^T at qpos0
+  m.tendon_length0.assign(m.ntendon, 0);
+  m.tendon_invweight0.assign(m.ntendon, 0);
+  for (int t = 0; t < m.ntendon; t++) {
+    std::vector<double> jt(nv, 0.0);
+    double len = 0;
+    for (int w = m.tendon_adr[t]; w < m.tendon_adr[t] + m.tendon_num[t]; w++) {
+      const int j = m.wrap_joint[w];
+      len += m.wrap_coef[w] * m.qpos0[m.jnt_qposadr[j]];
+      jt[m.jnt_dofadr[j]] += m.wrap_coef[w];
+    }
+    std::vector<double> x = jt;
+    chol_solve(L, nv, x.data());
+    double iw = 0;
+    for (int i = 0; i < nv; i++) iw += jt[i] * x[i];
+    m.tendon_length0[t] = len;
+    m.tendon_invweight0[t] = iw;
+    // springlength "-1 -1" (the default) means the length at qpos0
+    if (m.tendon_lengthspring[2 * t] == -1 && m.tendon_lengthspring[2 * t + 1] == -1) m.tendon_lengthspring[2 * t] = m.tendon_lengthspring[2 * t + 1] = len;
+  }
   // body invweights: A = J M^-1 J^T at the body COM
   std::vector<double> J(6 * nv), X(6 * nv);
   for (int b = 1; b < nb; b++) {
@@ -1365,10 +1450,15 @@ void finalize_model(Model& m, const LoadOptions& opt) {
   compute_invweights(m);
   // joint equality regulariser: sum of the coupled dofs' invweights
   for (size_t e = 0; e < m.eq_type.size(); e++) {
-    if (m.eq_type[e] != 2) continue;
-    double w = m.dof_invweight0[m.jnt_dofadr[m.eq_obj1[e]]];
-    if (m.eq_obj2[e] >= 0) w += m.dof_invweight0[m.jnt_dofadr[m.eq_obj2[e]]];
-    m.eq_invweight[e] = w;
+    if (m.eq_type[e] == 2) {
+      double w = m.dof_invweight0[m.jnt_dofadr[m.eq_obj1[e]]];
+      if (m.eq_obj2[e] >= 0) w += m.dof_invweight0[m.jnt_dofadr[m.eq_obj2[e]]];
+      m.eq_invweight[e] = w;
+    } else if (m.eq_type[e] == 3) {
+      double w = m.tendon_invweight0[m.eq_obj1[e]];
+      if (m.eq_obj2[e] >= 0) w += m.tendon_invweight0[m.eq_obj2[e]];
+      m.eq_invweight[e] = w;
+    }
   }
   build_pairs(m);
 }
@@ -1420,11 +1510,17 @@ std::string dump_model(const Model& m) {
   dd("geom_solref", m.geom_solref); dd("geom_solimp", m.geom_solimp); dd("geom_solmix", m.geom_solmix);
   dd("geom_margin", m.geom_margin); dd("geom_gap", m.geom_gap); dd("geom_rbound", m.geom_rbound);
   di("mesh_vertadr", m.mesh_vertadr); di("mesh_vertnum", m.mesh_vertnum); dd("mesh_vert", m.mesh_vert);
-  di("actuator_trnid", m.actuator_trnid); di("actuator_gaintype", m.actuator_gaintype); di("actuator_biastype", m.actuator_biastype);
+  di("actuator_trntype", m.actuator_trntype); di("actuator_trnid", m.actuator_trnid); di("actuator_gaintype", m.actuator_gaintype); di("actuator_biastype", m.actuator_biastype);
   di("actuator_ctrllimited", m.actuator_ctrllimited); di("actuator_forcelimited", m.actuator_forcelimited);
   dd("actuator_gear", m.actuator_gear); dd("actuator_gainprm", m.actuator_gainprm); dd("actuator_biasprm", m.actuator_biasprm);
   dd("actuator_ctrlrange", m.actuator_ctrlrange); dd("actuator_forcerange", m.actuator_forcerange);
   di("exclude_body1", m.exclude_body1); di("exclude_body2", m.exclude_body2);
+  di("tendon_adr", m.tendon_adr); di("tendon_num", m.tendon_num); di("tendon_limited", m.tendon_limited); di("wrap_joint", m.wrap_joint);
+  dd("wrap_coef", m.wrap_coef); dd("tendon_range", m.tendon_range); dd("tendon_margin", m.tendon_margin);
+  dd("tendon_frictionloss", m.tendon_frictionloss); dd("tendon_stiffness", m.tendon_stiffness); dd("tendon_damping", m.tendon_damping);
+  dd("tendon_lengthspring", m.tendon_lengthspring); dd("tendon_solref_lim", m.tendon_solref_lim); dd("tendon_solimp_lim", m.tendon_solimp_lim);
+  dd("tendon_solref_fri", m.tendon_solref_fri); dd("tendon_solimp_fri", m.tendon_solimp_fri); dd("tendon_length0", m.tendon_length0);
+  dd("tendon_invweight0", m.tendon_invweight0);
   di("eq_type", m.eq_type); di("eq_obj1", m.eq_obj1); di("eq_obj2", m.eq_obj2); di("eq_active", m.eq_active);
   dd("eq_data", m.eq_data); dd("eq_solref", m.eq_solref); dd("eq_solimp", m.eq_solimp); dd("eq_invweight", m.eq_invweight);
   std::vector<int> ep_i;

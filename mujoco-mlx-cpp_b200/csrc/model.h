@@ -86,6 +86,14 @@ struct Model {
   };
   std::vector<ExplicitPair> explicit_pairs;
 
+  // <tendon><fixed>: length = sum of coef * qpos over its joints (hinge /
+  // slide); spatial tendons are not in this build
+  int ntendon = 0;
+  std::vector<int> tendon_adr, tendon_num, tendon_limited, wrap_joint;
+  std::vector<double> wrap_coef, tendon_range, tendon_margin, tendon_frictionloss, tendon_stiffness, tendon_damping, tendon_lengthspring,
+      tendon_solref_lim, tendon_solimp_lim, tendon_solref_fri, tendon_solimp_fri, tendon_length0, tendon_invweight0;
+  std::vector<std::string> tendon_name;
+
   // <equality>: type 0 connect, 1 weld, 2 joint, 3 tendon (this build steps
   // joint equalities: q1 - q1_0 = poly(q2 - q2_0), poly from 5 coefficients)
   std::vector<int> eq_type, eq_obj1, eq_obj2, eq_active;

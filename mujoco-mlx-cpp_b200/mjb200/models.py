@@ -277,11 +277,19 @@ def arm_xml(iterations: int = 16, tolerance: float = 1e-8, timestep: float = 0.0
 
 
 def joint_ranges(model) -> np.ndarray:
-    """Ranges [nu, 2] of the joints the model's actuators drive (position targets)."""
+    """Ranges [nu, 2] of the joints (or fixed tendons) the model's actuators
+    drive, as position targets; an unlimited tendon gets [-0.2, 0.2]."""
     d = model.dump()
     trn = d["actuator_trnid"]
+    kind = d.get("actuator_trntype", np.zeros_like(trn))
     rng = d["jnt_range"].reshape(-1, 2)
-    return rng[trn]
+    out = np.zeros((len(trn), 2))
+    for a, (k, i) in enumerate(zip(kind, trn)):
+        if k == 3:
+            out[a] = d["tendon_range"].reshape(-1, 2)[i] if d["tendon_limited"][i] else (-0.2, 0.2)
+        else:
+            out[a] = rng[i]
+    return out
 
 
 def random_state(model, num_envs: int, seed: int, height=None, noise: float = 0.1):
@@ -347,6 +355,37 @@ def chain_xml(n: int, cfg: str, iterations: int = 50) -> str:
             f'<option timestep="0.002" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
             f'<worldbody><geom type="plane" size="5 5 0.1" pos="0 0 {floor_z:.4f}"{floor_col}/>'
             + "".join(body) + "</body>" * n + "</worldbody>" + eq + "</mujoco>")
+
+
+def tendon_chain_xml(n: int = 8, iterations: int = 50) -> str:
+    """Hinge chain (as chain_xml, n >= 8, no contact) coupled by fixed
+    tendons: t0 = j0 + 0.5 j1 (limited +-0.3, frictionloss, spring with a
+    dead band, damper), t1 = j2 - j3 + 0.5 j4 (auto-limited +-0.4, margin
+    0.02), t2 = j1 + j5 (frictionloss, spring to its rest length), t3, t4
+    held by a tendon equality t3 - t3_0 = 0.8 (t4 - t4_0); a motor on t0 and
+    a position actuator (kp 5) on t1."""
+    assert n >= 8
+    H = n * CHAIN_LINK + 0.05
+    body = []
+    for i in range(n):
+        axis = "1 0 0" if i % 2 else "0 1 0"
+        z = H if i == 0 else -CHAIN_LINK
+        body.append(f'<body pos="0 0 {z:.4f}"><joint name="j{i}" type="hinge" axis="{axis}" damping="0.02"/>'
+                    f'<geom type="capsule" fromto="0 0 0 0 0 {-CHAIN_LINK}" size="0.02" density="500" contype="0" conaffinity="0"/>')
+    ten = ('<tendon>'
+           '<fixed name="t0" limited="true" range="-0.3 0.3" frictionloss="0.03" stiffness="2" springlength="-0.05 0.05" damping="0.05">'
+           '<joint joint="j0" coef="1"/><joint joint="j1" coef="0.5"/></fixed>'
+           '<fixed name="t1" range="-0.4 0.4" margin="0.02"><joint joint="j2" coef="1"/><joint joint="j3" coef="-1"/><joint joint="j4" coef="0.5"/></fixed>'
+           '<fixed name="t2" frictionloss="0.02" stiffness="1"><joint joint="j1" coef="1"/><joint joint="j5" coef="1"/></fixed>'
+           '<fixed name="t3"><joint joint="j6" coef="1"/><joint joint="j7" coef="0.7"/></fixed>'
+           '<fixed name="t4"><joint joint="j4" coef="1"/><joint joint="j5" coef="-0.3"/></fixed>'
+           '</tendon>')
+    eq = '<equality><tendon tendon1="t3" tendon2="t4" polycoef="0 0.8 0 0 0"/></equality>'
+    act = ('<actuator><motor tendon="t0" gear="1" ctrllimited="true" ctrlrange="-1 1"/>'
+           '<position tendon="t1" kp="5"/></actuator>')
+    return (f'<mujoco model="tendon_chain{n}"><compiler angle="radian"/>'
+            f'<option timestep="0.002" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            '<worldbody>' + "".join(body) + "</body>" * n + "</worldbody>" + ten + eq + act + "</mujoco>")
 
 
 def chain_state(n: int, cfg: str, num_envs: int, seed: int):

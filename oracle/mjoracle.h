@@ -52,6 +52,12 @@ typedef struct OModel {
   int neq;
   const int *eq_type, *eq_obj1, *eq_obj2, *eq_active;
   const double *eq_data, *eq_solref, *eq_solimp, *eq_invweight;
+  /* fixed tendons: length = sum over wraps of coef * qpos (hinge / slide
+     joints); actuator_trntype 0 = joint, 3 = tendon (actuator_trnid) */
+  int ntendon;
+  const int *tendon_adr, *tendon_num, *tendon_limited, *wrap_joint, *actuator_trntype;
+  const double *wrap_coef, *tendon_range, *tendon_margin, *tendon_frictionloss, *tendon_stiffness, *tendon_damping, *tendon_lengthspring;
+  const double *tendon_solref_lim, *tendon_solimp_lim, *tendon_solref_fri, *tendon_solimp_fri, *tendon_length0, *tendon_invweight0;
 } OModel;
 
 /* per-env randomisation (NULL pointers = identity) */
@@ -96,6 +102,8 @@ void oracle_com(const OModel* m, OData* d, const ORand* r);
 void oracle_crb(const OModel* m, OData* d, const ORand* r);
 void oracle_rne(const OModel* m, OData* d, const ORand* r);   /* cvel, cdof_dot, qfrc_bias */
 void oracle_smooth_forces(const OModel* m, OData* d, const ORand* r);  /* passive, actuation, smooth, qacc_smooth */
+/* length, velocity and Jacobian (J: nv doubles, may be NULL) of fixed tendon t */
+void oracle_tendon(const OModel* m, const OData* d, int t, double* len, double* vel, double* J);
 void oracle_collide(const OModel* m, OData* d);
 void oracle_make_constraints(const OModel* m, OData* d, const ORand* r);
 void oracle_solve(const OModel* m, OData* d, int max_iter);

@@ -261,9 +261,26 @@ void oracle_rne(const OModel* m, OData* d, const ORand* rnd) {
   }
 }
 
+/* Fixed tendon (reference: tendon.hpp emit_tendon_phase; MuJoCo
+ * mj_tendon): length = sum coef * qpos, J = sum coef * e_dof. */
+void oracle_tendon(const OModel* m, const OData* d, int t, double* len, double* vel, double* J) {
+  double l = 0, v = 0;
+  if (J) memset(J, 0, m->nv * sizeof(double));
+  for (int w = m->tendon_adr[t]; w < m->tendon_adr[t] + m->tendon_num[t]; w++) {
+    int j = m->wrap_joint[w];
+    double c = m->wrap_coef[w];
+    l += c * d->qpos[m->jnt_qposadr[j]];
+    v += c * d->qvel[m->jnt_dofadr[j]];
+    if (J) J[m->jnt_dofadr[j]] += c;
+  }
+  *len = l;
+  *vel = v;
+}
+
 void oracle_smooth_forces(const OModel* m, OData* d, const ORand* rnd) {
   int nv = m->nv;
   memset(d->qfrc_passive, 0, nv * sizeof(double));
+  double* tJ = d->work;  /* nv */
   if (!(m->disableflags & (1 << 5))) {
     for (int j = 0; j < m->njnt; j++) {
       int t = m->jnt_type[j];
@@ -273,19 +290,40 @@ void oracle_smooth_forces(const OModel* m, OData* d, const ORand* rnd) {
       }
     }
     for (int i = 0; i < nv; i++) d->qfrc_passive[i] -= m->dof_damping[i] * d->qvel[i];
+    /* tendon spring with a dead band [lengthspring lo, hi] and damper
+       (reference: tendon.hpp:360-377) */
+    for (int t = 0; t < m->ntendon; t++) {
+      double k = m->tendon_stiffness[t], c = m->tendon_damping[t];
+      if (k == 0 && c == 0) continue;
+      double len, vel, f = 0;
+      oracle_tendon(m, d, t, &len, &vel, tJ);
+      double lo = m->tendon_lengthspring[2 * t], hi = m->tendon_lengthspring[2 * t + 1];
+      if (len > hi) f += k * (hi - len);
+      else if (len < lo) f += k * (lo - len);
+      f -= c * vel;
+      for (int i = 0; i < nv; i++) d->qfrc_passive[i] += tJ[i] * f;
+    }
   }
   memset(d->qfrc_actuator, 0, nv * sizeof(double));
   if (!(m->disableflags & (1 << 10))) {
     for (int a = 0; a < m->nu; a++) {
-      int j = m->actuator_trnid[a];
-      int qa = m->jnt_qposadr[j], da = m->jnt_dofadr[j];
+      const int tendon = m->actuator_trntype[a] == 3;
       double gear = m->actuator_gear[a];
+      double tl = 0, tv = 0;
+      int qa = 0, da = 0;
+      if (tendon) {
+        oracle_tendon(m, d, m->actuator_trnid[a], &tl, &tv, tJ);
+      } else {
+        int j = m->actuator_trnid[a];
+        qa = m->jnt_qposadr[j];
+        da = m->jnt_dofadr[j];
+      }
       double ctrl = d->ctrl[a];
       if (m->actuator_ctrllimited[a] && !(m->disableflags & (1 << 7))) {
         double lo = m->actuator_ctrlrange[2 * a], hi = m->actuator_ctrlrange[2 * a + 1];
         ctrl = ctrl < lo ? lo : ctrl > hi ? hi : ctrl;
       }
-      double len = gear * d->qpos[qa], vel = gear * d->qvel[da];
+      double len = gear * (tendon ? tl : d->qpos[qa]), vel = gear * (tendon ? tv : d->qvel[da]);
       const double* g = &m->actuator_gainprm[3 * a];
       const double* bp = &m->actuator_biasprm[3 * a];
       double gain = g[0] + (m->actuator_gaintype[a] ? g[1] * len + g[2] * vel : 0);
@@ -296,7 +334,10 @@ void oracle_smooth_forces(const OModel* m, OData* d, const ORand* rnd) {
         double lo = m->actuator_forcerange[2 * a], hi = m->actuator_forcerange[2 * a + 1];
         force = force < lo ? lo : force > hi ? hi : force;
       }
-      d->qfrc_actuator[da] += gear * force;
+      if (tendon)
+        for (int i = 0; i < nv; i++) d->qfrc_actuator[i] += gear * force * tJ[i];
+      else
+        d->qfrc_actuator[da] += gear * force;
     }
   }
   for (int i = 0; i < nv; i++) {

@@ -60,28 +60,45 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
   if (m->disableflags & 1) return;
   /* joint equalities first (reference: solver.hpp:259-289; bilateral) */
   if (!(m->disableflags & (1 << 1))) {
+    double* J2 = d->work;  /* nv */
     for (int e = 0; e < m->neq; e++) {
-      if (!m->eq_active[e] || m->eq_type[e] != 2) continue;
+      if (!m->eq_active[e] || (m->eq_type[e] != 2 && m->eq_type[e] != 3)) continue;
       if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
-      int j1 = m->eq_obj1[e], j2 = m->eq_obj2[e];
-      int d1 = m->jnt_dofadr[j1], q1 = m->jnt_qposadr[j1];
+      const int ten = m->eq_type[e] == 3;
+      int o1 = m->eq_obj1[e], o2 = m->eq_obj2[e];
+      /* joint: q - qpos0 / tendon: length - length0, and its rate */
+      double x1, v1, x2 = 0, v2 = 0;
+      int r = add_row(d, nv, T_EQUALITY);
+      double* J = &d->efc_J[r * nv];
+      if (ten) {
+        oracle_tendon(m, d, o1, &x1, &v1, J);
+        x1 -= m->tendon_length0[o1];
+        if (o2 >= 0) {
+          oracle_tendon(m, d, o2, &x2, &v2, J2);
+          x2 -= m->tendon_length0[o2];
+        }
+      } else {
+        x1 = d->qpos[m->jnt_qposadr[o1]] - m->qpos0[m->jnt_qposadr[o1]];
+        v1 = d->qvel[m->jnt_dofadr[o1]];
+        J[m->jnt_dofadr[o1]] = 1;
+        if (o2 >= 0) {
+          memset(J2, 0, nv * sizeof(double));
+          x2 = d->qpos[m->jnt_qposadr[o2]] - m->qpos0[m->jnt_qposadr[o2]];
+          v2 = d->qvel[m->jnt_dofadr[o2]];
+          J2[m->jnt_dofadr[o2]] = 1;
+        }
+      }
       const double* c = &m->eq_data[5 * e];
       double poly = c[0], dpoly = 0;
-      int d2 = -1;
-      if (j2 >= 0) {
-        d2 = m->jnt_dofadr[j2];
-        int q2 = m->jnt_qposadr[j2];
-        double x = d->qpos[q2] - m->qpos0[q2];
-        poly = c[0] + x * (c[1] + x * (c[2] + x * (c[3] + x * c[4])));
-        dpoly = c[1] + x * (2 * c[2] + x * (3 * c[3] + x * 4 * c[4]));
+      if (o2 >= 0) {
+        poly = c[0] + x2 * (c[1] + x2 * (c[2] + x2 * (c[3] + x2 * c[4])));
+        dpoly = c[1] + x2 * (2 * c[2] + x2 * (3 * c[3] + x2 * 4 * c[4]));
+        for (int i = 0; i < nv; i++) J[i] -= dpoly * J2[i];
       }
-      double pos = d->qpos[q1] - m->qpos0[q1] - poly;
-      double vel = d->qvel[d1] - (d2 >= 0 ? dpoly * d->qvel[d2] : 0);
+      double pos = x1 - poly;
+      double vel = v1 - dpoly * v2;
       double k, b, imp;
       impedance(m, &m->eq_solref[2 * e], &m->eq_solimp[5 * e], pos, &k, &b, &imp);
-      int r = add_row(d, nv, T_EQUALITY);
-      d->efc_J[r * nv + d1] = 1;
-      if (d2 >= 0) d->efc_J[r * nv + d2] -= dpoly;
       double R = (1 - imp) / imp * m->eq_invweight[e];
       d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
       d->efc_D[r] = 1 / d->efc_R[r];
@@ -102,6 +119,20 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
       d->efc_aref[r] = -b * d->qvel[i];
       d->efc_floss[r] = m->dof_frictionloss[i];
     }
+    /* tendon frictionloss rows after the dof ones (reference: solver.hpp:320-342) */
+    for (int t = 0; t < m->ntendon; t++) {
+      if (m->tendon_frictionloss[t] <= 0) continue;
+      if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+      double k, b, imp, len, vel;
+      impedance(m, &m->tendon_solref_fri[2 * t], &m->tendon_solimp_fri[5 * t], 0, &k, &b, &imp);
+      int r = add_row(d, nv, T_FRICTION);
+      oracle_tendon(m, d, t, &len, &vel, &d->efc_J[r * nv]);
+      double R = (1 - imp) / imp * m->tendon_invweight0[t];
+      d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+      d->efc_D[r] = 1 / d->efc_R[r];
+      d->efc_aref[r] = -b * vel;
+      d->efc_floss[r] = m->tendon_frictionloss[t];
+    }
   }
   if (!(m->disableflags & (1 << 3))) {
     for (int j = 0; j < m->njnt; j++) {
@@ -121,6 +152,29 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
         d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
         d->efc_D[r] = 1 / d->efc_R[r];
         d->efc_aref[r] = -b * sg * d->qvel[da] - k * imp * pos;
+      }
+    }
+    /* tendon limits after the joint limits, lower side then upper side
+       (reference: solver.hpp:370-395) */
+    for (int t = 0; t < m->ntendon; t++) {
+      if (!m->tendon_limited[t]) continue;
+      double len, vel;
+      oracle_tendon(m, d, t, &len, &vel, NULL);
+      for (int side = 0; side < 2; side++) {
+        double dist = side == 0 ? len - m->tendon_range[2 * t] : m->tendon_range[2 * t + 1] - len;
+        double margin = m->tendon_margin[t];
+        if (!(dist < margin)) continue;
+        if (stop || d->nefc + 1 > d->nefc_max) { stop = 1; d->nefc_dropped++; d->status |= ORACLE_EFC_OVERFLOW; continue; }
+        double k, b, imp, pos = dist - margin;
+        impedance(m, &m->tendon_solref_lim[2 * t], &m->tendon_solimp_lim[5 * t], pos, &k, &b, &imp);
+        int r = add_row(d, nv, T_LIMIT);
+        double sg = side == 0 ? 1.0 : -1.0;
+        oracle_tendon(m, d, t, &len, &vel, &d->efc_J[r * nv]);
+        for (int i = 0; i < nv; i++) d->efc_J[r * nv + i] *= sg;
+        double R = (1 - imp) / imp * m->tendon_invweight0[t];
+        d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
+        d->efc_D[r] = 1 / d->efc_R[r];
+        d->efc_aref[r] = -b * sg * vel - k * imp * pos;
       }
     }
   }
@@ -397,7 +451,7 @@ void oracle_integrate(const OModel* m, OData* d) {
   for (int i = 0; i < nv; i++) damp[i] = m->dof_damping[i];
   if (m->integrator == 2 || m->integrator == 3) {
     for (int a = 0; a < m->nu; a++) {
-      if (!m->actuator_biastype[a]) continue;
+      if (!m->actuator_biastype[a] || m->actuator_trntype[a] != 0) continue;
       double gv = m->actuator_gaintype[a] ? m->actuator_gainprm[3 * a + 2] : 0;
       double bv = m->actuator_biasprm[3 * a + 2];
       if (gv != 0 || bv == 0) continue;

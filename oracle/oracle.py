@@ -38,12 +38,19 @@ _EQ_PTR = [("eq_type", "i"), ("eq_obj1", "i"), ("eq_obj2", "i"), ("eq_active", "
            ("eq_data", "f"), ("eq_solref", "f"), ("eq_solimp", "f"), ("eq_invweight", "f")]
 
 
+_TEN_PTR = [("tendon_adr", "i"), ("tendon_num", "i"), ("tendon_limited", "i"), ("wrap_joint", "i"), ("actuator_trntype", "i"),
+            ("wrap_coef", "f"), ("tendon_range", "f"), ("tendon_margin", "f"), ("tendon_frictionloss", "f"), ("tendon_stiffness", "f"),
+            ("tendon_damping", "f"), ("tendon_lengthspring", "f"), ("tendon_solref_lim", "f"), ("tendon_solimp_lim", "f"),
+            ("tendon_solref_fri", "f"), ("tendon_solimp_fri", "f"), ("tendon_length0", "f"), ("tendon_invweight0", "f")]
+
+
 class OModel(C.Structure):
     _fields_ = ([(n, C.c_int) for n in _MODEL_INT] +
                 [("timestep", C.c_double), ("gravity", C.c_double * 3), ("tolerance", C.c_double), ("ls_tolerance", C.c_double),
                  ("impratio", C.c_double), ("meaninertia", C.c_double)] +
                 [(n, _ip if k == "i" else _dp) for n, k in _MODEL_PTR] +
-                [("neq", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _EQ_PTR])
+                [("neq", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _EQ_PTR] +
+                [("ntendon", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _TEN_PTR])
 
 
 class ORand(C.Structure):
@@ -112,7 +119,8 @@ class OracleModel:
         m.gravity[0], m.gravity[1], m.gravity[2] = orr[1:4]
         m.tolerance, m.ls_tolerance, m.impratio, m.meaninertia = orr[4:8]
         m.neq = int(len(dump.get("eq_type", [])))
-        for n, k in _MODEL_PTR + _EQ_PTR:
+        m.ntendon = int(len(dump.get("tendon_adr", [])))
+        for n, k in _MODEL_PTR + _EQ_PTR + _TEN_PTR:
             a = dump[n] if n in dump else np.zeros(0)
             a = np.ascontiguousarray(a, dtype=np.int32 if k == "i" else np.float64)
             if a.size == 0:

@@ -339,3 +339,102 @@ def test_joint_equality_couples_joints():
             worst = max(worst, abs(q[1] - 0.5 * q[0]))
     assert worst < 0.02                              # soft-constraint tracking error while swinging
     assert abs(env.a["qpos"][0]) > 1e-3              # it did swing
+
+
+def _tendon_chain():
+    m = mjb200.load_model_from_string(mjb200.models.tendon_chain_xml(8))
+    om = oracle.OracleModel(m.dump())
+    return m, om
+
+
+# tendon wraps of the tendon chain: tendon -> {dof: coef}
+_TENDON_J = [{0: 1.0, 1: 0.5}, {2: 1.0, 3: -1.0, 4: 0.5}, {1: 1.0, 5: 1.0}, {6: 1.0, 7: 0.7}, {4: 1.0, 5: -0.3}]
+
+
+def _tjac(t, nv=8):
+    J = np.zeros(nv)
+    for k, c in _TENDON_J[t].items():
+        J[k] = c
+    return J
+
+
+def test_tendon_compile_known_answers():
+    """Fixed tendons compile to their wraps; auto limits from range=; rest
+    length and invweight J M^-1 J^T at qpos0; springlength defaults to the
+    rest length; tendon equality invweight = sum of both tendons'."""
+    m, om = _tendon_chain()
+    d = m.dump()
+    assert list(d["tendon_num"]) == [2, 3, 2, 2, 2]
+    assert list(d["tendon_limited"]) == [1, 1, 0, 0, 0]
+    np.testing.assert_allclose(d["tendon_lengthspring"].reshape(-1, 2)[0], [-0.05, 0.05])
+    np.testing.assert_allclose(d["tendon_lengthspring"].reshape(-1, 2)[2], [0.0, 0.0])
+    assert list(d["actuator_trntype"]) == [3, 3] and list(d["actuator_trnid"]) == [0, 1]
+    env = oracle.OracleEnv(om)
+    env.step()  # at qpos0: M is the mass matrix there
+    M = env.a["M"].reshape(8, 8)
+    for t in range(5):
+        J = _tjac(t)
+        assert d["tendon_invweight0"][t] == pytest.approx(J @ np.linalg.solve(M, J), rel=1e-9)
+    assert d["eq_invweight"][0] == pytest.approx(d["tendon_invweight0"][3] + d["tendon_invweight0"][4], rel=1e-12)
+    bad = mjb200.models.tendon_chain_xml(8).replace('<fixed name="t4">', '<spatial name="t5"><site site="x"/></spatial><fixed name="t4">')
+    with pytest.raises(Exception, match="spatial"):
+        mjb200.load_model_from_string(bad)
+
+
+def test_tendon_passive_actuator_and_rows():
+    """Passive force J^T (spring with dead band - damping * velocity), tendon
+    actuator force gear * force * J, and the row order equality -> tendon
+    frictionloss -> tendon limits, each row's J, aref and the Gauss
+    optimality of the solution."""
+    m, om = _tendon_chain()
+    env = oracle.OracleEnv(om)
+    q = np.array([0.5, 0.2, 0.3, -0.2, 0.1, -0.1, 0.2, 0.1])   # t0 = 0.6 > 0.3, t1 = 0.55 > 0.4
+    v = np.array([0.3, -0.2, 0.1, 0.4, -0.3, 0.2, 0.1, -0.1])
+    env.a["qpos"][:] = q
+    env.a["qvel"][:] = v
+    env.a["ctrl"][:2] = [0.7, 0.1]
+    env.step()
+    L = [_tjac(t) @ q for t in range(5)]
+    V = [_tjac(t) @ v for t in range(5)]
+    # passive: dof damping 0.02, t0 spring k=2 dead band [-0.05, 0.05] + damper 0.05, t2 spring k=1 to rest 0
+    f0 = 2.0 * (0.05 - L[0]) - 0.05 * V[0]
+    f2 = 1.0 * (0.0 - L[2])
+    pas = -0.02 * v + _tjac(0) * f0 + _tjac(2) * f2
+    np.testing.assert_allclose(env.a["qfrc_passive"], pas, rtol=1e-12, atol=1e-14)
+    # actuators: motor on t0 (ctrl 0.7), position kp 5 on t1 (target 0.1)
+    act = _tjac(0) * 0.7 + _tjac(1) * 5.0 * (0.1 - L[1])
+    np.testing.assert_allclose(env.a["qfrc_actuator"], act, rtol=1e-12, atol=1e-14)
+    e = env.efc()
+    assert list(e["type"]) == [5, 0, 0, 1, 1]
+    np.testing.assert_allclose(e["J"][0], _tjac(3) - 0.8 * _tjac(4), atol=1e-15)
+    np.testing.assert_allclose(e["J"][1], _tjac(0))
+    np.testing.assert_allclose(e["J"][2], _tjac(2))
+    np.testing.assert_allclose(e["J"][3], -_tjac(0))     # upper side of t0
+    np.testing.assert_allclose(e["J"][4], -_tjac(1))     # upper side of t1
+    # aref of the limit row: -b (J v) - k imp pos with pos = 0.3 - t0 (< 0, saturated imp = dmax)
+    dmax, tc = 0.95, 0.02
+    k, b = 1 / (dmax ** 2 * tc ** 2), 2 / (dmax * tc)
+    assert e["aref"][3] == pytest.approx(-b * (-V[0]) - k * dmax * (0.3 - L[0]), rel=1e-12)
+    res, f, force = _gauss_residual(om, env)
+    assert res < 1e-6
+
+
+def test_tendon_limit_and_equality_hold_in_rollout():
+    """Rolled out under random tendon controls, t0 stays near [-0.3, 0.3]
+    (soft limit), the equality t3 = 0.8 t4 holds to the soft-constraint
+    tracking error, and no env is flagged."""
+    m, om = _tendon_chain()
+    env = oracle.OracleEnv(om)
+    g = np.random.default_rng(2)
+    env.a["qpos"][:] = g.normal(0, 0.1, 8)
+    worst_lim, worst_eq = 0.0, 0.0
+    for s in range(1500):
+        if s % 100 == 0:
+            env.a["ctrl"][:2] = [g.uniform(-1, 1), g.uniform(-0.4, 0.4)]
+        env.step()
+        assert env.d.status == 0
+        q = env.a["qpos"]
+        if s > 50:
+            worst_lim = max(worst_lim, abs(_tjac(0) @ q) - 0.3)
+            worst_eq = max(worst_eq, abs(_tjac(3) @ q - 0.8 * (_tjac(4) @ q)))
+    assert worst_lim < 0.05 and worst_eq < 0.05
