@@ -133,6 +133,11 @@ MJMLX_API const float* mjb200_batched_get_qacc(MjmlxBatchedSim* sim, int* n_out)
  * counterpart in the reference (its get_pack copies to the host).  0 / -1. */
 MJMLX_API int mjb200_batched_pack_device(MjmlxBatchedSim* sim, float** pack_dev);
 
+/* Device pointer to the sensordata of all envs (layout of
+ * mjmlx_batched_get_sensordata; valid until the sim is freed, rewritten by
+ * each step) and its float count; NULL / 0 without sensors. */
+MJMLX_API int mjb200_batched_sensordata_device(MjmlxBatchedSim* sim, float** sensordata_dev, int* n);
+
 /* Per-stage SM clock totals of the lockstep step kernel (8 stages: state check
  * + kinematics, collision, COM + CRB, RNE + forces, unconstrained solve,
  * constraint build, Newton, integration).  enable 1 starts (and zeroes) the

@@ -55,9 +55,20 @@ MJMLX_API float mjmlx_model_opt_timestep(const MjmlxModel* model);
 MJMLX_API void mjmlx_model_set_opt_timestep(MjmlxModel* model, float dt);
 /* Replaces mjmlx.h:78.  Returns 0 for an out-of-range id. */
 MJMLX_API float mjmlx_model_body_mass(const MjmlxModel* model, int body_id);
-/* Replaces mjmlx.h:83.  obj_type: 1 body, 3 joint, 5 geom, 19 actuator
- * (MuJoCo mjtObj numbering).  Returns -1 if not found. */
+/* Replaces mjmlx.h:83.  obj_type: 1 body, 3 joint, 5 geom, 6 site,
+ * 18 tendon, 19 actuator, 20 sensor (MuJoCo mjtObj numbering).  Returns -1
+ * if not found. */
 MJMLX_API int mjmlx_name2id(const MjmlxModel* model, int obj_type, const char* name);
+
+/* MJCF <sensor> metadata: MuJoCo's sensor_type (mjtSensor code), sensor_adr
+ * and sensor_dim, and the name (NULL when unnamed).  -1 / NULL for an
+ * out-of-range id.  Replaces mjmlx.h:86-91. */
+MJMLX_API int mjmlx_model_nsensor(const MjmlxModel* model);
+MJMLX_API int mjmlx_model_nsensordata(const MjmlxModel* model);
+MJMLX_API const char* mjmlx_model_sensor_name(const MjmlxModel* model, int sensor_id);
+MJMLX_API int mjmlx_model_sensor_type(const MjmlxModel* model, int sensor_id);
+MJMLX_API int mjmlx_model_sensor_adr(const MjmlxModel* model, int sensor_id);
+MJMLX_API int mjmlx_model_sensor_dim(const MjmlxModel* model, int sensor_id);
 
 /* ---------------------------------------------------------------- batched */
 
@@ -92,6 +103,22 @@ MJMLX_API const float* mjmlx_batched_get_cinert(const MjmlxBatchedSim* sim, int*
 MJMLX_API const float* mjmlx_batched_get_cvel(const MjmlxBatchedSim* sim, int* n_out);
 MJMLX_API const float* mjmlx_batched_get_qfrc_actuator(const MjmlxBatchedSim* sim, int* n_out);
 MJMLX_API const float* mjmlx_batched_get_cfrc_ext(const MjmlxBatchedSim* sim, int* n_out);
+
+/* Sensor values float[num_envs * nsensordata], each env laid out as MuJoCo's
+ * d->sensordata (sensor_adr).  Like the other getters they belong to the
+ * start state of the last physics step, i.e. MuJoCo's sensordata after
+ * mj_step.  Computed on the device inside the step (no extra launch):
+ * joint / tendon / actuator positions and velocities, joint actuator force,
+ * ball joints, subtree COM, frame pose / axes / velocities (world frame),
+ * gyro, velocimeter, magnetometer, and the accelerometer as the one-step
+ * difference of the site's world velocity minus gravity, in the site frame
+ * (zero difference on the first step after creation or reset).  Other
+ * sensor types, and frame sensors relative to another frame, read 0.
+ * nsensordata: per env; -1 for a mixed-model sim (get_sensordata then
+ * returns every env's values back to back).  NULL / 0 without sensors.
+ * Replace mjmlx.h:220-221. */
+MJMLX_API int mjmlx_batched_nsensordata(const MjmlxBatchedSim* sim);
+MJMLX_API const float* mjmlx_batched_get_sensordata(const MjmlxBatchedSim* sim, int* n_out);
 
 /* Per-env state setters.  Replace mjmlx.h:224-225. */
 MJMLX_API void mjmlx_batched_set_env_qpos(MjmlxBatchedSim* sim, int env_idx, const float* qpos, int nq);

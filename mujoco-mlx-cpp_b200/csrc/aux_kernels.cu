@@ -5,11 +5,13 @@
 #include "devmodel.h"
 
 __global__ void mjb_reset_kernel(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
-                                 float* qpos, float* qvel, float* warm) {
+                                 float* qpos, float* qvel, float* warm, int* sens_valid) {
   int env = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   int lane = threadIdx.x & 31;
   if (env >= B || !mask[env]) return;
   const DevModelDesc& m = models[env_model[env]];
+  // accelerometers restart without a previous velocity (sensor.cpp sensor_mark_reset)
+  if (sens_valid && lane == 0) sens_valid[env] = 0;
   for (int i = lane; i < m.nq; i += 32) qpos[qadr[env] + i] = ftab[m.f_qpos0 + i];
   for (int i = lane; i < m.nv; i += 32) {
     qvel[vadr[env] + i] = 0.f;
@@ -18,11 +20,11 @@ __global__ void mjb_reset_kernel(const DevModelDesc* models, const int* env_mode
 }
 
 cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
-                             float* qpos, float* qvel, float* warm, cudaStream_t s) {
+                             float* qpos, float* qvel, float* warm, int* sens_valid, cudaStream_t s) {
   int warps = 8;
   int grid = (B + warps - 1) / warps;
   if (grid < 1) grid = 1;
-  mjb_reset_kernel<<<grid, warps * 32, 0, s>>>(models, env_model, qadr, vadr, ftab, mask, B, qpos, qvel, warm);
+  mjb_reset_kernel<<<grid, warps * 32, 0, s>>>(models, env_model, qadr, vadr, ftab, mask, B, qpos, qvel, warm, sens_valid);
   return cudaGetLastError();
 }
 

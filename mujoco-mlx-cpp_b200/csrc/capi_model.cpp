@@ -129,13 +129,29 @@ MJMLX_API int mjmlx_name2id(const MjmlxModel* model, int obj_type, const char* n
     case 1: names = &m.body_name; break;
     case 3: names = &m.jnt_name; break;
     case 5: names = &m.geom_name; break;
+    case 6: names = &m.site_name; break;
+    case 18: names = &m.tendon_name; break;
     case 19: names = &m.actuator_name; break;
+    case 20: names = &m.sensor_name; break;
     default: return -1;
   }
   for (size_t k = 0; k < names->size(); k++)
     if ((*names)[k] == name) return (int)k;
   return -1;
 }
+
+MJMLX_API int mjmlx_model_nsensor(const MjmlxModel* model) { return model ? model->model.nsensor : 0; }
+MJMLX_API int mjmlx_model_nsensordata(const MjmlxModel* model) { return model ? model->model.nsensordata : 0; }
+
+static bool sensor_ok(const MjmlxModel* model, int id) { return model && id >= 0 && id < model->model.nsensor; }
+
+MJMLX_API const char* mjmlx_model_sensor_name(const MjmlxModel* model, int sensor_id) {
+  if (!sensor_ok(model, sensor_id) || model->model.sensor_name[sensor_id].empty()) return nullptr;
+  return model->model.sensor_name[sensor_id].c_str();
+}
+MJMLX_API int mjmlx_model_sensor_type(const MjmlxModel* model, int sensor_id) { return sensor_ok(model, sensor_id) ? model->model.sensor_type[sensor_id] : -1; }
+MJMLX_API int mjmlx_model_sensor_adr(const MjmlxModel* model, int sensor_id) { return sensor_ok(model, sensor_id) ? model->model.sensor_adr[sensor_id] : -1; }
+MJMLX_API int mjmlx_model_sensor_dim(const MjmlxModel* model, int sensor_id) { return sensor_ok(model, sensor_id) ? model->model.sensor_dim[sensor_id] : -1; }
 
 MJMLX_API int mjb200_model_dump(const MjmlxModel* model, char* buf, int bufsize) {
   if (!model) return -1;

@@ -148,6 +148,20 @@ MJMLX_API const float* mjmlx_batched_get_cvel(const MjmlxBatchedSim* sim, int* n
 MJMLX_API const float* mjmlx_batched_get_qfrc_actuator(const MjmlxBatchedSim* sim, int* n) { return getter(sim, "qfrc_actuator", n); }
 MJMLX_API const float* mjmlx_batched_get_cfrc_ext(const MjmlxBatchedSim* sim, int* n) { return getter(sim, "cfrc_ext", n); }
 
+MJMLX_API int mjmlx_batched_nsensordata(const MjmlxBatchedSim* sim) {
+  if (!sim || !sim->engine) return 0;
+  if (!sim->engine->uniform()) return -1;
+  return sim->engine->model(0).nsensordata;
+}
+MJMLX_API const float* mjmlx_batched_get_sensordata(const MjmlxBatchedSim* sim, int* n) { return getter(sim, "sensordata", n); }
+
+MJMLX_API int mjb200_batched_sensordata_device(MjmlxBatchedSim* sim, float** sensordata_dev, int* n) {
+  if (!sim || !sim->engine) return -1;
+  if (n) *n = sim->engine->total_sensordata();
+  if (sensordata_dev) *sensordata_dev = sim->engine->total_sensordata() ? sim->engine->sensordata_device() : nullptr;
+  return 0;
+}
+
 MJMLX_API void mjmlx_batched_set_env_qpos(MjmlxBatchedSim* sim, int env_idx, const float* qpos, int nq) {
   if (!sim || !qpos || env_idx < 0 || env_idx >= sim->engine->num_envs()) return;
   (void)nq;

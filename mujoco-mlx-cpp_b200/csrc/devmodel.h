@@ -33,6 +33,8 @@ struct DevModelDesc {
   int ntfloss, i_tfloss;       // tendons with frictionloss (tendon ids)
   int ntlimit, i_tlimit;       // limited tendons (tendon ids)
   int npten, i_pten;           // tendons with stiffness or damping (tendon ids)
+  int nsensor, nsensordata, nsens_acc;
+  int i_sensor;  // MJB_SENSOR_INTS per sensor: mjtSensor type (-1 = reads zero), adr, dim, body, root body, a, b, accelerometer slot
   int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
   int i_mesh;    // 2 per mesh: vertadr vertnum
 
@@ -48,6 +50,8 @@ struct DevModelDesc {
   int f_act;     // 11 per actuator: gear gain(3) bias(3) ctrlrange(2) forcerange(2)
   int f_wrap;    // 1 per wrap: coef
   int f_ten;     // MJB_TEN_FLOATS per tendon (layout below)
+  int f_sensor;  // MJB_SENSOR_FLOATS per sensor: object frame in its body (pos 3, quat 4), actuator gear
+  float magnetic[3];
   int f_mesh_vert;
 
   // per-env shared-memory workspace (float offsets from the warp's base)
@@ -66,6 +70,9 @@ struct DevModelDesc {
 #define MJB_TEN_FLOATS 24
 enum { TEN_LO = 0, TEN_HI, TEN_MARGIN, TEN_FLOSS, TEN_STIFF, TEN_DAMP, TEN_SPRLO, TEN_SPRHI, TEN_SRLIM, TEN_SILIM = 10, TEN_SRFRI = 15,
        TEN_SIFRI = 17, TEN_INVW = 22, TEN_LEN0 = 23 };
+
+#define MJB_SENSOR_INTS 8
+#define MJB_SENSOR_FLOATS 8
 
 // efc row metadata stride (floats) in the workspace: aref D floss type y force q
 #define MJB_EFC_FIELDS 8

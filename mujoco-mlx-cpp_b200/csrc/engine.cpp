@@ -17,7 +17,7 @@ cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, 
 cudaError_t mjb_launch_ray(int B, int nray, const int* env_model, const int* geom_base, const int* geom_count, const float* ginfo, const float* gpose,
                            int ng_max, const float* pnt, const float* vec, float* dist, int* geomid, cudaStream_t s);
 cudaError_t mjb_launch_reset(const DevModelDesc* models, const int* env_model, const int* qadr, const int* vadr, const float* ftab, const int* mask, int B,
-                             float* qpos, float* qvel, float* warm, cudaStream_t s);
+                             float* qpos, float* qvel, float* warm, int* sens_valid, cudaStream_t s);
 
 namespace mjb {
 
@@ -134,6 +134,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.ls_iterations = m.ls_iterations;
     d.timestep = (float)m.timestep;
     for (int k = 0; k < 3; k++) d.gravity[k] = (float)m.gravity[k];
+    for (int k = 0; k < 3; k++) d.magnetic[k] = (float)m.magnetic[k];
     d.tolerance = (float)(cfg.tolerance > 0 ? cfg.tolerance : m.tolerance);
     d.impratio = (float)m.impratio;
     d.scale = (float)(1.0 / (m.meaninertia * std::max(1, m.nv)));
@@ -241,6 +242,45 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.i_tlimit = tb.ai(tlim);
     d.npten = (int)tpas.size();
     d.i_pten = tb.ai(tpas);
+    // sensors (reference: make_sensor_ctx, sensor.cpp:99-210): the object
+    // frame of frame / site sensors relative to its body, state addresses of
+    // joint / actuator / tendon sensors, a slot per accelerometer
+    std::vector<int> si;
+    std::vector<double> sf;
+    int nacc = 0;
+    for (int k = 0; k < m.nsensor; k++) {
+      const int type = m.sensor_supported[k] ? m.sensor_type[k] : -1, ot = m.sensor_objtype[k], id = m.sensor_objid[k];
+      int body = 0, a = 0, b = -1, slot = -1;
+      double lp[3] = {0, 0, 0}, lq[4] = {1, 0, 0, 0}, gear = 1;
+      if (ot == OBJ_SITE) { body = m.site_bodyid[id]; std::copy_n(&m.site_pos[3 * id], 3, lp); std::copy_n(&m.site_quat[4 * id], 4, lq); }
+      else if (ot == OBJ_GEOM) { body = m.geom_bodyid[id]; std::copy_n(&m.geom_pos[3 * id], 3, lp); std::copy_n(&m.geom_quat[4 * id], 4, lq); }
+      else if (ot == OBJ_BODY || ot == OBJ_XBODY) {
+        body = id;
+        if (ot == OBJ_BODY && type != SENS_SUBTREECOM) { std::copy_n(&m.body_ipos[3 * id], 3, lp); std::copy_n(&m.body_iquat[4 * id], 4, lq); }
+      }
+      switch (type) {
+        case SENS_JOINTPOS: case SENS_BALLQUAT: a = m.jnt_qposadr[id]; break;
+        case SENS_JOINTVEL: case SENS_JOINTACTFRC: case SENS_BALLANGVEL: a = m.jnt_dofadr[id]; break;
+        case SENS_TENDONPOS: case SENS_TENDONVEL: a = id; break;
+        case SENS_SUBTREECOM: a = id; break;
+        case SENS_ACTUATORPOS: case SENS_ACTUATORVEL:
+          gear = m.actuator_gear[id];
+          if (m.actuator_trntype[id] == 3) { a = m.actuator_trnid[id]; b = -1; }
+          else { a = m.jnt_qposadr[m.actuator_trnid[id]]; b = m.jnt_dofadr[m.actuator_trnid[id]]; }
+          break;
+        case SENS_ACCELEROMETER: slot = nacc++; break;
+        default: break;
+      }
+      si.insert(si.end(), {type, m.sensor_adr[k], m.sensor_dim[k], body, m.body_rootid[body], a, b, slot});
+      sf.insert(sf.end(), lp, lp + 3);
+      sf.insert(sf.end(), lq, lq + 4);
+      sf.push_back(gear);
+    }
+    d.nsensor = m.nsensor;
+    d.nsensordata = m.nsensordata;
+    d.nsens_acc = nacc;
+    d.i_sensor = tb.ai(si);
+    d.f_sensor = tb.af(sf);
     // joint and tendon equalities (reference: build_solver_equality_table,
     // batched.cpp:411-455; tendon ones measure length - tendon_length0)
     std::vector<int> qi;
@@ -387,6 +427,26 @@ void Engine::alloc_state() {
       q += m.nq; v += m.nv; u += std::max(m.nu, 0); b += m.nbody;
     }
   tot_q_ = q; tot_v_ = v; tot_u_ = u; tot_b_ = b;
+  // sensordata and accelerometer history addresses
+  h_sadr_.assign(B_, 0);
+  h_aadr_.assign(B_, 0);
+  int sd = 0, ac = 0;
+  for (int i = 0; i < B_; i++) {
+    const DevModelDesc& dm = layouts_[h_model_[i]].desc;
+    h_sadr_[i] = sd;
+    h_aadr_[i] = ac;
+    sd += dm.nsensordata;
+    ac += 3 * dm.nsens_acc;
+  }
+  tot_s_ = sd;
+  tot_a_ = ac;
+  d_sadr_.upload(h_sadr_, stream_);
+  d_aadr_.upload(h_aadr_, stream_);
+  sensordata_.alloc(std::max(sd, 1));
+  check(cudaMemsetAsync(sensordata_.p, 0, sizeof(float) * std::max(sd, 1), stream_), "sensordata zero");
+  sens_prev_.alloc(std::max(ac, 1));
+  sens_valid_.alloc(B_);
+  check(cudaMemsetAsync(sens_valid_.p, 0, sizeof(int) * B_, stream_), "sensor history zero");
   d_model_.upload(h_model_, stream_);
   d_qadr_.upload(h_qadr_, stream_);
   d_vadr_.upload(h_vadr_, stream_);
@@ -582,6 +642,15 @@ StepParams Engine::params(int n, bool record) {
     P.rand_friction = rand_fric_.p;
     P.rand_gain = rand_gain_.p;
   }
+  if (tot_s_ > 0) {
+    if (record) P.sensordata = sensordata_.p;
+    P.env_sadr = d_sadr_.p;
+    if (tot_a_ > 0) {
+      P.sens_prev = sens_prev_.p;
+      P.env_aadr = d_aadr_.p;
+      P.sens_valid = sens_valid_.p;
+    }
+  }
   return P;
 }
 
@@ -765,7 +834,7 @@ void Engine::reset(const int* mask) {
   DevBuf<int> dm;
   std::vector<int> hm(mask, mask + B_);
   dm.upload(hm, stream_);
-  check(mjb_launch_reset(d_models_.p, d_model_.p, d_qadr_.p, d_vadr_.p, d_ftab_.p, dm.p, B_, qpos_.p, qvel_.p, warm_.p, stream_), "reset kernel");
+  check(mjb_launch_reset(d_models_.p, d_model_.p, d_qadr_.p, d_vadr_.p, d_ftab_.p, dm.p, B_, qpos_.p, qvel_.p, warm_.p, sens_valid_.p, stream_), "reset kernel");
   sync();
 }
 
@@ -783,6 +852,14 @@ const float* Engine::get_host(const char* what, int* n) {
   else if (w == "qfrc_actuator") { src = rec_qfa_.p; cnt = tot_v_; }
   else if (w == "cfrc_ext") { src = rec_cfrc_.p; cnt = 6 * tot_b_; }
   else if (w == "qacc") { src = rec_qacc_.p; cnt = tot_v_; }
+  else if (w == "sensordata") {
+    if (tot_s_ == 0) {
+      if (n) *n = 0;
+      return nullptr;
+    }
+    src = sensordata_.p;
+    cnt = tot_s_;
+  }
   else return nullptr;
   auto it = h_stage_.find(w);
   if (it == h_stage_.end()) {

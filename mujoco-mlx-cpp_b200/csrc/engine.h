@@ -66,6 +66,8 @@ class Engine {
   int total_q() const { return tot_q_; }
   int total_v() const { return tot_v_; }
   int total_u() const { return tot_u_; }
+  int total_sensordata() const { return tot_s_; }
+  float* sensordata_device() { return sensordata_.p; }
   int total_b() const { return tot_b_; }
   bool uniform() const { return models_.size() == 1; }
 
@@ -178,7 +180,10 @@ class Engine {
   std::vector<ModelLayout> layouts_;
   std::vector<int> h_itab_;
   std::vector<float> h_ftab_;
-  std::vector<int> h_model_, h_qadr_, h_vadr_, h_uadr_, h_badr_;
+  std::vector<int> h_model_, h_qadr_, h_vadr_, h_uadr_, h_badr_, h_sadr_, h_aadr_;
+  int tot_s_ = 0, tot_a_ = 0;   // sensordata floats, accelerometer history floats
+  DevBuf<int> d_sadr_, d_aadr_, sens_valid_;
+  DevBuf<float> sensordata_, sens_prev_;
   DevBuf<DevModelDesc> d_models_;
   DevBuf<int> d_itab_, d_model_, d_qadr_, d_vadr_, d_uadr_, d_badr_;
   DevBuf<float> d_ftab_;

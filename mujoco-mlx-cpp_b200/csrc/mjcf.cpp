@@ -557,6 +557,17 @@ struct Compiler {
     m.geom_mass.push_back(gmass);
   }
 
+  void add_site(const XmlNode& n, const std::string& cls, int body) {
+    m.nsite++;
+    auto nm = n.attr("name");
+    m.site_name.push_back(nm ? *nm : std::string());
+    m.site_bodyid.push_back(body);
+    double pos[3], quat[4];
+    read_frame(n, cls, pos, quat, "site");
+    m.site_pos.insert(m.site_pos.end(), pos, pos + 3);
+    m.site_quat.insert(m.site_quat.end(), quat, quat + 4);
+  }
+
   void parse_body(const XmlNode& n, int parent, const std::string& childclass) {
     std::string cls = childclass;
     if (auto v = n.attr("childclass")) cls = *v;
@@ -606,8 +617,10 @@ struct Compiler {
         add_geom(ch, cls, b);
       } else if (ch.tag == "body") {
         parse_body(ch, b, cls);
-      } else if (ch.tag == "joint" || ch.tag == "freejoint" || ch.tag == "site" || ch.tag == "camera" || ch.tag == "light") {
-        // joints handled above; sites/cameras/lights are not used by the step
+      } else if (ch.tag == "site") {
+        add_site(ch, cls, b);
+      } else if (ch.tag == "joint" || ch.tag == "freejoint" || ch.tag == "camera" || ch.tag == "light") {
+        // joints handled above; cameras/lights are not used by the step
       } else {
         fail("unsupported element <" + ch.tag + "> inside <body> (line " + std::to_string(ch.line) + ")");
       }
@@ -806,6 +819,99 @@ struct Compiler {
     }
   }
 
+  static int index_of(const std::vector<std::string>& names, const std::string& s, const char* what) {
+    for (size_t i = 0; i < names.size(); i++)
+      if (names[i] == s) return (int)i;
+    fail(std::string("unknown ") + what + " '" + s + "'");
+  }
+
+  // <sensor> (reference: sensor.cpp make_sensor_ctx; MuJoCo's sensor list).
+  // Types outside the batched set compile with their MuJoCo dimension and
+  // read as zeros, with a warning, as in the reference.
+  void parse_sensor(const XmlNode& n) {
+    struct Kind { int type, dim; const char* obj; };
+    static const std::map<std::string, Kind> kinds = {
+        {"touch", {SENS_TOUCH, 1, "site"}}, {"accelerometer", {SENS_ACCELEROMETER, 3, "site"}}, {"velocimeter", {SENS_VELOCIMETER, 3, "site"}},
+        {"gyro", {SENS_GYRO, 3, "site"}}, {"force", {SENS_FORCE, 3, "site"}}, {"torque", {SENS_TORQUE, 3, "site"}},
+        {"magnetometer", {SENS_MAGNETOMETER, 3, "site"}}, {"rangefinder", {SENS_RANGEFINDER, 1, "site"}},
+        {"jointpos", {SENS_JOINTPOS, 1, "joint"}}, {"jointvel", {SENS_JOINTVEL, 1, "joint"}}, {"tendonpos", {SENS_TENDONPOS, 1, "tendon"}},
+        {"tendonvel", {SENS_TENDONVEL, 1, "tendon"}}, {"actuatorpos", {SENS_ACTUATORPOS, 1, "actuator"}},
+        {"actuatorvel", {SENS_ACTUATORVEL, 1, "actuator"}}, {"actuatorfrc", {SENS_ACTUATORFRC, 1, "actuator"}},
+        {"jointactuatorfrc", {SENS_JOINTACTFRC, 1, "joint"}}, {"tendonactuatorfrc", {SENS_TENDONACTFRC, 1, "tendon"}},
+        {"ballquat", {SENS_BALLQUAT, 4, "joint"}}, {"ballangvel", {SENS_BALLANGVEL, 3, "joint"}},
+        {"jointlimitpos", {SENS_JOINTLIMITPOS, 1, "joint"}}, {"jointlimitvel", {SENS_JOINTLIMITVEL, 1, "joint"}},
+        {"jointlimitfrc", {SENS_JOINTLIMITFRC, 1, "joint"}}, {"tendonlimitpos", {SENS_TENDONLIMITPOS, 1, "tendon"}},
+        {"tendonlimitvel", {SENS_TENDONLIMITVEL, 1, "tendon"}}, {"tendonlimitfrc", {SENS_TENDONLIMITFRC, 1, "tendon"}},
+        {"framepos", {SENS_FRAMEPOS, 3, "frame"}}, {"framequat", {SENS_FRAMEQUAT, 4, "frame"}}, {"framexaxis", {SENS_FRAMEXAXIS, 3, "frame"}},
+        {"frameyaxis", {SENS_FRAMEYAXIS, 3, "frame"}}, {"framezaxis", {SENS_FRAMEZAXIS, 3, "frame"}},
+        {"framelinvel", {SENS_FRAMELINVEL, 3, "frame"}}, {"frameangvel", {SENS_FRAMEANGVEL, 3, "frame"}},
+        {"framelinacc", {SENS_FRAMELINACC, 3, "frame"}}, {"frameangacc", {SENS_FRAMEANGACC, 3, "frame"}},
+        {"subtreecom", {SENS_SUBTREECOM, 3, "body"}}, {"subtreelinvel", {SENS_SUBTREELINVEL, 3, "body"}},
+        {"subtreeangmom", {SENS_SUBTREEANGMOM, 3, "body"}}};
+    for (auto& c : n.children) {
+      auto it = kinds.find(c.tag);
+      if (it == kinds.end()) fail("unsupported sensor <" + c.tag + ">");
+      const Kind& k = it->second;
+      const std::string obj = k.obj;
+      auto need = [&](const char* attr) {
+        auto v = c.attr(attr);
+        if (!v) fail("sensor <" + c.tag + "> needs " + attr + "=");
+        return *v;
+      };
+      int objtype = OBJ_UNKNOWN, objid = -1;
+      bool supported = true;
+      if (obj == "site") {
+        objtype = OBJ_SITE;
+        objid = index_of(m.site_name, need("site"), "site");
+      } else if (obj == "joint") {
+        objtype = OBJ_JOINT;
+        objid = joint_by_name(need("joint"));
+        const int jt = m.jnt_type[objid];
+        const bool ball = k.type == SENS_BALLQUAT || k.type == SENS_BALLANGVEL;
+        if (ball != (jt == JNT_BALL) || jt == JNT_FREE) fail("sensor <" + c.tag + "> on a joint of the wrong type");
+      } else if (obj == "tendon") {
+        objtype = OBJ_TENDON;
+        objid = tendon_by_name(need("tendon"));
+      } else if (obj == "actuator") {
+        objtype = OBJ_ACTUATOR;
+        objid = index_of(m.actuator_name, need("actuator"), "actuator");
+      } else if (obj == "body") {
+        objtype = OBJ_BODY;
+        objid = body_by_name(need("body"));
+      } else {  // frame sensors: objtype body / xbody / geom / site
+        const std::string ot = need("objtype"), on = need("objname");
+        if (ot == "body") { objtype = OBJ_BODY; objid = body_by_name(on); }
+        else if (ot == "xbody") { objtype = OBJ_XBODY; objid = body_by_name(on); }
+        else if (ot == "geom") { objtype = OBJ_GEOM; objid = geom_by_name(on); }
+        else if (ot == "site") { objtype = OBJ_SITE; objid = index_of(m.site_name, on, "site"); }
+        else fail("frame sensor objtype must be body, xbody, geom or site");
+        if (c.attr("reftype") || c.attr("refname")) supported = false;  // relative frames: not in the batched set
+      }
+      switch (k.type) {
+        case SENS_ACCELEROMETER: case SENS_VELOCIMETER: case SENS_GYRO: case SENS_MAGNETOMETER: case SENS_JOINTPOS: case SENS_JOINTVEL:
+        case SENS_TENDONPOS: case SENS_TENDONVEL: case SENS_ACTUATORPOS: case SENS_ACTUATORVEL: case SENS_JOINTACTFRC: case SENS_BALLQUAT:
+        case SENS_BALLANGVEL: case SENS_FRAMEPOS: case SENS_FRAMEQUAT: case SENS_FRAMEXAXIS: case SENS_FRAMEYAXIS: case SENS_FRAMEZAXIS:
+        case SENS_FRAMELINVEL: case SENS_FRAMEANGVEL: case SENS_SUBTREECOM:
+          break;
+        default:
+          supported = false;
+      }
+      auto nm = c.attr("name");
+      if (!supported)
+        std::fprintf(stderr, "mjb200: sensor '%s' (<%s>) is outside the batched sensor set; its sensordata stays 0\n", nm ? nm->c_str() : "",
+                     c.tag.c_str());
+      m.sensor_name.push_back(nm ? *nm : std::string());
+      m.sensor_type.push_back(k.type);
+      m.sensor_objtype.push_back(objtype);
+      m.sensor_objid.push_back(objid);
+      m.sensor_dim.push_back(k.dim);
+      m.sensor_adr.push_back(m.nsensordata);
+      m.sensor_supported.push_back(supported);
+      m.nsensordata += k.dim;
+      m.nsensor++;
+    }
+  }
+
   int tendon_by_name(const std::string& s) const {
     for (int t = 0; t < m.ntendon; t++)
       if (m.tendon_name[t] == s) return t;
@@ -899,6 +1005,8 @@ struct Compiler {
     m.timestep = num(n, "timestep", cls, m.timestep);
     auto g = nums(n, "gravity", cls, {m.gravity[0], m.gravity[1], m.gravity[2]});
     for (int k = 0; k < 3; k++) m.gravity[k] = g.at(k);
+    auto mg = nums(n, "magnetic", cls, {m.magnetic[0], m.magnetic[1], m.magnetic[2]});
+    for (int k = 0; k < 3; k++) m.magnetic[k] = mg.at(k);
     m.iterations = (int)num(n, "iterations", cls, m.iterations);
     m.tolerance = num(n, "tolerance", cls, m.tolerance);
     m.ls_iterations = (int)num(n, "ls_iterations", cls, m.ls_iterations);
@@ -971,7 +1079,8 @@ struct Compiler {
         for (auto& ch : c.children) {
           if (ch.tag == "body") parse_body(ch, 0, std::string());
           else if (ch.tag == "geom") add_geom(ch, std::string(), 0);
-          else if (ch.tag == "site" || ch.tag == "camera" || ch.tag == "light") continue;
+          else if (ch.tag == "site") add_site(ch, std::string(), 0);
+          else if (ch.tag == "camera" || ch.tag == "light") continue;
           else fail("unsupported element <" + ch.tag + "> inside <worldbody>");
         }
       }
@@ -983,11 +1092,14 @@ struct Compiler {
       if (c.tag == "actuator") parse_actuator(c);
       else if (c.tag == "contact") parse_contact(c);
       else if (c.tag == "equality") parse_equality(c);
-      else if (c.tag == "tendon" || c.tag == "compiler" || c.tag == "default" || c.tag == "asset" || c.tag == "option" || c.tag == "worldbody" || c.tag == "size" ||
+      else if (c.tag == "tendon" || c.tag == "sensor" || c.tag == "compiler" || c.tag == "default" || c.tag == "asset" || c.tag == "option" || c.tag == "worldbody" || c.tag == "size" ||
                c.tag == "visual" || c.tag == "statistic" || c.tag == "keyframe")
         continue;
       else fail("unsupported top-level element <" + c.tag + ">");
     }
+    // sensors last: they name joints, tendons, actuators, bodies, geoms and sites
+    for (auto& c : root.children)
+      if (c.tag == "sensor") parse_sensor(c);
     finish_inertia();
     // meshes into the model
     m.nmesh = (int)mesh_props.size();
@@ -1521,6 +1633,10 @@ std::string dump_model(const Model& m) {
   dd("tendon_lengthspring", m.tendon_lengthspring); dd("tendon_solref_lim", m.tendon_solref_lim); dd("tendon_solimp_lim", m.tendon_solimp_lim);
   dd("tendon_solref_fri", m.tendon_solref_fri); dd("tendon_solimp_fri", m.tendon_solimp_fri); dd("tendon_length0", m.tendon_length0);
   dd("tendon_invweight0", m.tendon_invweight0);
+  di("site_bodyid", m.site_bodyid); dd("site_pos", m.site_pos); dd("site_quat", m.site_quat);
+  di("sensor_type", m.sensor_type); di("sensor_objtype", m.sensor_objtype); di("sensor_objid", m.sensor_objid);
+  di("sensor_dim", m.sensor_dim); di("sensor_adr", m.sensor_adr); di("sensor_supported", m.sensor_supported);
+  dd("magnetic", {m.magnetic[0], m.magnetic[1], m.magnetic[2]});
   di("eq_type", m.eq_type); di("eq_obj1", m.eq_obj1); di("eq_obj2", m.eq_obj2); di("eq_active", m.eq_active);
   dd("eq_data", m.eq_data); dd("eq_solref", m.eq_solref); dd("eq_solimp", m.eq_solimp); dd("eq_invweight", m.eq_invweight);
   std::vector<int> ep_i;

@@ -17,6 +17,18 @@ namespace mjb {
 enum GeomType { GEOM_PLANE = 0, GEOM_HFIELD = 1, GEOM_SPHERE = 2, GEOM_CAPSULE = 3, GEOM_ELLIPSOID = 4, GEOM_CYLINDER = 5, GEOM_BOX = 6, GEOM_MESH = 7 };
 enum JointType { JNT_FREE = 0, JNT_BALL = 1, JNT_SLIDE = 2, JNT_HINGE = 3 };
 enum ConeType { CONE_PYRAMIDAL = 0, CONE_ELLIPTIC = 1 };
+// MuJoCo 3.x mjtSensor codes of the sensor elements this compiler knows
+// (ordering as in MuJoCo's mjtSensor; not checked against 3.5.0's header,
+// which is absent here)
+enum SensorType {
+  SENS_TOUCH = 0, SENS_ACCELEROMETER, SENS_VELOCIMETER, SENS_GYRO, SENS_FORCE, SENS_TORQUE, SENS_MAGNETOMETER, SENS_RANGEFINDER,
+  SENS_CAMPROJECTION, SENS_JOINTPOS, SENS_JOINTVEL, SENS_TENDONPOS, SENS_TENDONVEL, SENS_ACTUATORPOS, SENS_ACTUATORVEL, SENS_ACTUATORFRC,
+  SENS_JOINTACTFRC, SENS_TENDONACTFRC, SENS_BALLQUAT, SENS_BALLANGVEL, SENS_JOINTLIMITPOS, SENS_JOINTLIMITVEL, SENS_JOINTLIMITFRC,
+  SENS_TENDONLIMITPOS, SENS_TENDONLIMITVEL, SENS_TENDONLIMITFRC, SENS_FRAMEPOS, SENS_FRAMEQUAT, SENS_FRAMEXAXIS, SENS_FRAMEYAXIS,
+  SENS_FRAMEZAXIS, SENS_FRAMELINVEL, SENS_FRAMEANGVEL, SENS_FRAMELINACC, SENS_FRAMEANGACC, SENS_SUBTREECOM, SENS_SUBTREELINVEL,
+  SENS_SUBTREEANGMOM
+};
+enum ObjType { OBJ_UNKNOWN = 0, OBJ_BODY = 1, OBJ_XBODY = 2, OBJ_JOINT = 3, OBJ_GEOM = 5, OBJ_SITE = 6, OBJ_TENDON = 18, OBJ_ACTUATOR = 19 };
 enum DisableBit {
   DSBL_CONSTRAINT = 1 << 0, DSBL_EQUALITY = 1 << 1, DSBL_FRICTIONLOSS = 1 << 2, DSBL_LIMIT = 1 << 3,
   DSBL_CONTACT = 1 << 4, DSBL_PASSIVE = 1 << 5, DSBL_GRAVITY = 1 << 6, DSBL_CLAMPCTRL = 1 << 7,
@@ -47,6 +59,7 @@ struct Model {
   double tolerance = 1e-8, ls_tolerance = 0.01, impratio = 1;
   int iterations = 100, ls_iterations = 50, cone = CONE_PYRAMIDAL, integrator = 0, disableflags = 0;
   double meaninertia = 1;   // mean diagonal of M at qpos0 (MuJoCo stat.meaninertia)
+  double magnetic[3] = {0, -0.5, 0};
 
   std::vector<std::string> body_name, jnt_name, geom_name, actuator_name, mesh_name;
 
@@ -85,6 +98,20 @@ struct Model {
     double friction[5], solref[2], solimp[5], margin, gap;
   };
   std::vector<ExplicitPair> explicit_pairs;
+
+  // sites (frames fixed to bodies)
+  int nsite = 0;
+  std::vector<int> site_bodyid;
+  std::vector<double> site_pos, site_quat;
+  std::vector<std::string> site_name;
+
+  // <sensor>: sensor_type is MuJoCo's mjtSensor code, sensor_objtype its
+  // mjtObj code (1 body, 2 xbody, 3 joint, 5 geom, 6 site, 18 tendon,
+  // 19 actuator); sensor_supported 0 = computed as zeros (types outside the
+  // batched sensor set), as the reference does
+  int nsensor = 0, nsensordata = 0;
+  std::vector<int> sensor_type, sensor_objtype, sensor_objid, sensor_dim, sensor_adr, sensor_supported;
+  std::vector<std::string> sensor_name;
 
   // <tendon><fixed>: length = sum of coef * qpos over its joints (hinge /
   // slide); spatial tendons are not in this build

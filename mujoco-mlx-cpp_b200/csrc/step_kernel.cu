@@ -143,6 +143,103 @@ __device__ __noinline__ void record_dyn(Env& E, const StepParams& P, int badr, i
   for (int k = lane; k < m.nv; k += 32) P.rec_qfrc_actuator[vadr + k] = ws[m.w_qfa + k];
 }
 
+// Sensors at the substep's start state (reference: sensor_compute,
+// sensor.cpp:265-356; MuJoCo's position / velocity stage formulas), one lane
+// per sensor, after RNE while kinematics, cvel and qfrc_actuator are in the
+// workspace.  write: store sensordata (last substep); save: store each
+// accelerometer frame's world linear velocity as the next one's previous
+// value.  prev_ok: the stored previous velocity is valid.
+__device__ __noinline__ void record_sensors(Env& E, const StepParams& P, bool write, bool save, bool prev_ok) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  const float* ws = E.ws;
+  const float* qpos = ws + m.w_qpos;
+  const float* qvel = ws + m.w_qvel;
+  float* out = write ? P.sensordata + P.env_sadr[E.env] : nullptr;
+  float* prev = P.sens_prev ? P.sens_prev + P.env_aadr[E.env] : nullptr;
+#pragma unroll 1
+  for (int s = E.lane; s < m.nsensor; s += 32) {
+    const int* si = it + m.i_sensor + MJB_SENSOR_INTS * s;
+    const float* sf = ft + m.f_sensor + MJB_SENSOR_FLOATS * s;
+    const int type = ldi(si, 0), adr = ldi(si, 1), dim = ldi(si, 2), a = ldi(si, 5), b = ldi(si, 6), slot = ldi(si, 7);
+    if (!write && type != 1) continue;   // history only: accelerometers
+    float y[4] = {0.f, 0.f, 0.f, 0.f};
+    switch (type) {
+      case 9: y[0] = qpos[a]; break;                      // jointpos
+      case 10: y[0] = qvel[a]; break;                     // jointvel
+      case 16: y[0] = ws[m.w_qfa + a]; break;             // jointactuatorfrc
+      case 11: case 12: {                                 // tendonpos / tendonvel
+        float len, vel;
+        d_tendon_lv(m, it, ft, qpos, qvel, a, len, vel);
+        y[0] = type == 11 ? len : vel;
+        break;
+      }
+      case 13: case 14: {                                 // actuatorpos / actuatorvel
+        float len, vel;
+        if (b < 0) d_tendon_lv(m, it, ft, qpos, qvel, a, len, vel);
+        else { len = qpos[a]; vel = qvel[b]; }
+        y[0] = ldf(sf, 7) * (type == 13 ? len : vel);
+        break;
+      }
+      case 18: {                                          // ballquat
+        float q[4] = {qpos[a], qpos[a + 1], qpos[a + 2], qpos[a + 3]};
+        const float inv = rsqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        for (int k = 0; k < 4; k++) y[k] = q[k] * inv;
+        break;
+      }
+      case 19: for (int k = 0; k < 3; k++) y[k] = qvel[a + k]; break;                  // ballangvel
+      case 35: for (int k = 0; k < 3; k++) y[k] = ws[m.w_scom + 3 * a + k]; break;     // subtreecom
+      case 1: case 2: case 3: case 6: case 26: case 27: case 28: case 29: case 30: case 31: case 32: {
+        // object frame: body pose composed with the object's local frame
+        const int body = ldi(si, 3), root = ldi(si, 4);
+        const float* bp = ws + m.w_xpos + 3 * body;
+        const float bq[4] = {ws[m.w_xquat + 4 * body], ws[m.w_xquat + 4 * body + 1], ws[m.w_xquat + 4 * body + 2], ws[m.w_xquat + 4 * body + 3]};
+        const float lp[3] = {ldf(sf, 0), ldf(sf, 1), ldf(sf, 2)}, lq[4] = {ldf(sf, 3), ldf(sf, 4), ldf(sf, 5), ldf(sf, 6)};
+        float off[3], pos[3], quat[4], R[9];
+        qrot(bq, lp, off);
+        for (int k = 0; k < 3; k++) pos[k] = bp[k] + off[k];
+        qmul(bq, lq, quat);
+        q2mat(quat, R);
+        // velocity of the frame origin: cvel moved from the root subtree COM
+        const float* cv = ws + m.w_cvel + 6 * body;
+        const float w[3] = {cv[0], cv[1], cv[2]};
+        const float r[3] = {pos[0] - ws[m.w_scom + 3 * root], pos[1] - ws[m.w_scom + 3 * root + 1], pos[2] - ws[m.w_scom + 3 * root + 2]};
+        float wxr[3], v[3];
+        cross3(w, r, wxr);
+        for (int k = 0; k < 3; k++) v[k] = cv[3 + k] + wxr[k];
+        switch (type) {
+          case 26: for (int k = 0; k < 3; k++) y[k] = pos[k]; break;
+          case 27: { const float sg = quat[0] < 0.f ? -1.f : 1.f; for (int k = 0; k < 4; k++) y[k] = sg * quat[k]; break; }
+          case 28: case 29: case 30: for (int k = 0; k < 3; k++) y[k] = R[3 * k + (type - 28)]; break;
+          case 31: for (int k = 0; k < 3; k++) y[k] = v[k]; break;
+          case 32: for (int k = 0; k < 3; k++) y[k] = w[k]; break;
+          case 3: mulmatT(R, w, y); break;
+          case 2: mulmatT(R, v, y); break;
+          case 6: mulmatT(R, m.magnetic, y); break;
+          case 1: {
+            // one-substep difference of the world linear velocity, minus gravity, in the site frame
+            float acc[3] = {0.f, 0.f, 0.f};
+            if (prev_ok)
+              for (int k = 0; k < 3; k++) acc[k] = (v[k] - prev[3 * slot + k]) / m.timestep;
+            for (int k = 0; k < 3; k++) acc[k] -= m.gravity[k];
+            mulmatT(R, acc, y);
+            if (save)
+              for (int k = 0; k < 3; k++) prev[3 * slot + k] = v[k];
+            break;
+          }
+          default: break;
+        }
+        break;
+      }
+      default: break;   // outside the batched set: zeros
+    }
+    if (write)
+      for (int k = 0; k < dim; k++) out[adr + k] = y[k];
+  }
+  __syncwarp();
+}
+
 // unconstrained acceleration qacc_smooth = M^-1 qfrc_smooth
 __device__ __noinline__ void d_qacc_smooth(Env& E) {
   const DevModelDesc& m = *E.md;
@@ -221,7 +318,7 @@ __device__ __noinline__ void write_features(Env& E, const StepParams& P, int nco
   }
 }
 
-__device__ __noinline__ void check_state(Env& E) {
+__device__ __noinline__ bool check_state(Env& E) {
   const DevModelDesc& m = *E.md;
   const float* ws = E.ws;
   bool bad = false;
@@ -232,7 +329,9 @@ __device__ __noinline__ void check_state(Env& E) {
   if (__any_sync(FULL_MASK, bad)) {
     E.status |= MJB_STATUS_BADSTATE;
     reset_env(E);
+    return true;
   }
+  return false;
 }
 
 }  // namespace
@@ -324,6 +423,9 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       __syncwarp();
     }
     const int max_iter = valid ? (P.max_iter > 0 ? P.max_iter : E.md->iterations) : 0;
+    // accelerometer history of this env is valid (cleared by resets)
+    bool sens_ok = valid && P.sens_valid ? P.sens_valid[env] != 0 : false;
+    const bool sensors = valid && E.md->nsensor > 0 && P.env_sadr;
     int nsum = 0, nmax = 0, ncon = 0, nefc = 0, choice = 0;
     float* vec = valid ? ws + E.md->w_vec : ws;
     float* qfc = vec + 5 * nv;
@@ -334,7 +436,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       const bool last = s == P.nsub - 1;
       stage_id = 0;
       if (valid) {
-        check_state(E);
+        if (check_state(E)) sens_ok = false;
         d_kinematics(E);
       }
       STAGE_SYNC();
@@ -350,6 +452,11 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
         d_rne(E, bias);
         d_forces(E, P, bias);
         if (last && P.rec_xpos) record_dyn(E, P, badr, vadr);
+        if (sensors) {
+          const bool write = last && P.sensordata, save = P.sens_prev && s >= P.nsub - 2;
+          if (write || save) record_sensors(E, P, write, save, sens_ok);
+          if (save) sens_ok = true;
+        }
       }
       STAGE_SYNC();
       if (valid) d_qacc_smooth(E);
@@ -393,6 +500,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
         if (P.ncon_out) P.ncon_out[env] = ncon;
         if (P.nefc_out) P.nefc_out[env] = nefc;
         if (P.warm_choice) P.warm_choice[env] = choice;
+        if (P.sens_valid) P.sens_valid[env] = sens_ok;
       }
       __syncwarp();
     }

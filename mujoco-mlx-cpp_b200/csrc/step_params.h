@@ -51,6 +51,16 @@ struct StepParams {
   float* rec_cfrc_ext;
   float* rec_qacc;
 
+  // sensors of the last substep's start state (nullable): sensordata at
+  // env_sadr[env]; accelerometers keep the previous substep's frame linear
+  // velocity (3 floats per accelerometer at env_aadr[env]) and a per-env
+  // flag saying it is valid
+  float* sensordata;
+  const int* env_sadr;
+  float* sens_prev;
+  const int* env_aadr;
+  int* sens_valid;
+
   // parity/debug outputs on the last substep (nullable)
   float* dbg_contacts;      // [B][dbg_ncon_max][MJB_CONTACT_FLOATS]
   int dbg_ncon_max;

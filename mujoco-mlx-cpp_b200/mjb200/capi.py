@@ -99,7 +99,17 @@ def _load():
         "mjb200_batched_stage_timing": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)]),
         "mjb200_batched_get_debug": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
     }
-    for g in ("qpos", "qvel", "xpos", "xquat", "subtree_com", "cinert", "cvel", "qfrc_actuator", "cfrc_ext"):
+    sig.update({
+        "mjmlx_model_nsensor": (C.c_int, [C.c_void_p]),
+        "mjmlx_model_nsensordata": (C.c_int, [C.c_void_p]),
+        "mjmlx_model_sensor_name": (C.c_char_p, [C.c_void_p, C.c_int]),
+        "mjmlx_model_sensor_type": (C.c_int, [C.c_void_p, C.c_int]),
+        "mjmlx_model_sensor_adr": (C.c_int, [C.c_void_p, C.c_int]),
+        "mjmlx_model_sensor_dim": (C.c_int, [C.c_void_p, C.c_int]),
+        "mjmlx_batched_nsensordata": (C.c_int, [C.c_void_p]),
+        "mjb200_batched_sensordata_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), _i32p]),
+    })
+    for g in ("qpos", "qvel", "xpos", "xquat", "subtree_com", "cinert", "cvel", "qfrc_actuator", "cfrc_ext", "sensordata"):
         sig[f"mjmlx_batched_get_{g}"] = (_f32p, [C.c_void_p, _i32p])
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -160,6 +170,19 @@ class Model:
 
     def name2id(self, objtype: int, name: str) -> int:
         return lib.mjmlx_name2id(self.handle, objtype, name.encode())
+
+    @property
+    def nsensordata(self) -> int:
+        return lib.mjmlx_model_nsensordata(self.handle)
+
+    def sensors(self):
+        """[(name, mjtSensor type, adr, dim)] of the model's sensors."""
+        out = []
+        for i in range(lib.mjmlx_model_nsensor(self.handle)):
+            nm = lib.mjmlx_model_sensor_name(self.handle, i)
+            out.append((nm.decode() if nm else "", lib.mjmlx_model_sensor_type(self.handle, i), lib.mjmlx_model_sensor_adr(self.handle, i),
+                        lib.mjmlx_model_sensor_dim(self.handle, i)))
+        return out
 
 
 def load_model_from_string(xml: str, self_collision: int = 1, max_condim: int = 0) -> Model:
@@ -363,6 +386,14 @@ class BatchedSim:
             raise RuntimeError("pack_device: " + last_error())
         return p.value
 
+    def sensordata_pointer(self):
+        """(device pointer, float count) of every env's sensordata."""
+        p = C.c_void_p()
+        n = C.c_int()
+        if lib.mjb200_batched_sensordata_device(self.handle, C.byref(p), C.byref(n)) != 0:
+            raise RuntimeError("sensordata_device: " + last_error())
+        return p.value, n.value
+
     def raycast(self, pnt, vec, bodyexclude: int = -1, geomgroup=None, flg_static: int = 1):
         """Rays pnt/vec [num_envs, nray, 3] (world frame, per env) against each
         env's geoms at its current qpos: (dist [num_envs, nray], geom id)."""
@@ -424,6 +455,14 @@ class BatchedSim:
         if not p:
             raise RuntimeError(f"get {name} failed: " + last_error())
         return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def sensordata(self):
+        """Sensor values [num_envs, nsensordata] (uniform batch) of the last
+        step's start state."""
+        nsd = lib.mjmlx_batched_nsensordata(self.handle)
+        if nsd <= 0:
+            return np.zeros((self.num_envs, 0), np.float32)
+        return self.get("sensordata").reshape(self.num_envs, nsd)
 
     def stats(self):
         B = self.num_envs

@@ -388,6 +388,80 @@ def tendon_chain_xml(n: int = 8, iterations: int = 50) -> str:
             '<worldbody>' + "".join(body) + "</body>" * n + "</worldbody>" + ten + eq + act + "</mujoco>")
 
 
+def sensor_xml(floor: bool = False) -> str:
+    """Floating torso with an IMU site (tilted), a two-hinge arm with a tip
+    site, a slider, a ball-jointed pendulum and a fixed tendon over the arm
+    hinges; motors, a position actuator and a tendon motor; one sensor of
+    every type in the batched set, plus a touch sensor and a relative frame
+    sensor (outside the set, read as zeros).  floor: a collidable plane
+    under the torso (otherwise the robot floats in free fall)."""
+    plane = '<geom name="floor" type="plane" size="5 5 0.1" pos="0 0 -0.2"/>' if floor else ""
+    return (
+        '<mujoco model="sensor_rig"><compiler angle="radian"/>'
+        '<option timestep="0.004" iterations="30" tolerance="1e-8" integrator="Euler" magnetic="0.1 -0.4 0.3"/>'
+        '<worldbody>' + plane +
+        '<body name="torso" pos="0 0 0.4"><freejoint/>'
+        '<geom name="torso_g" type="box" size="0.12 0.08 0.04" mass="1.5"/>'
+        '<site name="imu" pos="0.02 -0.01 0.03" euler="0.2 0.4 -0.3"/>'
+        '<body name="arm" pos="0.12 0 0"><joint name="shoulder" type="hinge" axis="0 1 0" damping="0.05"/>'
+        '<geom name="arm_g" type="capsule" fromto="0 0 0 0.18 0 0" size="0.02" mass="0.25"/>'
+        '<site name="tip" pos="0.18 0 0" quat="0.8 0.6 0 0"/>'
+        '<body name="fore" pos="0.18 0 0"><joint name="elbow" type="hinge" axis="0 1 0" damping="0.05"/>'
+        '<geom name="fore_g" type="capsule" fromto="0 0 0 0.12 0 0" size="0.015" mass="0.15"/></body></body>'
+        '<body name="slider" pos="-0.12 0 0"><joint name="slide" type="slide" axis="0 0 1" range="-0.08 0.08" damping="0.4"/>'
+        '<geom name="slider_g" type="sphere" size="0.025" mass="0.2" pos="0.01 0 0"/>'
+        '<site name="slider_site" pos="0 0.01 -0.025"/></body>'
+        '<body name="pend" pos="0 0.1 0"><joint name="ballj" type="ball" damping="0.01"/>'
+        '<geom name="pend_g" type="box" size="0.015 0.015 0.04" pos="0 0 -0.04" mass="0.2"/></body>'
+        '</body></worldbody>'
+        '<tendon><fixed name="tsum"><joint joint="shoulder" coef="1"/><joint joint="elbow" coef="0.5"/></fixed></tendon>'
+        '<actuator><motor name="m_sh" joint="shoulder" gear="2"/><motor name="m_el" joint="elbow"/>'
+        '<position name="p_sl" joint="slide" kp="15" gear="1.5"/><motor name="m_t" tendon="tsum" gear="0.5"/></actuator>'
+        '<sensor>'
+        '<gyro name="imu_gyro" site="imu"/><accelerometer name="imu_acc" site="imu"/><velocimeter name="imu_vel" site="imu"/>'
+        '<magnetometer name="imu_mag" site="imu"/><accelerometer name="tip_acc" site="tip"/><gyro name="tip_gyro" site="tip"/>'
+        '<framepos name="imu_pos" objtype="site" objname="imu"/><framequat name="imu_quat" objtype="site" objname="imu"/>'
+        '<framexaxis name="tip_x" objtype="site" objname="tip"/><frameyaxis name="tip_y" objtype="site" objname="tip"/>'
+        '<framezaxis name="tip_z" objtype="site" objname="tip"/><framelinvel name="tip_v" objtype="site" objname="tip"/>'
+        '<frameangvel name="tip_w" objtype="site" objname="tip"/><framepos name="arm_ipos" objtype="body" objname="arm"/>'
+        '<framequat name="arm_iquat" objtype="body" objname="arm"/><framelinvel name="fore_v" objtype="body" objname="fore"/>'
+        '<framepos name="fore_xpos" objtype="xbody" objname="fore"/><framequat name="fore_gq" objtype="geom" objname="fore_g"/>'
+        '<framepos name="slider_gp" objtype="geom" objname="slider_g"/>'
+        '<jointpos name="q_sh" joint="shoulder"/><jointvel name="v_sh" joint="shoulder"/><jointpos name="q_sl" joint="slide"/>'
+        '<jointvel name="v_sl" joint="slide"/><jointactuatorfrc name="f_sh" joint="shoulder"/><jointactuatorfrc name="f_sl" joint="slide"/>'
+        '<ballquat name="ball_q" joint="ballj"/><ballangvel name="ball_w" joint="ballj"/>'
+        '<actuatorpos name="ap_sh" actuator="m_sh"/><actuatorvel name="av_sh" actuator="m_sh"/>'
+        '<actuatorpos name="ap_t" actuator="m_t"/><actuatorvel name="av_t" actuator="m_t"/>'
+        '<tendonpos name="t_pos" tendon="tsum"/><tendonvel name="t_vel" tendon="tsum"/>'
+        '<subtreecom name="com" body="torso"/><subtreecom name="arm_com" body="arm"/>'
+        '<touch name="touch_tip" site="tip"/><framepos name="rel_pos" objtype="site" objname="tip" reftype="body" refname="torso"/>'
+        '</sensor></mujoco>')
+
+
+def sensor_state(model, num_envs: int, seed: int, qnoise: float = 0.3, vnoise: float = 1.0):
+    """qpos0 with N(0, qnoise) on the hinges, slide and ball (renormalised),
+    the free root rotated by up to 0.5 rad; N(0, vnoise) velocities."""
+    d = model.dump()
+    g = np.random.Generator(np.random.Philox(key=seed))
+    q = np.tile(d["qpos0"].astype(np.float64), (num_envs, 1))
+    jt, qa = d["jnt_type"], d["jnt_qposadr"]
+    for j in range(len(jt)):
+        a = qa[j]
+        if jt[j] in (2, 3):
+            q[:, a] += g.normal(0, qnoise, num_envs)
+            if jt[j] == 2:
+                q[:, a] = np.clip(q[:, a], -0.07, 0.07)
+        else:
+            o = a + 3 if jt[j] == 0 else a
+            ax = g.normal(size=(num_envs, 3))
+            ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+            ang = g.uniform(0, 0.5, num_envs)
+            q[:, o] = np.cos(ang / 2)
+            q[:, o + 1: o + 4] = ax * np.sin(ang / 2)[:, None]
+    v = g.normal(0, vnoise, size=(num_envs, model.nv))
+    return q, v
+
+
 def chain_state(n: int, cfg: str, num_envs: int, seed: int):
     """Random joint angles N(0, 0.5) (beyond the limits for some envs), the
     first joint swung by 1.2 rad for contact configurations, random joint

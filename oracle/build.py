@@ -13,7 +13,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRCS = ["o_dyn.c", "o_collide.c", "o_solver.c", "o_ray.c"]
+SRCS = ["o_dyn.c", "o_collide.c", "o_solver.c", "o_ray.c", "o_sensor.c"]
 OUT = os.path.join(HERE, "liboracle.so")
 
 

@@ -58,6 +58,11 @@ typedef struct OModel {
   const int *tendon_adr, *tendon_num, *tendon_limited, *wrap_joint, *actuator_trntype;
   const double *wrap_coef, *tendon_range, *tendon_margin, *tendon_frictionloss, *tendon_stiffness, *tendon_damping, *tendon_lengthspring;
   const double *tendon_solref_lim, *tendon_solimp_lim, *tendon_solref_fri, *tendon_solimp_fri, *tendon_length0, *tendon_invweight0;
+  /* sites and sensors (sensor_type: MuJoCo mjtSensor code; objtype: mjtObj
+     code 1 body, 2 xbody, 3 joint, 5 geom, 6 site, 18 tendon, 19 actuator) */
+  int nsite, nsensor;
+  const int *site_bodyid, *sensor_type, *sensor_objtype, *sensor_objid, *sensor_dim, *sensor_adr, *sensor_supported;
+  const double *site_pos, *site_quat, *magnetic;
 } OModel;
 
 /* per-env randomisation (NULL pointers = identity) */
@@ -112,6 +117,14 @@ void oracle_integrate(const OModel* m, OData* d);
 /* one full physics step (mj_step with the Euler integrator); max_iter <= 0
  * uses the model's iteration count */
 void oracle_step(const OModel* m, OData* d, const ORand* r, int max_iter);
+
+/* Sensor values of one env after oracle_step, from the quantities that step
+ * computed at its start state (q0, v0): sensordata[nsensordata].  Frame
+ * linear velocities (3 per sensor, world frame) go to linvel_out when not
+ * NULL; accelerometers difference them against prev_linvel (the previous
+ * step's, NULL when there is none) over one timestep. */
+void oracle_sensors(const OModel* m, const OData* d, const double* q0, const double* v0, const double* prev_linvel, double* linvel_out,
+                    double* sensordata);
 
 /* nearest ray hit t (pnt + t vec) among the geoms with include[g] != 0 at
  * the poses of the last oracle_kinematics call; -1 and geomid -1 when none */

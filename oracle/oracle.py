@@ -44,13 +44,18 @@ _TEN_PTR = [("tendon_adr", "i"), ("tendon_num", "i"), ("tendon_limited", "i"), (
             ("tendon_solref_fri", "f"), ("tendon_solimp_fri", "f"), ("tendon_length0", "f"), ("tendon_invweight0", "f")]
 
 
+_SENS_PTR = [("site_bodyid", "i"), ("sensor_type", "i"), ("sensor_objtype", "i"), ("sensor_objid", "i"), ("sensor_dim", "i"),
+             ("sensor_adr", "i"), ("sensor_supported", "i"), ("site_pos", "f"), ("site_quat", "f"), ("magnetic", "f")]
+
+
 class OModel(C.Structure):
     _fields_ = ([(n, C.c_int) for n in _MODEL_INT] +
                 [("timestep", C.c_double), ("gravity", C.c_double * 3), ("tolerance", C.c_double), ("ls_tolerance", C.c_double),
                  ("impratio", C.c_double), ("meaninertia", C.c_double)] +
                 [(n, _ip if k == "i" else _dp) for n, k in _MODEL_PTR] +
                 [("neq", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _EQ_PTR] +
-                [("ntendon", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _TEN_PTR])
+                [("ntendon", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _TEN_PTR] +
+                [("nsite", C.c_int), ("nsensor", C.c_int)] + [(n, _ip if k == "i" else _dp) for n, k in _SENS_PTR])
 
 
 class ORand(C.Structure):
@@ -90,6 +95,7 @@ def _load():
     lib.oracle_step.argtypes = [C.POINTER(OModel), C.POINTER(OData), C.POINTER(ORand), C.c_int]
     lib.oracle_ray.restype = C.c_double
     lib.oracle_ray.argtypes = [C.POINTER(OModel), C.POINTER(OData), _dp, _dp, _ip, _ip]
+    lib.oracle_sensors.argtypes = [C.POINTER(OModel), C.POINTER(OData), _dp, _dp, _dp, _dp, _dp]
     lib.oracle_step_batch.argtypes = [C.POINTER(OModel), C.POINTER(C.POINTER(OData)), C.c_int, C.c_int, C.c_int, C.c_int]
     return lib
 
@@ -120,7 +126,10 @@ class OracleModel:
         m.tolerance, m.ls_tolerance, m.impratio, m.meaninertia = orr[4:8]
         m.neq = int(len(dump.get("eq_type", [])))
         m.ntendon = int(len(dump.get("tendon_adr", [])))
-        for n, k in _MODEL_PTR + _EQ_PTR + _TEN_PTR:
+        m.nsite = int(len(dump.get("site_bodyid", [])))
+        m.nsensor = int(len(dump.get("sensor_type", [])))
+        self.nsensordata = int(np.sum(dump.get("sensor_dim", [])))
+        for n, k in _MODEL_PTR + _EQ_PTR + _TEN_PTR + _SENS_PTR:
             a = dump[n] if n in dump else np.zeros(0)
             a = np.ascontiguousarray(a, dtype=np.int32 if k == "i" else np.float64)
             if a.size == 0:
@@ -169,6 +178,25 @@ class OracleEnv:
 
     def kinematics(self):
         lib.oracle_kinematics(C.byref(self.om.c), C.byref(self.d))
+
+    def step_sensors(self, max_iter: int = 0, rand: ORand | None = None):
+        """One step, then the sensordata of its start state; accelerometers
+        difference against the previous call's frame velocities (none after
+        construction or reset_sensor_history)."""
+        q0 = self.a["qpos"].copy()
+        v0 = self.a["qvel"].copy()
+        self.step(max_iter, rand)
+        ns = max(self.om.c.nsensor, 1)
+        out = np.zeros(max(self.om.nsensordata, 1))
+        lin = np.zeros(3 * ns)
+        prev = getattr(self, "_linvel", None)
+        lib.oracle_sensors(C.byref(self.om.c), C.byref(self.d), _ptr(q0, "f"), _ptr(v0, "f"), None if prev is None else _ptr(prev, "f"),
+                           _ptr(lin, "f"), _ptr(out, "f"))
+        self._linvel = lin
+        return out[: self.om.nsensordata]
+
+    def reset_sensor_history(self):
+        self._linvel = None
 
     def set_predicted(self, qacc):
         if qacc is None:

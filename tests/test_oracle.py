@@ -438,3 +438,96 @@ def test_tendon_limit_and_equality_hold_in_rollout():
             worst_lim = max(worst_lim, abs(_tjac(0) @ q) - 0.3)
             worst_eq = max(worst_eq, abs(_tjac(3) @ q - 0.8 * (_tjac(4) @ q)))
     assert worst_lim < 0.05 and worst_eq < 0.05
+
+
+def _quat2mat(q):
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+
+_FLOATER = ('<mujoco><option timestep="0.005" gravity="0 0 -9.81" magnetic="0.2 -0.5 0.1"/><worldbody>'
+            '<body name="b" pos="0 0 1"><freejoint/><geom type="box" size="0.1 0.2 0.3" mass="2"/>'
+            '<site name="s" pos="0.1 -0.05 0.2"/></body></worldbody>'
+            '<sensor><gyro site="s"/><velocimeter site="s"/><accelerometer site="s"/><magnetometer site="s"/>'
+            '<framequat objtype="site" objname="s"/><framexaxis objtype="site" objname="s"/><framezaxis objtype="site" objname="s"/>'
+            '<framepos objtype="xbody" objname="b"/><touch site="s"/></sensor></mujoco>')
+
+
+def test_sensor_known_answers_free_body():
+    """Free body with a site at p (identity site frame), start state q0, v0:
+    gyro = the free joint's local angular velocity, velocimeter = R^T v +
+    w_local x p, magnetometer = R^T magnetic, frame axes = columns of R,
+    framequat = +-q0 with w >= 0, framepos(xbody) = root position; the
+    accelerometer reads R^T(-g) without history and, for a non-rotating
+    body in free fall, 0 once the previous velocity is known; touch (outside
+    the batched set) reads 0."""
+    m = mjb200.load_model_from_string(_FLOATER)
+    om = oracle.OracleModel(m.dump())
+    env = oracle.OracleEnv(om)
+    q0 = np.array([0.3, -0.2, 1.1, 0.6, 0.3, -0.5, 0.2])
+    q0[3:] /= np.linalg.norm(q0[3:])
+    v0 = np.array([0.4, -0.3, 0.2, 1.5, -0.7, 0.9])
+    env.a["qpos"][:] = q0
+    env.a["qvel"][:] = v0
+    sd = env.step_sensors()
+    R = _quat2mat(q0[3:])
+    p = np.array([0.1, -0.05, 0.2])
+    wl = v0[3:]
+    np.testing.assert_allclose(sd[0:3], wl, atol=1e-12)
+    np.testing.assert_allclose(sd[3:6], R.T @ v0[:3] + np.cross(wl, p), atol=1e-12)
+    np.testing.assert_allclose(sd[6:9], R.T @ np.array([0, 0, 9.81]), atol=1e-12)
+    np.testing.assert_allclose(sd[9:12], R.T @ np.array([0.2, -0.5, 0.1]), atol=1e-12)
+    qs = q0[3:] * (1 if q0[3] >= 0 else -1)
+    np.testing.assert_allclose(sd[12:16], qs, atol=1e-12)
+    np.testing.assert_allclose(sd[16:19], R[:, 0], atol=1e-12)
+    np.testing.assert_allclose(sd[19:22], R[:, 2], atol=1e-12)
+    np.testing.assert_allclose(sd[22:25], q0[:3], atol=1e-12)
+    assert sd[25] == 0.0
+    # no rotation: free fall, accelerometer 0 once a previous velocity exists
+    env.a["qvel"][3:] = 0.0
+    env.step_sensors()
+    sd = env.step_sensors()
+    np.testing.assert_allclose(sd[6:9], 0.0, atol=1e-9)
+    env.reset_sensor_history()
+    sd = env.step_sensors()
+    R = _quat2mat(env.a["qpos"][3:])   # rotation unchanged (no angular velocity)
+    np.testing.assert_allclose(sd[6:9], R.T @ np.array([0, 0, 9.81]), atol=1e-9)
+
+
+def test_sensor_rig_joint_tendon_actuator_values():
+    """Joint, ball, actuator (joint and tendon transmission), tendon and
+    joint actuator force sensors equal the start state's values; sensor
+    adr / dim follow the declaration order; the relative frame sensor and
+    the touch sensor read 0."""
+    m = mjb200.load_model_from_string(mjb200.models.sensor_xml())
+    om = oracle.OracleModel(m.dump())
+    S = {nm: (t, a, dm) for nm, t, a, dm in m.sensors()}
+    assert S["imu_gyro"] == (3, 0, 3) and S["imu_acc"][1:] == (3, 3) and m.nsensordata == sum(v[2] for v in S.values())
+    q, v = mjb200.models.sensor_state(m, 1, 5)
+    env = oracle.OracleEnv(om)
+    env.a["qpos"][:] = q[0]
+    env.a["qvel"][:] = v[0]
+    env.a["ctrl"][:4] = [0.3, -0.2, 0.05, 0.4]
+    sd = env.step_sensors()
+    d = m.dump()
+    jq, jd = d["jnt_qposadr"], d["jnt_dofadr"]
+    val = lambda nm: sd[S[nm][1]: S[nm][1] + S[nm][2]]
+    # joints: 0 free, 1 shoulder, 2 elbow, 3 slide, 4 ball
+    assert val("q_sh")[0] == q[0, jq[1]] and val("v_sh")[0] == v[0, jd[1]]
+    assert val("q_sl")[0] == q[0, jq[3]] and val("v_sl")[0] == v[0, jd[3]]
+    np.testing.assert_allclose(val("ball_q"), q[0, jq[4]: jq[4] + 4] / np.linalg.norm(q[0, jq[4]: jq[4] + 4]))
+    np.testing.assert_allclose(val("ball_w"), v[0, jd[4]: jd[4] + 3])
+    assert val("ap_sh")[0] == pytest.approx(2 * q[0, jq[1]]) and val("av_sh")[0] == pytest.approx(2 * v[0, jd[1]])
+    tl = q[0, jq[1]] + 0.5 * q[0, jq[2]]
+    tv = v[0, jd[1]] + 0.5 * v[0, jd[2]]
+    assert val("t_pos")[0] == pytest.approx(tl) and val("t_vel")[0] == pytest.approx(tv)
+    assert val("ap_t")[0] == pytest.approx(0.5 * tl) and val("av_t")[0] == pytest.approx(0.5 * tv)
+    # shoulder: motor gear 2 (ctrl 0.3) + tendon motor gear 0.5 (ctrl 0.4) through J = 1
+    assert val("f_sh")[0] == pytest.approx(2 * 0.3 + 0.5 * 0.4 * 1.0)
+    # slide: position actuator kp 15, gear 1.5, target 0.05
+    assert val("f_sl")[0] == pytest.approx(1.5 * 15 * (0.05 - 1.5 * q[0, jq[3]]))
+    np.testing.assert_allclose(val("fore_xpos"), env.a["xpos"][3 * 3: 3 * 4])
+    np.testing.assert_allclose(val("com"), env.a["subtree_com"][3:6])
+    assert not val("touch_tip").any() and not val("rel_pos").any()
