@@ -130,6 +130,7 @@ __device__ __noinline__ void d_kinematics(Env& E) {
 }
 
 // Broadphase + narrowphase; contacts in pair order.  Returns ncon.
+template <bool CVX>
 __device__ __noinline__ int d_collide(Env& E) {
   const DevModelDesc& m = *E.md;
   const int* it = E.it;
@@ -152,15 +153,20 @@ __device__ __noinline__ int d_collide(Env& E) {
       float margin = ldf(ft, m.f_pair + 16 * p);
       float s1[3] = {ldf(ft, m.f_geom_size + 3 * g1), ldf(ft, m.f_geom_size + 3 * g1 + 1), ldf(ft, m.f_geom_size + 3 * g1 + 2)};
       float s2[3] = {ldf(ft, m.f_geom_size + 3 * g2), ldf(ft, m.f_geom_size + 3 * g2 + 1), ldf(ft, m.f_geom_size + 3 * g2 + 2)};
-      const float* mesh2 = nullptr;
-      int nvert2 = 0;
+      const float *mesh1 = nullptr, *mesh2 = nullptr;
+      int nvert1 = 0, nvert2 = 0;
+      if (t1 == 7) {
+        int md = ldi(it, m.i_geom_dataid + g1);
+        mesh1 = ft + m.f_mesh_vert + 3 * ldi(it, m.i_mesh + 2 * md);
+        nvert1 = ldi(it, m.i_mesh + 2 * md + 1);
+      }
       if (t2 == 7) {
         int md = ldi(it, m.i_geom_dataid + g2);
         mesh2 = ft + m.f_mesh_vert + 3 * ldi(it, m.i_mesh + 2 * md);
         nvert2 = ldi(it, m.i_mesh + 2 * md + 1);
       }
-      n = c_collide_pair(t1, t2, gxpos + 3 * g1, gxmat + 9 * g1, s1, ldf(ft, m.f_geom_rbound + g1), gxpos + 3 * g2, gxmat + 9 * g2, s2,
-                         ldf(ft, m.f_geom_rbound + g2), mesh2, nvert2, margin, cs);
+      n = c_collide_pair<CVX>(t1, t2, gxpos + 3 * g1, gxmat + 9 * g1, s1, ldf(ft, m.f_geom_rbound + g1), mesh1, nvert1, gxpos + 3 * g2, gxmat + 9 * g2,
+                         s2, ldf(ft, m.f_geom_rbound + g2), mesh2, nvert2, margin, cs);
       if (n < 0) { unsup = true; n = 0; }
     }
     if (__any_sync(FULL_MASK, unsup)) E.status |= MJB_STATUS_UNSUPPORTED_PAIR;

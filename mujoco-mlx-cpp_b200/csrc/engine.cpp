@@ -9,7 +9,7 @@
 #include <numeric>
 
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
-cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
+cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int convex, int* blocks_per_sm);
 cudaError_t mjb_sub(int n, const float* a, const float* b, float* out, cudaStream_t s);
 cudaError_t mjb_launch_pack(int B, int nq, int nv, int nbody, const float* qpos, const float* qvel, const float* cfrc, const float* qfa, const int* bodies,
                             int nsel, int dof_lo, int ndof, int stride, float* out, cudaStream_t s);
@@ -66,12 +66,19 @@ struct TableBuilder {
 };
 
 // Supported narrowphase type combinations (type-ordered).
+// pair needing the GJK / EPA collider (no analytic one)
+bool pair_convex(int t1, int t2) {
+  if (t1 > t2) std::swap(t1, t2);
+  if (t1 == GEOM_PLANE) return false;
+  const bool analytic = (t1 == GEOM_SPHERE && (t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX)) ||
+                        (t1 == GEOM_CAPSULE && (t2 == GEOM_CAPSULE || t2 == GEOM_BOX)) || (t1 == GEOM_BOX && t2 == GEOM_BOX);
+  return !analytic;
+}
+
 bool pair_supported(int t1, int t2) {
   if (t1 == GEOM_PLANE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX || t2 == GEOM_ELLIPSOID || t2 == GEOM_CYLINDER || t2 == GEOM_MESH;
-  if (t1 == GEOM_SPHERE) return t2 == GEOM_SPHERE || t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
-  if (t1 == GEOM_CAPSULE) return t2 == GEOM_CAPSULE || t2 == GEOM_BOX;
-  if (t1 == GEOM_BOX) return t2 == GEOM_BOX;
-  return false;
+  // every pair of convex primitives / meshes: analytic or GJK / EPA
+  return t1 >= GEOM_SPHERE && t2 >= GEOM_SPHERE && t1 <= GEOM_MESH && t2 <= GEOM_MESH;
 }
 
 }  // namespace
@@ -116,6 +123,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
       int t1 = m.geom_type[p.g1], t2 = m.geom_type[p.g2];
       if (!pair_supported(t1, t2))
         throw std::runtime_error("engine: collision pair of geom types " + std::to_string(t1) + "-" + std::to_string(t2) + " has no collider in this build");
+      if (pair_convex(t1, t2)) convex_ = true;
     }
     for (auto& p : m.pairs)
       if (p.condim != 1 && p.condim != 3 && p.condim != 4 && p.condim != 6) throw std::runtime_error("engine: condim must be 1, 3, 4 or 6");
@@ -492,7 +500,7 @@ void Engine::choose_launch() {
   }
   if (smem_ > 227 * 1024) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
   int bps = 0;
-  check(mjb_occupancy(warps_, smem_, &bps), "occupancy");
+  check(mjb_occupancy(warps_, smem_, convex_, &bps), "occupancy");
   if (bps < 1) throw std::runtime_error("engine: kernel cannot be resident with this configuration");
   if (cfg_.blocks_per_sm > 0) bps = std::min(bps, cfg_.blocks_per_sm);
   persistent_ = lockstep_ ? 1 : (cfg_.persistent < 0 ? 1 : cfg_.persistent);
@@ -605,6 +613,7 @@ StepParams Engine::params(int n, bool record) {
   P.qvel = qvel_.p;
   P.ctrl = ctrl_.p;
   P.qacc_warm = warm_.p;
+  P.convex = convex_;
   P.nsub = n;
   P.max_iter = 0;
   P.work_counter = (persistent_ && !lockstep_) ? counter_.p : nullptr;
@@ -670,6 +679,7 @@ StepParams Engine::external_params(float* qpos, float* qvel, const float* ctrl, 
   P.qvel = qvel;
   P.ctrl = ctrl;
   P.qacc_warm = qacc_warm;
+  P.convex = convex_;
   P.nsub = n;
   P.work_counter = work_counter;
   P.lockstep = 0;

@@ -66,6 +66,7 @@ class Engine {
   int total_q() const { return tot_q_; }
   int total_v() const { return tot_v_; }
   int total_u() const { return tot_u_; }
+  bool convex() const { return convex_; }
   int total_sensordata() const { return tot_s_; }
   float* sensordata_device() { return sensordata_.p; }
   int total_b() const { return tot_b_; }
@@ -175,6 +176,7 @@ class Engine {
   int B_ = 0, tot_q_ = 0, tot_v_ = 0, tot_u_ = 0, tot_b_ = 0, nv_max_ = 0;
   EngineConfig cfg_;
   bool rand_on_ = false;
+  bool convex_ = false;   // some model has a pair for the GJK / EPA collider
   cudaStream_t stream_ = nullptr;
 
   std::vector<ModelLayout> layouts_;

@@ -38,7 +38,7 @@
 #include "step_params.h"
 
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
-cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm);
+cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int convex, int* blocks_per_sm);
 
 #define MJB200_NOALLOC_MAX_ENVS 65536
 #define MJB200_NOALLOC_HEAD_WORDS 64  // queue head, padded to 256 bytes
@@ -92,7 +92,7 @@ extern "C" MJMLX_API int mjb200_batched_step_noalloc(MjmlxBatchedSim* sim, float
   cudaError_t e = scratch_address(&scratch);
   const size_t smem = (size_t)kWarpsPerBlock * (E.desc_words() + E.ws_stride()) * 4;
   int bps = 0;
-  if (e == cudaSuccess) e = mjb_occupancy(kWarpsPerBlock, smem, &bps);
+  if (e == cudaSuccess) e = mjb_occupancy(kWarpsPerBlock, smem, E.convex() ? 1 : 0, &bps);
   if (e == cudaSuccess && bps < 1) e = cudaErrorInvalidConfiguration;
   if (e == cudaSuccess) e = cudaMemsetAsync(scratch, 0, sizeof(int), s);
   if (e == cudaSuccess) {

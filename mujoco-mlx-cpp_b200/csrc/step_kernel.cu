@@ -343,6 +343,7 @@ __device__ __noinline__ bool check_state(Env& E) {
 //    envs together and meet at a barrier after every stage, so all warps of
 //    the CTA execute the same stage code at the same time (instruction-cache
 //    locality); envs whose Newton solve ends early wait at the barrier.
+template <bool CVX>
 __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = blockDim.x >> 5;
@@ -440,7 +441,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
         d_kinematics(E);
       }
       STAGE_SYNC();
-      if (valid) ncon = d_collide(E);
+      if (valid) ncon = d_collide<CVX>(E);
       STAGE_SYNC();
       if (valid) {
         d_com(E, P);
@@ -567,19 +568,29 @@ cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, 
   return cudaGetLastError();
 }
 
+// P.convex selects the instance with the GJK / EPA collider (models with
+// general convex pairs); both instances share every other stage.
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
-  static size_t configured = 0;
-  if (smem_bytes > configured) {
-    cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  static size_t configured[2] = {0, 0};
+  const int k = P.convex ? 1 : 0;
+  if (smem_bytes > configured[k]) {
+    cudaError_t e = k ? cudaFuncSetAttribute(mjb_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes)
+                      : cudaFuncSetAttribute(mjb_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (e != cudaSuccess) return e;
-    configured = smem_bytes;
+    configured[k] = smem_bytes;
   }
-  mjb_step_kernel<<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
+  if (k) mjb_step_kernel<true><<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
+  else mjb_step_kernel<false><<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
   return cudaGetLastError();
 }
 
-cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int* blocks_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int convex, int* blocks_per_sm) {
+  if (convex) {
+    cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel<true>, warps_per_block * 32, smem_bytes);
+  }
+  cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel, warps_per_block * 32, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel<false>, warps_per_block * 32, smem_bytes);
 }

@@ -495,6 +495,58 @@ def box_pile_xml(nbox: int = 4, seed: int = 0, iterations: int = 30) -> str:
             '<worldbody><geom name="floor" type="plane" size="0 0 1"/>' + "".join(bodies) + '</worldbody></mujoco>')
 
 
+def noisy_sphere_vertices(npts: int, radius: float, noise: float, g) -> np.ndarray:
+    """npts points on a sphere of the given radius, each radius x U[1 -
+    noise, 1 + noise] (a rock-like convex hull)."""
+    d = g.normal(size=(npts, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return d * (radius * g.uniform(1 - noise, 1 + noise, size=(npts, 1)))
+
+
+CONVEX_SHAPES = ("ellipsoid", "cylinder", "mesh", "capsule", "sphere", "box")
+
+
+def convex_pile_xml(nbody: int = 6, seed: int = 0, iterations: int = 30, condim: int = 3) -> str:
+    """nbody free bodies cycling through ellipsoid, cylinder, 32-point noisy
+    sphere hull (r = 0.05 +- 20 %), capsule, sphere and box (sizes about
+    0.04-0.06 m), stacked loosely in a 0.1 m column above a plane, for the
+    GJK / EPA convex pairs (the bin workload's shapes at a size the dense
+    solver holds: nv = 6 nbody <= 64)."""
+    g = np.random.Generator(np.random.Philox(key=seed))
+    assets, bodies = [], []
+    z = 0.0
+    for i in range(nbody):
+        kind = CONVEX_SHAPES[i % len(CONVEX_SHAPES)]
+        if kind == "ellipsoid":
+            a = g.uniform(0.03, 0.06, 3)
+            geom, h = f'type="ellipsoid" size="{a[0]:.4f} {a[1]:.4f} {a[2]:.4f}"', a.max()
+        elif kind == "cylinder":
+            r, hh = g.uniform(0.03, 0.05), g.uniform(0.03, 0.05)
+            geom, h = f'type="cylinder" size="{r:.4f} {hh:.4f}"', max(r, hh)
+        elif kind == "mesh":
+            v = noisy_sphere_vertices(32, 0.05, 0.2, g)
+            assets.append(f'<mesh name="rock{i}" vertex="' + " ".join(f"{x:.5f}" for x in v.reshape(-1)) + '"/>')
+            geom, h = f'type="mesh" mesh="rock{i}"', 0.06
+        elif kind == "capsule":
+            r, hh = g.uniform(0.02, 0.035), g.uniform(0.03, 0.05)
+            geom, h = f'type="capsule" size="{r:.4f} {hh:.4f}"', r + hh
+        elif kind == "sphere":
+            r = g.uniform(0.03, 0.05)
+            geom, h = f'type="sphere" size="{r:.4f}"', r
+        else:
+            a = g.uniform(0.025, 0.045, 3)
+            geom, h = f'type="box" size="{a[0]:.4f} {a[1]:.4f} {a[2]:.4f}"', np.linalg.norm(a)
+        z += h + 0.002
+        x, y = g.uniform(-0.03, 0.03, 2)
+        bodies.append(f'<body name="b{i}" pos="{x:.4f} {y:.4f} {z:.4f}"><freejoint/><geom {geom} mass="{g.uniform(0.1, 0.4):.3f}"/></body>')
+        z += h
+    return (f'<mujoco model="convex_pile{nbody}"><compiler angle="radian"/>'
+            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            f'<default><geom condim="{condim}" friction="0.7 0.01 0.001"/></default>'
+            + (f'<asset>{"".join(assets)}</asset>' if assets else "")
+            + '<worldbody><geom name="floor" type="plane" size="0 0 1"/>' + "".join(bodies) + '</worldbody></mujoco>')
+
+
 def box_pile_state(model, num_envs: int, seed: int):
     """qpos0 with each box's position jittered by U[-0.03, 0.03] m and its
     orientation rotated by up to 0.4 rad about a random axis."""

@@ -404,6 +404,512 @@ static int box_box(const double* c1, const double* R1, const double* h1, const d
   return ns;
 }
 
+/* ------------------------------------------------------------------ convex
+ * General convex pairs (MuJoCo's convex collider semantics, not the
+ * reference's fixed-direction penetration estimate, collision.hpp:393-487):
+ * GJK distance between the shapes' cores and, when the cores overlap, EPA
+ * penetration (minimum translation distance).  Spheres and capsules enter as
+ * their core point / segment and their radius is added afterwards.  One
+ * contact: normal from geom1 to geom2, position at the midpoint of the two
+ * witness points, dist = separation (negative = penetration).  Tolerance
+ * CVX_TOL absolute (MuJoCo's ccd_tolerance default 1e-6), at most
+ * CVX_ITER GJK iterations and CVX_EPA_ITER EPA expansions.  Unverified
+ * against MuJoCo C. */
+#define CVX_TOL 1e-6
+#define CVX_ITER 64
+#define CVX_EPA_ITER 24
+#define CVX_MAXV (CVX_EPA_ITER + 8)
+#define CVX_MAXF (2 * CVX_MAXV)
+#define CVX_MAXE 48   /* horizon edges per expansion */
+
+typedef struct {
+  int type, dataid;
+  const double *c, *R, *sz;
+  double core;          /* radius added around the core */
+  double rbound;        /* bounding radius of the geom */
+} Shape;
+
+typedef struct { double w[3], a[3]; } SV;   /* Minkowski point w = a - b */
+
+static void core_support(const OModel* m, const Shape* s, const double* dir, double* out) {
+  if (s->type == 2) { memcpy(out, s->c, 3 * sizeof(double)); return; }
+  if (s->type == 3) {
+    double ax = s->R[2] * dir[0] + s->R[5] * dir[1] + s->R[8] * dir[2], h = ax >= 0 ? s->sz[1] : -s->sz[1];
+    for (int k = 0; k < 3; k++) out[k] = s->c[k] + s->R[3 * k + 2] * h;
+    return;
+  }
+  support(s->type, s->c, s->R, s->sz, m, s->dataid, dir, out);
+}
+
+static void mk_support(const OModel* m, const Shape* A, const Shape* B, const double* dir, SV* v) {
+  double nd[3] = {-dir[0], -dir[1], -dir[2]}, b[3];
+  core_support(m, A, dir, v->a);
+  core_support(m, B, nd, b);
+  for (int k = 0; k < 3; k++) v->w[k] = v->a[k] - b[k];
+}
+
+static double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* closest point to the origin on simplex S (n points): v, barycentric lam;
+ * S and lam reduced to the supporting subset.  Returns the new size. */
+static int simplex_closest(SV* S, int n, double* lam, double* v) {
+  if (n == 1) { lam[0] = 1; memcpy(v, S[0].w, 3 * sizeof(double)); return 1; }
+  if (n == 2) {
+    double e[3] = {S[1].w[0] - S[0].w[0], S[1].w[1] - S[0].w[1], S[1].w[2] - S[0].w[2]}, ee = dot3(e, e);
+    double t = ee > 0 ? -dot3(S[0].w, e) / ee : 0;
+    if (t <= 0) { lam[0] = 1; memcpy(v, S[0].w, 3 * sizeof(double)); return 1; }
+    if (t >= 1) { S[0] = S[1]; lam[0] = 1; memcpy(v, S[0].w, 3 * sizeof(double)); return 1; }
+    lam[0] = 1 - t; lam[1] = t;
+    for (int k = 0; k < 3; k++) v[k] = S[0].w[k] + t * e[k];
+    return 2;
+  }
+  if (n == 3) {
+    /* closest point of triangle (A, B, C) to the origin by Voronoi regions */
+    const double *A = S[0].w, *B = S[1].w, *C = S[2].w;
+    double ab[3], ac[3], ap[3] = {-A[0], -A[1], -A[2]};
+    for (int k = 0; k < 3; k++) { ab[k] = B[k] - A[k]; ac[k] = C[k] - A[k]; }
+    double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+    if (d1 <= 0 && d2 <= 0) { lam[0] = 1; memcpy(v, A, 3 * sizeof(double)); return 1; }
+    double bp[3] = {-B[0], -B[1], -B[2]}, d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+    if (d3 >= 0 && d4 <= d3) { S[0] = S[1]; lam[0] = 1; memcpy(v, S[0].w, 3 * sizeof(double)); return 1; }
+    double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+      double t = d1 / (d1 - d3);
+      lam[0] = 1 - t; lam[1] = t;
+      for (int k = 0; k < 3; k++) v[k] = A[k] + t * ab[k];
+      return 2;
+    }
+    double cp[3] = {-C[0], -C[1], -C[2]}, d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+    if (d6 >= 0 && d5 <= d6) { S[0] = S[2]; lam[0] = 1; memcpy(v, S[0].w, 3 * sizeof(double)); return 1; }
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+      double t = d2 / (d2 - d6);
+      S[1] = S[2];
+      lam[0] = 1 - t; lam[1] = t;
+      for (int k = 0; k < 3; k++) v[k] = A[k] + t * ac[k];
+      return 2;
+    }
+    double va = d3 * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+      double t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+      S[0] = S[1]; S[1] = S[2];
+      lam[0] = 1 - t; lam[1] = t;
+      for (int k = 0; k < 3; k++) v[k] = S[0].w[k] + t * (S[1].w[k] - S[0].w[k]);
+      return 2;
+    }
+    double den = 1 / (va + vb + vc), sb = vb * den, sc = vc * den;
+    lam[0] = 1 - sb - sc; lam[1] = sb; lam[2] = sc;
+    for (int k = 0; k < 3; k++) v[k] = A[k] + ab[k] * sb + ac[k] * sc;
+    return 3;
+  }
+  /* tetrahedron: origin inside -> 4; else the closest of the faces that
+     see the origin */
+  static const int F[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 3, 1}, {1, 2, 3, 0}};
+  int best = -1, bn = 0;
+  double bd = 1e300, bl[3], bv[3];
+  SV bs[3];
+  for (int f = 0; f < 4; f++) {
+    const double *P0 = S[F[f][0]].w, *P1 = S[F[f][1]].w, *P2 = S[F[f][2]].w, *Q = S[F[f][3]].w;
+    double e1[3], e2[3], nrm[3];
+    for (int k = 0; k < 3; k++) { e1[k] = P1[k] - P0[k]; e2[k] = P2[k] - P0[k]; }
+    o_cross(e1, e2, nrm);
+    double so = -dot3(nrm, P0), sq = dot3(nrm, Q) - dot3(nrm, P0);
+    if (so * sq >= 0) continue;   /* origin on the same side as the 4th point */
+    SV T[3] = {S[F[f][0]], S[F[f][1]], S[F[f][2]]};
+    double l[3], vv[3];
+    int k = simplex_closest(T, 3, l, vv);
+    double dd = dot3(vv, vv);
+    if (dd < bd) { bd = dd; best = f; bn = k; memcpy(bl, l, sizeof(bl)); memcpy(bv, vv, sizeof(bv)); memcpy(bs, T, sizeof(bs)); }
+  }
+  if (best < 0) { lam[0] = lam[1] = lam[2] = lam[3] = 0.25; v[0] = v[1] = v[2] = 0; return 4; }
+  for (int i = 0; i < bn; i++) { S[i] = bs[i]; lam[i] = bl[i]; }
+  memcpy(v, bv, 3 * sizeof(double));
+  return bn;
+}
+
+typedef struct { int v[3]; double n[3], d; int alive; } Face;
+
+static int epa_face(const SV* V, int i, int j, int k, const double* inner, Face* f) {
+  double e1[3], e2[3], n[3];
+  for (int q = 0; q < 3; q++) { e1[q] = V[j].w[q] - V[i].w[q]; e2[q] = V[k].w[q] - V[i].w[q]; }
+  o_cross(e1, e2, n);
+  double l = o_norm3(n);
+  if (l < 1e-300) return 0;
+  for (int q = 0; q < 3; q++) n[q] /= l;
+  double o[3] = {V[i].w[0] - inner[0], V[i].w[1] - inner[1], V[i].w[2] - inner[2]};
+  if (dot3(n, o) < 0) { int t = j; j = k; k = t; for (int q = 0; q < 3; q++) n[q] = -n[q]; }
+  f->v[0] = i; f->v[1] = j; f->v[2] = k;
+  memcpy(f->n, n, sizeof(n));
+  f->d = dot3(n, V[i].w);
+  f->alive = 1;
+  return 1;
+}
+
+/* penetration of overlapping cores: depth, normal A->B, witness points on
+ * the core surfaces; returns 0 when the polytope could not be built */
+static int epa(const OModel* m, const Shape* A, const Shape* B, SV* S, int n, double* depth, double* nrm, double* pa, double* pb) {
+  SV V[CVX_MAXV];
+  Face Fc[CVX_MAXF];
+  int nv = n, nf = 0;
+  for (int i = 0; i < n; i++) V[i] = S[i];
+  /* grow a degenerate simplex into a tetrahedron */
+  static const double dirs[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  for (int t = 0; nv == 1 && t < 6; t++) {
+    mk_support(m, A, B, dirs[t], &V[1]);
+    double e[3] = {V[1].w[0] - V[0].w[0], V[1].w[1] - V[0].w[1], V[1].w[2] - V[0].w[2]};
+    if (o_norm3(e) > CVX_TOL) nv = 2;
+  }
+  if (nv == 2) {
+    double e[3] = {V[1].w[0] - V[0].w[0], V[1].w[1] - V[0].w[1], V[1].w[2] - V[0].w[2]}, p[3], q[3];
+    const double* ax = fabs(e[0]) < fabs(e[1]) ? (fabs(e[0]) < fabs(e[2]) ? dirs[0] : dirs[4]) : (fabs(e[1]) < fabs(e[2]) ? dirs[2] : dirs[4]);
+    o_cross(e, ax, p);
+    o_cross(e, p, q);
+    const double* cand[4] = {p, q, NULL, NULL};
+    double np_[3] = {-p[0], -p[1], -p[2]}, nq[3] = {-q[0], -q[1], -q[2]};
+    cand[2] = np_; cand[3] = nq;
+    for (int t = 0; nv == 2 && t < 4; t++) {
+      mk_support(m, A, B, cand[t], &V[2]);
+      double f1[3], f2[3], c[3];
+      for (int k = 0; k < 3; k++) { f1[k] = V[1].w[k] - V[0].w[k]; f2[k] = V[2].w[k] - V[0].w[k]; }
+      o_cross(f1, f2, c);
+      if (o_norm3(c) > CVX_TOL * CVX_TOL) nv = 3;
+    }
+  }
+  if (nv == 3) {
+    double f1[3], f2[3], c[3];
+    for (int k = 0; k < 3; k++) { f1[k] = V[1].w[k] - V[0].w[k]; f2[k] = V[2].w[k] - V[0].w[k]; }
+    o_cross(f1, f2, c);
+    for (int sg = 0; nv == 3 && sg < 2; sg++) {
+      double d[3] = {sg ? -c[0] : c[0], sg ? -c[1] : c[1], sg ? -c[2] : c[2]};
+      mk_support(m, A, B, d, &V[3]);
+      double e3[3] = {V[3].w[0] - V[0].w[0], V[3].w[1] - V[0].w[1], V[3].w[2] - V[0].w[2]};
+      if (fabs(dot3(e3, c)) > CVX_TOL * o_norm3(c)) nv = 4;
+    }
+  }
+  if (nv < 4) return 0;
+  double inner[3] = {0, 0, 0};
+  for (int i = 0; i < 4; i++)
+    for (int k = 0; k < 3; k++) inner[k] += 0.25 * V[i].w[k];
+  static const int T4[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+  for (int f = 0; f < 4; f++)
+    if (!epa_face(V, T4[f][0], T4[f][1], T4[f][2], inner, &Fc[nf])) return 0;
+    else nf++;
+  int best = 0;
+  for (int it = 0;; it++) {
+    best = -1;
+    for (int f = 0; f < nf; f++)
+      if (Fc[f].alive && (best < 0 || Fc[f].d < Fc[best].d)) best = f;
+    if (best < 0) return 0;
+    if (it >= CVX_EPA_ITER || nv >= CVX_MAXV) break;
+    SV w;
+    mk_support(m, A, B, Fc[best].n, &w);
+    if (dot3(w.w, Fc[best].n) - Fc[best].d < CVX_TOL) break;
+    /* remove the faces that see w; collect the horizon edges */
+    int edges[CVX_MAXE][2], ne = 0, full = 0;
+    for (int f = 0; f < nf; f++) {
+      if (!Fc[f].alive) continue;
+      double o[3] = {w.w[0] - V[Fc[f].v[0]].w[0], w.w[1] - V[Fc[f].v[0]].w[1], w.w[2] - V[Fc[f].v[0]].w[2]};
+      if (dot3(Fc[f].n, o) <= 0) continue;
+      Fc[f].alive = 0;
+      for (int e = 0; e < 3; e++) {
+        int a = Fc[f].v[e], b = Fc[f].v[(e + 1) % 3], found = -1;
+        for (int q = 0; q < ne; q++)
+          if (edges[q][0] == b && edges[q][1] == a) { found = q; break; }
+        if (found >= 0) { edges[found][0] = edges[ne - 1][0]; edges[found][1] = edges[ne - 1][1]; ne--; }
+        else if (ne < CVX_MAXE) { edges[ne][0] = a; edges[ne][1] = b; ne++; }
+        else full = 1;
+      }
+    }
+    if (full) {   /* horizon too long for the edge buffer: keep the polytope as it was */
+      for (int f = 0; f < nf; f++) Fc[f].alive = 1;
+      break;
+    }
+    /* compact the face list, then add the new faces */
+    int k = 0;
+    for (int f = 0; f < nf; f++)
+      if (Fc[f].alive) Fc[k++] = Fc[f];
+    nf = k;
+    if (nf + ne > CVX_MAXF) break;
+    V[nv] = w;
+    for (int q = 0; q < ne; q++)
+      if (epa_face(V, edges[q][0], edges[q][1], nv, inner, &Fc[nf])) nf++;
+    nv++;
+  }
+  /* witness points: barycentric coordinates of d n in the closest face */
+  const Face* f = &Fc[best];
+  const double *P0 = V[f->v[0]].w, *P1 = V[f->v[1]].w, *P2 = V[f->v[2]].w;
+  double p[3] = {f->d * f->n[0], f->d * f->n[1], f->d * f->n[2]}, e1[3], e2[3], e0[3];
+  for (int q = 0; q < 3; q++) { e1[q] = P1[q] - P0[q]; e2[q] = P2[q] - P0[q]; e0[q] = p[q] - P0[q]; }
+  double d00 = dot3(e1, e1), d01 = dot3(e1, e2), d11 = dot3(e2, e2), d20 = dot3(e0, e1), d21 = dot3(e0, e2);
+  double den = d00 * d11 - d01 * d01, l1 = 0, l2 = 0;
+  if (fabs(den) > 1e-300) { l1 = (d11 * d20 - d01 * d21) / den; l2 = (d00 * d21 - d01 * d20) / den; }
+  double l0 = 1 - l1 - l2;
+  for (int q = 0; q < 3; q++) {
+    pa[q] = l0 * V[f->v[0]].a[q] + l1 * V[f->v[1]].a[q] + l2 * V[f->v[2]].a[q];
+    pb[q] = pa[q] - p[q];
+    nrm[q] = f->n[q];
+  }
+  *depth = f->d;
+  return 1;
+}
+
+/* Newton refinement of the contact normal on curved boundaries.  Depth and
+ * separation are both -min over unit n of h(n) = s(n).n, with s the support
+ * of A - B; EPA's polytope approximates curved patches only coarsely and
+ * GJK's duality-gap stop leaves the normal sqrt(tolerance)-accurate, so a
+ * few tangent-space Newton steps on h finish the minimisation.  Each shape's
+ * support is probed at n +- 1e-3 t1, t2: a shape whose support jumps there
+ * (a capsule core's end switching, a box or mesh edge) has a kink across
+ * the jump's tangent direction, which stays fixed; the step moves only in
+ * the direction left free, with the curvature measured along it.  Two
+ * independent kinks (a face, a vertex against a face) leave nothing to
+ * refine.  Steps are kept only when h decreases.  *depth receives h at the
+ * final normal (the support-plane distance, second-order accurate in the
+ * normal), sv the support there; returns 1 when the normal moved. */
+static int refine_normal(const OModel* m, const Shape* A, const Shape* B, double* n, double* depth, SV* sv) {
+  int moved = 0;
+  SV cur;
+  mk_support(m, A, B, n, &cur);
+  double h = dot3(cur.w, n);
+  const double eps = 1e-3;
+  for (int it = 0; it < 8; it++) {
+    double t1[3], t2[3], ax[3] = {0, 0, 0};
+    ax[fabs(n[0]) < 0.6 ? 0 : (fabs(n[1]) < 0.6 ? 1 : 2)] = 1;
+    o_cross(n, ax, t1);
+    double l = o_norm3(t1);
+    for (int k = 0; k < 3; k++) t1[k] /= l;
+    o_cross(n, t1, t2);
+    const double* T[2] = {t1, t2};
+    /* probe: per shape the largest support move and its tangent direction */
+    SV pr[4];
+    double jump[2] = {0, 0}, kd[2][2] = {{0, 0}, {0, 0}}, jv[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    for (int q = 0; q < 4; q++) {
+      const double* t = T[q & 1];
+      const double e = q < 2 ? eps : -eps;
+      double d[3] = {n[0] + e * t[0], n[1] + e * t[1], n[2] + e * t[2]};
+      mk_support(m, A, B, d, &pr[q]);
+      for (int sh = 0; sh < 2; sh++) {
+        double mv[3];
+        for (int k = 0; k < 3; k++)
+          mv[k] = sh == 0 ? pr[q].a[k] - cur.a[k] : (pr[q].a[k] - pr[q].w[k]) - (cur.a[k] - cur.w[k]);
+        double lm = o_norm3(mv);
+        if (lm > jump[sh]) {
+          jump[sh] = lm;
+          kd[sh][0] = dot3(mv, t1);
+          kd[sh][1] = dot3(mv, t2);
+          for (int k = 0; k < 3; k++) jv[sh][k] = mv[k] / lm;
+        }
+      }
+    }
+    const double rb[2] = {A->rbound, B->rbound};
+    double free_dir[2] = {0, 0}, kink3[3] = {0, 0, 0};
+    int nk = 0, blocked = 0;
+    for (int sh = 0; sh < 2; sh++) {
+      if (jump[sh] <= 20 * eps * rb[sh]) continue;   /* smooth: moves about eps x curvature radius */
+      double lk = sqrt(kd[sh][0] * kd[sh][0] + kd[sh][1] * kd[sh][1]);
+      if (lk < 0.5 * jump[sh]) { blocked = 1; continue; }   /* jump mostly along n */
+      double f[2] = {-kd[sh][1] / lk, kd[sh][0] / lk};
+      if (nk && fabs(f[0] * free_dir[1] - f[1] * free_dir[0]) > 0.1) blocked = 1;   /* two kinks */
+      free_dir[0] = f[0];
+      free_dir[1] = f[1];
+      memcpy(kink3, jv[sh], sizeof(kink3));
+      nk++;
+    }
+    if (blocked) break;
+    if (nk) {
+      /* the kink's minimum lies where the jumping support switches: n
+         orthogonal to the jump (a segment's axis, an edge) */
+      double nn[3], dn = dot3(n, kink3);
+      for (int k = 0; k < 3; k++) nn[k] = n[k] - dn * kink3[k];
+      double ln = o_norm3(nn);
+      for (int k = 0; k < 3; k++) nn[k] /= ln;
+      SV w;
+      mk_support(m, A, B, nn, &w);
+      double hn = dot3(w.w, nn);
+      if (hn < h - 1e-15) {
+        memcpy(n, nn, sizeof(nn));
+        h = hn;
+        cur = w;
+        moved = 1;
+      }
+    }
+    double u[2];
+    if (nk == 0) {
+      double H[2][2], g[2] = {dot3(cur.w, t1), dot3(cur.w, t2)};
+      for (int j2 = 0; j2 < 2; j2++)
+        for (int i2 = 0; i2 < 2; i2++) H[i2][j2] = (dot3(pr[j2].w, T[i2]) - dot3(pr[j2 + 2].w, T[i2])) / (2 * eps) - (i2 == j2 ? h : 0);
+      double a = H[0][0], b = 0.5 * (H[0][1] + H[1][0]), c = H[1][1], det = a * c - b * b;
+      if (!(a > 0 && det > 0)) break;
+      u[0] = -(c * g[0] - b * g[1]) / det;
+      u[1] = -(a * g[1] - b * g[0]) / det;
+    } else {
+      double e3[3], dp[3], dm[3];
+      for (int k = 0; k < 3; k++) {
+        e3[k] = free_dir[0] * t1[k] + free_dir[1] * t2[k];
+        dp[k] = n[k] + eps * e3[k];
+        dm[k] = n[k] - eps * e3[k];
+      }
+      SV sp, sm;
+      mk_support(m, A, B, dp, &sp);
+      mk_support(m, A, B, dm, &sm);
+      double He = (dot3(sp.w, e3) - dot3(sm.w, e3)) / (2 * eps) - h, ge = dot3(cur.w, e3);
+      if (!(He > 0)) break;
+      u[0] = -ge / He * free_dir[0];
+      u[1] = -ge / He * free_dir[1];
+    }
+    if (sqrt(u[0] * u[0] + u[1] * u[1]) < 1e-12) break;
+    int accepted = 0;
+    for (int ls = 0; ls < 4 && !accepted; ls++, u[0] *= 0.5, u[1] *= 0.5) {
+      double nn[3];
+      for (int k = 0; k < 3; k++) nn[k] = n[k] + u[0] * t1[k] + u[1] * t2[k];
+      double ln = o_norm3(nn);
+      for (int k = 0; k < 3; k++) nn[k] /= ln;
+      SV w;
+      mk_support(m, A, B, nn, &w);
+      double hn = dot3(w.w, nn);
+      if (hn < h - 1e-15) {
+        memcpy(n, nn, sizeof(nn));
+        h = hn;
+        cur = w;
+        accepted = moved = 1;
+      }
+    }
+    if (!accepted) break;
+  }
+  *depth = h;   /* support-plane distance at the final normal */
+  *sv = cur;
+  return moved;
+}
+
+/* largest move of a shape's core support point when the direction tilts by
+ * 1e-3 rad: about 1e-3 x the curvature radius where the support is unique,
+ * a jump across a face or an edge where it is not */
+static double support_jump(const OModel* m, const Shape* s, const double* n) {
+  double t1[3], t2[3], ax[3] = {0, 0, 0}, s0[3], j = 0;
+  ax[fabs(n[0]) < 0.6 ? 0 : (fabs(n[1]) < 0.6 ? 1 : 2)] = 1;
+  o_cross(n, ax, t1);
+  double l = o_norm3(t1);
+  for (int k = 0; k < 3; k++) t1[k] /= l;
+  o_cross(n, t1, t2);
+  core_support(m, s, n, s0);
+  for (int i = 0; i < 4; i++) {   /* +-t1, +-t2: a kink on either side shows */
+    const double* t = (i & 1) ? t2 : t1;
+    const double tilt = i < 2 ? 1e-3 : -1e-3;
+    double d[3] = {n[0] + tilt * t[0], n[1] + tilt * t[1], n[2] + tilt * t[2]}, s1[3];
+    core_support(m, s, d, s1);
+    double e[3] = {s1[0] - s0[0], s1[1] - s0[1], s1[2] - s0[2]}, le = o_norm3(e);
+    if (le > j) j = le;
+  }
+  return j;
+}
+
+/* centre of a shape's support set at direction n (a face, an edge or a
+ * point): the mean of the supports along 16 directions tilted by 0.05 rad
+ * around n; *spread = the largest distance of a sample from the mean */
+static void support_set_center(const OModel* m, const Shape* s, const double* n, double* c, double* spread) {
+  double t1[3], t2[3], ax[3] = {0, 0, 0}, p[16][3];
+  ax[fabs(n[0]) < 0.6 ? 0 : (fabs(n[1]) < 0.6 ? 1 : 2)] = 1;
+  o_cross(n, ax, t1);
+  double l = o_norm3(t1);
+  for (int k = 0; k < 3; k++) t1[k] /= l;
+  o_cross(n, t1, t2);
+  c[0] = c[1] = c[2] = 0;
+  for (int i = 0; i < 16; i++) {
+    double th = 0.39269908169872414 * i, ct = cos(th), st = sin(th), d[3];
+    for (int k = 0; k < 3; k++) d[k] = n[k] + 0.05 * (ct * t1[k] + st * t2[k]);
+    core_support(m, s, d, p[i]);
+    for (int k = 0; k < 3; k++) c[k] += p[i][k] / 16;
+  }
+  *spread = 0;
+  for (int i = 0; i < 16; i++) {
+    double e[3] = {p[i][0] - c[0], p[i][1] - c[1], p[i][2] - c[2]}, le = o_norm3(e);
+    if (le > *spread) *spread = le;
+  }
+}
+
+/* Witness points (core surfaces, pb = pa + sep n): where one shape's
+ * support point is unique at the normal (a curved patch, a vertex, a
+ * sphere's centre) it is that shape's support point; where both touch with
+ * a face or an edge the contact point is not unique: it is the centre of
+ * the smaller of the two support sets (a face's or an edge's middle), a
+ * choice that does not depend on how GJK / EPA reached the normal. */
+static void polish_witness(const OModel* m, const Shape* A, const Shape* B, const double* n, double sep, double* pa, double* pb) {
+  double nn[3] = {-n[0], -n[1], -n[2]};
+  double jA = support_jump(m, A, n), jB = support_jump(m, B, nn);
+  int sa = jA <= 4e-3 * A->rbound, sb = jB <= 4e-3 * B->rbound;
+  if (sa && (!sb || jA <= jB)) {
+    core_support(m, A, n, pa);
+    for (int k = 0; k < 3; k++) pb[k] = pa[k] + sep * n[k];
+  } else if (sb) {
+    core_support(m, B, nn, pb);
+    for (int k = 0; k < 3; k++) pa[k] = pb[k] - sep * n[k];
+  } else {
+    double cA[3], cB[3], sprA, sprB;
+    support_set_center(m, A, n, cA, &sprA);
+    support_set_center(m, B, nn, cB, &sprB);
+    if (sprA <= sprB) {
+      for (int k = 0; k < 3; k++) { pa[k] = cA[k]; pb[k] = cA[k] + sep * n[k]; }
+    } else {
+      for (int k = 0; k < 3; k++) { pb[k] = cB[k]; pa[k] = cB[k] - sep * n[k]; }
+    }
+  }
+}
+
+static int convex_pair(const OModel* m, const Shape* A, const Shape* B, double margin, Con* out) {
+  double dir[3] = {B->c[0] - A->c[0], B->c[1] - A->c[1], B->c[2] - A->c[2]};
+  if (o_norm3(dir) < 1e-12) { dir[0] = 1; dir[1] = dir[2] = 0; }
+  SV S[4];
+  double lam[4], v[3];
+  /* GJK on the Minkowski difference A - B */
+  mk_support(m, A, B, dir, &S[0]);
+  int n = 1, overlap = 0;
+  memcpy(v, S[0].w, sizeof(v));
+  lam[0] = 1;
+  for (int it = 0; it < CVX_ITER; it++) {
+    double vv = dot3(v, v);
+    if (vv < CVX_TOL * CVX_TOL) { overlap = 1; break; }
+    double nd[3] = {-v[0], -v[1], -v[2]};
+    SV w;
+    mk_support(m, A, B, nd, &w);
+    if (vv - dot3(v, w.w) <= CVX_TOL * sqrt(vv)) break;   /* no progress: v is the closest point */
+    S[n++] = w;
+    n = simplex_closest(S, n, lam, v);
+    if (n == 4) { overlap = 1; break; }
+  }
+  double pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0}, nrm[3], dist;
+  if (!overlap) {
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) { pa[k] += lam[i] * S[i].a[k]; pb[k] += lam[i] * (S[i].a[k] - S[i].w[k]); }
+    double len = o_norm3(v), h = -len;
+    for (int k = 0; k < 3; k++) nrm[k] = -v[k] / len;
+    /* the separation is -min_n h(n) too: GJK's duality-gap stop leaves the
+       normal only sqrt(tolerance)-accurate on curved shapes */
+    SV sv;
+    if (refine_normal(m, A, B, nrm, &h, &sv))
+      for (int k = 0; k < 3; k++) { pa[k] = sv.a[k]; pb[k] = sv.a[k] - sv.w[k]; }
+    if (-h > 0) len = -h;
+    polish_witness(m, A, B, nrm, len, pa, pb);
+    dist = len - A->core - B->core;
+  } else {
+    double depth;
+    if (!epa(m, A, B, S, n, &depth, nrm, pa, pb)) return 0;
+    SV sv;
+    if (refine_normal(m, A, B, nrm, &depth, &sv))
+      for (int k = 0; k < 3; k++) { pa[k] = sv.a[k]; pb[k] = sv.a[k] - sv.w[k]; }
+    polish_witness(m, A, B, nrm, -depth, pa, pb);
+    dist = -depth - A->core - B->core;
+  }
+  if (!(dist < margin)) return 0;
+  for (int k = 0; k < 3; k++) {
+    pa[k] += A->core * nrm[k];
+    pb[k] -= B->core * nrm[k];
+    out->pos[k] = 0.5 * (pa[k] + pb[k]);
+    out->n[k] = nrm[k];
+  }
+  out->dist = dist;
+  return 1;
+}
+
 static int add_contacts(const OModel* m, OData* d, int pair, const Con* cs, int n) {
   const int* pi = &m->pair_int[6 * pair];
   const double* pr = &m->pair_real[16 * pair];
@@ -473,7 +979,11 @@ void oracle_collide(const OModel* m, OData* d) {
       } else if (t1 == 2 && t2 == 6) n = sphere_box(c1, s1[0], c2, R2, s2, margin, cs);
       else if (t1 == 3 && t2 == 6) n = capsule_box(c1, R1, s1, c2, R2, s2, margin, cs);
       else if (t1 == 6 && t2 == 6) n = box_box(c1, R1, s1, c2, R2, s2, margin, cs);
-      else { d->status |= ORACLE_UNSUPPORTED; continue; }
+      else if (t1 >= 2 && t2 >= 2 && t1 <= 7 && t2 <= 7) {
+        Shape A = {t1, m->geom_dataid[g1], c1, R1, s1, t1 == 2 || t1 == 3 ? s1[0] : 0, m->geom_rbound[g1]};
+        Shape B = {t2, m->geom_dataid[g2], c2, R2, s2, t2 == 2 || t2 == 3 ? s2[0] : 0, m->geom_rbound[g2]};
+        n = convex_pair(m, &A, &B, margin, cs);
+      } else { d->status |= ORACLE_UNSUPPORTED; continue; }
     }
     add_contacts(m, d, p, cs, n);
   }

@@ -531,3 +531,129 @@ def test_sensor_rig_joint_tendon_actuator_values():
     np.testing.assert_allclose(val("fore_xpos"), env.a["xpos"][3 * 3: 3 * 4])
     np.testing.assert_allclose(val("com"), env.a["subtree_com"][3:6])
     assert not val("touch_tip").any() and not val("rel_pos").any()
+
+
+def _pair_contacts(g1, g2, pose1, pose2, margin=0.0):
+    """Contacts of one geom pair (two free bodies, no gravity) at the given
+    poses (pos3 + quat4 each), from the oracle's collision stage alone."""
+    import ctypes as C
+    xml = (f'<mujoco><option gravity="0 0 0"/><worldbody><body name="a"><freejoint/><geom {g1} margin="{margin}"/></body>'
+           f'<body name="b" pos="0 0 1"><freejoint/><geom {g2} margin="{margin}"/></body></worldbody></mujoco>')
+    m = mjb200.load_model_from_string(xml)
+    om = oracle.OracleModel(m.dump())
+    env = oracle.OracleEnv(om)
+    env.a["qpos"][:] = np.concatenate([pose1, pose2])
+    oracle.lib.oracle_kinematics(C.byref(om.c), C.byref(env.d))
+    oracle.lib.oracle_collide(C.byref(om.c), C.byref(env.d))
+    return env.contacts(), env.d.status, m.dump()["geom_type"]
+
+
+def _rand_quat(g):
+    q = g.normal(size=4)
+    return q / np.linalg.norm(q)
+
+
+def test_convex_gjk_epa_curved_known_answers():
+    """GJK distance (separated, within margin) and EPA + Newton refinement
+    (penetrating) between a sphere and a sphere-shaped ellipsoid, and
+    between two sphere-shaped ellipsoids, against the closed form: dist =
+    |c2 - c1| - r1 - r2, normal along c2 - c1, position at the midpoint of
+    the surface points."""
+    g = np.random.default_rng(7)
+    for g1, r1, g2, r2 in (('type="sphere" size="0.1"', 0.1, 'type="ellipsoid" size="0.2 0.2 0.2"', 0.2),
+                           ('type="ellipsoid" size="0.15 0.15 0.15"', 0.15, 'type="ellipsoid" size="0.2 0.2 0.2"', 0.2)):
+        for dist in (0.1, 0.01, -0.02, -0.12):
+            u = g.normal(size=3)
+            u /= np.linalg.norm(u)
+            c1 = g.normal(size=3) * 0.3
+            c2 = c1 + u * (r1 + r2 + dist)
+            cs, st, gt = _pair_contacts(g1, g2, np.r_[c1, _rand_quat(g)], np.r_[c2, _rand_quat(g)], margin=0.2)
+            assert st == 0 and len(cs) == 1
+            sgn = 1 if gt[0] <= gt[1] else -1   # pair order is by geom type
+            assert cs[0, 12] == pytest.approx(dist, abs=1e-8)
+            np.testing.assert_allclose(cs[0, 3:6], sgn * u, atol=1e-6)
+            mid = 0.5 * ((c1 + r1 * u) + (c2 - r2 * u))
+            np.testing.assert_allclose(cs[0, :3], mid, atol=1e-6)
+
+
+def test_convex_capsule_side_against_curved_known_answer():
+    """Capsule side (its core segment is flat along the axis, so the depth
+    has a kink there and curvature across it) against a sphere-shaped
+    ellipsoid: dist = distance from the centre to the core segment - r - R,
+    normal from the closest segment point to the centre."""
+    g = np.random.default_rng(11)
+    r, hl, R = 0.03, 0.06, 0.05
+    for dist in (0.02, -0.004, -0.03):
+        for trial in range(4):
+            q1 = _rand_quat(g)
+            w, x, y, z = q1
+            axis = np.array([2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)])
+            perp = np.cross(axis, g.normal(size=3))
+            perp /= np.linalg.norm(perp)
+            s = g.uniform(-0.8, 0.8) * hl
+            c1 = g.normal(size=3) * 0.1
+            c2 = c1 + s * axis + perp * (r + R + dist)
+            cs, st, gt = _pair_contacts('type="capsule" size="%g %g"' % (r, hl), 'type="ellipsoid" size="%g %g %g"' % (R, R, R),
+                                        np.r_[c1, q1], np.r_[c2, _rand_quat(g)], margin=0.05)
+            assert len(cs) == 1
+            assert cs[0, 12] == pytest.approx(dist, abs=1e-8)
+            np.testing.assert_allclose(cs[0, 3:6], perp, atol=1e-6)   # capsule (3) is geom1
+
+
+def test_convex_mesh_cube_matches_box_colliders():
+    """A mesh whose hull is a 0.2 m cube against a sphere and a capsule:
+    GJK / EPA on the hull give the analytic sphere-box depth and normal
+    (face, edge and vertex regions, separated and penetrating) and the
+    capsule-box distance when separated; when a capsule penetrates, the
+    minimum translation distance is at least the deepest-point depth of the
+    analytic capsule-box collider."""
+    cube = " ".join(f"{x} {y} {z}" for x in (-0.1, 0.1) for y in (-0.1, 0.1) for z in (-0.1, 0.1))
+    g = np.random.default_rng(8)
+    for other in ('type="sphere" size="0.07"', 'type="capsule" size="0.04 0.08"'):
+        for trial in range(12):
+            q1, q2 = _rand_quat(g), _rand_quat(g)
+            c2 = g.uniform(-0.22, 0.22, size=3)
+            xml_mesh = f'type="mesh" mesh="cube"'
+            mesh_model = ('<asset><mesh name="cube" vertex="' + cube + '"/></asset>')
+            import ctypes as C
+            outs = []
+            for shape in (xml_mesh, 'type="box" size="0.1 0.1 0.1"'):
+                xml = (f'<mujoco><option gravity="0 0 0"/>{mesh_model}<worldbody><body name="a"><freejoint/><geom {shape} margin="0.1"/></body>'
+                       f'<body name="b" pos="0 0 1"><freejoint/><geom {other} margin="0.1"/></body></worldbody></mujoco>')
+                m = mjb200.load_model_from_string(xml)
+                om = oracle.OracleModel(m.dump())
+                env = oracle.OracleEnv(om)
+                env.a["qpos"][:] = np.concatenate([[0, 0, 0], q1, c2, q2])
+                oracle.lib.oracle_kinematics(C.byref(om.c), C.byref(env.d))
+                oracle.lib.oracle_collide(C.byref(om.c), C.byref(env.d))
+                outs.append((env.contacts(), m.dump()["geom_type"]))
+            (cm, tm), (cb, tb) = outs
+            assert len(cm) == len(cb)
+            if len(cm):
+                # mesh (type 7) and box (6) are both geom2 of their pair
+                if other.startswith('type="sphere"') or cb[0, 12] > 0:
+                    assert cm[0, 12] == pytest.approx(cb[0, 12], abs=1e-7)
+                    np.testing.assert_allclose(cm[0, 3:6], cb[0, 3:6], atol=1e-5)
+                else:
+                    assert cm[0, 12] <= cb[0, 12] + 1e-9
+
+
+def test_convex_flat_and_order_symmetry():
+    """Cylinder standing on a box: depth and normal exact, position between
+    the faces; swapping the two bodies flips nothing in dist and keeps the
+    normal pointing from geom1 to geom2."""
+    I = [1, 0, 0, 0]
+    cs, st, gt = _pair_contacts('type="box" size="0.3 0.3 0.1"', 'type="cylinder" size="0.1 0.2"', np.r_[0, 0, 0, I], np.r_[0.05, 0.02, 0.29, I])
+    assert len(cs) == 1 and cs[0, 12] == pytest.approx(-0.01, abs=1e-9)
+    np.testing.assert_allclose(cs[0, 3:6], [0, 0, -1], atol=1e-9)   # cylinder (type 5) is geom1
+    assert cs[0, 2] == pytest.approx(0.095, abs=1e-9)
+    g = np.random.default_rng(9)
+    for trial in range(8):
+        p1 = np.r_[g.normal(size=3) * 0.1, _rand_quat(g)]
+        p2 = np.r_[p1[:3] + g.normal(size=3) * 0.12, _rand_quat(g)]
+        a, _, ta = _pair_contacts('type="ellipsoid" size="0.12 0.08 0.05"', 'type="cylinder" size="0.05 0.07"', p1, p2, margin=0.05)
+        b, _, tb = _pair_contacts('type="cylinder" size="0.05 0.07"', 'type="ellipsoid" size="0.12 0.08 0.05"', p2, p1, margin=0.05)
+        assert len(a) == len(b)
+        if len(a):
+            assert a[0, 12] == pytest.approx(b[0, 12], abs=1e-7)
+            np.testing.assert_allclose(a[0, 3:6], b[0, 3:6], atol=1e-5)
