@@ -126,12 +126,16 @@ MJMLX_API void mjmlx_batched_set_env_qvel(MjmlxBatchedSim* sim, int env_idx, con
 
 /* Per-env physics randomisation (config->domain_rand == 1 only).  For each
  * env_idx[i] (env_idx == NULL: n == num_envs, all envs) update the non-NULL
- * arrays: mass_scale[n*nbody], com_delta[n*nbody*3], friction_scale[n],
- * gain_scale[n*nu].  Returns 0 ok, -1 bad handle / domain_rand off / bad n,
- * -2 env index out of range.  Replaces mjmlx.h:233. */
+ * arrays: mass_scale[n*nbody] (mass and inertia), com_delta[n*nbody*3] (COM
+ * offset in the body frame), friction_scale[n] (pair friction),
+ * gain_scale[n*nu] (actuator force).  Returns 0 ok, -1 bad handle /
+ * domain_rand off / bad n, -2 env index out of range.  Replaces
+ * mjmlx.h:233. */
 MJMLX_API int mjmlx_batched_set_env_params(MjmlxBatchedSim* sim, const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale);
-/* Quadratic drag F = -k|v|v on free joints, drag_k[n * nfree].  Returns as
- * above, -3 if the model has no free joint.  Replaces mjmlx.h:237-238. */
+/* Quadratic drag F = -k|v|v [N s^2/m^2] on the translational dofs of each
+ * free joint (MJCF order), drag_k[n * nfree]; 0 (no drag) until set.
+ * Returns as above, -3 if no model of the sim has a free joint.  Replaces
+ * mjmlx.h:237-238. */
 MJMLX_API int mjmlx_batched_set_free_drag(MjmlxBatchedSim* sim, const int* env_idx, int n, const float* drag_k);
 MJMLX_API int mjmlx_batched_num_free_joints(const MjmlxBatchedSim* sim);
 

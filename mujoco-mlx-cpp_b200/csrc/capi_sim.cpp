@@ -181,12 +181,8 @@ MJMLX_API int mjmlx_batched_set_env_params(MjmlxBatchedSim* sim, const int* env_
 }
 
 MJMLX_API int mjmlx_batched_set_free_drag(MjmlxBatchedSim* sim, const int* env_idx, int n, const float* drag_k) {
-  (void)env_idx;
-  (void)n;
-  (void)drag_k;
-  if (!sim || !sim->engine->domain_rand()) return -1;
-  set_error("mjmlx_batched_set_free_drag: free-joint drag is not supported by this build");
-  return -1;
+  if (!sim || !sim->engine) return -1;
+  return guard("mjmlx_batched_set_free_drag", [&]() { return sim->engine->set_free_drag(env_idx, n, drag_k); }, -1);
 }
 
 MJMLX_API int mjmlx_batched_num_free_joints(const MjmlxBatchedSim* sim) {

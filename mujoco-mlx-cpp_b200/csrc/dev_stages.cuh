@@ -202,9 +202,22 @@ __device__ __noinline__ void d_com(Env& E, const StepParams& P) {
   const float* ft = E.ft;
   float* ws = E.ws;
   float* tmp = ws + m.w_tmp;  // 4 per body: mass, mass*xipos
-  const float* xipos = ws + m.w_xipos;
+  float* xipos = ws + m.w_xipos;
   const float* xquat = ws + m.w_xquat;
   float* scom = ws + m.w_scom;
+  if (P.rand_com) {
+    // per-env COM offset in the body frame (reference: forward.hpp:110-115)
+    const float* cd = P.rand_com + 3 * P.env_badr[E.env];
+    const float* xmat = ws + m.w_xmat;
+    #pragma unroll 1
+    for (int b = 1 + E.lane; b < m.nbody; b += 32) {
+      const float d[3] = {cd[3 * b], cd[3 * b + 1], cd[3 * b + 2]};
+      float w[3];
+      mulmat(xmat + 9 * b, d, w);
+      for (int k = 0; k < 3; k++) xipos[3 * b + k] += w[k];
+    }
+    __syncwarp();
+  }
   #pragma unroll 1
   for (int b = E.lane; b < m.nbody; b += 32) {
     float mb = ldf(ft, m.f_body_mass + b) * msc(P, E, b);
@@ -516,6 +529,36 @@ __device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* 
         pas -= st * (qpos[qa] - ldf(ft, m.f_qpos_spring + qa));
       }
       pas -= ldf(ft, m.f_dof_damping + i) * qvel[i];
+      // gravity compensation at each compensated body's COM, through cdof
+      // (reference: forward.hpp:438-452)
+      const int db = ldi(it, m.i_dof_bodyid + i), dsub = ldi(it, m.i_body_subtreesize + db);
+      const int ngc = (m.disableflags & (1 << 6)) ? 0 : m.ngcomp;   // nothing to compensate without gravity
+      #pragma unroll 1
+      for (int k = 0; k < ngc; k++) {
+        const int b = ldi(it, m.i_gcomp + k);
+        if (b < db || b >= db + dsub) continue;
+        const float mb = ldf(ft, m.f_body_mass + b) * ldf(ft, m.f_gcomp + k) * msc(P, E, b);
+        const int root = ldi(it, m.i_body_rootid + b);
+        const float* xi = ws + m.w_xipos + 3 * b;
+        const float* rc = ws + m.w_scom + 3 * root;
+        const float f[3] = {-mb * m.gravity[0], -mb * m.gravity[1], -mb * m.gravity[2]};
+        const float o[3] = {xi[0] - rc[0], xi[1] - rc[1], xi[2] - rc[2]};
+        float tq[3];
+        cross3(o, f, tq);
+        const float* cd = ws + m.w_cdof + 6 * i;
+        pas += cd[0] * tq[0] + cd[1] * tq[1] + cd[2] * tq[2] + cd[3] * f[0] + cd[4] * f[1] + cd[5] * f[2];
+      }
+      // quadratic drag on the translational dofs of free joints (per env;
+      // reference: forward.hpp:455-464)
+      if (P.rand_drag) {
+        #pragma unroll 1
+        for (int k = 0; k < m.nfree; k++) {
+          const int da = ldi(it, m.i_free + k);
+          if (i < da || i >= da + 3) continue;
+          const float vx = qvel[da], vy = qvel[da + 1], vz = qvel[da + 2];
+          pas += -P.rand_drag[P.env_fadr[E.env] + k] * sqrtf(vx * vx + vy * vy + vz * vz) * qvel[i];
+        }
+      }
       // tendon spring with a dead band and damper, through J^T
       // (reference: tendon.hpp:360-377)
       #pragma unroll 1

@@ -33,6 +33,8 @@ struct DevModelDesc {
   int ntfloss, i_tfloss;       // tendons with frictionloss (tendon ids)
   int ntlimit, i_tlimit;       // limited tendons (tendon ids)
   int npten, i_pten;           // tendons with stiffness or damping (tendon ids)
+  int ngcomp, i_gcomp;   // bodies with gravity compensation (body ids)
+  int nfree, i_free;     // free joints in MJCF order (dof address of each)
   int nsensor, nsensordata, nsens_acc;
   int i_sensor;  // MJB_SENSOR_INTS per sensor: mjtSensor type (-1 = reads zero), adr, dim, body, root body, a, b, accelerometer slot
   int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
@@ -51,6 +53,7 @@ struct DevModelDesc {
   int f_wrap;    // 1 per wrap: coef
   int f_ten;     // MJB_TEN_FLOATS per tendon (layout below)
   int f_sensor;  // MJB_SENSOR_FLOATS per sensor: object frame in its body (pos 3, quat 4), actuator gear
+  int f_gcomp;   // gravcomp per body
   float magnetic[3];
   int f_mesh_vert;
 

@@ -131,8 +131,6 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     for (int j = 0; j < m.njnt; j++)
       if (m.jnt_limited[j] && m.jnt_type[j] == JNT_BALL) throw std::runtime_error("engine: limited ball joints are not supported");
     if (m.nv > 64) throw std::runtime_error("engine: models with more than 64 dofs are not supported by this build");
-    for (double g : m.body_gravcomp)
-      if (g != 0) throw std::runtime_error("engine: gravcomp is not supported");
     DevModelDesc d;
     std::memset(&d, 0, sizeof(d));
     d.nq = m.nq; d.nv = m.nv; d.nu = m.nu; d.nbody = m.nbody; d.njnt = m.njnt; d.ngeom = m.ngeom;
@@ -250,6 +248,18 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.i_tlimit = tb.ai(tlim);
     d.npten = (int)tpas.size();
     d.i_pten = tb.ai(tpas);
+    // gravity compensation and free joints (reference: forward.hpp:438-464)
+    std::vector<int> gci, fri;
+    std::vector<double> gcf;
+    for (int b = 1; b < m.nbody; b++)
+      if (m.body_gravcomp[b] != 0) { gci.push_back(b); gcf.push_back(m.body_gravcomp[b]); }
+    for (int j = 0; j < m.njnt; j++)
+      if (m.jnt_type[j] == JNT_FREE) fri.push_back(m.jnt_dofadr[j]);
+    d.ngcomp = (int)gci.size();
+    d.i_gcomp = tb.ai(gci);
+    d.f_gcomp = tb.af(gcf);
+    d.nfree = (int)fri.size();
+    d.i_free = tb.ai(fri);
     // sensors (reference: make_sensor_ctx, sensor.cpp:99-210): the object
     // frame of frame / site sensors relative to its body, state addresses of
     // joint / actuator / tendon sensors, a slot per accelerometer
@@ -435,6 +445,14 @@ void Engine::alloc_state() {
       q += m.nq; v += m.nv; u += std::max(m.nu, 0); b += m.nbody;
     }
   tot_q_ = q; tot_v_ = v; tot_u_ = u; tot_b_ = b;
+  h_fadr_.assign(B_, 0);
+  int fr = 0;
+  for (int i = 0; i < B_; i++) {
+    h_fadr_[i] = fr;
+    fr += layouts_[h_model_[i]].desc.nfree;
+  }
+  tot_f_ = fr;
+  d_fadr_.upload(h_fadr_, stream_);
   // sensordata and accelerometer history addresses
   h_sadr_.assign(B_, 0);
   h_aadr_.assign(B_, 0);
@@ -480,9 +498,13 @@ void Engine::alloc_state() {
     h_rand_mass_.assign(b, 1.f);
     h_rand_fric_.assign(B_, 1.f);
     h_rand_gain_.assign(std::max(u, 1), 1.f);
+    h_rand_com_.assign(3 * std::max(b, 1), 0.f);
+    h_rand_drag_.assign(std::max(tot_f_, 1), 0.f);
     rand_mass_.upload(h_rand_mass_, stream_);
     rand_fric_.upload(h_rand_fric_, stream_);
     rand_gain_.upload(h_rand_gain_, stream_);
+    rand_com_.upload(h_rand_com_, stream_);
+    rand_drag_.upload(h_rand_drag_, stream_);
   }
   check(cudaStreamSynchronize(stream_), "init sync");
 }
@@ -650,6 +672,11 @@ StepParams Engine::params(int n, bool record) {
     P.rand_mass = rand_mass_.p;
     P.rand_friction = rand_fric_.p;
     P.rand_gain = rand_gain_.p;
+    if (com_on_) P.rand_com = rand_com_.p;
+    if (drag_on_) {
+      P.rand_drag = rand_drag_.p;
+      P.env_fadr = d_fadr_.p;
+    }
   }
   if (tot_s_ > 0) {
     if (record) P.sensordata = sensordata_.p;
@@ -695,6 +722,11 @@ StepParams Engine::external_params(float* qpos, float* qvel, const float* ctrl, 
     P.rand_mass = rand_mass_.p;
     P.rand_friction = rand_fric_.p;
     P.rand_gain = rand_gain_.p;
+    if (com_on_) P.rand_com = rand_com_.p;
+    if (drag_on_) {
+      P.rand_drag = rand_drag_.p;
+      P.env_fadr = d_fadr_.p;
+    }
   }
   return P;
 }
@@ -922,19 +954,13 @@ int Engine::set_env_params(const int* env_idx, int n, const float* mass_scale, c
   if (!env_idx && n != B_) return -1;
   for (int i = 0; i < n; i++)
     if (env_idx && (env_idx[i] < 0 || env_idx[i] >= B_)) return -2;
-  if (com_delta) {
-    for (int i = 0; i < n; i++) {
-      int e = env_idx ? env_idx[i] : i;
-      int nb = models_[h_model_[e]]->nbody;
-      for (int k = 0; k < 3 * nb; k++)
-        if (com_delta[(size_t)i * 3 * nb + k] != 0.f) return -1;  // COM offsets are not supported by this build
-    }
-  }
   for (int i = 0; i < n; i++) {
     int e = env_idx ? env_idx[i] : i;
     const Model& m = *models_[h_model_[e]];
     if (mass_scale)
       for (int b = 0; b < m.nbody; b++) h_rand_mass_[h_badr_[e] + b] = mass_scale[(size_t)i * m.nbody + b];
+    if (com_delta)
+      for (int k = 0; k < 3 * m.nbody; k++) h_rand_com_[3 * h_badr_[e] + k] = com_delta[(size_t)i * 3 * m.nbody + k];
     if (friction_scale) h_rand_fric_[e] = friction_scale[i];
     if (gain_scale)
       for (int a = 0; a < m.nu; a++) h_rand_gain_[h_uadr_[e] + a] = gain_scale[(size_t)i * m.nu + a];
@@ -943,6 +969,30 @@ int Engine::set_env_params(const int* env_idx, int n, const float* mass_scale, c
   rand_mass_.upload(h_rand_mass_, stream_);
   rand_fric_.upload(h_rand_fric_, stream_);
   rand_gain_.upload(h_rand_gain_, stream_);
+  if (com_delta) {
+    rand_com_.upload(h_rand_com_, stream_);
+    if (!com_on_) invalidate_graphs();
+    com_on_ = true;
+  }
+  sync();
+  return 0;
+}
+
+int Engine::set_free_drag(const int* env_idx, int n, const float* drag_k) {
+  if (!rand_on_ || n < 0 || !drag_k) return -1;
+  if (tot_f_ == 0) return -3;
+  if (!env_idx && n != B_) return -1;
+  for (int i = 0; i < n; i++)
+    if (env_idx && (env_idx[i] < 0 || env_idx[i] >= B_)) return -2;
+  for (int i = 0; i < n; i++) {
+    const int e = env_idx ? env_idx[i] : i;
+    const int nf = layouts_[h_model_[e]].desc.nfree;
+    for (int f = 0; f < nf; f++) h_rand_drag_[h_fadr_[e] + f] = drag_k[(size_t)i * nf + f];
+  }
+  sync();
+  rand_drag_.upload(h_rand_drag_, stream_);
+  if (!drag_on_) invalidate_graphs();
+  drag_on_ = true;
   sync();
   return 0;
 }

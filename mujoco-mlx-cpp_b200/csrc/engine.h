@@ -94,6 +94,8 @@ class Engine {
 
   // domain randomisation
   int set_env_params(const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale);
+  // per-env quadratic drag F = -k |v| v on each free joint (domain_rand sims)
+  int set_free_drag(const int* env_idx, int n, const float* drag_k);
   bool domain_rand() const { return rand_on_; }
 
   // learned warm start
@@ -195,8 +197,12 @@ class Engine {
   DevBuf<float> rec_xpos_, rec_xquat_, rec_scom_, rec_cinert_, rec_cvel_, rec_qfa_, rec_cfrc_, rec_qacc_;
   DevBuf<float> dbg_con_, dbg_efc_, dbg_vec_;
   int dbg_ncon_ = 0, dbg_nefc_ = 0;
-  DevBuf<float> rand_mass_, rand_fric_, rand_gain_;
-  std::vector<float> h_rand_mass_, h_rand_fric_, h_rand_gain_;
+  DevBuf<float> rand_mass_, rand_fric_, rand_gain_, rand_com_, rand_drag_;
+  std::vector<float> h_rand_mass_, h_rand_fric_, h_rand_gain_, h_rand_com_, h_rand_drag_;
+  std::vector<int> h_fadr_;
+  DevBuf<int> d_fadr_;
+  int tot_f_ = 0;                            // free joints over all envs
+  bool com_on_ = false, drag_on_ = false;    // COM offsets / drag set at least once
   DevBuf<float> feat_, tmp_prev_;
   DevBuf<unsigned long long> stage_cycles_;
   bool timing_ = false;

@@ -74,6 +74,9 @@ struct StepParams {
   const float* rand_mass;      // [badr + body]
   const float* rand_friction;  // [env]
   const float* rand_gain;      // [uadr + actuator]
+  const float* rand_com;       // [3 badr + 3 body + k]: COM offset in the body frame
+  const float* rand_drag;      // [env_fadr + free joint]: quadratic drag coefficient
+  const int* env_fadr;
 
   // learned warm start: feature rows written after each substep (nullable):
   // qpos[feat_qskip:nq], qvel, converged qacc, then MJB_FEAT_CONTACTS x

@@ -57,6 +57,7 @@ def _load():
         "mjmlx_batched_set_env_qpos": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
         "mjmlx_batched_set_env_qvel": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
         "mjmlx_batched_set_env_params": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p, _f32p, _f32p, _f32p]),
+        "mjmlx_batched_set_free_drag": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p]),
         "mjmlx_batched_set_pack_spec": (C.c_int, [C.c_void_p, _i32p, C.c_int, C.c_int, C.c_int]),
         "mjmlx_batched_get_pack": (C.c_int, [C.c_void_p, _f32p]),
         "mjmlx_batched_raycast": (C.c_int, [C.c_void_p, _f32p, _f32p, C.c_int, C.c_int, C.POINTER(C.c_ubyte), C.c_int, _f32p, _i32p]),
@@ -470,12 +471,19 @@ class BatchedSim:
         lib.mjb200_batched_stats(self.handle, *[_ip(out[k]) for k in ("status", "niter_sum", "niter_max", "ncon", "nefc", "warm_choice")])
         return out
 
-    def set_env_params(self, env_idx=None, mass_scale=None, friction_scale=None, gain_scale=None):
+    def set_env_params(self, env_idx=None, mass_scale=None, friction_scale=None, gain_scale=None, com_delta=None):
         n = self.num_envs if env_idx is None else len(env_idx)
         ei = None if env_idx is None else np.ascontiguousarray(env_idx, np.int32)
         conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1)
-        ms, fs, gs = conv(mass_scale), conv(friction_scale), conv(gain_scale)
-        return lib.mjmlx_batched_set_env_params(self.handle, _ip(ei), n, _fp(ms), None, _fp(fs), _fp(gs))
+        ms, fs, gs, cd = conv(mass_scale), conv(friction_scale), conv(gain_scale), conv(com_delta)
+        return lib.mjmlx_batched_set_env_params(self.handle, _ip(ei), n, _fp(ms), _fp(cd), _fp(fs), _fp(gs))
+
+    def set_free_drag(self, drag_k, env_idx=None):
+        """Quadratic drag coefficients [n, nfree] of the free joints."""
+        n = self.num_envs if env_idx is None else len(env_idx)
+        ei = None if env_idx is None else np.ascontiguousarray(env_idx, np.int32)
+        dk = np.ascontiguousarray(drag_k, np.float32).reshape(-1)
+        return lib.mjmlx_batched_set_free_drag(self.handle, _ip(ei), n, _fp(dk))
 
     # ---- debug capture
     def set_debug(self, ncon_max: int = 32, nefc_max: int = 128):

@@ -63,6 +63,8 @@ typedef struct OModel {
   int nsite, nsensor;
   const int *site_bodyid, *sensor_type, *sensor_objtype, *sensor_objid, *sensor_dim, *sensor_adr, *sensor_supported;
   const double *site_pos, *site_quat, *magnetic;
+  /* gravity compensation per body (fraction of its weight) */
+  const double* body_gravcomp;
 } OModel;
 
 /* per-env randomisation (NULL pointers = identity) */
@@ -70,6 +72,8 @@ typedef struct ORand {
   const double* mass_scale;     /* [nbody] */
   double friction_scale;
   const double* gain_scale;     /* [nu] */
+  const double* com_delta;      /* [nbody][3]: COM offset in the body frame */
+  const double* drag_k;         /* [free joints]: quadratic drag F = -k |v| v */
 } ORand;
 
 #define ORACLE_CONTACT_STRIDE 20  /* pos3 frame9 dist pair g1 g2 dim mu0 includemargin efc_adr */

@@ -83,6 +83,13 @@ void oracle_com(const OModel* m, OData* d, const ORand* rnd) {
   int nb = m->nbody, nv = m->nv;
   double* mass = d->work;           /* nb */
   double* mc = d->work + nb;        /* 3 nb */
+  /* per-env COM offset, body frame (reference: forward.hpp:110-115 XIP) */
+  if (rnd && rnd->com_delta)
+    for (int b = 1; b < nb; b++) {
+      double w[3];
+      o_mulmat(&d->xmat[9 * b], &rnd->com_delta[3 * b], w);
+      for (int k = 0; k < 3; k++) d->xipos[3 * b + k] += w[k];
+    }
   for (int b = 0; b < nb; b++) {
     mass[b] = m->body_mass[b] * msc(rnd, b);
     for (int k = 0; k < 3; k++) mc[3 * b + k] = mass[b] * d->xipos[3 * b + k];
@@ -290,6 +297,35 @@ void oracle_smooth_forces(const OModel* m, OData* d, const ORand* rnd) {
       }
     }
     for (int i = 0; i < nv; i++) d->qfrc_passive[i] -= m->dof_damping[i] * d->qvel[i];
+    /* gravity compensation: -gravcomp * m * gravity at the body's COM,
+       through cdof (reference: forward.hpp:438-452) */
+    for (int b = 1; b < m->nbody && !(m->disableflags & (1 << 6)); b++) {
+      double gc = m->body_gravcomp[b];
+      if (gc == 0) continue;
+      double mb = m->body_mass[b] * gc * msc(rnd, b), f[3], o[3], w[6];
+      const double* rc = &d->subtree_com[3 * m->body_rootid[b]];
+      for (int k = 0; k < 3; k++) { f[k] = -mb * m->gravity[k]; o[k] = d->xipos[3 * b + k] - rc[k]; }
+      o_cross(o, f, w);
+      w[3] = f[0]; w[4] = f[1]; w[5] = f[2];
+      for (int i = 0; i < nv; i++) {
+        int db = m->dof_bodyid[i];
+        if (!(db <= b && b < db + m->body_subtreesize[db])) continue;
+        double s = 0;
+        for (int k = 0; k < 6; k++) s += d->cdof[6 * i + k] * w[k];
+        d->qfrc_passive[i] += s;
+      }
+    }
+    /* quadratic drag on free joints, per env (reference: forward.hpp:455-464) */
+    if (rnd && rnd->drag_k) {
+      int f = 0;
+      for (int j = 0; j < m->njnt; j++) {
+        if (m->jnt_type[j] != 0) continue;
+        int da = m->jnt_dofadr[j];
+        const double* v = &d->qvel[da];
+        double kd = -rnd->drag_k[f++] * sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; k++) d->qfrc_passive[da + k] += kd * v[k];
+      }
+    }
     /* tendon spring with a dead band [lengthspring lo, hi] and damper
        (reference: tendon.hpp:360-377) */
     for (int t = 0; t < m->ntendon; t++) {

@@ -45,7 +45,8 @@ _TEN_PTR = [("tendon_adr", "i"), ("tendon_num", "i"), ("tendon_limited", "i"), (
 
 
 _SENS_PTR = [("site_bodyid", "i"), ("sensor_type", "i"), ("sensor_objtype", "i"), ("sensor_objid", "i"), ("sensor_dim", "i"),
-             ("sensor_adr", "i"), ("sensor_supported", "i"), ("site_pos", "f"), ("site_quat", "f"), ("magnetic", "f")]
+             ("sensor_adr", "i"), ("sensor_supported", "i"), ("site_pos", "f"), ("site_quat", "f"), ("magnetic", "f"),
+             ("body_gravcomp", "f")]
 
 
 class OModel(C.Structure):
@@ -59,7 +60,7 @@ class OModel(C.Structure):
 
 
 class ORand(C.Structure):
-    _fields_ = [("mass_scale", _dp), ("friction_scale", C.c_double), ("gain_scale", _dp)]
+    _fields_ = [("mass_scale", _dp), ("friction_scale", C.c_double), ("gain_scale", _dp), ("com_delta", _dp), ("drag_k", _dp)]
 
 
 _DATA_D = ["qpos", "qvel", "ctrl", "qacc_warmstart", "qacc_predicted",

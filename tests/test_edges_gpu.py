@@ -124,3 +124,44 @@ def test_implicitfast_integrator_parity():
         for e in range(B):
             assert np.abs(g["qpos"][e] - o[e]["qpos"]).max() < 1e-5
             assert np.abs(g["qvel"][e] - o[e]["qvel"]).max() < 1e-4 * max(1.0, np.abs(o[e]["qvel"]).max())
+
+
+def test_gravcomp_com_offset_drag_parity():
+    """Gravity compensation on the thighs (gravcomp 0.6), per-env COM offsets
+    (U[-1, 1] cm per body, body frame) and per-env quadratic drag on the
+    trunk's free joint (k U[0, 3]) against the oracle at visited states."""
+    xml = mjb200.models.quadruped_xml().replace('_thigh" pos=', '_thigh" gravcomp="0.6" pos=')
+    assert xml.count('gravcomp="0.6"') == 4
+    model = mjb200.load_model_from_string(xml)
+    om = oracle.OracleModel(model.dump())
+    B = 24
+    (qp, qv, ctrl), = visited_states(om, nsteps=(40,), B=B)
+    sim = mjb200.BatchedSim(model, B, domain_rand=1)
+    nb = int(model.dump()["sizes"][3])
+    rng = np.random.default_rng(21)
+    cd = rng.uniform(-0.01, 0.01, size=(B, nb, 3)).astype(np.float32)
+    cd[:, 0] = 0
+    drag = rng.uniform(0, 3, size=(B, 1)).astype(np.float32)
+    assert sim.set_env_params(com_delta=cd) == 0
+    assert sim.set_free_drag(drag) == 0
+    qv = qv.copy()
+    qv[:, :3] += rng.normal(0, 1.0, size=(B, 3)).astype(np.float32)   # drag needs a moving trunk
+    g = gpu_step_from(sim, qp, qv, ctrl, 64, 256)
+    errs = []
+    for e in range(B):
+        env = oracle.OracleEnv(om)
+        env.a["qpos"][:] = qp[e]
+        env.a["qvel"][:] = qv[e]
+        env.a["ctrl"][: om.nu] = ctrl[e]
+        c64 = np.ascontiguousarray(cd[e].astype(np.float64).reshape(-1))
+        k64 = np.ascontiguousarray(drag[e].astype(np.float64))
+        rand = oracle.ORand(None, 1.0, None, c64.ctypes.data_as(C.POINTER(C.c_double)), k64.ctypes.data_as(C.POINTER(C.c_double)))
+        env.step(0, rand)
+        assert g["stats"]["status"][e] == 0 and env.d.status == 0
+        errs.append(rel_err(g["vec"][e, 2, : om.nv], env.a["qacc"]))
+        assert np.abs(g["qpos"][e] - env.a["qpos"]).max() < 1e-5
+    assert np.median(errs) <= 1e-4 and max(errs) <= 2e-3, (np.median(errs), max(errs))
+    # the three terms change the step: without them the accelerations differ
+    plain = mjb200.BatchedSim(mjb200.load_model_from_string(mjb200.models.quadruped_xml()), B)
+    gp = gpu_step_from(plain, qp, qv, ctrl, 64, 256)
+    assert np.abs(gp["vec"][:, 2] - g["vec"][:, 2]).max() > 1e-2

@@ -657,3 +657,65 @@ def test_convex_flat_and_order_symmetry():
         if len(a):
             assert a[0, 12] == pytest.approx(b[0, 12], abs=1e-7)
             np.testing.assert_allclose(a[0, 3:6], b[0, 3:6], atol=1e-5)
+
+
+def _dp(a):
+    import ctypes as C
+    return np.ascontiguousarray(a, np.float64).ctypes.data_as(C.POINTER(C.c_double))
+
+
+_CHAIN3 = ('<mujoco><option timestep="0.002"/><worldbody>'
+           '<body><joint type="hinge" axis="0 1 0"/><geom type="capsule" fromto="0 0 0 0.3 0 0" size="0.03" mass="1"/>'
+           '<body pos="0.3 0 0"><joint type="hinge" axis="1 0 0"/><geom type="capsule" fromto="0 0 0 0.25 0 0.1" size="0.03" mass="0.6"/>'
+           '<body pos="0.25 0 0.1"><joint type="hinge" axis="0 1 0"/><geom type="sphere" size="0.05" mass="0.4" pos="0.1 0 0"/>'
+           '</body></body></body></worldbody></mujoco>')
+
+
+def test_gravcomp_known_answers():
+    """Gravity compensation (gravcomp = 1 on every body) cancels gravity: at
+    zero velocity qacc = 0; gravcomp = 0.5 halves the zero-velocity
+    acceleration of the uncompensated chain."""
+    q = np.array([0.3, -0.4, 0.7])
+    acc = {}
+    for gc in ("0", "0.5", "1"):
+        xml = _CHAIN3.replace("<body>", f'<body gravcomp="{gc}">').replace('<body pos', f'<body gravcomp="{gc}" pos')
+        om, env = env_from_xml(xml)
+        env.a["qpos"][:] = q
+        env.step()
+        acc[gc] = env.a["qacc"].copy()
+    np.testing.assert_allclose(acc["1"], 0.0, atol=1e-12)
+    np.testing.assert_allclose(acc["0.5"], 0.5 * acc["0"], rtol=1e-10)
+    assert np.abs(acc["0"]).max() > 1.0
+
+
+def test_com_offset_and_drag_known_answers():
+    """Per-env COM offset: a hinged sphere (COM at L on the arm, axis y,
+    horizontal arm) accelerates at m g (L + d) / (I + m (L + d)^2) with the
+    COM moved by d along the arm.  Per-env drag: a free body in zero gravity
+    (COM at its origin) decelerates at -k |v| v / m."""
+    import ctypes as C
+    L, mass, r = 0.3, 2.0, 0.05
+    xml = (f'<mujoco><option timestep="0.002"/><worldbody><body><joint type="hinge" axis="0 1 0"/>'
+           f'<geom type="sphere" size="{r}" pos="{L} 0 0" mass="{mass}"/></body></worldbody></mujoco>')
+    om, env = env_from_xml(xml)
+    I = 0.4 * mass * r * r
+    for d in (0.0, 0.05, -0.1):
+        env.a["qpos"][:] = 0
+        env.a["qvel"][:] = 0
+        cd = np.zeros((2, 3))
+        cd[1, 0] = d
+        keep = np.ascontiguousarray(cd.reshape(-1))
+        rand = oracle.ORand(None, 1.0, None, keep.ctypes.data_as(C.POINTER(C.c_double)), None)
+        env.step(0, rand)
+        Ld = L + d
+        assert env.a["qacc"][0] == pytest.approx(mass * 9.81 * Ld / (I + mass * Ld * Ld), rel=1e-10)
+    xml = ('<mujoco><option timestep="0.002" gravity="0 0 0"/><worldbody><body><freejoint/>'
+           '<geom type="box" size="0.1 0.2 0.3" mass="3"/></body></worldbody></mujoco>')
+    om, env = env_from_xml(xml)
+    v = np.array([0.4, -1.2, 0.7])
+    env.a["qvel"][:3] = v
+    k = np.array([0.8])
+    rand = oracle.ORand(None, 1.0, None, None, k.ctypes.data_as(C.POINTER(C.c_double)))
+    env.step(0, rand)
+    np.testing.assert_allclose(env.a["qacc"][:3], -0.8 * np.linalg.norm(v) * v / 3.0, rtol=1e-10)
+    np.testing.assert_allclose(env.a["qacc"][3:], 0.0, atol=1e-12)
