@@ -103,7 +103,33 @@ __device__ __forceinline__ void d_chol(float* A, int n, int lane, float* idiag) 
 // x := (L L')^-1 x.  The running vector lives in registers (element i on lane
 // i; a second slot covers n up to 64) and each solved entry is broadcast with a
 // shuffle, so the substitution needs no shared-memory round trip per step.
+__device__ __noinline__ void d_chol_solve_mem(const float* L, const float* idiag, int n, float* x, int lane) {
+  // n > 64: the running vector stays in the workspace, column by column
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    const float xk = x[k] * idiag[k];
+    __syncwarp();
+    if (lane == 0) x[k] = xk;
+#pragma unroll 1
+    for (int i = k + 1 + lane; i < n; i += 32) x[i] -= L[i * n + k] * xk;
+    __syncwarp();
+  }
+#pragma unroll 1
+  for (int k = n - 1; k >= 0; k--) {
+    const float xk = x[k] * idiag[k];
+    __syncwarp();
+    if (lane == 0) x[k] = xk;
+#pragma unroll 1
+    for (int i = lane; i < k; i += 32) x[i] -= L[k * n + i] * xk;
+    __syncwarp();
+  }
+}
+
 __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, int n, float* x, int lane) {
+  if (n > 64) {
+    d_chol_solve_mem(L, idiag, n, x, lane);
+    return;
+  }
   float x0 = lane < n ? x[lane] : 0.f;
   float x1 = lane + 32 < n ? x[lane + 32] : 0.f;
 #pragma unroll 1

@@ -130,7 +130,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     if (m.cone != CONE_PYRAMIDAL) throw std::runtime_error("engine: the elliptic cone is not supported by this build");
     for (int j = 0; j < m.njnt; j++)
       if (m.jnt_limited[j] && m.jnt_type[j] == JNT_BALL) throw std::runtime_error("engine: limited ball joints are not supported");
-    if (m.nv > 64) throw std::runtime_error("engine: models with more than 64 dofs are not supported by this build");
+    if (m.nv > 1024) throw std::runtime_error("engine: models with more than 1024 dofs are not supported by this build");
     DevModelDesc d;
     std::memset(&d, 0, sizeof(d));
     d.nq = m.nq; d.nv = m.nv; d.nu = m.nu; d.nbody = m.nbody; d.njnt = m.njnt; d.ngeom = m.ngeom;
@@ -511,24 +511,31 @@ void Engine::alloc_state() {
 
 void Engine::choose_launch() {
   lockstep_ = cfg_.lockstep ? 1 : 0;
-  const int per_warp = (desc_words_ + ws_stride_) * 4;
+  // a workspace that does not fit shared memory (large models: the bin of
+  // free bodies, nv in the hundreds) lives in HBM, one per resident warp;
+  // shared memory then holds the model descriptors only
+  gws_mode_ = (desc_words_ + ws_stride_) * 4 > 227 * 1024;
+  const int per_warp = (desc_words_ + (gws_mode_ ? 0 : ws_stride_)) * 4;
   if (cfg_.warps_per_block > 0) warps_ = cfg_.warps_per_block;
+  else if (gws_mode_) warps_ = 4;
   else if (lockstep_) warps_ = std::max(1, std::min(8, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs of up to 8 warps per SM
   else warps_ = 4;
-  smem_ = warps_ * (desc_words_ + ws_stride_) * 4;
+  smem_ = warps_ * per_warp;
   if (smem_ > 227 * 1024) {
-    warps_ = std::max(1, (227 * 1024) / ((desc_words_ + ws_stride_) * 4));
-    smem_ = warps_ * (desc_words_ + ws_stride_) * 4;
+    warps_ = std::max(1, (227 * 1024) / per_warp);
+    smem_ = warps_ * per_warp;
   }
   if (smem_ > 227 * 1024) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
   int bps = 0;
   check(mjb_occupancy(warps_, smem_, convex_, &bps), "occupancy");
   if (bps < 1) throw std::runtime_error("engine: kernel cannot be resident with this configuration");
   if (cfg_.blocks_per_sm > 0) bps = std::min(bps, cfg_.blocks_per_sm);
-  persistent_ = lockstep_ ? 1 : (cfg_.persistent < 0 ? 1 : cfg_.persistent);
+  persistent_ = (lockstep_ || gws_mode_) ? 1 : (cfg_.persistent < 0 ? 1 : cfg_.persistent);
   if (persistent_) grid_ = std::min(sm_count_ * bps, (B_ + warps_ - 1) / warps_);
   else grid_ = (B_ + warps_ - 1) / warps_;
   grid_ = std::max(grid_, 1);
+  if (gws_mode_) gws_.alloc((size_t)grid_ * warps_ * ws_stride_);
+  else gws_.alloc(0);
 }
 
 void Engine::configure(const EngineConfig& cfg) {
@@ -557,7 +564,7 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
     copy(warm_.p, sw.p, tot_v_);
   };
   const EngineConfig orig = cfg_;
-  const int per_warp = (desc_words_ + ws_stride_) * 4;
+  const int per_warp = (desc_words_ + (gws_mode_ ? 0 : ws_stride_)) * 4;
   std::vector<TuneCandidate> out;
   cudaEvent_t e0, e1;
   check(cudaEventCreate(&e0), "event");
@@ -643,6 +650,10 @@ StepParams Engine::params(int n, bool record) {
   P.stage_cycles = timing_ ? stage_cycles_.p : nullptr;
   P.ws_stride = ws_stride_;
   P.desc_words = desc_words_;
+  if (gws_mode_) {
+    P.gws = gws_.p;
+    P.gws_blocks = grid_;
+  }
   P.poison_workspace = poison_;
   P.status = status_.p;
   P.niter_sum = niter_sum_.p;

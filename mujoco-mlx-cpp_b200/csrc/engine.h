@@ -67,6 +67,7 @@ class Engine {
   int total_v() const { return tot_v_; }
   int total_u() const { return tot_u_; }
   bool convex() const { return convex_; }
+  bool hbm_workspace() const { return gws_mode_; }
   int total_sensordata() const { return tot_s_; }
   float* sensordata_device() { return sensordata_.p; }
   int total_b() const { return tot_b_; }
@@ -179,6 +180,8 @@ class Engine {
   EngineConfig cfg_;
   bool rand_on_ = false;
   bool convex_ = false;   // some model has a pair for the GJK / EPA collider
+  bool gws_mode_ = false; // workspaces in HBM (too large for shared memory)
+  DevBuf<float> gws_;
   cudaStream_t stream_ = nullptr;
 
   std::vector<ModelLayout> layouts_;

@@ -86,6 +86,10 @@ extern "C" MJMLX_API int mjb200_batched_step_noalloc(MjmlxBatchedSim* sim, float
                    " envs; the allocation-free step supports at most 65536 (MJB200_NOALLOC_MAX_ENVS)");
     return -2;
   }
+  if (E.hbm_workspace()) {
+    mjb::set_error("mjb200_batched_step_noalloc: the model's workspace does not fit shared memory (it needs the HBM workspace of the regular step)");
+    return -1;
+  }
   if (n == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* scratch = nullptr;

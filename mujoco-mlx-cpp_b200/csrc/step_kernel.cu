@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
   const int W = blockDim.x >> 5;
   const bool lockstep = P.lockstep != 0;
   int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
-  float* ws = mjb_smem + W * P.desc_words + warp * P.ws_stride;
+  float* ws = P.gws ? P.gws + ((size_t)blockIdx.x * W + warp) * P.ws_stride : mjb_smem + W * P.desc_words + warp * P.ws_stride;
   // optional per-stage timing: thread 0 of each CTA accumulates the clock
   // between consecutive stage barriers
   const bool timing = lockstep && P.stage_cycles != nullptr && threadIdx.x == 0;
@@ -527,32 +527,34 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
 __global__ void __launch_bounds__(512) mjb_geom_pose_kernel(StepParams P, float* gpose, int ng_max) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
   int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
-  float* ws = mjb_smem + W * P.desc_words + warp * P.ws_stride;
-  const int env = blockIdx.x * W + warp;
-  if (env >= P.num_envs) return;
-  const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
+  float* ws = P.gws ? P.gws + ((size_t)blockIdx.x * W + warp) * P.ws_stride : mjb_smem + W * P.desc_words + warp * P.ws_stride;
 #pragma unroll 1
-  for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
-  __syncwarp();
-  Env E;
-  E.it = P.itab;
-  E.ft = P.ftab;
-  E.ws = ws;
-  E.lane = lane;
-  E.env = env;
-  E.status = 0;
-  E.md = reinterpret_cast<const DevModelDesc*>(dsm);
-  const DevModelDesc& m = *E.md;
-  const int qadr = P.env_qadr[env];
+  for (int env = blockIdx.x * W + warp; env < P.num_envs; env += gridDim.x * W) {
+    const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
 #pragma unroll 1
-  for (int i = lane; i < m.nq; i += 32) ws[m.w_qpos + i] = P.qpos[qadr + i];
-  __syncwarp();
-  d_kinematics(E);
-  float* out = gpose + (size_t)env * ng_max * 12;
+    for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
+    __syncwarp();
+    Env E;
+    E.it = P.itab;
+    E.ft = P.ftab;
+    E.ws = ws;
+    E.lane = lane;
+    E.env = env;
+    E.status = 0;
+    E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+    const DevModelDesc& m = *E.md;
+    const int qadr = P.env_qadr[env];
 #pragma unroll 1
-  for (int k = lane; k < m.ngeom * 12; k += 32) {
-    const int g = k / 12, q = k % 12;
-    out[k] = q < 3 ? ws[m.w_gxpos + 3 * g + q] : ws[m.w_gxmat + 9 * g + (q - 3)];
+    for (int i = lane; i < m.nq; i += 32) ws[m.w_qpos + i] = P.qpos[qadr + i];
+    __syncwarp();
+    d_kinematics(E);
+    float* out = gpose + (size_t)env * ng_max * 12;
+#pragma unroll 1
+    for (int k = lane; k < m.ngeom * 12; k += 32) {
+      const int g = k / 12, q = k % 12;
+      out[k] = q < 3 ? ws[m.w_gxpos + 3 * g + q] : ws[m.w_gxmat + 9 * g + (q - 3)];
+    }
+    __syncwarp();
   }
 }
 
@@ -563,7 +565,8 @@ cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, 
     if (e != cudaSuccess) return e;
     configured = smem_bytes;
   }
-  const int grid = (P.num_envs + warps_per_block - 1) / warps_per_block;
+  int grid = (P.num_envs + warps_per_block - 1) / warps_per_block;
+  if (P.gws && grid > P.gws_blocks) grid = P.gws_blocks;   // one HBM workspace per resident warp
   mjb_geom_pose_kernel<<<grid, warps_per_block * 32, smem_bytes, stream>>>(P, gpose, ng_max);
   return cudaGetLastError();
 }

@@ -31,7 +31,10 @@ struct StepParams {
   int* work_counter;        // persistent scheduling queue head (nullable = static env mapping)
   int lockstep;             // 1: the warps of a CTA run each stage together (barrier between stages)
   unsigned long long* stage_cycles;  // nullable: per-stage SM clock totals (lockstep mode, 8 stages)
-  int ws_stride;            // floats of shared workspace per warp
+  int ws_stride;            // floats of workspace per warp
+  float* gws;               // non-null: workspaces in HBM (ws_stride floats per resident warp, by global warp index)
+                            // for models whose workspace exceeds shared memory; shared memory then holds the descriptors only
+  int gws_blocks;           // CTAs the HBM workspaces cover
   int desc_words;           // 32-bit words of DevModelDesc copied into shared memory
 
   // per-env statistics of this launch

@@ -547,6 +547,53 @@ def convex_pile_xml(nbody: int = 6, seed: int = 0, iterations: int = 30, condim:
             + '<worldbody><geom name="floor" type="plane" size="0 0 1"/>' + "".join(bodies) + '</worldbody></mujoco>')
 
 
+BIN_SHAPES = ("box", "capsule", "ellipsoid", "mesh")
+
+
+def bin_xml(nbody: int = 64, size: float = 1.0, seed: int = 0, condim: int = 3, iterations: int = 30) -> str:
+    """A square bin (floor plus four inward-facing wall planes, side `size`)
+    holding nbody free bodies cycling through boxes, capsules, ellipsoids and
+    convex hulls of 32 points on a 0.05 m sphere with +-20 % radial noise,
+    placed on a jittered grid in layers above the floor with random
+    orientations (the collision-heavy bin workload; nv = 6 nbody)."""
+    g = np.random.Generator(np.random.Philox(key=seed))
+    half = 0.5 * size
+    walls = ['<geom name="floor" type="plane" size="0 0 1"/>']
+    for k, (x, y, zx) in enumerate([(half, 0, "-1 0 0"), (-half, 0, "1 0 0"), (0, half, "0 -1 0"), (0, -half, "0 1 0")]):
+        walls.append(f'<geom name="wall{k}" type="plane" pos="{x:.4f} {y:.4f} 0" zaxis="{zx}" size="{half:.4f} {half:.4f} 0.1"/>')
+    per_side = max(1, int(np.ceil(np.sqrt(min(nbody, 16)))))
+    pitch = (size - 0.16) / max(per_side - 1, 1) if per_side > 1 else 0.0
+    assets, bodies = [], []
+    for i in range(nbody):
+        kind = BIN_SHAPES[i % len(BIN_SHAPES)]
+        if kind == "box":
+            a = g.uniform(0.025, 0.045, 3)
+            geom = f'type="box" size="{a[0]:.4f} {a[1]:.4f} {a[2]:.4f}"'
+        elif kind == "capsule":
+            geom = f'type="capsule" size="{g.uniform(0.02, 0.03):.4f} {g.uniform(0.03, 0.045):.4f}"'
+        elif kind == "ellipsoid":
+            a = g.uniform(0.03, 0.055, 3)
+            geom = f'type="ellipsoid" size="{a[0]:.4f} {a[1]:.4f} {a[2]:.4f}"'
+        else:
+            v = noisy_sphere_vertices(32, 0.05, 0.2, g)
+            assets.append(f'<mesh name="hull{i}" vertex="' + " ".join(f"{x:.5f}" for x in v.reshape(-1)) + '"/>')
+            geom = f'type="mesh" mesh="hull{i}"'
+        layer, cell = divmod(i, per_side * per_side)
+        cx, cy = divmod(cell, per_side)
+        x = -half + 0.08 + cx * pitch + g.uniform(-0.02, 0.02)
+        y = -half + 0.08 + cy * pitch + g.uniform(-0.02, 0.02)
+        z = 0.08 + 0.14 * layer + g.uniform(0.0, 0.02)
+        q = g.normal(size=4)
+        q /= np.linalg.norm(q)
+        bodies.append(f'<body name="b{i}" pos="{x:.4f} {y:.4f} {z:.4f}" quat="{q[0]:.5f} {q[1]:.5f} {q[2]:.5f} {q[3]:.5f}"><freejoint/>'
+                      f'<geom {geom} mass="{g.uniform(0.1, 0.5):.3f}"/></body>')
+    return (f'<mujoco model="bin{nbody}"><compiler angle="radian"/>'
+            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            f'<default><geom condim="{condim}" friction="0.8 0.01 0.001"/></default>'
+            + (f'<asset>{"".join(assets)}</asset>' if assets else "")
+            + '<worldbody>' + "".join(walls) + "".join(bodies) + '</worldbody></mujoco>')
+
+
 def box_pile_state(model, num_envs: int, seed: int):
     """qpos0 with each box's position jittered by U[-0.03, 0.03] m and its
     orientation rotated by up to 0.4 rad about a random axis."""
