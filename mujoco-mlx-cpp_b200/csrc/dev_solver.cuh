@@ -95,8 +95,55 @@ __device__ __noinline__ void d_chol_reg(float* A, int n, int lane, float* idiag)
   }
 }
 
-__device__ __forceinline__ void d_chol(float* A, int n, int lane, float* idiag) {
+// Right-looking Cholesky that skips exact zeros (large models): after
+// column k is scaled, its nonzero rows below the diagonal are listed with a
+// ballot scan and only their pairs are updated.  The arithmetic on the
+// nonzero entries is the dense algorithm's; for the bin of free bodies M is
+// 6 x 6 block-diagonal and H keeps the contact graph's block pattern plus
+// fill-in, so most of the n^3 / 6 updates of the dense version vanish.
+// nz: n ints of scratch.
+__device__ __noinline__ void d_chol_sparse(float* A, int n, int lane, float* idiag, int* nz) {
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    const float d = sqrtf(fmaxf(A[k * n + k], 1e-30f));
+    const float id = 1.f / d;
+    __syncwarp();
+    int cnt = 0;
+#pragma unroll 1
+    for (int base = k + 1; base < n; base += 32) {
+      const int i = base + lane;
+      bool on = false;
+      if (i < n) {
+        const float v = A[i * n + k];
+        on = v != 0.f;
+        if (on) A[i * n + k] = v * id;
+      }
+      const unsigned bal = __ballot_sync(FULL_MASK, on);
+      if (on) nz[cnt + __popc(bal & ((1u << lane) - 1u))] = i;
+      cnt += __popc(bal);
+    }
+    if (lane == 0) {
+      A[k * n + k] = d;
+      idiag[k] = id;
+    }
+    __syncwarp();
+    const int T = cnt * (cnt + 1) / 2;
+#pragma unroll 1
+    for (int t = lane; t < T; t += 32) {
+      int p = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+      if ((p + 1) * (p + 2) / 2 <= t) p++;
+      else if (p * (p + 1) / 2 > t) p--;
+      const int q = t - p * (p + 1) / 2;
+      const int i = nz[p], j = nz[q];
+      A[i * n + j] -= A[i * n + k] * A[j * n + k];
+    }
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void d_chol(float* A, int n, int lane, float* idiag, int* nz = nullptr) {
   if (n <= 32) d_chol_reg(A, n, lane, idiag);
+  else if (n > 64 && nz) d_chol_sparse(A, n, lane, idiag, nz);
   else d_chol_smem(A, n, lane, idiag);
 }
 
@@ -192,13 +239,57 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
   d_chol(L, n, lane, idiag);
 }
 
+// Row-sparse variant for large models (nv > 64, HBM workspaces): a contact
+// row touches only the dofs of its two bodies' chains (12 for two free
+// bodies out of hundreds), so H = M + sum D_r J_r' J_r is accumulated row by
+// row over each row's nonzero columns (found with a ballot scan) instead of
+// entry by entry over every active row.
+__device__ __noinline__ void d_factor_sparse(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
+                                             int n, int lane, int* nz, float* L, float* idiag) {
+#pragma unroll 1
+  for (int i = 0; i < n; i++) {
+#pragma unroll 1
+    for (int j = lane; j <= i; j += 32) L[i * n + j] = M[i * n + j] + ((i == j && ddiag) ? dscale * ldf(ddiag, i) : 0.f);
+  }
+  __syncwarp();
+#pragma unroll 1
+  for (int a = 0; a < nact; a++) {
+    const int r = act[a];
+    const float* row = J + r * n;
+    int cnt = 0;
+#pragma unroll 1
+    for (int base = 0; base < n; base += 32) {
+      const int c = base + lane;
+      const bool on = c < n && row[c] != 0.f;
+      const unsigned bal = __ballot_sync(FULL_MASK, on);
+      if (on) nz[cnt + __popc(bal & ((1u << lane) - 1u))] = c;
+      cnt += __popc(bal);
+    }
+    __syncwarp();
+    const float d = eD[r];
+    const int T = cnt * (cnt + 1) / 2;
+#pragma unroll 1
+    for (int t = lane; t < T; t += 32) {
+      int p = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+      if ((p + 1) * (p + 2) / 2 <= t) p++;
+      else if (p * (p + 1) / 2 > t) p--;
+      const int q = t - p * (p + 1) / 2;
+      const int i = nz[p], j = nz[q];   // nz ascending: i >= j
+      L[i * n + j] += d * row[i] * row[j];
+    }
+    __syncwarp();
+  }
+  d_chol(L, n, lane, idiag, nz);
+}
+
 __device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const float* ddiag, float dscale, float* L, float* idiag) {
   const DevModelDesc& m = *E.md;
   const int nv = m.nv;
   const float* M = E.ws + m.w_M;
   const float* J = E.ws + m.w_J;
   const float* eD = E.ws + m.w_efc + EFC_D * m.nefc_max;
-  d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag);
+  if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag);
+  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag);
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {

@@ -64,7 +64,7 @@ struct DevModelDesc {
   int w_con, w_rowcon;
   // phase region K (kinematics / dynamics), aliased by region S (solver)
   int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;
-  int w_J, w_efc, w_H, w_active;
+  int w_J, w_efc, w_H, w_active, w_nz;   // w_nz: nv ints, nonzero columns of one row (row-sparse H build)
 };
 
 // per-tendon floats: range lo, hi, margin, frictionloss, stiffness, damping,

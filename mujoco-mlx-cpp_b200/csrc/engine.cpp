@@ -408,6 +408,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     int kend = off;
     off = kbase;
     d.w_J = take(d.nefc_max * nv); d.w_efc = take(MJB_EFC_FIELDS * d.nefc_max); d.w_H = take(nv * nv); d.w_active = take(d.nefc_max);
+    d.w_nz = take(nv);
     int send = off;
     d.ws_size = std::max(kend, send);
     ws_stride_ = std::max(ws_stride_, d.ws_size);

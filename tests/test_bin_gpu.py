@@ -48,3 +48,34 @@ def test_bin_parity_and_rollout(nbody, side, B, ncon, nefc, steps):
         errs = np.array(errs)
         print(nbody, "ncon", list(g["stats"]["ncon"]), "median %.2e max %.2e" % (np.median(errs), errs.max()))
         assert np.median(errs) <= 1e-4 and errs.max() <= 5e-3, (np.median(errs), errs.max())
+
+
+def test_bin_workload_2048_envs_sampled_parity():
+    """The bin workload at its batch size: 2048 envs of 64 free bodies,
+    stepped 80 substeps from seeded poses; 64 sampled envs (every 32nd)
+    checked against the oracle as above (contact pairs, row counts, qacc)."""
+    model = mjb200.load_model_from_string(mjb200.models.bin_xml(64, 1.0, seed=1))
+    om = oracle.OracleModel(model.dump())
+    B, ncon, nefc = 2048, 400, 1600
+    q, v = mjb200.models.box_pile_state(model, B, seed=7)
+    sim = mjb200.BatchedSim(model, B, ncon_max=ncon, nefc_max=nefc)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    sim.step(None, 80)
+    qp, qv = sim.state()
+    assert np.all(sim.stats()["status"] == 0) and np.isfinite(qp).all()
+    g = gpu_step_from(sim, qp, qv, None, ncon, nefc)
+    idx = np.arange(0, B, 32)
+    o = oracle_step_from(om, qp[idx].astype(np.float64), qv[idx].astype(np.float64), np.zeros((len(idx), 1)), ncon_max=ncon, nefc_max=nefc)
+    errs, flips = [], 0
+    for k, e in enumerate(idx):
+        assert g["stats"]["status"][e] == 0 and o[k]["status"] == 0
+        ok, nb = contact_sets_match(g["con"][e], o[k]["contacts"], g["stats"]["ncon"][e])
+        assert ok, e
+        flips += nb
+        if nb == 0:
+            assert g["stats"]["nefc"][e] == o[k]["nefc"]
+            errs.append(rel_err(g["vec"][e, 2, : om.nv], o[k]["qacc"]))
+    errs = np.array(errs)
+    print("sampled", len(idx), "boundary flips", flips, "ncon mean", g["stats"]["ncon"][idx].mean(), "median %.2e max %.2e" % (np.median(errs), errs.max()))
+    assert len(errs) >= 60
+    assert np.median(errs) <= 1e-4 and errs.max() <= 5e-3, (np.median(errs), errs.max())
