@@ -340,8 +340,8 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       const float* f = ft + m.f_eq + 15 * r;
       float x1, v1, x2 = 0.f, v2 = 0.f;
       if (ten) {
-        d_tendon_lv(m, it, ft, qpos, qvel, o1, x1, v1);
-        if (o2 >= 0) d_tendon_lv(m, it, ft, qpos, qvel, o2, x2, v2);
+        d_tendon_lv(m, ws, o1, x1, v1);
+        if (o2 >= 0) d_tendon_lv(m, ws, o2, x2, v2);
       } else {
         x1 = qpos[ldi(qi, 3)];
         v1 = qvel[o1];
@@ -361,11 +361,11 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       impedance(m, ldf(f, 7), ldf(f, 8), si, pos, k, b, imp);
       const float R = fmaxf((1.f - imp) / imp * ldf(f, 14), 1e-15f);
       if (ten) {
-        d_tendon_row(m, it, ft, o1, 1.f, J + r * nv);
+        d_tendon_row(m, ws, o1, 1.f, J + r * nv);
         if (o2 >= 0) {
-          const int adr = ldi(it, m.i_ten + 3 * o2), num = ldi(it, m.i_ten + 3 * o2 + 1);
+          const float* J2 = ws + m.w_ten + o2 * (nv + 2) + 2;
           #pragma unroll 1
-          for (int w = adr; w < adr + num; w++) J[r * nv + ldi(it, m.i_wrap + 2 * w)] -= dpoly * ldf(ft, m.f_wrap + w);
+          for (int c = 0; c < nv; c++) J[r * nv + c] -= dpoly * J2[c];
         }
       } else {
         #pragma unroll 1
@@ -418,9 +418,9 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       float si[5] = {ldf(tf, TEN_SIFRI), ldf(tf, TEN_SIFRI + 1), ldf(tf, TEN_SIFRI + 2), ldf(tf, TEN_SIFRI + 3), ldf(tf, TEN_SIFRI + 4)};
       float k, b, imp, len, vel;
       impedance(m, ldf(tf, TEN_SRFRI), ldf(tf, TEN_SRFRI + 1), si, 0.f, k, b, imp);
-      d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+      d_tendon_lv(m, ws, t, len, vel);
       const float R = fmaxf((1.f - imp) / imp * ldf(tf, TEN_INVW), 1e-15f);
-      d_tendon_row(m, it, ft, t, 1.f, J + r * nv);
+      d_tendon_row(m, ws, t, 1.f, J + r * nv);
       EfcRef e{efc + r, ne};
       e[EFC_D] = 1.f / R;
       e[EFC_AREF] = -b * vel;
@@ -484,7 +484,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       if (li < m.ntlimit) {
         t = ldi(it, m.i_tlimit + li);
         const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
-        d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+        d_tendon_lv(m, ws, t, len, vel);
         dist[0] = len - ldf(tf, TEN_LO);
         dist[1] = ldf(tf, TEN_HI) - len;
         act[0] = dist[0] < ldf(tf, TEN_MARGIN);
@@ -502,7 +502,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
         float pos = dist[s] - ldf(tf, TEN_MARGIN), k, b, imp;
         impedance(m, ldf(tf, TEN_SRLIM), ldf(tf, TEN_SRLIM + 1), si, pos, k, b, imp);
         const float sg = s == 0 ? 1.f : -1.f;
-        d_tendon_row(m, it, ft, t, sg, J + r * nv);
+        d_tendon_row(m, ws, t, sg, J + r * nv);
         const float R = fmaxf((1.f - imp) / imp * ldf(tf, TEN_INVW), 1e-15f);
         EfcRef e{efc + r, ne};
         e[EFC_D] = 1.f / R;

@@ -9,6 +9,7 @@
 //   d_forces      <- forward.hpp:399-469
 #pragma once
 #include "dev_collide.cuh"
+#include "tendon_wrap.h"
 #include "step_params.h"
 
 namespace mjbdev {
@@ -471,39 +472,146 @@ __device__ __noinline__ void d_rne(Env& E, float* bias) {
   __syncwarp();
 }
 
-// Fixed tendon t: length = sum coef * qpos and velocity = sum coef * qvel
-// over its wraps (reference: tendon.hpp emit_tendon_phase, fixed branch).
-__device__ __forceinline__ void d_tendon_lv(const DevModelDesc& m, const int* it, const float* ft, const float* qpos, const float* qvel, int t,
-                                            float& len, float& vel) {
-  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
-  float l = 0.f, v = 0.f;
-  #pragma unroll 1
-  for (int w = adr; w < adr + num; w++) {
-    const float c = ldf(ft, m.f_wrap + w);
-    l += c * qpos[ldi(it, m.i_wrap + 2 * w + 1)];
-    v += c * qvel[ldi(it, m.i_wrap + 2 * w)];
-  }
-  len = l;
-  vel = v;
+// Tendons of this substep: length, velocity and Jacobian of every tendon
+// into the persistent workspace (w_ten: per tendon [length, velocity,
+// J(nv)]), computed once after the COM pass and read by the forces, the
+// constraint rows and the sensors (reference: tendon.hpp emit_tendon_phase,
+// MuJoCo mj_tendon).  Fixed tendons: length = sum coef * qpos, J = sum coef
+// e_dof.  Spatial tendons: lane 0 walks the path (sites, wrapping sphere /
+// cylinder geoms, pulley divisors) and lists its straight pieces; every
+// lane then sums, for its dofs, piece direction x (Jacobian at the piece's
+// end - Jacobian at its start), the tangent points of a wrap moving with the
+// geom; velocity = J qvel.
+__device__ __forceinline__ void d_site_world(const DevModelDesc& m, const int* it, const float* ft, const float* ws, int s, float* p) {
+  const int b = ldi(it, m.i_site_body + s);
+  const float q[4] = {ws[m.w_xquat + 4 * b], ws[m.w_xquat + 4 * b + 1], ws[m.w_xquat + 4 * b + 2], ws[m.w_xquat + 4 * b + 3]};
+  const float l[3] = {ldf(ft, m.f_site + 3 * s), ldf(ft, m.f_site + 3 * s + 1), ldf(ft, m.f_site + 3 * s + 2)};
+  float r[3];
+  qrot(q, l, r);
+  for (int k = 0; k < 3; k++) p[k] = ws[m.w_xpos + 3 * b + k] + r[k];
 }
 
-// Component of tendon t's (constant) Jacobian on dof i.
-__device__ __forceinline__ float d_tendon_jac(const DevModelDesc& m, const int* it, const float* ft, int t, int i) {
-  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
-  float j = 0.f;
-  #pragma unroll 1
-  for (int w = adr; w < adr + num; w++)
-    if (ldi(it, m.i_wrap + 2 * w) == i) j += ldf(ft, m.f_wrap + w);
-  return j;
+// lane 0: append the straight piece p0 (body b0) -> p1 (body b1), scaled
+__device__ __forceinline__ void d_piece(float* seg, int& np, const float* p0, int b0, const float* p1, int b1, float scale) {
+  float* q = seg + 9 * np++;
+  for (int k = 0; k < 3; k++) { q[k] = p0[k]; q[3 + k] = p1[k]; }
+  q[6] = __int_as_float(b0);
+  q[7] = __int_as_float(b1);
+  q[8] = scale;
 }
+
+__device__ __noinline__ void d_tendons(Env& E) {
+  const DevModelDesc& m = *E.md;
+  const int* it = E.it;
+  const float* ft = E.ft;
+  float* ws = E.ws;
+  const int nv = m.nv, lane = E.lane;
+  const float* qpos = ws + m.w_qpos;
+  const float* qvel = ws + m.w_qvel;
+  float* seg = ws + m.w_tseg;
+  #pragma unroll 1
+  for (int t = 0; t < m.ntendon; t++) {
+    float* row = ws + m.w_ten + t * (nv + 2);
+    const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
+    int np = 0;
+    float len = 0.f;
+    if (lane == 0) {
+      float scale = 1.f;
+      #pragma unroll 1
+      for (int w = adr; w < adr + num; w++) {
+        const int* wi = it + m.i_wrap + 3 * w;
+        const int ty = ldi(wi, 0);
+        if (ty == 1) {
+          len += ldf(ft, m.f_wrap + w) * qpos[ldi(wi, 2)];
+        } else if (ty == 2) {
+          scale = 1.f / ldf(ft, m.f_wrap + w);
+        } else if (ty == 3 && w + 1 < adr + num) {
+          const int* wn = wi + 3;
+          const int tn = ldi(wn, 0);
+          if (tn == 3) {
+            float p0[3], p1[3];
+            d_site_world(m, it, ft, ws, ldi(wi, 1), p0);
+            d_site_world(m, it, ft, ws, ldi(wn, 1), p1);
+            const float e[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            len += scale * norm3(e);
+            d_piece(seg, np, p0, ldi(wi, 2), p1, ldi(wn, 2), scale);
+          } else if ((tn == 4 || tn == 5) && w + 2 < adr + num) {
+            const int* w2 = wi + 6;
+            const int g = ldi(wn, 1), ss = ldi(wn, 2), gb = ldi(it, m.i_geom_bodyid + g);
+            float p0[3], p1[3], sp[3], t0[3], t1[3];
+            d_site_world(m, it, ft, ws, ldi(wi, 1), p0);
+            d_site_world(m, it, ft, ws, ldi(w2, 1), p1);
+            if (ss >= 0) d_site_world(m, it, ft, ws, ss, sp);
+            bool wrapped = false;
+            const float full = mjbwrap::geom<float>(tn == 4 ? 2 : 5, ws + m.w_gxpos + 3 * g, ws + m.w_gxmat + 9 * g, ldf(ft, m.f_geom_size + 3 * g), p0,
+                                                    p1, ss >= 0 ? sp : nullptr, t0, t1, wrapped);
+            len += scale * full;
+            if (!wrapped) {
+              d_piece(seg, np, p0, ldi(wi, 2), p1, ldi(w2, 2), scale);
+            } else {
+              d_piece(seg, np, p0, ldi(wi, 2), t0, gb, scale);
+              d_piece(seg, np, t1, gb, p1, ldi(w2, 2), scale);
+            }
+            w += 1;
+          }
+        }
+      }
+    }
+    np = __shfl_sync(FULL_MASK, np, 0);
+    len = __shfl_sync(FULL_MASK, len, 0);
+    __syncwarp();
+    float vpart = 0.f;
+    #pragma unroll 1
+    for (int i = lane; i < nv; i += 32) {
+      float j = 0.f;
+      #pragma unroll 1
+      for (int w = adr; w < adr + num; w++)
+        if (ldi(it, m.i_wrap + 3 * w) == 1 && ldi(it, m.i_wrap + 3 * w + 1) == i) j += ldf(ft, m.f_wrap + w);
+      const int db = ldi(it, m.i_dof_bodyid + i), dsub = ldi(it, m.i_body_subtreesize + db);
+      const float* cd = ws + m.w_cdof + 6 * i;
+      #pragma unroll 1
+      for (int p = 0; p < np; p++) {
+        const float* q = seg + 9 * p;
+        float e[3] = {q[3] - q[0], q[4] - q[1], q[5] - q[2]};
+        const float l = norm3(e);
+        if (l < 1e-12f) continue;
+        for (int k = 0; k < 3; k++) e[k] /= l;
+        for (int side = 0; side < 2; side++) {
+          const int b = __float_as_int(q[6 + side]);
+          if (b < db || b >= db + dsub) continue;
+          const int root = ldi(it, m.i_body_rootid + b);
+          const float* pt = q + 3 * side;
+          const float off[3] = {pt[0] - ws[m.w_scom + 3 * root], pt[1] - ws[m.w_scom + 3 * root + 1], pt[2] - ws[m.w_scom + 3 * root + 2]};
+          const float jp[3] = {cd[3] + cd[1] * off[2] - cd[2] * off[1], cd[4] + cd[2] * off[0] - cd[0] * off[2], cd[5] + cd[0] * off[1] - cd[1] * off[0]};
+          j += (side ? 1.f : -1.f) * q[8] * (e[0] * jp[0] + e[1] * jp[1] + e[2] * jp[2]);
+        }
+      }
+      row[2 + i] = j;
+      vpart += j * qvel[i];
+    }
+    const float vel = warp_sum(vpart);
+    if (lane == 0) {
+      row[0] = len;
+      row[1] = vel;
+    }
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void d_tendon_lv(const DevModelDesc& m, const float* ws, int t, float& len, float& vel) {
+  const float* row = ws + m.w_ten + t * (m.nv + 2);
+  len = row[0];
+  vel = row[1];
+}
+
+// Component of tendon t's Jacobian on dof i.
+__device__ __forceinline__ float d_tendon_jac(const DevModelDesc& m, const float* ws, int t, int i) { return ws[m.w_ten + t * (m.nv + 2) + 2 + i]; }
 
 // row[0..nv) = sg * (Jacobian of tendon t), written by one lane.
-__device__ __forceinline__ void d_tendon_row(const DevModelDesc& m, const int* it, const float* ft, int t, float sg, float* row) {
+__device__ __forceinline__ void d_tendon_row(const DevModelDesc& m, const float* ws, int t, float sg, float* row) {
+  const float* J = ws + m.w_ten + t * (m.nv + 2) + 2;
   #pragma unroll 1
-  for (int c = 0; c < m.nv; c++) row[c] = 0.f;
-  const int adr = ldi(it, m.i_ten + 3 * t), num = ldi(it, m.i_ten + 3 * t + 1);
-  #pragma unroll 1
-  for (int w = adr; w < adr + num; w++) row[ldi(it, m.i_wrap + 2 * w)] += sg * ldf(ft, m.f_wrap + w);
+  for (int c = 0; c < m.nv; c++) row[c] = sg * J[c];
 }
 
 // passive + actuation + smooth force
@@ -564,11 +672,11 @@ __device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* 
       #pragma unroll 1
       for (int k = 0; k < m.npten; k++) {
         const int t = ldi(it, m.i_pten + k);
-        const float jt = d_tendon_jac(m, it, ft, t, i);
+        const float jt = d_tendon_jac(m, ws, t, i);
         if (jt == 0.f) continue;
         const float* tf = ft + m.f_ten + MJB_TEN_FLOATS * t;
         float len, vel;
-        d_tendon_lv(m, it, ft, qpos, qvel, t, len, vel);
+        d_tendon_lv(m, ws, t, len, vel);
         const float kst = ldf(tf, TEN_STIFF), lo = ldf(tf, TEN_SPRLO), hi = ldf(tf, TEN_SPRHI);
         float f = 0.f;
         if (len > hi) f += kst * (hi - len);
@@ -585,9 +693,9 @@ __device__ __noinline__ void d_forces(Env& E, const StepParams& P, const float* 
         float moment = 1.f, len, vel;
         if (ten >= 0) {
           // tendon transmission: length / velocity / moment from the tendon
-          moment = d_tendon_jac(m, it, ft, ten, i);
+          moment = d_tendon_jac(m, ws, ten, i);
           if (moment == 0.f) continue;
-          d_tendon_lv(m, it, ft, qpos, qvel, ten, len, vel);
+          d_tendon_lv(m, ws, ten, len, vel);
         } else {
           if (ldi(ai, 0) != i) continue;
           len = qpos[ldi(ai, 1)];

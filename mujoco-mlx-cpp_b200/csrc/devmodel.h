@@ -29,7 +29,9 @@ struct DevModelDesc {
   int neq, i_eq;  // joint / tendon equalities: 5 ints each (kind 0 joint 1 tendon, obj1, obj2 or -1, qposadr1, qposadr2);
                   // obj = dof for joints, tendon id for tendons
   int i_act;     // 7 per actuator: dof qposadr gaintype biastype ctrllimited forcelimited tendon (-1 = joint transmission)
-  int ntendon, i_ten, i_wrap;  // fixed tendons: 3 ints each (wrapadr wrapnum limited); 2 per wrap (dof qposadr)
+  int ntendon, i_ten, i_wrap;  // tendons: 3 ints each (wrapadr wrapnum limited); 3 per wrap element: type (1 joint, 2 pulley,
+                               // 3 site, 4 sphere, 5 cylinder) then (dof, qposadr) / (0, 0) / (site, body) / (geom, side site or -1)
+  int i_site_body;             // body of each site
   int ntfloss, i_tfloss;       // tendons with frictionloss (tendon ids)
   int ntlimit, i_tlimit;       // limited tendons (tendon ids)
   int npten, i_pten;           // tendons with stiffness or damping (tendon ids)
@@ -50,7 +52,8 @@ struct DevModelDesc {
   int f_floss;   // 8 per frictionloss dof: floss solref(2) solimp(5)
   int f_eq;      // 15 per joint equality: qpos0 ref1, ref2, polycoef(5), solref(2), solimp(5), invweight
   int f_act;     // 11 per actuator: gear gain(3) bias(3) ctrlrange(2) forcerange(2)
-  int f_wrap;    // 1 per wrap: coef
+  int f_wrap;    // 1 per wrap: joint coef or pulley divisor
+  int f_site;    // 3 per site: position in its body
   int f_ten;     // MJB_TEN_FLOATS per tendon (layout below)
   int f_sensor;  // MJB_SENSOR_FLOATS per sensor: object frame in its body (pos 3, quat 4), actuator gear
   int f_gcomp;   // gravcomp per body
@@ -61,6 +64,8 @@ struct DevModelDesc {
   int ws_size;
   int w_qpos, w_qvel, w_ctrl, w_x, w_xwarm;
   int w_scom, w_cdof, w_M, w_qfs, w_qas, w_qfa, w_vec;   // w_vec: 8*nv solver vectors
+  int w_ten;     // per tendon [length, velocity, J(nv)] of the current substep
+  int w_tseg;    // kinematics-region scratch: straight pieces of one spatial tendon path (9 floats each)
   int w_con, w_rowcon;
   // phase region K (kinematics / dynamics), aliased by region S (solver)
   int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;

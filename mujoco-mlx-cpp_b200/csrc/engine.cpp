@@ -233,10 +233,18 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
       if (m.tendon_limited[t]) tlim.push_back(t);
       if (m.tendon_stiffness[t] != 0 || m.tendon_damping[t] != 0) tpas.push_back(t);
     }
-    for (size_t w = 0; w < m.wrap_joint.size(); w++) {
-      wi.insert(wi.end(), {m.jnt_dofadr[m.wrap_joint[w]], m.jnt_qposadr[m.wrap_joint[w]]});
-      wf.push_back(m.wrap_coef[w]);
+    int max_pieces = 1;
+    for (int t = 0; t < m.ntendon; t++) max_pieces = std::max(max_pieces, m.tendon_num[t]);
+    for (size_t w = 0; w < m.wrap_objid.size(); w++) {
+      const int ty = m.wrap_type[w], id = m.wrap_objid[w];
+      if (ty == 1) wi.insert(wi.end(), {1, m.jnt_dofadr[id], m.jnt_qposadr[id]});
+      else if (ty == 2) wi.insert(wi.end(), {2, 0, 0});
+      else if (ty == 3) wi.insert(wi.end(), {3, id, m.site_bodyid[id]});
+      else wi.insert(wi.end(), {ty, id, (int)m.wrap_prm[w]});
+      wf.push_back(ty == 1 || ty == 2 ? m.wrap_prm[w] : 0.0);
     }
+    d.i_site_body = tb.ai(m.site_bodyid);
+    d.f_site = tb.af(m.site_pos);
     d.ntendon = m.ntendon;
     d.i_ten = tb.ai(ti);
     d.i_wrap = tb.ai(wi);
@@ -400,11 +408,13 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.w_qpos = take(m.nq); d.w_qvel = take(nv); d.w_ctrl = take(nu); d.w_x = take(nv); d.w_xwarm = take(nv);
     d.w_scom = take(3 * nb); d.w_cdof = take(6 * nv); d.w_M = take(nv * nv); d.w_qfs = take(nv); d.w_qas = take(nv); d.w_qfa = take(nv);
     d.w_vec = take(9 * nv); d.w_con = take(MJB_CONTACT_FLOATS * d.ncon_max); d.w_rowcon = 0;
+    d.w_ten = take(std::max(1, m.ntendon * (nv + 2)));
     int kbase = off;
     d.w_xpos = take(3 * nb); d.w_xquat = take(4 * nb); d.w_xmat = take(9 * nb); d.w_xipos = take(3 * nb);
     d.w_xanchor = take(3 * nj); d.w_xaxis = take(3 * nj); d.w_gxpos = take(3 * ng); d.w_gxmat = take(9 * ng);
     d.w_cinert = take(10 * nb); d.w_crb = take(10 * nb); d.w_cvel = take(6 * nb); d.w_cdofdot = take(6 * nv);
     d.w_cacc = take(6 * nb); d.w_tmp = take(4 * nb);
+    d.w_tseg = take(9 * max_pieces);
     int kend = off;
     off = kbase;
     d.w_J = take(d.nefc_max * nv); d.w_efc = take(MJB_EFC_FIELDS * d.nefc_max); d.w_H = take(nv * nv); d.w_active = take(d.nefc_max);

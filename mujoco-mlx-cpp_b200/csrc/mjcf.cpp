@@ -20,6 +20,7 @@
 
 #include "hull.h"
 #include "model.h"
+#include "tendon_wrap.h"
 #include "xml.h"
 
 namespace mjb {
@@ -776,22 +777,60 @@ struct Compiler {
 
   void parse_tendon(const XmlNode& n) {
     for (auto& t : n.children) {
-      if (t.tag == "spatial") fail("spatial tendons are not supported by this build (fixed tendons are)");
-      if (t.tag != "fixed") fail("unsupported element <" + t.tag + "> inside <tendon>");
+      if (t.tag != "fixed" && t.tag != "spatial") fail("unsupported element <" + t.tag + "> inside <tendon>");
       std::string cls;
       auto nm = t.attr("name");
       m.tendon_name.push_back(nm ? *nm : std::string());
-      m.tendon_adr.push_back((int)m.wrap_joint.size());
-      for (auto& w : t.children) {
-        if (w.tag != "joint") fail("fixed tendon elements must be <joint>");
-        auto jn = w.attr("joint");
-        if (!jn) fail("tendon joint needs joint=");
-        int j = joint_by_name(*jn);
-        if (m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE) fail("fixed tendons use hinge or slide joints");
-        m.wrap_joint.push_back(j);
-        m.wrap_coef.push_back(num(w, "coef", cls, 1));
+      m.tendon_adr.push_back((int)m.wrap_objid.size());
+      if (t.tag == "fixed") {
+        for (auto& w : t.children) {
+          if (w.tag != "joint") fail("fixed tendon elements must be <joint>");
+          auto jn = w.attr("joint");
+          if (!jn) fail("tendon joint needs joint=");
+          int j = joint_by_name(*jn);
+          if (m.jnt_type[j] != JNT_HINGE && m.jnt_type[j] != JNT_SLIDE) fail("fixed tendons use hinge or slide joints");
+          m.wrap_type.push_back(1);
+          m.wrap_objid.push_back(j);
+          m.wrap_prm.push_back(num(w, "coef", cls, 1));
+        }
+      } else {
+        // spatial path: branches of sites separated by pulleys; a sphere or
+        // cylinder geom may sit between two sites of a branch
+        int prev = 0;   // 0 branch start, 3 site, 4 geom
+        for (auto& w : t.children) {
+          if (w.tag == "site") {
+            auto sn = w.attr("site");
+            if (!sn) fail("spatial tendon site needs site=");
+            m.wrap_type.push_back(3);
+            m.wrap_objid.push_back(index_of(m.site_name, *sn, "site"));
+            m.wrap_prm.push_back(0);
+            prev = 3;
+          } else if (w.tag == "geom") {
+            auto gn = w.attr("geom");
+            if (!gn) fail("spatial tendon geom needs geom=");
+            if (prev != 3) fail("a wrapping geom must follow a site in a spatial tendon");
+            const int g = geom_by_name(*gn);
+            if (m.geom_type[g] != GEOM_SPHERE && m.geom_type[g] != GEOM_CYLINDER) fail("spatial tendons wrap around sphere and cylinder geoms only");
+            m.wrap_type.push_back(m.geom_type[g] == GEOM_SPHERE ? 4 : 5);
+            m.wrap_objid.push_back(g);
+            auto ss = w.attr("sidesite");
+            m.wrap_prm.push_back(ss ? index_of(m.site_name, *ss, "site") : -1);
+            prev = 4;
+          } else if (w.tag == "pulley") {
+            if (prev != 3) fail("a pulley must follow a site in a spatial tendon");
+            const double dv = num(w, "divisor", cls, 0);
+            if (!(dv > 0)) fail("pulley divisor must be positive");
+            m.wrap_type.push_back(2);
+            m.wrap_objid.push_back(-1);
+            m.wrap_prm.push_back(dv);
+            prev = 0;
+          } else {
+            fail("spatial tendon elements must be <site>, <geom> or <pulley>");
+          }
+        }
+        if (prev != 3) fail("a spatial tendon (and each pulley branch) must end with a site");
       }
-      m.tendon_num.push_back((int)m.wrap_joint.size() - m.tendon_adr.back());
+      m.tendon_num.push_back((int)m.wrap_objid.size() - m.tendon_adr.back());
       auto rng = nums(t, "range", cls, {0, 0});
       auto lim = t.attr("limited");
       const bool auto_lim = !lim || *lim == "auto";
@@ -1326,16 +1365,82 @@ void compute_invweights(Model& m) {
       m.dof_invweight0[a] = minv_diag[a];
     }
   }
-  // fixed tendons: rest length and invweight J M^-1 J^T at qpos0
+  // tendons: rest length and invweight J M^-1 J^T at qpos0
   m.tendon_length0.assign(m.ntendon, 0);
   m.tendon_invweight0.assign(m.ntendon, 0);
+  // world point / body of site s and geom poses at qpos0
+  auto site_world = [&](int sidx, double* p) {
+    const int b = m.site_bodyid[sidx];
+    double r[3];
+    quat_rot(&d.xquat[4 * b], &m.site_pos[3 * sidx], r);
+    for (int k = 0; k < 3; k++) p[k] = d.xpos[3 * b + k] + r[k];
+  };
+  // add scale * dir' (point Jacobian of body b at world point p) to jt
+  auto add_point = [&](std::vector<double>& jt, int b, const double* p, const double* dir, double scale) {
+    const double* rc = &d.subtree_com[3 * m.body_rootid[b]];
+    const double off[3] = {p[0] - rc[0], p[1] - rc[1], p[2] - rc[2]};
+    for (int i = 0; i < nv; i++) {
+      const int db = m.dof_bodyid[i];
+      if (!(db <= b && b < db + m.body_subtreesize[db])) continue;
+      const double* c = &d.cdof[6 * i];
+      const double jp[3] = {c[3] + (c[1] * off[2] - c[2] * off[1]), c[4] + (c[2] * off[0] - c[0] * off[2]), c[5] + (c[0] * off[1] - c[1] * off[0])};
+      jt[i] += scale * (dir[0] * jp[0] + dir[1] * jp[1] + dir[2] * jp[2]);
+    }
+  };
+  // straight piece from p0 on body b0 to p1 on body b1
+  auto add_piece = [&](std::vector<double>& jt, double& len, const double* p0, int b0, const double* p1, int b1, double scale) {
+    double e[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const double l = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+    len += scale * l;
+    if (l < 1e-12) return;
+    for (int k = 0; k < 3; k++) e[k] /= l;
+    add_point(jt, b1, p1, e, scale);
+    add_point(jt, b0, p0, e, -scale);
+  };
   for (int t = 0; t < m.ntendon; t++) {
     std::vector<double> jt(nv, 0.0);
     double len = 0;
-    for (int w = m.tendon_adr[t]; w < m.tendon_adr[t] + m.tendon_num[t]; w++) {
-      const int j = m.wrap_joint[w];
-      len += m.wrap_coef[w] * m.qpos0[m.jnt_qposadr[j]];
-      jt[m.jnt_dofadr[j]] += m.wrap_coef[w];
+    const int a0 = m.tendon_adr[t], a1 = a0 + m.tendon_num[t];
+    double scale = 1;
+    for (int w = a0; w < a1; w++) {
+      const int ty = m.wrap_type[w];
+      if (ty == 1) {
+        const int j = m.wrap_objid[w];
+        len += m.wrap_prm[w] * m.qpos0[m.jnt_qposadr[j]];
+        jt[m.jnt_dofadr[j]] += m.wrap_prm[w];
+      } else if (ty == 2) {
+        scale = 1.0 / m.wrap_prm[w];
+      } else if (ty == 3 && w + 1 < a1 && m.wrap_type[w + 1] == 3) {
+        double p0[3], p1[3];
+        site_world(m.wrap_objid[w], p0);
+        site_world(m.wrap_objid[w + 1], p1);
+        add_piece(jt, len, p0, m.site_bodyid[m.wrap_objid[w]], p1, m.site_bodyid[m.wrap_objid[w + 1]], scale);
+      } else if (ty == 3 && w + 2 < a1 && (m.wrap_type[w + 1] == 4 || m.wrap_type[w + 1] == 5)) {
+        const int s0 = m.wrap_objid[w], g = m.wrap_objid[w + 1], s1 = m.wrap_objid[w + 2], ss = (int)m.wrap_prm[w + 1];
+        double p0[3], p1[3], gc[3], gq[4], gR[9], sp[3], t0[3], t1[3], r[3];
+        site_world(s0, p0);
+        site_world(s1, p1);
+        const int gb = m.geom_bodyid[g];
+        quat_rot(&d.xquat[4 * gb], &m.geom_pos[3 * g], r);
+        for (int k = 0; k < 3; k++) gc[k] = d.xpos[3 * gb + k] + r[k];
+        quat_mul(&d.xquat[4 * gb], &m.geom_quat[4 * g], gq);
+        quat2mat(gq, gR);
+        if (ss >= 0) site_world(ss, sp);
+        bool wrapped = false;
+        mjbwrap::geom<double>(m.wrap_type[w + 1] == 4 ? 2 : 5, gc, gR, m.geom_size[3 * g], p0, p1, ss >= 0 ? sp : nullptr, t0, t1, wrapped);
+        if (!wrapped) {
+          add_piece(jt, len, p0, m.site_bodyid[s0], p1, m.site_bodyid[s1], scale);
+        } else {
+          const double l_before = len;
+          add_piece(jt, len, p0, m.site_bodyid[s0], t0, gb, scale);
+          add_piece(jt, len, t1, gb, p1, m.site_bodyid[s1], scale);
+          // the arc (helix) between the tangent points moves rigidly with the geom
+          const double full = mjbwrap::geom<double>(m.wrap_type[w + 1] == 4 ? 2 : 5, gc, gR, m.geom_size[3 * g], p0, p1, ss >= 0 ? sp : nullptr, t0, t1,
+                                                    wrapped);
+          len = l_before + scale * full;
+        }
+        w += 1;   // the geom; the next site starts the next piece
+      }
     }
     std::vector<double> x = jt;
     chol_solve(L, nv, x.data());
@@ -1627,8 +1732,8 @@ std::string dump_model(const Model& m) {
   dd("actuator_gear", m.actuator_gear); dd("actuator_gainprm", m.actuator_gainprm); dd("actuator_biasprm", m.actuator_biasprm);
   dd("actuator_ctrlrange", m.actuator_ctrlrange); dd("actuator_forcerange", m.actuator_forcerange);
   di("exclude_body1", m.exclude_body1); di("exclude_body2", m.exclude_body2);
-  di("tendon_adr", m.tendon_adr); di("tendon_num", m.tendon_num); di("tendon_limited", m.tendon_limited); di("wrap_joint", m.wrap_joint);
-  dd("wrap_coef", m.wrap_coef); dd("tendon_range", m.tendon_range); dd("tendon_margin", m.tendon_margin);
+  di("wrap_type", m.wrap_type); di("tendon_adr", m.tendon_adr); di("tendon_num", m.tendon_num); di("tendon_limited", m.tendon_limited); di("wrap_objid", m.wrap_objid);
+  dd("wrap_prm", m.wrap_prm); dd("tendon_range", m.tendon_range); dd("tendon_margin", m.tendon_margin);
   dd("tendon_frictionloss", m.tendon_frictionloss); dd("tendon_stiffness", m.tendon_stiffness); dd("tendon_damping", m.tendon_damping);
   dd("tendon_lengthspring", m.tendon_lengthspring); dd("tendon_solref_lim", m.tendon_solref_lim); dd("tendon_solimp_lim", m.tendon_solimp_lim);
   dd("tendon_solref_fri", m.tendon_solref_fri); dd("tendon_solimp_fri", m.tendon_solimp_fri); dd("tendon_length0", m.tendon_length0);

@@ -113,11 +113,15 @@ struct Model {
   std::vector<int> sensor_type, sensor_objtype, sensor_objid, sensor_dim, sensor_adr, sensor_supported;
   std::vector<std::string> sensor_name;
 
-  // <tendon><fixed>: length = sum of coef * qpos over its joints (hinge /
-  // slide); spatial tendons are not in this build
+  // <tendon>: fixed tendons (length = sum of coef * qpos over hinge / slide
+  // joints) and spatial tendons (paths through sites, optionally wrapping
+  // around sphere / cylinder geoms, split by pulleys).  Per wrap element:
+  // wrap_type (MuJoCo mjtWrap: 1 joint, 2 pulley, 3 site, 4 sphere geom,
+  // 5 cylinder geom), wrap_objid (joint / site / geom id, -1 for a pulley),
+  // wrap_prm (joint coef, pulley divisor, geom side site id or -1)
   int ntendon = 0;
-  std::vector<int> tendon_adr, tendon_num, tendon_limited, wrap_joint;
-  std::vector<double> wrap_coef, tendon_range, tendon_margin, tendon_frictionloss, tendon_stiffness, tendon_damping, tendon_lengthspring,
+  std::vector<int> tendon_adr, tendon_num, tendon_limited, wrap_objid, wrap_type;
+  std::vector<double> wrap_prm, tendon_range, tendon_margin, tendon_frictionloss, tendon_stiffness, tendon_damping, tendon_lengthspring,
       tendon_solref_lim, tendon_solimp_lim, tendon_solref_fri, tendon_solimp_fri, tendon_length0, tendon_invweight0;
   std::vector<std::string> tendon_name;
 

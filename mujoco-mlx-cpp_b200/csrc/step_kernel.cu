@@ -171,13 +171,13 @@ __device__ __noinline__ void record_sensors(Env& E, const StepParams& P, bool wr
       case 16: y[0] = ws[m.w_qfa + a]; break;             // jointactuatorfrc
       case 11: case 12: {                                 // tendonpos / tendonvel
         float len, vel;
-        d_tendon_lv(m, it, ft, qpos, qvel, a, len, vel);
+        d_tendon_lv(m, ws, a, len, vel);
         y[0] = type == 11 ? len : vel;
         break;
       }
       case 13: case 14: {                                 // actuatorpos / actuatorvel
         float len, vel;
-        if (b < 0) d_tendon_lv(m, it, ft, qpos, qvel, a, len, vel);
+        if (b < 0) d_tendon_lv(m, ws, a, len, vel);
         else { len = qpos[a]; vel = qvel[b]; }
         y[0] = ldf(sf, 7) * (type == 13 ? len : vel);
         break;
@@ -451,6 +451,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       STAGE_SYNC();
       if (valid) {
         d_rne(E, bias);
+        if (E.md->ntendon) d_tendons(E);
         d_forces(E, P, bias);
         if (last && P.rec_xpos) record_dyn(E, P, badr, vadr);
         if (sensors) {

@@ -462,6 +462,47 @@ def sensor_state(model, num_envs: int, seed: int, qnoise: float = 0.3, vnoise: f
     return q, v
 
 
+def spatial_tendon_xml(iterations: int = 50) -> str:
+    """Two-link arm (shoulder and elbow hinges about y) on a fixed base with
+    spatial tendons: 'flexor' runs from the base over a wrapping sphere at the
+    shoulder, a site on the upper arm, around a wrapping cylinder at the elbow
+    (with a side site) to the forearm (limited, spring, damper, frictionloss);
+    'rope' hangs a slider from a world site through a pulley (divisor 2)
+    shared with the forearm tip; 'strap' is a straight site-to-site tendon.
+    A motor pulls on the flexor, a position actuator on the slider."""
+    return (
+        '<mujoco model="spatial_tendons"><compiler angle="radian"/>'
+        f'<option timestep="0.002" iterations="{iterations}" tolerance="1e-8" integrator="Euler"/>'
+        '<worldbody>'
+        '<site name="top" pos="0.35 0 0.9"/>'
+        '<body name="base" pos="0 0 0.6">'
+        '<geom type="box" size="0.05 0.05 0.05" contype="0" conaffinity="0" mass="2"/>'
+        '<site name="origin" pos="-0.02 0 0.18"/>'
+        '<geom name="shoulder_wrap" type="sphere" size="0.06" pos="0 0 0.08" contype="0" conaffinity="0" mass="0.01"/>'
+        '<body name="upper" pos="0 0 0.08"><joint name="shoulder" type="hinge" axis="0 1 0" damping="0.1"/>'
+        '<geom type="capsule" fromto="0 0 0 0.3 0 0" size="0.025" contype="0" conaffinity="0" mass="0.8"/>'
+        '<site name="mid" pos="0.15 0 0.05"/>'
+        '<geom name="elbow_wrap" type="cylinder" size="0.04 0.03" pos="0.3 0 0" quat="0.7071068 0.7071068 0 0" contype="0" conaffinity="0" mass="0.01"/>'
+        '<site name="elbow_side" pos="0.3 0 0.1"/>'
+        '<body name="fore" pos="0.3 0 0"><joint name="elbow" type="hinge" axis="0 1 0" damping="0.1"/>'
+        '<geom type="capsule" fromto="0 0 0 0.25 0 0" size="0.02" contype="0" conaffinity="0" mass="0.5"/>'
+        '<site name="insert" pos="0.12 0 0.02"/><site name="tip" pos="0.25 0 0"/></body></body></body>'
+        '<body name="slider" pos="0.6 0 0.5"><joint name="slide" type="slide" axis="0 0 1" damping="0.5"/>'
+        '<geom type="sphere" size="0.03" contype="0" conaffinity="0" mass="0.3"/><site name="hook" pos="0 0 0.03"/></body>'
+        '</worldbody>'
+        '<tendon>'
+        '<spatial name="flexor" limited="true" range="0.435 0.46" stiffness="30" damping="0.5" frictionloss="0.05">'
+        '<site site="origin"/><geom geom="shoulder_wrap"/><site site="mid"/><geom geom="elbow_wrap" sidesite="elbow_side"/><site site="insert"/>'
+        '</spatial>'
+        '<spatial name="rope" stiffness="100" springlength="0.55">'
+        '<site site="tip"/><site site="top"/><pulley divisor="2"/><site site="top"/><site site="hook"/></spatial>'
+        '<spatial name="strap" frictionloss="0.02" range="0.5 0.56"><site site="origin"/><site site="tip"/></spatial>'
+        '</tendon>'
+        '<actuator><motor name="pull" tendon="flexor" gear="5" ctrllimited="true" ctrlrange="-1 1"/>'
+        '<position name="lift" joint="slide" kp="20"/></actuator>'
+        '</mujoco>')
+
+
 def chain_state(n: int, cfg: str, num_envs: int, seed: int):
     """Random joint angles N(0, 0.5) (beyond the limits for some envs), the
     first joint swung by 1.2 rad for contact configurations, random joint

@@ -55,8 +55,8 @@ typedef struct OModel {
   /* fixed tendons: length = sum over wraps of coef * qpos (hinge / slide
      joints); actuator_trntype 0 = joint, 3 = tendon (actuator_trnid) */
   int ntendon;
-  const int *tendon_adr, *tendon_num, *tendon_limited, *wrap_joint, *actuator_trntype;
-  const double *wrap_coef, *tendon_range, *tendon_margin, *tendon_frictionloss, *tendon_stiffness, *tendon_damping, *tendon_lengthspring;
+  const int *tendon_adr, *tendon_num, *tendon_limited, *wrap_objid, *actuator_trntype;
+  const double *wrap_prm, *tendon_range, *tendon_margin, *tendon_frictionloss, *tendon_stiffness, *tendon_damping, *tendon_lengthspring;
   const double *tendon_solref_lim, *tendon_solimp_lim, *tendon_solref_fri, *tendon_solimp_fri, *tendon_length0, *tendon_invweight0;
   /* sites and sensors (sensor_type: MuJoCo mjtSensor code; objtype: mjtObj
      code 1 body, 2 xbody, 3 joint, 5 geom, 6 site, 18 tendon, 19 actuator) */
@@ -65,6 +65,10 @@ typedef struct OModel {
   const double *site_pos, *site_quat, *magnetic;
   /* gravity compensation per body (fraction of its weight) */
   const double* body_gravcomp;
+  /* tendon wrap element types (mjtWrap: 1 joint, 2 pulley, 3 site, 4 sphere,
+     5 cylinder); wrap_objid / wrap_prm: joint, site or geom id / joint
+     coef, pulley divisor or the geom's side site (-1 none) */
+  const int* wrap_type;
 } OModel;
 
 /* per-env randomisation (NULL pointers = identity) */

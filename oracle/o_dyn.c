@@ -6,6 +6,7 @@
  *   oracle_rne          <- forward.hpp:281-397   (Phases C, D: cvel, cdof_dot, RNE bias)
  *   oracle_smooth_forces<- forward.hpp:399-469   (Phase E: passive, actuation, qfrc_smooth)
  */
+#include <math.h>
 #include "mjoracle.h"
 #include "o_util.h"
 
@@ -270,16 +271,200 @@ void oracle_rne(const OModel* m, OData* d, const ORand* rnd) {
 
 /* Fixed tendon (reference: tendon.hpp emit_tendon_phase; MuJoCo
  * mj_tendon): length = sum coef * qpos, J = sum coef * e_dof. */
-void oracle_tendon(const OModel* m, const OData* d, int t, double* len, double* vel, double* J) {
-  double l = 0, v = 0;
-  if (J) memset(J, 0, m->nv * sizeof(double));
-  for (int w = m->tendon_adr[t]; w < m->tendon_adr[t] + m->tendon_num[t]; w++) {
-    int j = m->wrap_joint[w];
-    double c = m->wrap_coef[w];
-    l += c * d->qpos[m->jnt_qposadr[j]];
-    v += c * d->qvel[m->jnt_dofadr[j]];
-    if (J) J[m->jnt_dofadr[j]] += c;
+/* ---- spatial tendon wrapping (MuJoCo's sphere / cylinder wrapping; the
+ * geometry of tangent lines to a circle, restated for the oracle) */
+
+static int seg_cross(const double* p1, const double* p2, const double* p3, const double* p4) {
+  double det = (p4[1] - p3[1]) * (p2[0] - p1[0]) - (p4[0] - p3[0]) * (p2[1] - p1[1]);
+  if (fabs(det) < 1e-15) return 0;
+  double a = ((p4[0] - p3[0]) * (p1[1] - p3[1]) - (p4[1] - p3[1]) * (p1[0] - p3[0])) / det;
+  double b = ((p2[0] - p1[0]) * (p1[1] - p3[1]) - (p2[1] - p1[1]) * (p1[0] - p3[0])) / det;
+  return a >= 0 && a <= 1 && b >= 0 && b <= 1;
+}
+
+/* 2D wrap of the path p0 -> p1 around the circle |x| = r; returns the arc
+ * length and the tangent points, or -1 when the straight segment is the
+ * path (it stays outside the circle, on the side point's side if given) */
+static double wrap_circle(const double* p0, const double* p1, double r, const double* side, double* t0, double* t1) {
+  double l0 = p0[0] * p0[0] + p0[1] * p0[1], l1 = p1[0] * p1[0] + p1[1] * p1[1];
+  if (r <= 0 || l0 <= r * r || l1 <= r * r) return -1;
+  double e[2] = {p1[0] - p0[0], p1[1] - p0[1]}, ee = e[0] * e[0] + e[1] * e[1];
+  double a = ee > 0 ? -(p0[0] * e[0] + p0[1] * e[1]) / ee : 0;
+  a = a < 0 ? 0 : a > 1 ? 1 : a;
+  double q[2] = {p0[0] + a * e[0], p0[1] + a * e[1]};
+  if (q[0] * q[0] + q[1] * q[1] > r * r && (!side || side[0] * q[0] + side[1] * q[1] >= 0)) return -1;
+  double ta[2][2], tb[2][2], arc[2], best_g = 0;
+  int best = -1;
+  for (int k = 0; k < 2; k++) {
+    double sg = k == 0 ? 1 : -1;   /* counter-clockwise, clockwise */
+    const double* pp[2] = {p0, p1};
+    for (int e2 = 0; e2 < 2; e2++) {
+      const double* p = pp[e2];
+      double dd = sqrt(p[0] * p[0] + p[1] * p[1]), c = r / dd, s = sqrt(1 - c * c) * (e2 == 0 ? sg : -sg);
+      double u[2] = {p[0] / dd, p[1] / dd}, *t = e2 == 0 ? ta[k] : tb[k];
+      t[0] = r * (c * u[0] - s * u[1]);
+      t[1] = r * (c * u[1] + s * u[0]);
+    }
+    double ang = atan2(ta[k][0] * tb[k][1] - ta[k][1] * tb[k][0], ta[k][0] * tb[k][0] + ta[k][1] * tb[k][1]) * sg;
+    if (ang < 0) ang += 6.283185307179586;
+    arc[k] = r * ang;
+    double g;
+    if (side) {
+      double mid[2] = {ta[k][0] + tb[k][0], ta[k][1] + tb[k][1]}, lm = sqrt(mid[0] * mid[0] + mid[1] * mid[1]);
+      if (lm > 1e-12) { mid[0] /= lm; mid[1] /= lm; } else { mid[0] = 1; mid[1] = 0; }
+      g = mid[0] * side[0] + mid[1] * side[1];
+    } else {
+      double dx = ta[k][0] - tb[k][0], dy = ta[k][1] - tb[k][1];
+      g = -(dx * dx + dy * dy);
+    }
+    if (seg_cross(p0, ta[k], p1, tb[k])) g = -1e4;
+    if (best < 0 || g > best_g) { best = k; best_g = g; }
   }
+  if (seg_cross(p0, ta[best], p1, tb[best])) return -1;
+  t0[0] = ta[best][0]; t0[1] = ta[best][1];
+  t1[0] = tb[best][0]; t1[1] = tb[best][1];
+  return arc[best];
+}
+
+/* path s0 -> s1 around a sphere (type 2) or cylinder (type 5) at c with
+ * rotation R and radius r; returns its length; *wrapped and the tangent
+ * points t0, t1 when it leaves the straight line */
+static double wrap_geom(int type, const double* c, const double* R, double r, const double* s0, const double* s1, const double* side, double* t0,
+                        double* t1, int* wrapped) {
+  double d0[3], d1[3], e1[3], e2[3], ax[3] = {R[2], R[5], R[8]}, z0 = 0, z1 = 0;
+  for (int k = 0; k < 3; k++) { d0[k] = s0[k] - c[k]; d1[k] = s1[k] - c[k]; }
+  double sv[3] = {s1[0] - s0[0], s1[1] - s0[1], s1[2] - s0[2]}, straight = o_norm3(sv);
+  *wrapped = 0;
+  if (type == 5) {
+    for (int k = 0; k < 3; k++) { e1[k] = R[3 * k]; e2[k] = R[3 * k + 1]; }
+    z0 = o_dot3(d0, ax);
+    z1 = o_dot3(d1, ax);
+  } else {
+    double l0 = o_norm3(d0);
+    if (l0 < 1e-12) return straight;
+    for (int k = 0; k < 3; k++) e1[k] = d0[k] / l0;
+    double p = o_dot3(d1, e1), w[3];
+    for (int k = 0; k < 3; k++) w[k] = d1[k] - p * e1[k];
+    double lw = o_norm3(w);
+    if (lw < 1e-12 * (1 + o_norm3(d1))) {
+      if (side) {
+        double ds[3] = {side[0] - c[0], side[1] - c[1], side[2] - c[2]}, ps = o_dot3(ds, e1);
+        for (int k = 0; k < 3; k++) w[k] = ds[k] - ps * e1[k];
+        lw = o_norm3(w);
+      }
+      if (lw < 1e-12) {
+        double a[3] = {fabs(e1[0]) < 0.6 ? 1 : 0, fabs(e1[0]) < 0.6 ? 0 : 1, 0}, pa = o_dot3(a, e1);
+        for (int k = 0; k < 3; k++) w[k] = a[k] - pa * e1[k];
+        lw = o_norm3(w);
+      }
+    }
+    for (int k = 0; k < 3; k++) e2[k] = w[k] / lw;
+  }
+  double p0[2] = {o_dot3(d0, e1), o_dot3(d0, e2)}, p1[2] = {o_dot3(d1, e1), o_dot3(d1, e2)}, sd[2], a2[2], b2[2];
+  const double* sdp = NULL;
+  if (side) {
+    double ds[3] = {side[0] - c[0], side[1] - c[1], side[2] - c[2]};
+    sd[0] = o_dot3(ds, e1);
+    sd[1] = o_dot3(ds, e2);
+    sdp = sd;
+  }
+  double arc = wrap_circle(p0, p1, r, sdp, a2, b2);
+  if (arc < 0) return straight;
+  *wrapped = 1;
+  double la = hypot(a2[0] - p0[0], a2[1] - p0[1]), lb = hypot(p1[0] - b2[0], p1[1] - b2[1]), L2 = la + arc + lb, len = L2, za = 0, zb = 0;
+  if (type == 5) {
+    double dz = z1 - z0;
+    za = z0 + (L2 > 0 ? dz * la / L2 : 0);
+    zb = z0 + (L2 > 0 ? dz * (la + arc) / L2 : 0);
+    len = sqrt(L2 * L2 + dz * dz);
+  }
+  for (int k = 0; k < 3; k++) {
+    t0[k] = c[k] + a2[0] * e1[k] + a2[1] * e2[k] + (type == 5 ? za * ax[k] : 0);
+    t1[k] = c[k] + b2[0] * e1[k] + b2[1] * e2[k] + (type == 5 ? zb * ax[k] : 0);
+  }
+  return len;
+}
+
+static void site_world(const OModel* m, const OData* d, int s, double* p) {
+  int b = m->site_bodyid[s];
+  double r[3];
+  o_quat_rot(&d->xquat[4 * b], &m->site_pos[3 * s], r);
+  for (int k = 0; k < 3; k++) p[k] = d->xpos[3 * b + k] + r[k];
+}
+
+/* J += scale * dir' (point Jacobian of body b at world point p) */
+static void point_jac(const OModel* m, const OData* d, int b, const double* p, const double* dir, double scale, double* J) {
+  const double* rc = &d->subtree_com[3 * m->body_rootid[b]];
+  double off[3] = {p[0] - rc[0], p[1] - rc[1], p[2] - rc[2]};
+  for (int i = 0; i < m->nv; i++) {
+    int db = m->dof_bodyid[i];
+    if (!(db <= b && b < db + m->body_subtreesize[db])) continue;
+    const double* c = &d->cdof[6 * i];
+    double jp[3] = {c[3] + (c[1] * off[2] - c[2] * off[1]), c[4] + (c[2] * off[0] - c[0] * off[2]), c[5] + (c[0] * off[1] - c[1] * off[0])};
+    J[i] += scale * o_dot3(dir, jp);
+  }
+}
+
+static void piece(const OModel* m, const OData* d, const double* p0, int b0, const double* p1, int b1, double scale, double* len, double* J) {
+  double e[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]}, l = o_norm3(e);
+  *len += scale * l;
+  if (l < 1e-12) return;
+  for (int k = 0; k < 3; k++) e[k] /= l;
+  point_jac(m, d, b1, p1, e, scale, J);
+  point_jac(m, d, b0, p0, e, -scale, J);
+}
+
+/* Fixed tendons (reference: tendon.hpp emit_tendon_phase; MuJoCo
+ * mj_tendon): length = sum coef * qpos, J = sum coef * e_dof.  Spatial
+ * tendons: the path length through the sites (around wrapping geoms, scaled
+ * by 1 / divisor after each pulley), J = sum over straight pieces of the
+ * piece direction times the difference of the end points' Jacobians, the
+ * tangent points moving with the wrapping geom; velocity = J qvel.  The
+ * kinematic quantities are those of the last oracle_kinematics / oracle_com. */
+void oracle_tendon(const OModel* m, const OData* d, int t, double* len, double* vel, double* J) {
+  int nv = m->nv;
+  double Jl[nv > 0 ? nv : 1];
+  double* JJ = J ? J : Jl;
+  double l = 0, scale = 1;
+  memset(JJ, 0, nv * sizeof(double));
+  int a0 = m->tendon_adr[t], a1 = a0 + m->tendon_num[t];
+  for (int w = a0; w < a1; w++) {
+    int ty = m->wrap_type[w];
+    if (ty == 1) {
+      int j = m->wrap_objid[w];
+      double c = m->wrap_prm[w];
+      l += c * d->qpos[m->jnt_qposadr[j]];
+      JJ[m->jnt_dofadr[j]] += c;
+    } else if (ty == 2) {
+      scale = 1 / m->wrap_prm[w];
+    } else if (ty == 3 && w + 1 < a1 && m->wrap_type[w + 1] == 3) {
+      double p0[3], p1[3];
+      int s0 = m->wrap_objid[w], s1 = m->wrap_objid[w + 1];
+      site_world(m, d, s0, p0);
+      site_world(m, d, s1, p1);
+      piece(m, d, p0, m->site_bodyid[s0], p1, m->site_bodyid[s1], scale, &l, JJ);
+    } else if (ty == 3 && w + 2 < a1 && (m->wrap_type[w + 1] == 4 || m->wrap_type[w + 1] == 5)) {
+      int s0 = m->wrap_objid[w], g = m->wrap_objid[w + 1], s1 = m->wrap_objid[w + 2], ss = (int)m->wrap_prm[w + 1];
+      double p0[3], p1[3], sp[3], t0[3], t1[3];
+      site_world(m, d, s0, p0);
+      site_world(m, d, s1, p1);
+      if (ss >= 0) site_world(m, d, ss, sp);
+      int wrapped = 0, gb = m->geom_bodyid[g];
+      double full = wrap_geom(m->wrap_type[w + 1] == 4 ? 2 : 5, &d->geom_xpos[3 * g], &d->geom_xmat[9 * g], m->geom_size[3 * g], p0, p1,
+                              ss >= 0 ? sp : NULL, t0, t1, &wrapped);
+      if (!wrapped) {
+        piece(m, d, p0, m->site_bodyid[s0], p1, m->site_bodyid[s1], scale, &l, JJ);
+      } else {
+        double dummy = 0;
+        piece(m, d, p0, m->site_bodyid[s0], t0, gb, scale, &dummy, JJ);
+        piece(m, d, t1, gb, p1, m->site_bodyid[s1], scale, &dummy, JJ);
+        l += scale * full;
+      }
+      w += 1;
+    }
+  }
+  double v = 0;
+  for (int i = 0; i < nv; i++) v += JJ[i] * d->qvel[i];
   *len = l;
   *vel = v;
 }

@@ -38,15 +38,15 @@ _EQ_PTR = [("eq_type", "i"), ("eq_obj1", "i"), ("eq_obj2", "i"), ("eq_active", "
            ("eq_data", "f"), ("eq_solref", "f"), ("eq_solimp", "f"), ("eq_invweight", "f")]
 
 
-_TEN_PTR = [("tendon_adr", "i"), ("tendon_num", "i"), ("tendon_limited", "i"), ("wrap_joint", "i"), ("actuator_trntype", "i"),
-            ("wrap_coef", "f"), ("tendon_range", "f"), ("tendon_margin", "f"), ("tendon_frictionloss", "f"), ("tendon_stiffness", "f"),
+_TEN_PTR = [("tendon_adr", "i"), ("tendon_num", "i"), ("tendon_limited", "i"), ("wrap_objid", "i"), ("actuator_trntype", "i"),
+            ("wrap_prm", "f"), ("tendon_range", "f"), ("tendon_margin", "f"), ("tendon_frictionloss", "f"), ("tendon_stiffness", "f"),
             ("tendon_damping", "f"), ("tendon_lengthspring", "f"), ("tendon_solref_lim", "f"), ("tendon_solimp_lim", "f"),
             ("tendon_solref_fri", "f"), ("tendon_solimp_fri", "f"), ("tendon_length0", "f"), ("tendon_invweight0", "f")]
 
 
 _SENS_PTR = [("site_bodyid", "i"), ("sensor_type", "i"), ("sensor_objtype", "i"), ("sensor_objid", "i"), ("sensor_dim", "i"),
              ("sensor_adr", "i"), ("sensor_supported", "i"), ("site_pos", "f"), ("site_quat", "f"), ("magnetic", "f"),
-             ("body_gravcomp", "f")]
+             ("body_gravcomp", "f"), ("wrap_type", "i")]
 
 
 class OModel(C.Structure):
@@ -96,6 +96,7 @@ def _load():
     lib.oracle_step.argtypes = [C.POINTER(OModel), C.POINTER(OData), C.POINTER(ORand), C.c_int]
     lib.oracle_ray.restype = C.c_double
     lib.oracle_ray.argtypes = [C.POINTER(OModel), C.POINTER(OData), _dp, _dp, _ip, _ip]
+    lib.oracle_tendon.argtypes = [C.POINTER(OModel), C.POINTER(OData), C.c_int, _dp, _dp, _dp]
     lib.oracle_sensors.argtypes = [C.POINTER(OModel), C.POINTER(OData), _dp, _dp, _dp, _dp, _dp]
     lib.oracle_step_batch.argtypes = [C.POINTER(OModel), C.POINTER(C.POINTER(OData)), C.c_int, C.c_int, C.c_int, C.c_int]
     return lib
@@ -179,6 +180,16 @@ class OracleEnv:
 
     def kinematics(self):
         lib.oracle_kinematics(C.byref(self.om.c), C.byref(self.d))
+
+    def tendon(self, t: int):
+        """(length, velocity, J[nv]) of tendon t at the current qpos / qvel
+        (runs kinematics and the COM pass first)."""
+        lib.oracle_kinematics(C.byref(self.om.c), C.byref(self.d))
+        lib.oracle_com(C.byref(self.om.c), C.byref(self.d), None)
+        ln, vl = C.c_double(), C.c_double()
+        J = np.zeros(max(self.om.nv, 1))
+        lib.oracle_tendon(C.byref(self.om.c), C.byref(self.d), t, C.byref(ln), C.byref(vl), _ptr(J, "f"))
+        return ln.value, vl.value, J[: self.om.nv]
 
     def step_sensors(self, max_iter: int = 0, rand: ORand | None = None):
         """One step, then the sensordata of its start state; accelerometers

@@ -376,8 +376,8 @@ def test_tendon_compile_known_answers():
         J = _tjac(t)
         assert d["tendon_invweight0"][t] == pytest.approx(J @ np.linalg.solve(M, J), rel=1e-9)
     assert d["eq_invweight"][0] == pytest.approx(d["tendon_invweight0"][3] + d["tendon_invweight0"][4], rel=1e-12)
-    bad = mjb200.models.tendon_chain_xml(8).replace('<fixed name="t4">', '<spatial name="t5"><site site="x"/></spatial><fixed name="t4">')
-    with pytest.raises(Exception, match="spatial"):
+    bad = mjb200.models.tendon_chain_xml(8).replace('<fixed name="t4">', '<spatial name="t5"><pulley divisor="2"/></spatial><fixed name="t4">')
+    with pytest.raises(Exception, match="pulley must follow a site"):
         mjb200.load_model_from_string(bad)
 
 
@@ -719,3 +719,56 @@ def test_com_offset_and_drag_known_answers():
     env.step(0, rand)
     np.testing.assert_allclose(env.a["qacc"][:3], -0.8 * np.linalg.norm(v) * v / 3.0, rtol=1e-10)
     np.testing.assert_allclose(env.a["qacc"][3:], 0.0, atol=1e-12)
+
+
+def test_spatial_tendon_wrap_known_answers():
+    """Static sites around a world sphere / cylinder: the wrapped length is
+    2 sqrt(a^2 - r^2) + r (pi - 2 acos(r / a)) for points at +-a through the
+    centre; a cylinder adds the axial rise as a helix, sqrt(L^2 + dz^2); a
+    path that misses the geom is straight; a pulley divides the next branch."""
+    a, r, dz = 0.3, 0.1, 0.2
+    L2 = 2 * np.sqrt(a * a - r * r) + r * (np.pi - 2 * np.arccos(r / a))
+    xml = (f'<mujoco><worldbody><geom name="ball" type="sphere" size="{r}" contype="0" conaffinity="0"/>'
+           f'<geom name="can" type="cylinder" size="{r} 0.5" pos="0 2 0" contype="0" conaffinity="0"/>'
+           f'<site name="s0" pos="{-a} 0 0"/><site name="s1" pos="{a} 0 0"/><site name="s2" pos="{a} 0.5 0.4"/>'
+           f'<site name="c0" pos="{-a} 2 0"/><site name="c1" pos="{a} 2 {dz}"/><site name="up" pos="0 0 1"/>'
+           '<body><joint type="slide" axis="0 0 1"/><geom type="sphere" size="0.01" mass="1" contype="0" conaffinity="0"/></body></worldbody>'
+           '<tendon><spatial><site site="s0"/><geom geom="ball"/><site site="s1"/></spatial>'
+           '<spatial><site site="c0"/><geom geom="can"/><site site="c1"/></spatial>'
+           '<spatial><site site="s0"/><geom geom="ball" sidesite="up"/><site site="s2"/></spatial>'
+           '<spatial><site site="s0"/><site site="s1"/><pulley divisor="4"/><site site="s1"/><site site="s2"/></spatial>'
+           '</tendon></mujoco>')
+    om, env = env_from_xml(xml)
+    l0 = env.tendon(0)[0]
+    assert l0 == pytest.approx(L2, rel=1e-12)
+    assert env.tendon(1)[0] == pytest.approx(np.sqrt(L2 * L2 + dz * dz), rel=1e-12)
+    # s0 -> s2 with the side site above: the straight line misses the ball (it
+    # passes above the centre, on the side site's side) -> straight
+    s0, s2 = np.array([-a, 0, 0]), np.array([a, 0.5, 0.4])
+    t = (np.dot(-s0, s2 - s0) / np.dot(s2 - s0, s2 - s0))
+    assert np.linalg.norm(s0 + t * (s2 - s0)) > r
+    assert env.tendon(2)[0] == pytest.approx(np.linalg.norm(s2 - s0), rel=1e-12)
+    assert env.tendon(3)[0] == pytest.approx(2 * a + np.linalg.norm(s2 - np.array([a, 0, 0])) / 4, rel=1e-12)
+
+
+def test_spatial_tendon_jacobian_matches_finite_differences():
+    """On the wrapped arm, the oracle's tendon Jacobian equals the finite
+    difference of its length (tangent points moving with their geom: the
+    envelope of the shortest wrapped path)."""
+    m = mjb200.load_model_from_string(mjb200.models.spatial_tendon_xml())
+    om = oracle.OracleModel(m.dump())
+    env = oracle.OracleEnv(om)
+    g = np.random.default_rng(3)
+    for trial in range(6):
+        q = np.array([g.uniform(-0.8, 0.8), g.uniform(-1.5, 1.5), g.uniform(-0.1, 0.1)])
+        for t in range(3):
+            env.a["qpos"][:] = q
+            _, _, J = env.tendon(t)
+            fd = np.zeros(3)
+            for i in range(3):
+                for sg in (1, -1):
+                    qq = q.copy()
+                    qq[i] += sg * 1e-6
+                    env.a["qpos"][:] = qq
+                    fd[i] += sg * env.tendon(t)[0] / 2e-6
+            np.testing.assert_allclose(J, fd, atol=1e-7)

@@ -96,3 +96,42 @@ def test_tendon_overflow_rule_matches_oracle():
         assert g["stats"]["nefc"][e] == o[e]["nefc"] == 2
         errs.append(rel_err(g["vec"][e, 2, :8], o[e]["qacc"]))
     assert np.median(errs) <= 1e-4 and max(errs) <= 2e-3
+
+
+def test_spatial_tendon_parity_and_rollout():
+    """Spatial tendons (sphere and cylinder wrapping with a side site, a
+    pulley, straight site pieces) on the wrapped arm: per env the row types
+    in order, D and aref, qfrc_smooth and qacc against the oracle (same
+    bounds as above), then a rollout under random motor commands that stays
+    finite and unflagged."""
+    model = mjb200.load_model_from_string(mjb200.models.spatial_tendon_xml())
+    om = oracle.OracleModel(model.dump())
+    B = 48
+    g = np.random.default_rng(17)
+    q = np.stack([g.uniform(-0.9, 0.9, B), g.uniform(-1.6, 1.6, B), g.uniform(-0.15, 0.15, B)], axis=1).astype(np.float32)
+    v = g.normal(0, 1.0, size=(B, 3)).astype(np.float32)
+    ctrl = np.stack([g.uniform(-1, 1, B), g.uniform(-0.1, 0.1, B)], axis=1).astype(np.float32)
+    sim = mjb200.BatchedSim(model, B, ncon_max=4, nefc_max=32)
+    gs = gpu_step_from(sim, q, v, ctrl, 4, 32)
+    o = oracle_step_from(om, q.astype(np.float64), v.astype(np.float64), ctrl.astype(np.float64), ncon_max=4, nefc_max=32)
+    errs, nlim = [], 0
+    for e in range(B):
+        assert gs["stats"]["status"][e] == 0 and o[e]["status"] == 0
+        n = o[e]["nefc"]
+        assert gs["stats"]["nefc"][e] == n
+        ot = o[e]["efc"]["type"]
+        assert list(gs["efc"][e, :n, 0].astype(int)) == list(ot)
+        nlim += int((ot == 1).sum())
+        np.testing.assert_allclose(gs["efc"][e, :n, 2], o[e]["efc"]["D"], rtol=1e-4)
+        np.testing.assert_allclose(gs["efc"][e, :n, 3], o[e]["efc"]["aref"], rtol=1e-4, atol=1e-4 * np.abs(o[e]["efc"]["aref"]).max())
+        assert rel_err(gs["vec"][e, 1, :3], o[e]["qfrc_smooth"]) <= 1e-5
+        errs.append(rel_err(gs["vec"][e, 2, :3], o[e]["qacc"]))
+    assert nlim > 0
+    errs = np.array(errs)
+    assert np.median(errs) <= 1e-4 and errs.max() <= 2e-3, (np.median(errs), errs.max())
+    sim.set_state(q, v)
+    for c in range(20):
+        sim.step(np.stack([g.uniform(-1, 1, B), g.uniform(-0.1, 0.1, B)], axis=1).astype(np.float32), 25)
+    qp, qv = sim.state()
+    assert np.isfinite(qp).all() and np.isfinite(qv).all()
+    assert np.all(sim.stats()["status"] == 0)
