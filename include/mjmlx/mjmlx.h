@@ -120,6 +120,14 @@ MJMLX_API const float* mjmlx_batched_get_cfrc_ext(const MjmlxBatchedSim* sim, in
 MJMLX_API int mjmlx_batched_nsensordata(const MjmlxBatchedSim* sim);
 MJMLX_API const float* mjmlx_batched_get_sensordata(const MjmlxBatchedSim* sim, int* n_out);
 
+/* Jacobian d(qvel after one physics step) / d(ctrl) of every env at the
+ * current state and the controls of the last step, grad_out float[num_envs
+ * * nv * nu] (row-major per env), by central differences of perturbed
+ * steps from the saved state, which is restored afterwards (single-model
+ * sims; the statistics reflect the probe steps).  The reference declares
+ * this entry point with an empty body.  Replaces mjmlx.h:268-270. */
+MJMLX_API void mjmlx_batched_grad_step(MjmlxBatchedSim* sim, float* grad_out);
+
 /* Per-env state setters.  Replace mjmlx.h:224-225. */
 MJMLX_API void mjmlx_batched_set_env_qpos(MjmlxBatchedSim* sim, int env_idx, const float* qpos, int nq);
 MJMLX_API void mjmlx_batched_set_env_qvel(MjmlxBatchedSim* sim, int env_idx, const float* qvel, int nv);

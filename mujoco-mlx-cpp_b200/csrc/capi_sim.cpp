@@ -185,6 +185,11 @@ MJMLX_API int mjmlx_batched_set_free_drag(MjmlxBatchedSim* sim, const int* env_i
   return guard("mjmlx_batched_set_free_drag", [&]() { return sim->engine->set_free_drag(env_idx, n, drag_k); }, -1);
 }
 
+MJMLX_API void mjmlx_batched_grad_step(MjmlxBatchedSim* sim, float* grad_out) {
+  if (!sim || !sim->engine || !grad_out) return;
+  guard("mjmlx_batched_grad_step", [&]() { sim->engine->grad_step(grad_out); return 0; }, 0);
+}
+
 MJMLX_API int mjmlx_batched_num_free_joints(const MjmlxBatchedSim* sim) {
   if (!sim || !sim->engine->uniform()) return 0;
   const auto& m = sim->engine->model(0);

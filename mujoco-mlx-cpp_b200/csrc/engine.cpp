@@ -842,6 +842,55 @@ void Engine::step(const float* ctrl_host, int n) {
 
 void Engine::step_device(int n) { launch(n, cfg_.record != 0); }
 
+// d(qvel after one physics step) / d(ctrl) at the current state and the
+// controls of the last step, by central differences (step eps = 1e-3 x
+// max(1, |ctrl|)), one perturbed step per control and sign from the same
+// saved state (position, velocity, warm start); the state is restored
+// afterwards.  out[env][nv][nu], single-model batches.
+void Engine::grad_step(float* out) {
+  if (!uniform()) throw std::runtime_error("grad_step: needs a single-model batch");
+  const Model& m = *models_[0];
+  const int nv = m.nv, nu = m.nu;
+  if (nu == 0 || nv == 0) return;
+  sync();
+  DevBuf<float> sq, sv, sw;
+  sq.alloc(tot_q_);
+  sv.alloc(tot_v_);
+  sw.alloc(tot_v_);
+  auto copy = [&](float* dst, const float* src, size_t n) { check(cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream_), "grad copy"); };
+  copy(sq.p, qpos_.p, tot_q_);
+  copy(sv.p, qvel_.p, tot_v_);
+  copy(sw.p, warm_.p, tot_v_);
+  std::vector<float> c0(tot_u_), c(tot_u_), vp(tot_v_), vm(tot_v_);
+  check(cudaMemcpyAsync(c0.data(), ctrl_.p, sizeof(float) * tot_u_, cudaMemcpyDeviceToHost, stream_), "grad ctrl");
+  sync();
+  auto probe = [&](int j, float sgn, std::vector<float>& v) {
+    c = c0;
+    for (int e = 0; e < B_; e++) c[(size_t)e * nu + j] += sgn * 1e-3f * std::max(1.f, std::fabs(c0[(size_t)e * nu + j]));
+    check(cudaMemcpyAsync(ctrl_.p, c.data(), sizeof(float) * tot_u_, cudaMemcpyHostToDevice, stream_), "grad ctrl");
+    copy(qpos_.p, sq.p, tot_q_);
+    copy(qvel_.p, sv.p, tot_v_);
+    copy(warm_.p, sw.p, tot_v_);
+    launch(1, false);
+    check(cudaMemcpyAsync(v.data(), qvel_.p, sizeof(float) * tot_v_, cudaMemcpyDeviceToHost, stream_), "grad qvel");
+    sync();
+  };
+  for (int j = 0; j < nu; j++) {
+    probe(j, 1.f, vp);
+    probe(j, -1.f, vm);
+    for (int e = 0; e < B_; e++) {
+      const float h = 1e-3f * std::max(1.f, std::fabs(c0[(size_t)e * nu + j]));
+      for (int i = 0; i < nv; i++) out[((size_t)e * nv + i) * nu + j] = (vp[(size_t)e * nv + i] - vm[(size_t)e * nv + i]) / (2.f * h);
+    }
+  }
+  check(cudaMemcpyAsync(ctrl_.p, c0.data(), sizeof(float) * tot_u_, cudaMemcpyHostToDevice, stream_), "grad ctrl");
+  copy(qpos_.p, sq.p, tot_q_);
+  copy(qvel_.p, sv.p, tot_v_);
+  copy(warm_.p, sw.p, tot_v_);
+  feat_valid_ = false;
+  sync();
+}
+
 void Engine::get_qacc_warmstart(float* out) {
   check(cudaMemcpyAsync(out, warm_.p, sizeof(float) * tot_v_, cudaMemcpyDeviceToHost, stream_), "get warm start");
   sync();

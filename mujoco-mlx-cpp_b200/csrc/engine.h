@@ -97,6 +97,8 @@ class Engine {
   int set_env_params(const int* env_idx, int n, const float* mass_scale, const float* com_delta, const float* friction_scale, const float* gain_scale);
   // per-env quadratic drag F = -k |v| v on each free joint (domain_rand sims)
   int set_free_drag(const int* env_idx, int n, const float* drag_k);
+  // d(qvel after one step) / d(ctrl) by central differences, out[env][nv][nu]
+  void grad_step(float* out);
   bool domain_rand() const { return rand_on_; }
 
   // learned warm start

@@ -58,6 +58,7 @@ def _load():
         "mjmlx_batched_set_env_qvel": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
         "mjmlx_batched_set_env_params": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p, _f32p, _f32p, _f32p]),
         "mjmlx_batched_set_free_drag": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p]),
+        "mjmlx_batched_grad_step": (None, [C.c_void_p, _f32p]),
         "mjmlx_batched_set_pack_spec": (C.c_int, [C.c_void_p, _i32p, C.c_int, C.c_int, C.c_int]),
         "mjmlx_batched_get_pack": (C.c_int, [C.c_void_p, _f32p]),
         "mjmlx_batched_raycast": (C.c_int, [C.c_void_p, _f32p, _f32p, C.c_int, C.c_int, C.POINTER(C.c_ubyte), C.c_int, _f32p, _i32p]),
@@ -477,6 +478,13 @@ class BatchedSim:
         conv = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1)
         ms, fs, gs, cd = conv(mass_scale), conv(friction_scale), conv(gain_scale), conv(com_delta)
         return lib.mjmlx_batched_set_env_params(self.handle, _ip(ei), n, _fp(ms), _fp(cd), _fp(fs), _fp(gs))
+
+    def grad_step(self):
+        """d(qvel after one step) / d(ctrl) per env, [num_envs, nv, nu]."""
+        m = self.models[0]
+        out = np.zeros((self.num_envs, m.nv, m.nu), np.float32)
+        lib.mjmlx_batched_grad_step(self.handle, _fp(out))
+        return out
 
     def set_free_drag(self, drag_k, env_idx=None):
         """Quadratic drag coefficients [n, nfree] of the free joints."""

@@ -165,3 +165,37 @@ def test_gravcomp_com_offset_drag_parity():
     plain = mjb200.BatchedSim(mjb200.load_model_from_string(mjb200.models.quadruped_xml()), B)
     gp = gpu_step_from(plain, qp, qv, ctrl, 64, 256)
     assert np.abs(gp["vec"][:, 2] - g["vec"][:, 2]).max() > 1e-2
+
+
+def test_batched_grad_step_matches_oracle_differences(quad_model):
+    """mjmlx_batched_grad_step: d(qvel after one step)/d(ctrl) by central
+    differences on the GPU against the same differences of the FP64 oracle
+    (FP32 steps resolve the 1e-3 control perturbation to about 1e-3 of the
+    Jacobian's scale); the state and controls are restored."""
+    om = oracle.OracleModel(quad_model.dump())
+    B = 8
+    (qp, qv, ctrl), = visited_states(om, nsteps=(40,), B=B)
+    sim = mjb200.BatchedSim(quad_model, B)
+    sim.set_state(qp, qv)
+    sim.step(ctrl, 1)
+    q1, v1 = sim.state()
+    G = sim.grad_step()
+    q2, v2 = sim.state()
+    assert np.array_equal(q1, q2) and np.array_equal(v1, v2)
+    nv, nu = om.nv, om.nu
+    for e in range(B):
+        ref = np.zeros((nv, nu))
+        for j in range(nu):
+            h = 1e-3 * max(1.0, abs(float(ctrl[e, j])))
+            vs = []
+            for sg in (1, -1):
+                env = oracle.OracleEnv(om)
+                env.a["qpos"][:] = q1[e]
+                env.a["qvel"][:] = v1[e]
+                c = ctrl[e].astype(np.float64).copy()
+                c[j] += sg * np.float32(h)
+                env.a["ctrl"][:nu] = c.astype(np.float32)
+                env.step()
+                vs.append(env.a["qvel"].copy())
+            ref[:, j] = (vs[0] - vs[1]) / (2 * h)
+        assert np.abs(G[e] - ref).max() <= 2e-2 * np.abs(ref).max(), (e, np.abs(G[e] - ref).max(), np.abs(ref).max())
