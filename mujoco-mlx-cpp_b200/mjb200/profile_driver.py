@@ -71,7 +71,7 @@ def _sensitivity(mjb200, m, B):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["step", "learned", "gemm", "sensitivity"])
+    ap.add_argument("what", choices=["step", "learned", "gemm", "sensitivity", "bin", "convex"])
     ap.add_argument("--envs", type=int, default=4096)
     ap.add_argument("--ctrl", type=int, default=3, help="control steps (4 substeps each)")
     ap.add_argument("--rows", type=int, default=16384)
@@ -95,6 +95,24 @@ def main(argv=None):
                     raise RuntimeError(mjb200.capi.last_error())
             torch.cuda.synchronize()
         print("gemm done")
+        return
+
+    if a.what in ("bin", "convex"):
+        # large-model path (HBM workspaces, row-sparse H, zero-skipping
+        # Cholesky) on the 64-body bin, or the GJK / EPA kernel instance on
+        # the 6-body convex pile; a.ctrl substeps after 20 settling substeps
+        xml = mjb200.models.bin_xml(64, 1.0, seed=1) if a.what == "bin" else mjb200.models.convex_pile_xml(6, seed=1)
+        m = mjb200.load_model_from_string(xml)
+        kw = dict(ncon_max=400, nefc_max=1600) if a.what == "bin" else dict(ncon_max=40, nefc_max=200)
+        sim = mjb200.BatchedSim(m, a.envs, record=0, **kw)
+        q, v = mjb200.models.box_pile_state(m, a.envs, seed=5)
+        sim.set_state(q.astype(np.float32), v.astype(np.float32))
+        sim.step(None, 20)
+        for c in range(a.ctrl):
+            sim.step(None, 1)
+        sim.sync()
+        st = sim.stats()
+        print(a.what, "done: shape", sim.launch_shape(), "ncon mean", st["ncon"].mean(), "nefc mean", st["nefc"].mean(), "status", np.unique(st["status"]))
         return
 
     m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
