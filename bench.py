@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--envs", type=int, default=16384)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
-    ap.add_argument("--train-ctrl-steps", type=int, default=32, help="control steps of the warm-start training rollouts")
-    ap.add_argument("--train-epochs", type=int, default=8)
+    ap.add_argument("--train-ctrl-steps", type=int, default=64, help="control steps of the warm-start training rollouts")
+    ap.add_argument("--train-epochs", type=int, default=16)
     return ap.parse_args()
 
 

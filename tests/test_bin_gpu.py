@@ -79,3 +79,28 @@ def test_bin_workload_2048_envs_sampled_parity():
     print("sampled", len(idx), "boundary flips", flips, "ncon mean", g["stats"]["ncon"][idx].mean(), "median %.2e max %.2e" % (np.median(errs), errs.max()))
     assert len(errs) >= 60
     assert np.median(errs) <= 1e-4 and errs.max() <= 5e-3, (np.median(errs), errs.max())
+
+
+def test_mixed_batch_with_large_model_matches_small_model_sim(quad_model):
+    """A batch mixing the quadruped with a 16-body bin runs every env with
+    HBM workspaces (the bin's does not fit shared memory); the quadruped envs
+    step bit-identically to a quadruped-only sim in shared memory."""
+    big = mjb200.load_model_from_string(mjb200.models.bin_xml(16, 0.5, seed=1))
+    Bq, Bb = 24, 8
+    mixed = mjb200.BatchedSim([quad_model, big], [Bq, Bb], ncon_max=128, nefc_max=512)
+    assert mixed.launch_shape()["smem_bytes"] < 64 * 1024
+    small = mjb200.BatchedSim(quad_model, Bq, ncon_max=128, nefc_max=512)
+    assert small.launch_shape()["smem_bytes"] > 64 * 1024
+    q, v = mjb200.models.quadruped_initial_state_fast(Bq, seed=3)
+    qb, vb = mjb200.models.box_pile_state(big, Bb, seed=4)
+    small.set_state(q.astype(np.float32), v.astype(np.float32))
+    mixed.set_state(np.concatenate([q.reshape(-1), qb.reshape(-1)]).astype(np.float32), np.concatenate([v.reshape(-1), vb.reshape(-1)]).astype(np.float32))
+    for c in range(10):
+        cq = mjb200.models.quadruped_controls_fast(Bq, c, seed=5).astype(np.float32)
+        small.step(cq, 4)
+        mixed.step(np.concatenate([cq.reshape(-1), np.zeros(0, np.float32)]), 4)
+    qs, vs = small.state()
+    qm, vm = mixed.state()
+    nq, nv = quad_model.nq, quad_model.nv
+    assert np.array_equal(qm[: Bq * nq].reshape(Bq, nq), qs) and np.array_equal(vm[: Bq * nv].reshape(Bq, nv), vs)
+    assert np.isfinite(qm).all() and np.all(mixed.stats()["status"] == 0)
