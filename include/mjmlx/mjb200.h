@@ -43,6 +43,8 @@ typedef struct MjbEngineConfig {
     double tolerance;      /* > 0 overrides the model's solver tolerance */
     int max_iter;          /* > 0 overrides the Newton iteration cap */
     int lockstep;          /* 1: the warps of a CTA run each stage together */
+    int predict_every;     /* learned warm start: predict at every k-th substep of a step call (1 = every substep);
+                              the substeps between run in one launch with the previous-step warm start */
 } MjbEngineConfig;
 
 /* Defaults of MjbEngineConfig. */

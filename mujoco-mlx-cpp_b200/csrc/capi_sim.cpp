@@ -28,6 +28,7 @@ mjb::EngineConfig to_cfg(const MjbEngineConfig* e) {
   c.tolerance = e->tolerance;
   c.max_iter = e->max_iter;
   c.lockstep = e->lockstep;
+  c.predict_every = e->predict_every > 0 ? e->predict_every : 1;
   return c;
 }
 
@@ -44,6 +45,7 @@ MjbEngineConfig from_cfg(const mjb::EngineConfig& c) {
   e.tolerance = c.tolerance;
   e.max_iter = c.max_iter;
   e.lockstep = c.lockstep;
+  e.predict_every = c.predict_every;
   return e;
 }
 

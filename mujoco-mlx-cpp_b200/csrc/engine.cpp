@@ -762,11 +762,17 @@ void Engine::launch_learned(int n, bool record) {
   const bool first_valid = feat_valid_;
   const Model& m = *models_[0];
   const int F = feature_count(), qskip = feature_qskip();
+  // a prediction at substeps s % k == 0; each launch runs up to the next
+  // prediction (the prediction is a warm-start candidate of its first
+  // substep only; the kernel writes the features of every substep, so the
+  // next prediction sees the latest)
+  const int k = std::max(1, cfg_.predict_every);
   auto body = [&]() {
-    for (int s = 0; s < n; s++) {
+    for (int s = 0; s < n;) {
       const bool have = first_valid || s > 0;
+      const int len = std::min(k, n - s);
       if (have) net_->infer(feat_.p, feat_stride_, F, ctrl_.p, m.nu, warm_.p, pred_.p, B_, stream_);
-      StepParams P = params(1, record && s == n - 1);
+      StepParams P = params(len, record && s + len == n);
       P.qacc_pred = have ? pred_.p : nullptr;
       P.features = feat_.p;
       P.feat_stride = feat_stride_;
@@ -774,6 +780,7 @@ void Engine::launch_learned(int n, bool record) {
       P.stats_accumulate = s > 0;
       if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
       check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+      s += len;
     }
   };
   feat_valid_ = true;

@@ -29,6 +29,7 @@ struct EngineConfig {
   double tolerance = -1;     // > 0 overrides the model tolerance
   int max_iter = 0;          // > 0 overrides the model / config iteration count
   int lockstep = 1;          // warps of a CTA run the stages together (instruction-cache locality)
+  int predict_every = 1;     // learned warm start: predict at substeps s % predict_every == 0 of a call
 };
 
 class CudaError : public std::runtime_error {

@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       if (valid) nefc = d_constraints(E, P, ncon);
       STAGE_SYNC();
       if (valid) {
-        const float* xpred = P.qacc_pred ? P.qacc_pred + vadr : nullptr;
+        const float* xpred = (P.qacc_pred && s == 0) ? P.qacc_pred + vadr : nullptr;   // a prediction serves the launch's first substep
         int it = d_newton(E, P, nefc, max_iter, xpred, choice);
         nsum += it;
         nmax = it > nmax ? it : nmax;

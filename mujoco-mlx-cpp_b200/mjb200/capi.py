@@ -29,7 +29,7 @@ class MjmlxBatchedConfig(C.Structure):
 class MjbEngineConfig(C.Structure):
     _fields_ = [("warps_per_block", C.c_int), ("persistent", C.c_int), ("blocks_per_sm", C.c_int), ("ncon_max", C.c_int),
                 ("nefc_max", C.c_int), ("use_graph", C.c_int), ("record", C.c_int), ("warmstart", C.c_int),
-                ("tolerance", C.c_double), ("max_iter", C.c_int), ("lockstep", C.c_int)]
+                ("tolerance", C.c_double), ("max_iter", C.c_int), ("lockstep", C.c_int), ("predict_every", C.c_int)]
 
 
 def _load():
