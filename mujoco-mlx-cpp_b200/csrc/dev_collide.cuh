@@ -505,6 +505,12 @@ __device__ int cvx_closest(CSV* S, int n, float* lam, float* v) {
   }
   if (n == 3) return cvx_triangle(S, lam, v);
   const int F[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 3, 1}, {1, 2, 3, 0}};
+  // a flat tetrahedron (volume below 1e-6 of its edge product) cannot be
+  // trusted to contain the origin: every face is then a candidate
+  float t1[3], t2[3], t3[3], c23[3];
+  for (int k = 0; k < 3; k++) { t1[k] = S[1].w[k] - S[0].w[k]; t2[k] = S[2].w[k] - S[0].w[k]; t3[k] = S[3].w[k] - S[0].w[k]; }
+  cross3(t2, t3, c23);
+  const bool flat = fabsf(dot3(t1, c23)) <= 1e-6f * norm3(t1) * norm3(t2) * norm3(t3);
   int best = -1, bn = 0;
   float bd = 3.0e38f, bl[3], bv[3];
   CSV bs[3];
@@ -514,7 +520,7 @@ __device__ int cvx_closest(CSV* S, int n, float* lam, float* v) {
     for (int k = 0; k < 3; k++) { e1[k] = P1[k] - P0[k]; e2[k] = P2[k] - P0[k]; }
     cross3(e1, e2, nrm);
     const float so = -dot3(nrm, P0), sq = dot3(nrm, Q) - dot3(nrm, P0);
-    if (so * sq >= 0.f) continue;
+    if (!flat && so * sq >= 0.f) continue;
     CSV T[3] = {S[F[f][0]], S[F[f][1]], S[F[f][2]]};
     float l[3], vv[3];
     const int k = cvx_triangle(T, l, vv);
@@ -879,6 +885,15 @@ __device__ __noinline__ int c_convex(const CShape& A, const CShape& B, float mar
     CSV w;
     cvx_support(A, B, nd, w);
     if (vv - dot3(v, w.w) <= CVX_TOL * sqrtf(vv)) break;
+    // a support point already in the simplex: v is as close as the simplex
+    // gets in this precision (on polytopes FP32 round-off in v can exceed
+    // the tolerance and return a vertex again); stop as separated
+    bool dup = false;
+    for (int i = 0; i < n; i++) {
+      const float e[3] = {w.w[0] - S[i].w[0], w.w[1] - S[i].w[1], w.w[2] - S[i].w[2]};
+      dup = dup || dot3(e, e) <= 1e-16f;
+    }
+    if (dup) break;
     S[n++] = w;
     n = cvx_closest(S, n, lam, v);
     if (n == 4) { overlap = true; break; }

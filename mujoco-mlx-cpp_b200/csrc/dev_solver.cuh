@@ -210,8 +210,33 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
 // built in shared memory from the lower-triangle entry table (entries spread
 // over the lanes), then factored by the right-looking shared-memory Cholesky
 // into the row-major lower triangle of L with idiag = 1 / L_jj.
+// Middle-zone elliptic cones add A A' - W W' per cone (A = sum_a HA_a J_a,
+// W = sum_a HU_a J_a over the cone's rows); their tangent rows' own terms
+// come in through the active list with weight HD.  cones[-k] (k < ncone)
+// holds normal row | dim << 16; hau = the HA field (HU follows at + ne).
+__device__ __forceinline__ float cone_entry(const float* J, const float* hau, int ne, const int* cones, int ncone, int n, int i, int j) {
+  float s = 0.f;
+#pragma unroll 1
+  for (int k = 0; k < ncone; k++) {
+    const int code = cones[-k], r = code & 0xffff, dim = code >> 16;
+    float Ai = 0.f, Aj = 0.f, Ui = 0.f, Uj = 0.f;
+#pragma unroll 1
+    for (int a = 0; a < dim; a++) {
+      const float* Jr = J + (r + a) * n;
+      const float ha = hau[r + a], hu = hau[ne + r + a], ji = Jr[i], jj = Jr[j];
+      Ai += ha * ji;
+      Aj += ha * jj;
+      Ui += hu * ji;
+      Uj += hu * jj;
+    }
+    s += Ai * Aj - Ui * Uj;
+  }
+  return s;
+}
+
 __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
-                                           int n, int lane, const int* it, int i_tri, float* L, float* idiag) {
+                                           int n, int lane, const int* it, int i_tri, float* L, float* idiag,
+                                           const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0) {
   const int ntri = n * (n + 1) / 2;
 #pragma unroll 1
   for (int t = lane; t < ntri; t += 32) {
@@ -233,6 +258,7 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
       int r0 = act[a];
       s0 += eD[r0] * J[r0 * n + i] * J[r0 * n + j];
     }
+    if (ncone) s1 += cone_entry(J, hau, ne, cones, ncone, n, i, j);
     L[i * n + j] = (s0 + s1) + (s2 + s3);
   }
   __syncwarp();
@@ -245,7 +271,8 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
 // row over each row's nonzero columns (found with a ballot scan) instead of
 // entry by entry over every active row.
 __device__ __noinline__ void d_factor_sparse(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
-                                             int n, int lane, int* nz, float* L, float* idiag) {
+                                             int n, int lane, int* nz, float* L, float* idiag,
+                                             const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0) {
 #pragma unroll 1
   for (int i = 0; i < n; i++) {
 #pragma unroll 1
@@ -279,17 +306,50 @@ __device__ __noinline__ void d_factor_sparse(const float* M, const float* J, con
     }
     __syncwarp();
   }
+  // middle-zone cones: A A' - W W' over the union of the cone rows' columns
+#pragma unroll 1
+  for (int k = 0; k < ncone; k++) {
+    const int code = cones[-k], r = code & 0xffff, dim = code >> 16;
+    int cnt = 0;
+#pragma unroll 1
+    for (int base = 0; base < n; base += 32) {
+      const int c = base + lane;
+      bool on = false;
+      if (c < n)
+        for (int a = 0; a < dim; a++) on = on || J[(r + a) * n + c] != 0.f;
+      const unsigned bal = __ballot_sync(FULL_MASK, on);
+      if (on) nz[cnt + __popc(bal & ((1u << lane) - 1u))] = c;
+      cnt += __popc(bal);
+    }
+    __syncwarp();
+    const int one[1] = {code};
+    const int T = cnt * (cnt + 1) / 2;
+#pragma unroll 1
+    for (int t = lane; t < T; t += 32) {
+      int p = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+      if ((p + 1) * (p + 2) / 2 <= t) p++;
+      else if (p * (p + 1) / 2 > t) p--;
+      const int q = t - p * (p + 1) / 2;
+      const int i = nz[p], j = nz[q];
+      L[i * n + j] += cone_entry(J, hau, ne, one, 1, n, i, j);
+    }
+    __syncwarp();
+  }
   d_chol(L, n, lane, idiag, nz);
 }
 
-__device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const float* ddiag, float dscale, float* L, float* idiag) {
+// ell: rows weigh with HD instead of D, plus the middle-zone cones
+__device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const float* ddiag, float dscale, float* L, float* idiag,
+                                         bool ell = false, const int* cones = nullptr, int ncone = 0) {
   const DevModelDesc& m = *E.md;
-  const int nv = m.nv;
+  const int nv = m.nv, ne = m.nefc_max;
   const float* M = E.ws + m.w_M;
   const float* J = E.ws + m.w_J;
-  const float* eD = E.ws + m.w_efc + EFC_D * m.nefc_max;
-  if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag);
-  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag);
+  const float* efc = E.ws + m.w_efc;
+  const float* eD = efc + (ell ? EFC_HD : EFC_D) * ne;
+  const float* hau = efc + EFC_HA * ne;
+  if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag, cones, ncone, hau, ne);
+  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne);
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
@@ -310,8 +370,14 @@ __device__ __forceinline__ int rows_of(float dim) { int d = (int)dim; return d =
 // Builds efc rows; returns nefc.  Row metadata: EFC_AREF (b during the
 // build), EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y (k*imp*pos during the build),
 // EFC_CON (contact index or -1).
+// EXT: the extended kernel instance, which also builds elliptic contacts
+// (reference model: MuJoCo's elliptic cone; normal row R_n = (1 - imp) / imp
+// * invweight, friction rows R_j = R_n (mu_0 / mu_j)^2 / impratio, friction
+// rows' aref without the position term).
+template <bool EXT>
 __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon) {
   const DevModelDesc& m = *E.md;
+  const bool ell = EXT && m.cone == 1;
   const int* it = E.it;
   const float* ft = E.ft;
   float* ws = E.ws;
@@ -524,7 +590,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       int c = base + E.lane;
       int nr = 0;
       float* cr = con + MJB_CONTACT_FLOATS * (c < ncon ? c : 0);
-      if (c < ncon) nr = (cr[12] < cr[15]) ? rows_of(cr[14]) : 0;
+      if (c < ncon) nr = (cr[12] < cr[15]) ? (ell && cr[14] > 1.f ? (int)cr[14] : rows_of(cr[14])) : 0;
       int incl = warp_incl_scan(nr, E.lane);
       int total = __shfl_sync(FULL_MASK, incl, 31);
       int r0 = nefc + incl - nr;
@@ -547,6 +613,29 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
         float invw = ldf(pf, 14);
         int dim = (int)cr[14];
         float D;
+        if (ell && dim > 1) {
+          const float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
+          const float mu0 = ldf(pf, 2) * fs;
+          const float Rn = fmaxf((1.f - imp) / imp * invw, 1e-15f);
+          #pragma unroll 1
+          for (int q = 0; q < nr; q++) {
+            EfcRef e{efc + r0 + q, ne};
+            e[EFC_AREF] = b;
+            e[EFC_CON] = (float)c;
+            if (q == 0) {
+              e[EFC_D] = 1.f / Rn;
+              e[EFC_Y] = k * imp * pos;
+              e[EFC_FLOSS] = mu0 / sqrtf(m.impratio);
+              e[EFC_TYPE] = ROW_ELLIPTIC;
+            } else {
+              const float mu = ldf(pf, 1 + q) * fs;
+              e[EFC_D] = 1.f / fmaxf(Rn * (mu0 * mu0) / (mu * mu) / m.impratio, 1e-15f);
+              e[EFC_Y] = 0.f;
+              e[EFC_FLOSS] = mu;
+              e[EFC_TYPE] = ROW_ELLFRIC;
+            }
+          }
+        } else {
         if (dim == 1) {
           D = 1.f / fmaxf((1.f - imp) / imp * invw, 1e-15f);
         } else {
@@ -564,6 +653,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
           e[EFC_FLOSS] = 0;
           e[EFC_TYPE] = dim == 1 ? ROW_FRICTIONLESS : ROW_PYRAMID;
           e[EFC_CON] = (float)c;
+        }
         }
       }
       nefc += total;
@@ -604,6 +694,17 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
         if (dim == 1) {
           J[r * nv + i] = jn;
           r++;
+          continue;
+        }
+        if (ell) {
+          J[r * nv + i] = jn;
+          #pragma unroll 1
+          for (int dir = 0; dir < dim - 1; dir++) {
+            const float* ax = (dir == 0 || dir == 3) ? fr + 3 : (dir == 1 || dir == 4) ? fr + 6 : fr;
+            const float* src = dir < 2 ? jp : jr;
+            J[(r + 1 + dir) * nv + i] = ax[0] * src[0] + ax[1] * src[1] + ax[2] * src[2];
+          }
+          r += dim;
           continue;
         }
         float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
@@ -661,8 +762,104 @@ __device__ __forceinline__ float row_cost_delta(int type, float D, float fl, flo
   return row_cost(type, D, fl, y + dy) - row_cost(type, D, fl, y);
 }
 
+// Elliptic contact group (MuJoCo's cone model; solver.hpp has pyramids
+// only): jar y over the normal row and dim - 1 friction rows, fl[0] = mu,
+// fl[j] = mu_j, U = (mu y_0, mu_j y_j), N = U_0, T = |U_t|.  Zones: top
+// (N >= mu T) no force; bottom (mu N + T <= 0) every row quadratic with its
+// own D; middle: cost 0.5 Dm (N - mu T)^2, Dm = D_0 / (mu^2 (1 + mu^2)).
+// Returns the cost.  f (may be null): forces -ds/dy.  q (may be null):
+// qhq = q' H q.  hd/ha/hu (may be null): the Hessian as row data, H = sum_j
+// hd_j e_j e_j' + ha ha' - hu hu' (middle zone: hd_j = c mu_j^2 on the
+// friction rows, ha = sqrt(Dm) grad(N - mu T), hu_j = sqrt(c) mu_j U_j / T,
+// c = -Dm (N - mu T) mu / T > 0).  Arrays are indexed below 6 only.
+__device__ __forceinline__ float cone_eval(int dim, const float* D, const float* fl, const float* y, const float* q, float* f, float& qhq,
+                                           float* hd, float* ha, float* hu) {
+  const float mu = fl[0];
+  float U[6], T2 = 0.f;
+  U[0] = mu * y[0];
+#pragma unroll
+  for (int j = 1; j < 6; j++) {
+    U[j] = j < dim ? fl[j] * y[j] : 0.f;
+    T2 += U[j] * U[j];
+  }
+  const float T = sqrtf(T2), N = U[0];
+  float cost = 0.f;
+  qhq = 0.f;
+  if (N >= mu * T || (T <= 0.f && N >= 0.f)) {
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      if (j < dim) {
+        if (f) f[j] = 0.f;
+        if (hd) { hd[j] = 0.f; ha[j] = 0.f; hu[j] = 0.f; }
+      }
+    return 0.f;
+  }
+  if (mu * N + T <= 0.f || (T <= 0.f && N < 0.f)) {
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      if (j < dim) {
+        if (f) f[j] = -D[j] * y[j];
+        cost += 0.5f * D[j] * y[j] * y[j];
+        if (q) qhq += D[j] * q[j] * q[j];
+        if (hd) { hd[j] = D[j]; ha[j] = 0.f; hu[j] = 0.f; }
+      }
+    return cost;
+  }
+  const float Dm = D[0] / (mu * mu * (1.f + mu * mu)), NmT = N - mu * T, iT = 1.f / T;
+  const float c = -Dm * NmT * mu * iT;
+  cost = 0.5f * Dm * NmT * NmT;
+  if (f) {
+    f[0] = -Dm * NmT * mu;
+#pragma unroll
+    for (int j = 1; j < 6; j++)
+      if (j < dim) f[j] = Dm * NmT * mu * U[j] * iT * fl[j];
+  }
+  if (q) {
+    float aq = mu * q[0], wq = 0.f, sq = 0.f;
+#pragma unroll
+    for (int j = 1; j < 6; j++)
+      if (j < dim) {
+        const float w = fl[j] * U[j] * iT;
+        aq -= mu * w * q[j];
+        wq += w * q[j];
+        sq += fl[j] * fl[j] * q[j] * q[j];
+      }
+    qhq = Dm * aq * aq + c * (sq - wq * wq);
+  }
+  if (hd) {
+    const float sDm = sqrtf(Dm), sc = sqrtf(c);
+    hd[0] = 0.f;
+    ha[0] = sDm * mu;
+    hu[0] = 0.f;
+#pragma unroll
+    for (int j = 1; j < 6; j++)
+      if (j < dim) {
+        const float w = fl[j] * U[j] * iT;
+        hd[j] = c * fl[j] * fl[j];
+        ha[j] = -sDm * mu * w;
+        hu[j] = sc * w;
+      }
+  }
+  return cost;
+}
+
+// rows of the elliptic group whose normal row is r (its contact's condim)
+__device__ __forceinline__ int cone_dim(const Env& E, const float* efc, int ne, int r) {
+  return (int)E.ws[E.md->w_con + MJB_CONTACT_FLOATS * (int)efc[EFC_CON * ne + r] + 14];
+}
+
+__device__ __forceinline__ void cone_load(const float* efc, int ne, int r, int dim, float* D, float* fl) {
+#pragma unroll
+  for (int j = 0; j < 6; j++)
+    if (j < dim) {
+      D[j] = efc[EFC_D * ne + r + j];
+      fl[j] = efc[EFC_FLOSS * ne + r + j];
+    }
+}
+
 // Cost of candidate x (Gauss term 0.5 d'M d with d = x - qacc_smooth, plus
 // row costs).  `tmp` is nv floats of scratch.  Warp-uniform result.
+template <bool EXT>
 __device__ __noinline__ float d_cost(Env& E, int nefc, const float* x, float* tmp) {
   const DevModelDesc& m = *E.md;
   const int nv = m.nv, ne = m.nefc_max, lane = E.lane;
@@ -678,11 +875,128 @@ __device__ __noinline__ float d_cost(Env& E, int nefc, const float* x, float* tm
   for (int i = lane; i < nv; i += 32) c += 0.5f * tmp[i] * dot_c(M + i * nv, tmp, nv);
 #pragma unroll 1
   for (int r = lane; r < nefc; r += 32) {
+    const int ty = (int)efc[EFC_TYPE * ne + r];
+    if (EXT && ty == ROW_ELLFRIC) continue;
+    if (EXT && ty == ROW_ELLIPTIC) {
+      const int dim = cone_dim(E, efc, ne, r);
+      float D[6], fl[6], y[6], qhq;
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+        if (j < dim) y[j] = dot_c(J + (r + j) * nv, x, nv) - efc[EFC_AREF * ne + r + j];
+      cone_load(efc, ne, r, dim, D, fl);
+      c += cone_eval(dim, D, fl, y, nullptr, nullptr, qhq, nullptr, nullptr, nullptr);
+      continue;
+    }
     float y = dot_c(J + r * nv, x, nv) - efc[EFC_AREF * ne + r];
-    c += row_cost((int)efc[EFC_TYPE * ne + r], efc[EFC_D * ne + r], efc[EFC_FLOSS * ne + r], y);
+    c += row_cost(ty, efc[EFC_D * ne + r], efc[EFC_FLOSS * ne + r], y);
   }
   __syncwarp();
   return warp_sum(c);
+}
+
+// Forces (and the Hessian row data HD / HA / HU) from the jar in EFC_Y, for
+// models with elliptic cones: the lane of a cone's normal row evaluates the
+// whole group.
+__device__ __noinline__ void d_forces_ell(Env& E, int nefc) {
+  const DevModelDesc& m = *E.md;
+  const int ne = m.nefc_max;
+  float* efc = E.ws + m.w_efc;
+#pragma unroll 1
+  for (int r = E.lane; r < nefc; r += 32) {
+    const int ty = (int)efc[EFC_TYPE * ne + r];
+    if (ty == ROW_ELLFRIC) continue;
+    if (ty == ROW_ELLIPTIC) {
+      const int dim = cone_dim(E, efc, ne, r);
+      float D[6], fl[6], y[6], qhq;
+      cone_load(efc, ne, r, dim, D, fl);
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+        if (j < dim) y[j] = efc[EFC_Y * ne + r + j];
+      // a group's rows are consecutive within each field: write in place
+      cone_eval(dim, D, fl, y, nullptr, efc + EFC_FORCE * ne + r, qhq, efc + EFC_HD * ne + r, efc + EFC_HA * ne + r, efc + EFC_HU * ne + r);
+      continue;
+    }
+    const float D = efc[EFC_D * ne + r], fl = efc[EFC_FLOSS * ne + r], y = efc[EFC_Y * ne + r];
+    efc[EFC_FORCE * ne + r] = row_force(ty, D, fl, y);
+    efc[EFC_HD * ne + r] = row_quad(ty, D, fl, y) ? D : 0.f;
+  }
+  __syncwarp();
+}
+
+// Line-search sums at step a along q = EFC_Q for elliptic models (per lane):
+// g1 = -sum q' force(y + a q), g2 = sum q' H q; the cone groups are
+// evaluated by their normal row's lane.
+__device__ __noinline__ void ls_sums_ell(const Env& E, const float* efc, int ne, int nefc, float a, float& g1, float& g2) {
+#pragma unroll 1
+  for (int r = E.lane; r < nefc; r += 32) {
+    const int ty = (int)efc[EFC_TYPE * ne + r];
+    if (ty == ROW_ELLFRIC) continue;
+    if (ty == ROW_ELLIPTIC) {
+      const int dim = cone_dim(E, efc, ne, r);
+      float D[6], fl[6], y[6], q[6], f[6], qhq;
+      cone_load(efc, ne, r, dim, D, fl);
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+        if (j < dim) {
+          q[j] = efc[EFC_Q * ne + r + j];
+          y[j] = efc[EFC_Y * ne + r + j] + a * q[j];
+        }
+      cone_eval(dim, D, fl, y, q, f, qhq, nullptr, nullptr, nullptr);
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+        if (j < dim) g1 -= q[j] * f[j];
+      g2 += qhq;
+      continue;
+    }
+    const float q = efc[EFC_Q * ne + r], y = efc[EFC_Y * ne + r] + a * q, D = efc[EFC_D * ne + r], fl = efc[EFC_FLOSS * ne + r];
+    g1 -= q * row_force(ty, D, fl, y);
+    if (row_quad(ty, D, fl, y)) g2 += D * q * q;
+  }
+}
+
+// Middle-zone cones (normal row with HA != 0) written downwards from
+// cones[0] as normal row | dim << 16; returns their count.
+__device__ __noinline__ int d_cone_list(const Env& E, int nefc, int* cones) {
+  const DevModelDesc& m = *E.md;
+  const int ne = m.nefc_max, lane = E.lane;
+  const float* efc = E.ws + m.w_efc;
+  int ncone = 0;
+#pragma unroll 1
+  for (int base = 0; base < nefc; base += 32) {
+    const int r = base + lane;
+    const bool cq = r < nefc && (int)efc[EFC_TYPE * ne + r] == ROW_ELLIPTIC && efc[EFC_HA * ne + r] != 0.f;
+    const unsigned b = __ballot_sync(FULL_MASK, cq);
+    if (cq) cones[-(ncone + __popc(b & ((1u << lane) - 1u)))] = r | (cone_dim(E, efc, ne, r) << 16);
+    ncone += __popc(b);
+  }
+  __syncwarp();
+  return ncone;
+}
+
+// Cost change of the rows along the step a q for elliptic models (per lane).
+__device__ __noinline__ float cost_delta_ell(const Env& E, const float* efc, int ne, int nefc, float a) {
+  float dc = 0.f;
+#pragma unroll 1
+  for (int r = E.lane; r < nefc; r += 32) {
+    const int ty = (int)efc[EFC_TYPE * ne + r];
+    if (ty == ROW_ELLFRIC) continue;
+    if (ty == ROW_ELLIPTIC) {
+      const int dim = cone_dim(E, efc, ne, r);
+      float D[6], fl[6], y0[6], y1[6], qhq;
+      cone_load(efc, ne, r, dim, D, fl);
+#pragma unroll
+      for (int j = 0; j < 6; j++)
+        if (j < dim) {
+          y0[j] = efc[EFC_Y * ne + r + j];
+          y1[j] = y0[j] + a * efc[EFC_Q * ne + r + j];
+        }
+      dc += cone_eval(dim, D, fl, y1, nullptr, nullptr, qhq, nullptr, nullptr, nullptr) -
+            cone_eval(dim, D, fl, y0, nullptr, nullptr, qhq, nullptr, nullptr, nullptr);
+      continue;
+    }
+    dc += row_cost_delta(ty, efc[EFC_D * ne + r], efc[EFC_FLOSS * ne + r], efc[EFC_Y * ne + r], a * efc[EFC_Q * ne + r]);
+  }
+  return dc;
 }
 
 // g = Md - J'force; returns ||g||^2 and the magnitude of the summed terms
@@ -708,9 +1022,11 @@ __device__ __forceinline__ float grad_update(const float* J, const float* force,
 // gradient below tolerance * meaninertia * nv, where the gradient test also
 // accepts the FP32 round-off floor of the gradient (16 eps times the norm of
 // the terms it is summed from) -- below that floor FP32 cannot resolve it.
+template <bool EXT>
 __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int max_iter, const float* xpred, int& choice) {
   (void)P;
   const DevModelDesc& m = *E.md;
+  const bool ell = EXT && m.cone == 1;
   const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations;
   float* ws = E.ws;
   const float* M = ws + m.w_M;
@@ -730,17 +1046,18 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   const float* eA = efc + EFC_AREF * ne;
   const float* eL = efc + EFC_FLOSS * ne;
   const float* eT = efc + EFC_TYPE * ne;
+  const float* eHD = efc + EFC_HD * ne;   // elliptic models only
   const float scale = m.scale, tol = m.tolerance;
 
   // warm start: lowest cost of smooth / previous / predicted
   choice = 0;
   const float* src = qas;
   if (!(m.disableflags & (1 << 8)) && nefc > 0) {
-    float best = d_cost(E, nefc, qas, tmp);
-    float cw = d_cost(E, nefc, xw, tmp);
+    float best = d_cost<EXT>(E, nefc, qas, tmp);
+    float cw = d_cost<EXT>(E, nefc, xw, tmp);
     if (cw < best) { best = cw; choice = 1; }
     if (xpred) {
-      float cp = d_cost(E, nefc, xpred, tmp);
+      float cp = d_cost<EXT>(E, nefc, xpred, tmp);
       if (cp <= best) { best = cp; choice = 2; }
     }
     src = choice == 1 ? xw : choice == 2 ? xpred : qas;
@@ -758,9 +1075,10 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   for (int r = lane; r < nefc; r += 32) {
     float y = dot_c(J + r * nv, x, nv) - eA[r];
     eY[r] = y;
-    eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
+    if (!ell) eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
   }
   __syncwarp();
+  if (ell) d_forces_ell(E, nefc);
   float terms;
   float gn = grad_update(J, eF, Md, grad, nv, nefc, lane, terms);
   __syncwarp();
@@ -776,7 +1094,7 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
 #pragma unroll 1
     for (int base = 0; base < nefc; base += 32) {
       int r = base + lane;
-      bool q = r < nefc && row_quad((int)eT[r], eD[r], eL[r], eY[r]);
+      bool q = r < nefc && (ell ? eHD[r] > 0.f : row_quad((int)eT[r], eD[r], eL[r], eY[r]));
       unsigned b = __ballot_sync(FULL_MASK, q);
       int pos = nact + __popc(b & ((1u << lane) - 1u));
       if (q) {
@@ -789,8 +1107,15 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     }
     if (nact != nact_prev) changed = true;
     __syncwarp();
+    // middle-zone cones (their Hessian moves with y: refactor every
+    // iteration while any is present), listed downwards from the end of the
+    // active-row list: active rows + cones <= nefc, as a middle-zone cone's
+    // normal row is not active
+    int* cones = act_list + ne - 1;
+    const int ncone = ell ? d_cone_list(E, nefc, cones) : 0;
+    if (ncone) changed = true;
     if (changed) {
-      d_factor(E, act_list, nact, nullptr, 0.f, H, idiag);
+      d_factor(E, act_list, nact, nullptr, 0.f, H, idiag, ell, cones, ncone);
       nact_prev = nact;
     }
 #pragma unroll 1
@@ -818,12 +1143,15 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     float d0, h0;
     {
       float g1 = 0, g2 = 0;
+      if (ell) ls_sums_ell(E, efc, ne, nefc, 0.f, g1, g2);
+      else {
 #pragma unroll 1
       for (int r = lane; r < nefc; r += 32) {
         int ty = (int)eT[r];
         float q = eQ[r], y = eY[r], D = eD[r], fl = eL[r];
         g1 -= q * row_force(ty, D, fl, y);
         if (row_quad(ty, D, fl, y)) g2 += D * q * q;
+      }
       }
       d0 = B + warp_sum(g1);
       h0 = A + warp_sum(g2);
@@ -836,12 +1164,15 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
 #pragma unroll 1
       for (int it2 = 0; it2 < ls_iter; it2++) {
         float g1 = 0, g2 = 0;
+        if (ell) ls_sums_ell(E, efc, ne, nefc, a, g1, g2);
+        else {
 #pragma unroll 1
         for (int r = lane; r < nefc; r += 32) {
           int ty = (int)eT[r];
           float q = eQ[r], y = eY[r] + a * q, D = eD[r], fl = eL[r];
           g1 -= q * row_force(ty, D, fl, y);
           if (row_quad(ty, D, fl, y)) g2 += D * q * q;
+        }
         }
         float dd = a * A + B + warp_sum(g1);
         float hh = A + warp_sum(g2);
@@ -860,8 +1191,11 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     if (alpha == 0.f) break;
     // cost change along the step (accurate for small steps)
     float dc = 0;
+    if (ell) dc = cost_delta_ell(E, efc, ne, nefc, alpha);
+    else {
 #pragma unroll 1
     for (int r = lane; r < nefc; r += 32) dc += row_cost_delta((int)eT[r], eD[r], eL[r], eY[r], alpha * eQ[r]);
+    }
     dc = warp_sum(dc) + 0.5f * alpha * alpha * A + alpha * B;
     // update x, Md, y, force, grad
 #pragma unroll 1
@@ -873,9 +1207,10 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     for (int r = lane; r < nefc; r += 32) {
       float y = eY[r] + alpha * eQ[r];
       eY[r] = y;
-      eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
+      if (!ell) eF[r] = row_force((int)eT[r], eD[r], eL[r], y);
     }
     __syncwarp();
+    if (ell) d_forces_ell(E, nefc);
     gn = grad_update(J, eF, Md, grad, nv, nefc, lane, terms);
     __syncwarp();
     float improvement = -scale * dc;

@@ -82,10 +82,18 @@ enum { TEN_LO = 0, TEN_HI, TEN_MARGIN, TEN_FLOSS, TEN_STIFF, TEN_DAMP, TEN_SPRLO
 #define MJB_SENSOR_INTS 8
 #define MJB_SENSOR_FLOATS 8
 
-// efc row metadata stride (floats) in the workspace: aref D floss type y force q
+// efc row metadata stride (floats) in the workspace: aref D floss type y
+// force q con; models with elliptic cones carry three more fields per row
+// for the Newton Hessian: HD (the row's diagonal weight: D in its quadratic
+// zone, else 0; for a cone's friction rows in the middle zone the tangent
+// curvature), HA (the rank-1 cone term's coefficient) and HU (the
+// tangent-projection term's coefficient)
 #define MJB_EFC_FIELDS 8
-enum { EFC_AREF = 0, EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y, EFC_FORCE, EFC_Q, EFC_CON };
-enum { ROW_FRICTION = 0, ROW_LIMIT = 1, ROW_PYRAMID = 2, ROW_FRICTIONLESS = 3, ROW_EQUALITY = 5 };
+#define MJB_EFC_FIELDS_ELLIPTIC 11
+enum { EFC_AREF = 0, EFC_D, EFC_FLOSS, EFC_TYPE, EFC_Y, EFC_FORCE, EFC_Q, EFC_CON, EFC_HD, EFC_HA, EFC_HU };
+// ROW_ELLIPTIC: an elliptic contact's normal row (floss = mu_0 / sqrt(impratio));
+// ROW_ELLFRIC: its friction rows, which follow it (floss = that direction's mu)
+enum { ROW_FRICTION = 0, ROW_LIMIT = 1, ROW_PYRAMID = 2, ROW_FRICTIONLESS = 3, ROW_ELLIPTIC = 4, ROW_EQUALITY = 5, ROW_ELLFRIC = 6 };
 
 // status bits (per env, OR over substeps)
 enum {

@@ -127,7 +127,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     }
     for (auto& p : m.pairs)
       if (p.condim != 1 && p.condim != 3 && p.condim != 4 && p.condim != 6) throw std::runtime_error("engine: condim must be 1, 3, 4 or 6");
-    if (m.cone != CONE_PYRAMIDAL) throw std::runtime_error("engine: the elliptic cone is not supported by this build");
+    if (m.cone == CONE_ELLIPTIC) convex_ = true;   // the extended kernel instance carries the elliptic solver
     for (int j = 0; j < m.njnt; j++)
       if (m.jnt_limited[j] && m.jnt_type[j] == JNT_BALL) throw std::runtime_error("engine: limited ball joints are not supported");
     if (m.nv > 1024) throw std::runtime_error("engine: models with more than 1024 dofs are not supported by this build");
@@ -398,7 +398,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     int ncb = std::max(1, m.max_contacts_bound);
     d.ncon_max = cfg.ncon_max > 0 ? cfg.ncon_max : std::min(ncb, 24);
     int rows_per_con = 1;
-    for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : 2 * (p.condim - 1));
+    for (auto& p : m.pairs) rows_per_con = std::max(rows_per_con, p.condim == 1 ? 1 : m.cone == CONE_ELLIPTIC ? p.condim : 2 * (p.condim - 1));
     int rows_bound = d.neq + d.nfloss + d.ntfloss + 2 * (d.nlimit + d.ntlimit) + rows_per_con * d.ncon_max;
     d.nefc_max = cfg.nefc_max > 0 ? cfg.nefc_max : std::max(1, std::min(rows_bound, 64));
     // workspace layout
@@ -417,7 +417,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.w_tseg = take(9 * max_pieces);
     int kend = off;
     off = kbase;
-    d.w_J = take(d.nefc_max * nv); d.w_efc = take(MJB_EFC_FIELDS * d.nefc_max); d.w_H = take(nv * nv); d.w_active = take(d.nefc_max);
+    d.w_J = take(d.nefc_max * nv); d.w_efc = take((m.cone == CONE_ELLIPTIC ? MJB_EFC_FIELDS_ELLIPTIC : MJB_EFC_FIELDS) * d.nefc_max); d.w_H = take(nv * nv); d.w_active = take(d.nefc_max);
     d.w_nz = take(nv);
     int send = off;
     d.ws_size = std::max(kend, send);

@@ -182,7 +182,7 @@ class Engine {
   int B_ = 0, tot_q_ = 0, tot_v_ = 0, tot_u_ = 0, tot_b_ = 0, nv_max_ = 0;
   EngineConfig cfg_;
   bool rand_on_ = false;
-  bool convex_ = false;   // some model has a pair for the GJK / EPA collider
+  bool convex_ = false;   // some model has a pair for the GJK / EPA collider or an elliptic cone (extended kernel instance)
   bool gws_mode_ = false; // workspaces in HBM (too large for shared memory)
   DevBuf<float> gws_;
   cudaStream_t stream_ = nullptr;

@@ -48,15 +48,22 @@ __device__ __noinline__ void record_cfrc(Env& E, const StepParams& P, int ncon, 
       if (c < 0) { r++; continue; }
       const float* cr = con + MJB_CONTACT_FLOATS * c;
       int dim = (int)cr[14];
-      int nr = dim == 1 ? 1 : 2 * (dim - 1);
+      const bool ell = (int)efc[EFC_TYPE * ne + r] == ROW_ELLIPTIC;
+      int nr = dim == 1 ? 1 : ell ? dim : 2 * (dim - 1);
       int p = (int)cr[13];
       const float* pf = E.ft + m.f_pair + 16 * p;
       float fs = P.rand_friction ? P.rand_friction[E.env] : 1.f;
       float fn = 0, ft[5] = {0, 0, 0, 0, 0};
-      #pragma unroll 1
-      for (int q = 0; q < nr; q++) fn += efc[EFC_FORCE * ne + r + q];
-      for (int d = 0; d + 1 < dim; d++)
-        ft[d] = ldf(pf, 2 + d) * fs * (efc[EFC_FORCE * ne + r + 2 * d] - efc[EFC_FORCE * ne + r + 2 * d + 1]);
+      if (ell) {
+        // elliptic: the normal row's force and one force per friction direction
+        fn = efc[EFC_FORCE * ne + r];
+        for (int d = 0; d + 1 < dim; d++) ft[d] = efc[EFC_FORCE * ne + r + 1 + d];
+      } else {
+        #pragma unroll 1
+        for (int q = 0; q < nr; q++) fn += efc[EFC_FORCE * ne + r + q];
+        for (int d = 0; d + 1 < dim; d++)
+          ft[d] = ldf(pf, 2 + d) * fs * (efc[EFC_FORCE * ne + r + 2 * d] - efc[EFC_FORCE * ne + r + 2 * d + 1]);
+      }
       const float* n = cr + 3;
       const float* t1 = cr + 6;
       const float* t2 = cr + 9;
@@ -463,11 +470,11 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       STAGE_SYNC();
       if (valid) d_qacc_smooth(E);
       STAGE_SYNC();
-      if (valid) nefc = d_constraints(E, P, ncon);
+      if (valid) nefc = d_constraints<CVX>(E, P, ncon);
       STAGE_SYNC();
       if (valid) {
         const float* xpred = (P.qacc_pred && s == 0) ? P.qacc_pred + vadr : nullptr;   // a prediction serves the launch's first substep
-        int it = d_newton(E, P, nefc, max_iter, xpred, choice);
+        int it = d_newton<CVX>(E, P, nefc, max_iter, xpred, choice);
         nsum += it;
         nmax = it > nmax ? it : nmax;
       }

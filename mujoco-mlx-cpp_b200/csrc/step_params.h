@@ -25,7 +25,7 @@ struct StepParams {
   float* qacc_warm;
   const float* qacc_pred;   // predicted warm start (nullable)
 
-  int convex;               // 1: some model has a general convex pair (kernel instance with GJK / EPA)
+  int convex;               // 1: some model has a general convex pair or an elliptic cone (kernel instance with GJK / EPA and the cone solver)
   int nsub;                 // substeps per launch (same ctrl)
   int max_iter;             // <= 0: model default
   int* work_counter;        // persistent scheduling queue head (nullable = static env mapping)

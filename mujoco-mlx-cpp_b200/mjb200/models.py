@@ -547,7 +547,7 @@ def noisy_sphere_vertices(npts: int, radius: float, noise: float, g) -> np.ndarr
 CONVEX_SHAPES = ("ellipsoid", "cylinder", "mesh", "capsule", "sphere", "box")
 
 
-def convex_pile_xml(nbody: int = 6, seed: int = 0, iterations: int = 30, condim: int = 3) -> str:
+def convex_pile_xml(nbody: int = 6, seed: int = 0, iterations: int = 30, condim: int = 3, cone: str = "pyramidal") -> str:
     """nbody free bodies cycling through ellipsoid, cylinder, 32-point noisy
     sphere hull (r = 0.05 +- 20 %), capsule, sphere and box (sizes about
     0.04-0.06 m), stacked loosely in a 0.1 m column above a plane, for the
@@ -582,16 +582,30 @@ def convex_pile_xml(nbody: int = 6, seed: int = 0, iterations: int = 30, condim:
         bodies.append(f'<body name="b{i}" pos="{x:.4f} {y:.4f} {z:.4f}"><freejoint/><geom {geom} mass="{g.uniform(0.1, 0.4):.3f}"/></body>')
         z += h
     return (f'<mujoco model="convex_pile{nbody}"><compiler angle="radian"/>'
-            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="{cone}" integrator="Euler"/>'
             f'<default><geom condim="{condim}" friction="0.7 0.01 0.001"/></default>'
             + (f'<asset>{"".join(assets)}</asset>' if assets else "")
             + '<worldbody><geom name="floor" type="plane" size="0 0 1"/>' + "".join(bodies) + '</worldbody></mujoco>')
 
 
+def pushed_box_xml(cone: str = "elliptic", condim: int = 3, mu: float = 0.5, impratio: float = 1.0) -> str:
+    """A 1 kg cube (half size 0.1 m) on a plane, on three slide joints (x,
+    y, z) and a ball joint, with a motor on the x slide: the friction-cone
+    known-answer model (sticks for pushes below mu m g, slides above).
+    Tangential friction mu, torsional 0.02, rolling 0.002; dt 0.002."""
+    fr = f'friction="{mu} 0.02 0.002" condim="{condim}"'
+    return (f'<mujoco model="pushed_box"><option timestep="0.002" iterations="100" tolerance="1e-10" cone="{cone}" impratio="{impratio}"/>'
+            f'<worldbody><geom name="floor" type="plane" size="0 0 1" {fr}/>'
+            f'<body name="box" pos="0 0 0.1"><joint name="sx" type="slide" axis="1 0 0"/><joint name="sy" type="slide" axis="0 1 0"/>'
+            f'<joint name="sz" type="slide" axis="0 0 1"/><joint name="rot" type="ball"/>'
+            f'<geom type="box" size="0.1 0.1 0.1" mass="1" {fr}/></body></worldbody>'
+            f'<actuator><motor name="push" joint="sx"/></actuator></mujoco>')
+
+
 BIN_SHAPES = ("box", "capsule", "ellipsoid", "mesh")
 
 
-def bin_xml(nbody: int = 64, size: float = 1.0, seed: int = 0, condim: int = 3, iterations: int = 30) -> str:
+def bin_xml(nbody: int = 64, size: float = 1.0, seed: int = 0, condim: int = 3, iterations: int = 30, cone: str = "pyramidal") -> str:
     """A square bin (floor plus four inward-facing wall planes, side `size`)
     holding nbody free bodies cycling through boxes, capsules, ellipsoids and
     convex hulls of 32 points on a 0.05 m sphere with +-20 % radial noise,
@@ -629,7 +643,7 @@ def bin_xml(nbody: int = 64, size: float = 1.0, seed: int = 0, condim: int = 3, 
         bodies.append(f'<body name="b{i}" pos="{x:.4f} {y:.4f} {z:.4f}" quat="{q[0]:.5f} {q[1]:.5f} {q[2]:.5f} {q[3]:.5f}"><freejoint/>'
                       f'<geom {geom} mass="{g.uniform(0.1, 0.5):.3f}"/></body>')
     return (f'<mujoco model="bin{nbody}"><compiler angle="radian"/>'
-            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="pyramidal" integrator="Euler"/>'
+            f'<option timestep="0.004" iterations="{iterations}" tolerance="1e-8" cone="{cone}" integrator="Euler"/>'
             f'<default><geom condim="{condim}" friction="0.8 0.01 0.001"/></default>'
             + (f'<asset>{"".join(assets)}</asset>' if assets else "")
             + '<worldbody>' + "".join(walls) + "".join(bodies) + '</worldbody></mujoco>')

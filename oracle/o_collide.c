@@ -505,6 +505,12 @@ static int simplex_closest(SV* S, int n, double* lam, double* v) {
   /* tetrahedron: origin inside -> 4; else the closest of the faces that
      see the origin */
   static const int F[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 3, 1}, {1, 2, 3, 0}};
+  /* a flat tetrahedron (volume below 1e-6 of its edge product) is not
+     trusted to contain the origin: every face is then a candidate */
+  double t1[3], t2[3], t3[3], c23[3];
+  for (int k = 0; k < 3; k++) { t1[k] = S[1].w[k] - S[0].w[k]; t2[k] = S[2].w[k] - S[0].w[k]; t3[k] = S[3].w[k] - S[0].w[k]; }
+  o_cross(t2, t3, c23);
+  const int flat = fabs(dot3(t1, c23)) <= 1e-6 * sqrt(dot3(t1, t1) * dot3(t2, t2) * dot3(t3, t3));
   int best = -1, bn = 0;
   double bd = 1e300, bl[3], bv[3];
   SV bs[3];
@@ -514,7 +520,7 @@ static int simplex_closest(SV* S, int n, double* lam, double* v) {
     for (int k = 0; k < 3; k++) { e1[k] = P1[k] - P0[k]; e2[k] = P2[k] - P0[k]; }
     o_cross(e1, e2, nrm);
     double so = -dot3(nrm, P0), sq = dot3(nrm, Q) - dot3(nrm, P0);
-    if (so * sq >= 0) continue;   /* origin on the same side as the 4th point */
+    if (!flat && so * sq >= 0) continue;   /* origin on the same side as the 4th point */
     SV T[3] = {S[F[f][0]], S[F[f][1]], S[F[f][2]]};
     double l[3], vv[3];
     int k = simplex_closest(T, 3, l, vv);
@@ -872,6 +878,13 @@ static int convex_pair(const OModel* m, const Shape* A, const Shape* B, double m
     SV w;
     mk_support(m, A, B, nd, &w);
     if (vv - dot3(v, w.w) <= CVX_TOL * sqrt(vv)) break;   /* no progress: v is the closest point */
+    /* a support point already in the simplex: no progress either */
+    int dup = 0;
+    for (int i = 0; i < n; i++) {
+      double e[3] = {w.w[0] - S[i].w[0], w.w[1] - S[i].w[1], w.w[2] - S[i].w[2]};
+      if (dot3(e, e) <= 1e-16) dup = 1;
+    }
+    if (dup) break;
     S[n++] = w;
     n = simplex_closest(S, n, lam, v);
     if (n == 4) { overlap = 1; break; }

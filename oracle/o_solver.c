@@ -19,7 +19,7 @@
 #include "mjoracle.h"
 #include "o_util.h"
 
-enum { T_FRICTION = 0, T_LIMIT = 1, T_PYRAMID = 2, T_FRICTIONLESS = 3, T_EQUALITY = 5 };
+enum { T_FRICTION = 0, T_LIMIT = 1, T_PYRAMID = 2, T_FRICTIONLESS = 3, T_ELLIPTIC = 4, T_EQUALITY = 5, T_ELLFRIC = 6 };
 
 static void impedance(const OModel* m, const double* solref, const double* solimp, double pos, double* k, double* b, double* imp) {
   double tc = solref[0], dr = solref[1];
@@ -190,7 +190,8 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
     const int* pi = &m->pair_int[6 * pair];
     const double* pr = &m->pair_real[16 * pair];
     int dim = pi[4];
-    int nrow = dim == 1 ? 1 : 2 * (dim - 1);
+    const int elliptic = m->cone == 1 && dim > 1;
+    int nrow = dim == 1 ? 1 : elliptic ? dim : 2 * (dim - 1);
     if (stop || d->nefc + nrow > d->nefc_max) { stop = 1; d->nefc_dropped += nrow; d->status |= ORACLE_EFC_OVERFLOW; continue; }
     double fs = (rnd ? rnd->friction_scale : 1.0);
     double mu[5];
@@ -227,6 +228,35 @@ void oracle_make_constraints(const OModel* m, OData* d, const ORand* rnd) {
       d->efc_R[r] = R < O_MINVAL ? O_MINVAL : R;
       d->efc_D[r] = 1 / d->efc_R[r];
       d->efc_aref[r] = -b * rowdot(Jn, d->qvel, nv) - k * imp * pos;
+      continue;
+    }
+    if (elliptic) {
+      /* elliptic cone (MuJoCo's model): the normal row and dim - 1 friction
+         rows along t1, t2 (translation), n (torsion), t1, t2 (rolling).
+         R_n from the translational invweight; friction R_j = R_n (mu_0 /
+         mu_j)^2 / impratio, so the cone's aspect in the solver is
+         mu = mu_0 / sqrt(impratio) (stored in the normal row's floss slot;
+         each friction row stores its own coefficient mu_j) */
+      double Rn = (1 - imp) / imp * pr[14];
+      if (Rn < O_MINVAL) Rn = O_MINVAL;
+      int r = add_row(d, nv, T_ELLIPTIC);
+      memcpy(&d->efc_J[r * nv], Jn, nv * sizeof(double));
+      d->efc_R[r] = Rn;
+      d->efc_D[r] = 1 / Rn;
+      d->efc_aref[r] = -b * rowdot(Jn, d->qvel, nv) - k * imp * pos;
+      d->efc_floss[r] = mu[0] / sqrt(m->impratio);
+      for (int dir = 0; dir < dim - 1; dir++) {
+        const double* ax = dir == 0 || dir == 3 ? fr + 3 : dir == 1 || dir == 4 ? fr + 6 : fr;
+        const double* src = dir < 2 ? jacp : jacr;
+        int rf = add_row(d, nv, T_ELLFRIC);
+        double* J = &d->efc_J[rf * nv];
+        for (int i = 0; i < nv; i++) J[i] = ax[0] * src[i] + ax[1] * src[nv + i] + ax[2] * src[2 * nv + i];
+        double Rf = Rn * (mu[0] * mu[0]) / (mu[dir] * mu[dir]) / m->impratio;
+        d->efc_R[rf] = Rf < O_MINVAL ? O_MINVAL : Rf;
+        d->efc_D[rf] = 1 / d->efc_R[rf];
+        d->efc_aref[rf] = -b * rowdot(J, d->qvel, nv);
+        d->efc_floss[rf] = mu[dir];
+      }
       continue;
     }
     double mu0 = mu[0];
@@ -288,6 +318,59 @@ static double row_cost_delta(int type, double D, double fl, double y, double dy)
   return row_cost(type, D, fl, y + dy) - row_cost(type, D, fl, y);
 }
 
+/* Elliptic contact group (rows r0 = normal, r0+1 .. r0+dim-1 = friction)
+ * with jar y[0..dim): MuJoCo's three zones in the cone space U_0 = mu y_0,
+ * U_j = mu_j y_j, N = U_0, T = |U_t|:
+ *  top (N >= mu T): no force;
+ *  bottom (mu N + T <= 0): every row quadratic, f_j = -D_j y_j;
+ *  middle: cost 0.5 Dm (N - mu T)^2 with Dm = D_0 / (mu^2 (1 + mu^2)).
+ * Returns the cost; fills the forces, the zone (0 top, 1 bottom, 2 middle)
+ * and, if H is not NULL, the dim x dim Hessian in jar space. */
+static double cone_eval(int dim, const double* D, const double* fl, const double* y, double* f, int* zone, double* H) {
+  double mu = fl[0], U[6], T = 0;
+  U[0] = mu * y[0];
+  for (int j = 1; j < dim; j++) { U[j] = fl[j] * y[j]; T += U[j] * U[j]; }
+  T = sqrt(T);
+  double N = U[0], cost = 0;
+  if (H) memset(H, 0, dim * dim * sizeof(double));
+  if (N >= mu * T || (T <= 0 && N >= 0)) {
+    for (int j = 0; j < dim; j++) f[j] = 0;
+    *zone = 0;
+  } else if (mu * N + T <= 0 || (T <= 0 && N < 0)) {
+    for (int j = 0; j < dim; j++) {
+      f[j] = -D[j] * y[j];
+      cost += 0.5 * D[j] * y[j] * y[j];
+      if (H) H[j * dim + j] = D[j];
+    }
+    *zone = 1;
+  } else {
+    double Dm = D[0] / (mu * mu * (1 + mu * mu)), NmT = N - mu * T;
+    cost = 0.5 * Dm * NmT * NmT;
+    f[0] = -Dm * NmT * mu;
+    for (int j = 1; j < dim; j++) f[j] = Dm * NmT * mu * U[j] / T * fl[j];
+    if (H) {
+      /* Dm (a a' + NmT S' grad^2(N - mu T) S), a = S' grad(N - mu T),
+         S = diag(mu, mu_1..) */
+      double a[6];
+      a[0] = mu;
+      for (int j = 1; j < dim; j++) a[j] = -mu * U[j] / T * fl[j];
+      for (int i = 0; i < dim; i++)
+        for (int j = 0; j < dim; j++) H[i * dim + j] = Dm * a[i] * a[j];
+      double c = -Dm * NmT * mu / T;   /* > 0 in the middle zone */
+      for (int i = 1; i < dim; i++)
+        for (int j = 1; j < dim; j++) H[i * dim + j] += c * fl[i] * fl[j] * ((i == j ? 1.0 : 0.0) - U[i] * U[j] / (T * T));
+    }
+    *zone = 2;
+  }
+  return cost;
+}
+
+static int group_dim(const int* type, int r, int ne) {
+  int dim = 1;
+  while (r + dim < ne && type[r + dim] == T_ELLFRIC) dim++;
+  return dim;
+}
+
 typedef struct {
   int nv, nefc;
   const double *M, *qfrc_smooth, *qacc_smooth, *J, *aref, *D, *floss;
@@ -305,8 +388,14 @@ static double eval_point(const Prob* P, const double* x, double* y, double* forc
     Md[i] = s;
   }
   for (int i = 0; i < nv; i++) cost += 0.5 * (x[i] - P->qacc_smooth[i]) * Md[i];
+  for (int r = 0; r < P->nefc; r++) y[r] = rowdot(&P->J[r * nv], x, nv) - P->aref[r];
   for (int r = 0; r < P->nefc; r++) {
-    y[r] = rowdot(&P->J[r * nv], x, nv) - P->aref[r];
+    if (P->type[r] == T_ELLFRIC) continue;
+    if (P->type[r] == T_ELLIPTIC) {
+      int dim = group_dim(P->type, r, P->nefc), zone;
+      cost += cone_eval(dim, &P->D[r], &P->floss[r], &y[r], &force[r], &zone, NULL);
+      continue;
+    }
     force[r] = row_force(P->type[r], P->D[r], P->floss[r], y[r]);
     cost += row_cost(P->type[r], P->D[r], P->floss[r], y[r]);
   }
@@ -322,6 +411,20 @@ static double eval_point(const Prob* P, const double* x, double* y, double* forc
 static void ls_deriv(const Prob* P, double A, double B, const double* y, const double* q, double a, double* d1, double* d2) {
   double g1 = a * A + B, g2 = A;
   for (int r = 0; r < P->nefc; r++) {
+    if (P->type[r] == T_ELLFRIC) continue;
+    if (P->type[r] == T_ELLIPTIC) {
+      /* d/da and d2/da2 of the group cost along q, from its jar-space
+         gradient (-force) and Hessian */
+      int dim = group_dim(P->type, r, P->nefc), zone;
+      double yy[6], f[6], H[36];
+      for (int j = 0; j < dim; j++) yy[j] = y[r + j] + a * q[r + j];
+      cone_eval(dim, &P->D[r], &P->floss[r], yy, f, &zone, H);
+      for (int i = 0; i < dim; i++) {
+        g1 -= q[r + i] * f[i];
+        for (int j = 0; j < dim; j++) g2 += q[r + i] * H[i * dim + j] * q[r + j];
+      }
+      continue;
+    }
     double yr = y[r] + a * q[r];
     double f = row_force(P->type[r], P->D[r], P->floss[r], yr);
     g1 -= q[r] * f;
@@ -354,7 +457,17 @@ static double linesearch(const Prob* P, const double* y, const double* q, double
     a = an;
   }
   double dc = 0.5 * a * a * A + a * B;
-  for (int r = 0; r < P->nefc; r++) dc += row_cost_delta(P->type[r], P->D[r], P->floss[r], y[r], a * q[r]);
+  for (int r = 0; r < P->nefc; r++) {
+    if (P->type[r] == T_ELLFRIC) continue;
+    if (P->type[r] == T_ELLIPTIC) {
+      int dim = group_dim(P->type, r, P->nefc), zone;
+      double yy[6], f[6];
+      for (int j = 0; j < dim; j++) yy[j] = y[r + j] + a * q[r + j];
+      dc += cone_eval(dim, &P->D[r], &P->floss[r], yy, f, &zone, NULL) - cone_eval(dim, &P->D[r], &P->floss[r], &y[r], f, &zone, NULL);
+      continue;
+    }
+    dc += row_cost_delta(P->type[r], P->D[r], P->floss[r], y[r], a * q[r]);
+  }
   *dcost = dc;
   return a;
 }
@@ -392,6 +505,26 @@ void oracle_solve(const OModel* m, OData* d, int max_iter) {
       /* H = M + sum_quadratic D J'J */
       memcpy(H, d->M, nv * nv * sizeof(double));
       for (int r = 0; r < ne; r++) {
+        if (d->efc_type[r] == T_ELLFRIC) continue;
+        if (d->efc_type[r] == T_ELLIPTIC) {
+          /* cone Hessian: J_c' Hc J_c over the group's rows */
+          int dim = group_dim(d->efc_type, r, ne), zone;
+          double f[6], Hc[36];
+          cone_eval(dim, &d->efc_D[r], &d->efc_floss[r], &d->efc_jar[r], f, &zone, Hc);
+          if (zone == 0) continue;
+          for (int a = 0; a < dim; a++)
+            for (int bb = 0; bb < dim; bb++) {
+              double hab = Hc[a * dim + bb];
+              if (hab == 0) continue;
+              const double* Ja = &d->efc_J[(r + a) * nv];
+              const double* Jb = &d->efc_J[(r + bb) * nv];
+              for (int i = 0; i < nv; i++) {
+                if (Ja[i] == 0) continue;
+                for (int j = 0; j <= i; j++) H[i * nv + j] += Ja[i] * hab * Jb[j];
+              }
+            }
+          continue;
+        }
         if (!row_quadratic(d->efc_type[r], d->efc_D[r], d->efc_floss[r], d->efc_jar[r])) continue;
         const double* J = &d->efc_J[r * nv];
         double Dr = d->efc_D[r];

@@ -772,3 +772,135 @@ def test_spatial_tendon_jacobian_matches_finite_differences():
                     env.a["qpos"][:] = qq
                     fd[i] += sg * env.tendon(t)[0] / 2e-6
             np.testing.assert_allclose(J, fd, atol=1e-7)
+
+
+def _cone_force(D0, mu, fric, y):
+    """MuJoCo's elliptic cone in numpy, written from the cost rather than
+    shared with the C code: s(y) over one contact's rows with U = (mu y0,
+    fric_j y_j), N = U0, T = |U_t|; top zone (N >= mu T) zero, bottom zone
+    (mu N + T <= 0) quadratic in every row, middle 0.5 Dm (N - mu T)^2 with
+    Dm = D0 / (mu^2 (1 + mu^2)).  Returns (cost, force = -ds/dy)."""
+    U = np.concatenate([[mu * y[0]], fric * y[1:]])
+    N, T = U[0], np.linalg.norm(U[1:])
+    if N >= mu * T or (T <= 0 and N >= 0):
+        return 0.0, np.zeros_like(y)
+    if mu * N + T <= 0 or (T <= 0 and N < 0):
+        return None, None   # bottom: the caller handles it with per-row D
+    Dm = D0 / (mu * mu * (1 + mu * mu))
+    g = np.concatenate([[mu], -mu * U[1:] / T * fric])   # d(N - mu T)/dy
+    return 0.5 * Dm * (N - mu * T) ** 2, -Dm * (N - mu * T) * g
+
+
+def _elliptic_cost_and_force(e, floss, y):
+    cost, f, r = 0.0, np.zeros_like(y), 0
+    while r < len(y):
+        t = e["type"][r]
+        if t == 4:
+            dim = 1
+            while r + dim < len(y) and e["type"][r + dim] == 6:
+                dim += 1
+            c, fc = _cone_force(e["D"][r], floss[r], floss[r + 1: r + dim], y[r: r + dim])
+            if c is None:
+                fc = -e["D"][r: r + dim] * y[r: r + dim]
+                c = 0.5 * float(e["D"][r: r + dim] @ (y[r: r + dim] ** 2))
+            cost += c
+            f[r: r + dim] = fc
+            r += dim
+        else:
+            assert t in (1, 3, 5)
+            fr = -e["D"][r] * (y[r] if t == 5 else min(y[r], 0.0))
+            cost += 0.5 * e["D"][r] * (y[r] ** 2 if t == 5 else min(y[r], 0.0) ** 2)
+            f[r] = fr
+            r += 1
+    return cost, f
+
+
+def _elliptic_box(condim, mu=0.5, impratio=1.0):
+    om, env = env_from_xml(mjb200.models.pushed_box_xml("elliptic", condim, mu, impratio))
+    env.a["qpos"][:] = 0
+    env.a["qpos"][2] = -0.0005
+    env.a["qpos"][3] = 1
+    return om, env
+
+
+@pytest.mark.parametrize("condim", [3, 4, 6])
+@pytest.mark.parametrize("impratio", [1.0, 4.0])
+def test_elliptic_cone_rows_and_gauss_optimality(condim, impratio):
+    """Elliptic contacts: dim rows per contact (normal type 4, friction type
+    6); R_j = R_n (mu_0 / mu_j)^2 / impratio; the Newton solution minimises
+    the Gauss cost with the cone term (gradient residual ~0 and no random
+    perturbation lowers the cost), for a box pushed with a tangential motor
+    both below and above mu m g, at rest and sliding."""
+    checked = 0
+    for push in (1.0, 9.0):
+        om, env = _elliptic_box(condim, impratio=impratio)
+        for t in range(60):
+            env.a["ctrl"][0] = push
+            env.a["qvel"][1] = 0.05   # a sideways component: both tangents carry force
+            env.step()
+            assert env.d.status == 0
+            e = env.efc()
+            n = env.d.nefc
+            nc = env.d.ncon
+            if t % 3 or nc == 0:
+                continue
+            checked += 1
+            assert n == nc * condim
+            assert list(e["type"][:condim]) == [4] + [6] * (condim - 1)
+            floss = env.a["efc_floss"][:n]
+            R = 1 / e["D"]
+            fr = np.array([0.5, 0.5, 0.02, 0.002, 0.002])
+            for c in range(nc):
+                r0 = c * condim
+                assert floss[r0] == pytest.approx(0.5 / np.sqrt(impratio), rel=1e-12)
+                for j in range(1, condim):
+                    assert floss[r0 + j] == pytest.approx(fr[j - 1], rel=1e-12)
+                    assert R[r0 + j] == pytest.approx(R[r0] * (0.5 / fr[j - 1]) ** 2 / impratio, rel=1e-9)
+            nv = om.nv
+            M = env.a["M"].reshape(nv, nv)
+            qacc, qs = env.a["qacc"].copy(), env.a["qacc_smooth"]
+            y = e["J"] @ qacc - e["aref"]
+
+            def total(x):
+                yx = e["J"] @ x - e["aref"]
+                return 0.5 * (x - qs) @ M @ (x - qs) + _elliptic_cost_and_force(e, floss, yx)[0]
+
+            c0, f = _elliptic_cost_and_force(e, floss, y)
+            np.testing.assert_allclose(f, e["force"], atol=1e-8 * max(1.0, np.abs(f).max()))
+            res = np.linalg.norm(M @ (qacc - qs) - e["J"].T @ f) / max(np.linalg.norm(M @ qs), 1.0)
+            assert res < 1e-7, res
+            # friction forces stay in the cone: |f_j / mu_j| over the tangents <= f_n / mu
+            for c in range(nc):
+                r0 = c * condim
+                ft = f[r0 + 1: r0 + condim] / floss[r0 + 1: r0 + condim]
+                assert f[r0] >= -1e-12
+                assert np.linalg.norm(ft) <= f[r0] / floss[r0] * (1 + 1e-9) + 1e-12
+            g = np.random.default_rng(condim)
+            base = total(qacc)
+            for k in range(20):
+                d = g.normal(size=nv) * 10.0 ** g.uniform(-6, -2)
+                assert total(qacc + d) >= base - 1e-10 * max(1.0, abs(base))
+    assert checked >= 20
+
+
+def test_elliptic_cone_stick_and_slide_known_answers():
+    """Pushed box (m = 1 kg, mu = 0.5, condim 3): below mu m g it sticks
+    (tangential velocity stays ~0); above it slides with a friction force on
+    the cone boundary, |f_t| = mu f_n per contact, so the net tangential
+    force is push - mu sum(f_n)."""
+    om, env = _elliptic_box(3)
+    for t in range(200):
+        env.a["ctrl"][0] = 3.0
+        env.step()
+    assert abs(env.a["qvel"][0]) < 2e-3
+    om, env = _elliptic_box(3)
+    for t in range(200):
+        env.a["ctrl"][0] = 9.0
+        env.step()
+        e = env.efc()
+        if env.d.nefc == 0 or env.a["qvel"][0] < 0.05:
+            continue
+        f = e["force"].reshape(-1, 3)
+        # every contact in the middle zone: friction on the boundary
+        np.testing.assert_allclose(np.linalg.norm(f[:, 1:], axis=1), 0.5 * f[:, 0], rtol=1e-6)
+    assert env.a["qvel"][0] > 0.5
