@@ -75,3 +75,67 @@ def test_convex_pile_parity_and_rollout(seed):
     qp, qv = sim.state()
     assert np.isfinite(qp).all() and np.isfinite(qv).all()
     assert np.all(sim.stats()["status"] == 0)
+
+
+def test_hull_pairs_near_touching_match_oracle():
+    """Two free noisy-sphere hulls (32 points each) in 1024 envs, random
+    orientations, the second placed along a random direction at the
+    oracle's touching distance plus d, |d| log-uniform in [1e-7, 1e-3] m
+    and of either sign.  The GPU's contact (present or not, and its
+    distance) must match the oracle's except within 1e-5 m of touching: a
+    polytope pair this close is where FP32 GJK can return a simplex vertex
+    again or close a flat tetrahedron around the origin."""
+    g = np.random.Generator(np.random.Philox(key=11))
+    va = mjb200.models.noisy_sphere_vertices(32, 0.05, 0.2, g)
+    vb = mjb200.models.noisy_sphere_vertices(32, 0.05, 0.2, g)
+    mesh = lambda nm, v: f'<mesh name="{nm}" vertex="' + " ".join(f"{x:.5f}" for x in v.reshape(-1)) + '"/>'
+    xml = ('<mujoco><option timestep="0.002" gravity="0 0 0"/><asset>' + mesh("ha", va) + mesh("hb", vb) + '</asset><worldbody>'
+           '<body name="a"><freejoint/><geom type="mesh" mesh="ha" mass="0.2"/></body>'
+           '<body name="b" pos="0.2 0 0"><freejoint/><geom type="mesh" mesh="hb" mass="0.2"/></body></worldbody></mujoco>')
+    model = mjb200.load_model_from_string(xml)
+    om = oracle.OracleModel(model.dump())
+    B = 1024
+    q = np.zeros((B, 14))
+
+    def rand_quat():
+        x = g.normal(size=4)
+        return x / np.linalg.norm(x)
+
+    def oracle_dist(qe):
+        env = oracle.OracleEnv(om, 4, 16)
+        env.a["qpos"][:] = qe
+        env.step()
+        c = env.contacts()
+        return float(c[0, 12]) if len(c) else None
+
+    for e in range(B):
+        q[e, 3:7], q[e, 10:14] = rand_quat(), rand_quat()
+        u = g.normal(size=3)
+        u /= np.linalg.norm(u)
+        lo, hi = 0.0, 0.2                       # lo overlaps, hi separates
+        for _ in range(36):
+            mid = 0.5 * (lo + hi)
+            q[e, 7:10] = mid * u
+            d = oracle_dist(q[e])
+            if d is not None and d < 0:
+                lo = mid
+            else:
+                hi = mid
+        q[e, 7:10] = (hi + g.choice([-1, 1]) * 10 ** g.uniform(-7, -3)) * u
+    q32 = q.astype(np.float32)
+    sim = mjb200.BatchedSim(model, B, ncon_max=4, nefc_max=16)
+    gs = gpu_step_from(sim, q32, np.zeros((B, 12), np.float32), None, 4, 16)
+    o = oracle_step_from(om, q32.astype(np.float64), np.zeros((B, 12)), np.zeros((B, 1)), ncon_max=4, nefc_max=16)
+    near, far = 0, 0
+    for e in range(B):
+        od = float(o[e]["contacts"][0, 12]) if o[e]["ncon"] else None
+        gd = float(gs["con"][e, 0, 12]) if gs["stats"]["ncon"][e] else None
+        if od is None and gd is None:
+            far += 1
+            continue
+        if od is None or gd is None:
+            assert abs(od if gd is None else gd) <= 1e-5, (e, od, gd)
+            near += 1
+            continue
+        assert abs(gd - od) <= 1e-5, (e, od, gd)
+    assert far > B // 4 and near < B // 10
