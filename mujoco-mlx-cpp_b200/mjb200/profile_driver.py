@@ -18,6 +18,7 @@ bounds what any predicted warm start can save.
 from __future__ import annotations
 
 import argparse
+import json
 
 import numpy as np
 
@@ -76,6 +77,9 @@ def main(argv=None):
     ap.add_argument("--ctrl", type=int, default=3, help="control steps (4 substeps each)")
     ap.add_argument("--rows", type=int, default=16384)
     ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--cone", default="pyramidal", choices=["pyramidal", "elliptic"], help="bin / convex: friction cone")
+    ap.add_argument("--condim", type=int, default=3, help="bin / convex: contact dimensionality")
+    ap.add_argument("--time", action="store_true", help="bin / convex: time the control steps with CUDA events")
     a = ap.parse_args(argv)
 
     import torch
@@ -101,18 +105,46 @@ def main(argv=None):
         # large-model path (HBM workspaces, row-sparse H, zero-skipping
         # Cholesky) on the 64-body bin, or the GJK / EPA kernel instance on
         # the 6-body convex pile; a.ctrl substeps after 20 settling substeps
-        xml = mjb200.models.bin_xml(64, 1.0, seed=1) if a.what == "bin" else mjb200.models.convex_pile_xml(6, seed=1)
+        # (--time: a.ctrl control steps of 4 substeps, CUDA events around
+        # each, Newton iterations per substep from the step statistics)
+        if a.what == "bin":
+            xml = mjb200.models.bin_xml(64, 1.0, seed=1, condim=a.condim, cone=a.cone)
+        else:
+            xml = mjb200.models.convex_pile_xml(6, seed=1, condim=a.condim, cone=a.cone)
         m = mjb200.load_model_from_string(xml)
-        kw = dict(ncon_max=400, nefc_max=1600) if a.what == "bin" else dict(ncon_max=40, nefc_max=200)
-        sim = mjb200.BatchedSim(m, a.envs, record=0, **kw)
+        rows = a.condim if (a.cone == "elliptic" and a.condim > 1) else max(1, 2 * (a.condim - 1))
+        ncon = 400 if a.what == "bin" else 40
+        sim = mjb200.BatchedSim(m, a.envs, record=0, ncon_max=ncon, nefc_max=ncon * rows)
         q, v = mjb200.models.box_pile_state(m, a.envs, seed=5)
         sim.set_state(q.astype(np.float32), v.astype(np.float32))
         sim.step(None, 20)
-        for c in range(a.ctrl):
-            sim.step(None, 1)
+        if not a.time:
+            for c in range(a.ctrl):
+                sim.step(None, 1)
+            sim.sync()
+            st = sim.stats()
+            print(a.what, "done: shape", sim.launch_shape(), "ncon mean", st["ncon"].mean(), "nefc mean", st["nefc"].mean(), "status", np.unique(st["status"]))
+            return
         sim.sync()
-        st = sim.stats()
-        print(a.what, "done: shape", sim.launch_shape(), "ncon mean", st["ncon"].mean(), "nefc mean", st["nefc"].mean(), "status", np.unique(st["status"]))
+        stream = torch.cuda.ExternalStream(sim.stream())   # the sim launches on its own stream
+        ms, its, itmax = [], [], []
+        for c in range(a.ctrl):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            sim.step(None, 4)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            st = sim.stats()
+            its.append(st["niter_sum"] / 4.0)
+            itmax.append(st["niter_max"])
+        its = np.concatenate(its)
+        out = dict(workload=f"{a.what} {a.cone} condim {a.condim}", envs=a.envs, ms_per_control_step=float(np.median(ms)),
+                   env_steps_per_s=a.envs * 1e3 / float(np.median(ms)), newton_iter_mean=float(its.mean()),
+                   newton_iter_p99=float(np.percentile(its, 99)), newton_iter_max=int(np.max(itmax)), ncon_mean=float(st["ncon"].mean()),
+                   nefc_mean=float(st["nefc"].mean()), status=[int(x) for x in np.unique(st["status"])], shape=sim.launch_shape())
+        print(json.dumps(out))
         return
 
     m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
