@@ -33,6 +33,15 @@ MJMLX_API void mjb200_warmstart_free(MjbWarmStart* net);
 /* Input width (features + controls) the sim's learned warm start expects, or -1. */
 MJMLX_API int mjb200_warmstart_input_width(const MjmlxBatchedSim* sim);
 
+/* The net shape a sim expects: input width, output width and rows per env.
+ * One row of nv outputs per env, except for models made only of free bodies
+ * (children of the world) with nv > 64 and no controls: one row per body of
+ * 45 features (height, orientation quaternion, the body's 6 velocities and 6
+ * converged accelerations, its first 4 contacts as normal along the force on
+ * the body, distance and contact point minus body position) and 6 outputs,
+ * rows_per_env = nbody - 1.  Any pointer may be NULL; 0 or -1. */
+MJMLX_API int mjb200_warmstart_layout(const MjmlxBatchedSim* sim, int* in_raw, int* nout, int* rows_per_env);
+
 /* Sizes: input width, padded input width, hidden width, output width, padded
  * output width, total parameter count.  Any pointer may be NULL. */
 MJMLX_API int mjb200_warmstart_dims(const MjbWarmStart* net, int* in_raw, int* in_pad, int* hidden, int* nout, int* out_pad, int* nparams);
@@ -62,9 +71,10 @@ MJMLX_API int mjb200_warmstart_train(MjbWarmStart* net, const float* xraw_dev, c
 
 /* Training data from a plain rollout of the sim (learned warm start off):
  * ctrl_dev holds nctrl control sets of total_u floats, each applied for
- * substeps_per_ctrl substeps; every substep after the first writes num_envs
- * rows xraw_dev[.][in_raw] and traw_dev[.][nv] while max_rows allows.
- * Returns the number of rows written, or -1. */
+ * substeps_per_ctrl substeps; every substep after the first writes
+ * num_envs x rows_per_env rows xraw_dev[.][in_raw] and traw_dev[.][nout]
+ * (mjb200_warmstart_layout) while max_rows allows.  Returns the number of
+ * rows written, or -1. */
 MJMLX_API int mjb200_batched_warmstart_collect(MjmlxBatchedSim* sim, const float* ctrl_dev, int nctrl, int substeps_per_ctrl, float* xraw_dev,
                                                float* traw_dev, int max_rows);
 /* Attaches a net to the sim (NULL detaches).  The net must outlive the

@@ -52,6 +52,18 @@ MJMLX_API int mjb200_warmstart_input_width(const MjmlxBatchedSim* sim) {
   });
 }
 
+MJMLX_API int mjb200_warmstart_layout(const MjmlxBatchedSim* sim, int* in_raw, int* nout, int* rows_per_env) {
+  if (!sim || !sim->engine) return -1;
+  return guarded("mjb200_warmstart_layout", [&] {
+    const auto& e = *sim->engine;
+    if (!e.uniform()) throw std::runtime_error("needs a single-model batch");
+    if (in_raw) *in_raw = e.feature_count() + (e.feature_per_body() ? 0 : e.model(0).nu);
+    if (nout) *nout = e.warmstart_outputs();
+    if (rows_per_env) *rows_per_env = e.rows_per_env();
+    return 0;
+  });
+}
+
 MJMLX_API int mjb200_warmstart_dims(const MjbWarmStart* w, int* in_raw, int* in_pad, int* hidden, int* nout, int* out_pad, int* nparams) {
   if (!w) return -1;
   const auto& n = *w->net;

@@ -762,6 +762,7 @@ void Engine::launch_learned(int n, bool record) {
   const bool first_valid = feat_valid_;
   const Model& m = *models_[0];
   const int F = feature_count(), qskip = feature_qskip();
+  const bool per_body = feature_per_body();
   // a prediction at substeps s % k == 0; each launch runs up to the next
   // prediction (the prediction is a warm-start candidate of its first
   // substep only; the kernel writes the features of every substep, so the
@@ -771,12 +772,14 @@ void Engine::launch_learned(int n, bool record) {
     for (int s = 0; s < n;) {
       const bool have = first_valid || s > 0;
       const int len = std::min(k, n - s);
-      if (have) net_->infer(feat_.p, feat_stride_, F, ctrl_.p, m.nu, warm_.p, pred_.p, B_, stream_);
+      // per-body mode: B * (nbody - 1) rows of 6 outputs, which are the env-major [B][nv] layout
+      if (have) net_->infer(feat_.p, feat_stride_, F, ctrl_.p, per_body ? 0 : m.nu, warm_.p, pred_.p, B_ * rows_per_env(), stream_);
       StepParams P = params(len, record && s + len == n);
       P.qacc_pred = have ? pred_.p : nullptr;
       P.features = feat_.p;
       P.feat_stride = feat_stride_;
       P.feat_qskip = qskip;
+      P.feat_body = per_body;
       P.stats_accumulate = s > 0;
       if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
       check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
@@ -1099,7 +1102,16 @@ int Engine::feature_qskip() const {
 
 int Engine::feature_count() const {
   const Model& m = *models_[0];
+  if (feature_per_body()) return MJB_FEAT_BODY;
   return m.nq - feature_qskip() + 2 * m.nv + 4 * MJB_FEAT_CONTACTS;
+}
+
+bool Engine::feature_per_body() const {
+  const Model& m = *models_[0];
+  if (m.nv <= WarmStartNet::kOutPad || m.nu != 0 || m.njnt != m.nbody - 1) return false;
+  for (int j = 0; j < m.njnt; j++)
+    if (m.jnt_type[j] != JNT_FREE || m.jnt_bodyid[j] != j + 1 || m.body_parentid[j + 1] != 0) return false;
+  return true;
 }
 
 void Engine::ensure_features() {
@@ -1109,7 +1121,7 @@ void Engine::ensure_features() {
   if (feat_.p && feat_stride_ == stride) return;
   sync();
   feat_stride_ = stride;
-  feat_.alloc((size_t)B_ * stride);
+  feat_.alloc((size_t)B_ * rows_per_env() * stride);
   feat_valid_ = false;
   invalidate_graphs();
 }
@@ -1119,9 +1131,9 @@ void Engine::set_warmstart(WarmStartNet* net) {
   if (net) {
     ensure_features();
     const Model& m = *models_[0];
-    if (net->in_raw() != feature_count() + m.nu || net->nout() != m.nv)
+    if (net->in_raw() != feature_count() + (feature_per_body() ? 0 : m.nu) || net->nout() != warmstart_outputs())
       throw std::runtime_error("learned warm start: the net's input / output widths do not match this model");
-    net->prepare_inference(B_);
+    net->prepare_inference(B_ * rows_per_env());
   }
   net_ = net;
   invalidate_graphs();
@@ -1130,7 +1142,9 @@ void Engine::set_warmstart(WarmStartNet* net) {
 int Engine::collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows) {
   ensure_features();
   const Model& m = *models_[0];
-  const int F = feature_count(), nu = m.nu, nv = m.nv, in_raw = F + nu;
+  const bool per_body = feature_per_body();
+  const int F = feature_count(), nu = per_body ? 0 : m.nu, nv = m.nv, in_raw = F + nu;
+  const int R = B_ * rows_per_env();   // training rows per substep
   tmp_prev_.alloc((size_t)B_ * nv);
   WarmStartNet* saved = net_;
   net_ = nullptr;
@@ -1139,10 +1153,10 @@ int Engine::collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* x
   for (int c = 0; c < nctrl; c++) {
     if (nu > 0) check(cudaMemcpyAsync(ctrl_.p, ctrl_seq + (size_t)c * tot_u_, sizeof(float) * tot_u_, cudaMemcpyDeviceToDevice, stream_), "collect ctrl");
     for (int s = 0; s < sub_per_ctrl; s++) {
-      const bool take = have && rows + B_ <= max_rows;
+      const bool take = have && rows + R <= max_rows;
       if (take) {
         float* xr = xraw + (size_t)rows * in_raw;
-        check(cudaMemcpy2DAsync(xr, sizeof(float) * in_raw, feat_.p, sizeof(float) * feat_stride_, sizeof(float) * F, B_, cudaMemcpyDeviceToDevice,
+        check(cudaMemcpy2DAsync(xr, sizeof(float) * in_raw, feat_.p, sizeof(float) * feat_stride_, sizeof(float) * F, R, cudaMemcpyDeviceToDevice,
                                 stream_),
               "collect features");
         if (nu > 0)
@@ -1154,11 +1168,13 @@ int Engine::collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* x
       P.features = feat_.p;
       P.feat_stride = feat_stride_;
       P.feat_qskip = feature_qskip();
+      P.feat_body = per_body;
       if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
       check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
       if (take) {
-        check(mjb_sub(B_ * nv, warm_.p, tmp_prev_.p, traw + (size_t)rows * nv, stream_), "collect target");
-        rows += B_;
+        // per-body mode: R rows of 6 targets are the same B * nv floats
+        check(mjb_sub(B_ * nv, warm_.p, tmp_prev_.p, traw + (size_t)rows * warmstart_outputs(), stream_), "collect target");
+        rows += R;
       }
       have = true;
     }

@@ -107,6 +107,13 @@ class Engine {
   // free-joint x, y; qvel; converged qacc; 16 x contact normal and distance).
   int feature_count() const;
   int feature_qskip() const;
+  // Per-body mode: models made only of free bodies (children of the world)
+  // with more dofs than a per-env net serves (nv > 64) and no controls get
+  // one feature row and 6 outputs per body (rows_per_env = nbody - 1);
+  // otherwise one row of nv outputs per env.
+  bool feature_per_body() const;
+  int rows_per_env() const { return feature_per_body() ? models_[0]->nbody - 1 : 1; }
+  int warmstart_outputs() const { return feature_per_body() ? 6 : models_[0]->nv; }
   // Attaches a trained net (null detaches): every substep then first runs the
   // net on the features of the previous substep and the current controls and
   // offers its prediction to the Newton solver as a warm-start candidate.

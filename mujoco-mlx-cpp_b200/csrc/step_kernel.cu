@@ -298,7 +298,49 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
 // the next substep starts from (qpos without the skipped leading
 // coordinates, qvel), the converged acceleration of this substep, and the
 // normal and distance of the first MJB_FEAT_CONTACTS contacts.
+// Per-body rows (P.feat_body): lane per body, contacts scanned in order.
+__device__ __noinline__ void write_body_features(Env& E, const StepParams& P, int ncon) {
+  const DevModelDesc& m = *E.md;
+  const float* ws = E.ws;
+  const int nb = m.nbody - 1;
+  float* base = P.features + (size_t)E.env * nb * P.feat_stride;
+#pragma unroll 1
+  for (int b = E.lane; b < nb; b += 32) {
+    const int body = b + 1, j = ldi(E.it, m.i_body_jntadr + body);
+    const int qa = ldi(E.it, m.i_jnt_qposadr + j), va = ldi(E.it, m.i_jnt_dofadr + j);
+    float* f = base + (size_t)b * P.feat_stride;
+    const float* q = ws + m.w_qpos + qa;
+    f[0] = q[2];
+    for (int k = 0; k < 4; k++) f[1 + k] = q[3 + k];
+    for (int k = 0; k < 6; k++) {
+      f[5 + k] = ws[m.w_qvel + va + k];
+      f[11 + k] = ws[m.w_x + va + k];
+    }
+    int n = 0;
+#pragma unroll 1
+    for (int c = 0; c < ncon && n < MJB_FEAT_BODY_CONTACTS; c++) {
+      const float* cr = ws + m.w_con + c * MJB_CONTACT_FLOATS;
+      const int p = (int)cr[13];
+      const int b1 = ldi(E.it, m.i_pair + 6 * p + 2), b2 = ldi(E.it, m.i_pair + 6 * p + 3);
+      if (b1 != body && b2 != body) continue;
+      const float sg = b2 == body ? 1.f : -1.f;   // the normal points from geom 1 to geom 2
+      float* o = f + 17 + 7 * n;
+      for (int k = 0; k < 3; k++) {
+        o[k] = sg * cr[3 + k];
+        o[4 + k] = cr[k] - q[k];
+      }
+      o[3] = cr[12];
+      n++;
+    }
+    for (int k = 17 + 7 * n; k < MJB_FEAT_BODY; k++) f[k] = 0.f;
+  }
+}
+
 __device__ __noinline__ void write_features(Env& E, const StepParams& P, int ncon) {
+  if (P.feat_body) {
+    write_body_features(E, P, ncon);
+    return;
+  }
   const DevModelDesc& m = *E.md;
   const float* ws = E.ws;
   const int nv = m.nv, lane = E.lane;

@@ -84,11 +84,20 @@ struct StepParams {
   // learned warm start: feature rows written after each substep (nullable):
   // qpos[feat_qskip:nq], qvel, converged qacc, then MJB_FEAT_CONTACTS x
   // (contact normal, distance) in contact order, zero padded
+  // feat_body = 1 (models made only of free bodies, children of the world):
+  // one row per body instead, [B][nbody - 1][feat_stride], of MJB_FEAT_BODY
+  // floats: height, orientation quaternion, the body's 6 velocities and 6
+  // converged accelerations, then its first MJB_FEAT_BODY_CONTACTS contacts
+  // in contact order as (normal along the force on this body, distance,
+  // contact point minus body position), zero padded
   float* features;             // [B][feat_stride]
   int feat_stride;
   int feat_qskip;
+  int feat_body;
   int stats_accumulate;        // 1: add this launch's Newton iterations to niter_sum / max into niter_max
   int poison_workspace;        // 1: fill each env's shared workspace with NaN before its first stage (test aid)
 };
 
 #define MJB_FEAT_CONTACTS 16
+#define MJB_FEAT_BODY_CONTACTS 4
+#define MJB_FEAT_BODY (17 + 7 * MJB_FEAT_BODY_CONTACTS)

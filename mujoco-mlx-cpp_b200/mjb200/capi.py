@@ -73,6 +73,7 @@ def _load():
         "mjb200_warmstart_create": (C.c_void_p, [C.c_int, C.c_int, C.c_ulonglong]),
         "mjb200_warmstart_free": (None, [C.c_void_p]),
         "mjb200_warmstart_input_width": (C.c_int, [C.c_void_p]),
+        "mjb200_warmstart_layout": (C.c_int, [C.c_void_p, _i32p, _i32p, _i32p]),
         "mjb200_warmstart_dims": (C.c_int, [C.c_void_p] + [_i32p] * 6),
         "mjb200_warmstart_get_params": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_warmstart_set_params": (C.c_int, [C.c_void_p, _f32p]),
@@ -414,6 +415,13 @@ class BatchedSim:
     # ---- learned warm start
     def warmstart_input_width(self) -> int:
         return lib.mjb200_warmstart_input_width(self.handle)
+
+    def warmstart_layout(self):
+        """(in_raw, nout, rows_per_env) of the learned warm start for this sim."""
+        d = [C.c_int() for _ in range(3)]
+        if lib.mjb200_warmstart_layout(self.handle, *[C.byref(x) for x in d]) < 0:
+            raise RuntimeError(last_error())
+        return tuple(x.value for x in d)
 
     def warmstart_collect(self, ctrl_ptr: int, nctrl: int, substeps_per_ctrl: int, xraw_ptr: int, traw_ptr: int, max_rows: int) -> int:
         rc = lib.mjb200_batched_warmstart_collect(self.handle, C.c_void_p(ctrl_ptr), nctrl, substeps_per_ctrl, C.c_void_p(xraw_ptr),

@@ -80,6 +80,9 @@ def main(argv=None):
     ap.add_argument("--cone", default="pyramidal", choices=["pyramidal", "elliptic"], help="bin / convex: friction cone")
     ap.add_argument("--condim", type=int, default=3, help="bin / convex: contact dimensionality")
     ap.add_argument("--time", action="store_true", help="bin / convex: time the control steps with CUDA events")
+    ap.add_argument("--learned", action="store_true", help="bin --time: also train the per-body warm start and time it")
+    ap.add_argument("--train-substeps", type=int, default=24, help="bin --learned: substeps of the collection rollout")
+    ap.add_argument("--train-epochs", type=int, default=8)
     a = ap.parse_args(argv)
 
     import torch
@@ -126,25 +129,59 @@ def main(argv=None):
             print(a.what, "done: shape", sim.launch_shape(), "ncon mean", st["ncon"].mean(), "nefc mean", st["nefc"].mean(), "status", np.unique(st["status"]))
             return
         sim.sync()
-        stream = torch.cuda.ExternalStream(sim.stream())   # the sim launches on its own stream
-        ms, its, itmax = [], [], []
-        for c in range(a.ctrl):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        net = None
+        if a.learned:
+            # per-body warm start trained on a rollout from other seeded poses
+            col = mjb200.BatchedSim(m, a.envs, record=0, ncon_max=ncon, nefc_max=ncon * rows)
+            qc, vc = mjb200.models.box_pile_state(m, a.envs, seed=905)
+            col.set_state(qc.astype(np.float32), vc.astype(np.float32))
+            col.step(None, 20)
+            in_raw, nout, rpe = col.warmstart_layout()
+            n = a.envs * rpe * (a.train_substeps - 1)
+            x = torch.empty(n, in_raw, device="cuda")
+            t = torch.empty(n, nout, device="cuda")
+            dummy = torch.zeros(1, device="cuda")
             torch.cuda.synchronize()
-            e0.record(stream)
-            sim.step(None, 4)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1))
-            st = sim.stats()
-            its.append(st["niter_sum"] / 4.0)
-            itmax.append(st["niter_max"])
-        its = np.concatenate(its)
-        out = dict(workload=f"{a.what} {a.cone} condim {a.condim}", envs=a.envs, ms_per_control_step=float(np.median(ms)),
-                   env_steps_per_s=a.envs * 1e3 / float(np.median(ms)), newton_iter_mean=float(its.mean()),
-                   newton_iter_p99=float(np.percentile(its, 99)), newton_iter_max=int(np.max(itmax)), ncon_mean=float(st["ncon"].mean()),
-                   nefc_mean=float(st["nefc"].mean()), status=[int(x) for x in np.unique(st["status"])], shape=sim.launch_shape())
-        print(json.dumps(out))
+            got = col.warmstart_collect(dummy.data_ptr(), 1, a.train_substeps, x.data_ptr(), t.data_ptr(), n)
+            net = mjb200.WarmStart(in_raw, nout, seed=906)
+            net.fit_normalization(x.data_ptr(), t.data_ptr(), got)
+            _, hist = net.train(x.data_ptr(), t.data_ptr(), got, epochs=a.train_epochs, batch=4096, lr=1e-3, seed=907)
+            print(json.dumps(dict(train_rows=got, layout=[in_raw, nout, rpe], epoch_loss=[float(h) for h in hist])))
+            del x, t
+            col.close()
+        modes = ("plain", "learned") if a.learned else ("plain",)
+        for mode in modes:
+            s2 = sim if mode == "plain" else mjb200.BatchedSim(m, a.envs, record=0, ncon_max=ncon, nefc_max=ncon * rows)
+            if mode == "learned":
+                s2.set_warmstart(net)
+                s2.set_state(q.astype(np.float32), v.astype(np.float32))
+                s2.step(None, 20)
+                s2.sync()
+            else:
+                s2.set_state(q.astype(np.float32), v.astype(np.float32))
+                s2.step(None, 20)
+                s2.sync()
+            stream = torch.cuda.ExternalStream(s2.stream())   # the sim launches on its own stream
+            ms, its, itmax, chosen = [], [], [], []
+            for c in range(a.ctrl):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(stream)
+                s2.step(None, 4)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                st = s2.stats()
+                its.append(st["niter_sum"] / 4.0)
+                itmax.append(st["niter_max"])
+                chosen.append(st["warm_choice"])
+            its = np.concatenate(its)
+            out = dict(workload=f"{a.what} {a.cone} condim {a.condim}", mode=mode, envs=a.envs, ms_per_control_step=float(np.median(ms)),
+                       env_steps_per_s=a.envs * 1e3 / float(np.median(ms)), newton_iter_mean=float(its.mean()),
+                       newton_iter_p99=float(np.percentile(its, 99)), newton_iter_max=int(np.max(itmax)),
+                       learned_choice_share=float(np.mean(np.concatenate(chosen) == 2)), ncon_mean=float(st["ncon"].mean()),
+                       nefc_mean=float(st["nefc"].mean()), status=[int(x) for x in np.unique(st["status"])], shape=s2.launch_shape())
+            print(json.dumps(out))
         return
 
     m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
