@@ -81,6 +81,7 @@ def main(argv=None):
     ap.add_argument("--condim", type=int, default=3, help="bin / convex: contact dimensionality")
     ap.add_argument("--time", action="store_true", help="bin / convex: time the control steps with CUDA events")
     ap.add_argument("--learned", action="store_true", help="bin --time: also train the per-body warm start and time it")
+    ap.add_argument("--stages", action="store_true", help="bin --time: per-stage share of the warps' cycles over one control step")
     ap.add_argument("--train-substeps", type=int, default=24, help="bin --learned: substeps of the collection rollout")
     ap.add_argument("--train-epochs", type=int, default=8)
     a = ap.parse_args(argv)
@@ -182,6 +183,12 @@ def main(argv=None):
                        learned_choice_share=float(np.mean(np.concatenate(chosen) == 2)), ncon_mean=float(st["ncon"].mean()),
                        nefc_mean=float(st["nefc"].mean()), status=[int(x) for x in np.unique(st["status"])], shape=s2.launch_shape())
             print(json.dumps(out))
+            if a.stages and mode == "plain":
+                s2.stage_timing(1)
+                s2.step(None, 4)
+                cyc = s2.stage_timing(0)
+                tot = sum(cyc.values()) or 1
+                print(json.dumps({k: round(v / tot, 4) for k, v in cyc.items() if v}))
         return
 
     m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
