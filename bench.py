@@ -10,8 +10,8 @@ step.  Data are synthetic (seeded Philox), there is no dataset.
 
   value   whole-job env-steps/s of the learned-warm-start engine with the
           per-step controls already resident in HBM (device-to-device copy
-          into the sim, then per substep: feature gather + 4 tcgen05 GEMMs of
-          the MLP + the step kernel), CUDA events on the sim's stream, L2
+          into the sim, then per substep: the fused tcgen05 inference kernel
+          (feature gather and the MLP's 4 layers) + the step kernel), CUDA events on the sim's stream, L2
           flushed (256 MB write) before every timed step.  The net is trained
           first, on the GPU, from plain rollouts with disjoint seeds
           (--train-ctrl-steps x 4 substeps x envs pairs, --train-epochs).
@@ -365,7 +365,8 @@ def run_ours(args, world, rank, local):
             "data": "synthetic", "config": workload_config(B),
             "e2e": {"value": L["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,
-            "gpu_launches": K * SUBSTEPS * 6,
+            # learned path: per substep one fused inference kernel (mlp_infer_kernel) and one step kernel
+            "gpu_launches": K * SUBSTEPS * 2,
             "solver": {"value_is": "learned warm start (previous-step and qacc_smooth candidates kept as fallback), same tolerance 1e-8",
                        "learned": L, "plain": P, "learned_over_plain": L["value"] / P["value"],
                        "learned_first_substep": res["learned_first"],
