@@ -89,26 +89,38 @@ MJMLX_API int mjb200_batched_get_qacc_warmstart(MjmlxBatchedSim* sim, float* qac
 MJMLX_API int mjb200_batched_set_qacc_warmstart(MjmlxBatchedSim* sim, const float* qacc);
 /* Allocation-free step.  No counterpart in the reference.
  *
- * For callers that must not have the library allocate device memory while
- * they step: code recording the step into a CUDA graph by stream capture,
- * programs that reserve their whole device memory budget up front, real-time
- * control loops that cannot wait on an allocator.  Runs n physics steps of
- * the sim's model(s) on state held in the caller's device buffers, laid out
- * like the sim's own (mjb200_batched_layout offsets): qpos[total_q],
- * qvel[total_v], ctrl[total_u] (may be NULL when total_u == 0) and
- * qacc_warmstart[total_v] (zeros for a cold start), all updated in place.
- * The launch is ordered on `stream` (cudaStream_t; NULL = legacy default
- * stream).  Per-env statistics of the call are not kept (mjb200_batched_stats
- * still reports the sim's own last step).
+ * For callers that cannot let a library allocate device memory while they
+ * step: a trainer that hands all free device memory to its own caching
+ * allocator at start-up (cudaMalloc then fails or fragments its pool), a
+ * real-time control loop that cannot wait on cudaMalloc / cudaFree (they may
+ * synchronise the device), a host that fixes its device-memory budget when it
+ * starts.  Runs n physics steps of the sim's model(s) on state held in the
+ * caller's device buffers, laid out like the sim's own (mjb200_batched_layout
+ * offsets): qpos[total_q], qvel[total_v], ctrl[total_u] (may be NULL when
+ * total_u == 0) and qacc_warmstart[total_v] (zeros for a cold start), all
+ * updated in place, with the sim's own launch shape, so the results equal
+ * the regular step's.  The launch is ordered on `stream` (cudaStream_t;
+ * NULL = legacy default stream).
+ *
+ * What it leaves out: per-env statistics of the call are not kept
+ * (mjb200_batched_stats still reports the sim's own last step); sensors are
+ * not computed (sensordata and the accelerometer history keep the sim's own
+ * last step); a learned warm-start net attached to the sim is not used (the
+ * previous-step warm start in qacc_warmstart is); recorded quantities (xpos,
+ * cfrc_ext, ...) are not written.  A model whose workspace needs the HBM
+ * workspace of the regular step (too large for shared memory) is refused
+ * with -1.
  *
  * Scratch comes from a fixed area inside the library, sized for at most
  * 65536 envs; a larger sim is rejected (return -2, mjb200_last_error says
- * why).  Make the first call on each device before any stream capture: it
- * looks up the scratch address once for that device.  The scratch is shared
- * by every sim on a device, so calls whose kernels may overlap in time race;
- * order them on one stream.
+ * why).  The first call on each device looks up the scratch area's device
+ * address and caches it; make that first call before any stream capture.
+ * The scratch is shared by every sim on a device and keeps the last call's
+ * contents, so calls whose kernels may overlap on the GPU race; order them
+ * on one stream.
  *
- * Returns 0 on success, -1 bad arguments, -2 too many envs, -3 CUDA error. */
+ * Returns 0 on success, -1 bad arguments or refused model, -2 too many envs,
+ * -3 CUDA error. */
 MJMLX_API int mjb200_batched_step_noalloc(MjmlxBatchedSim* sim, float* qpos, float* qvel, const float* ctrl, float* qacc_warmstart, int n,
                                           void* stream);
 /* Device pointers of the HBM-resident state (float, env-major records). */

@@ -1,32 +1,36 @@
 // Allocation-free physics step: mjb200_batched_step_noalloc.
 //
-// Some callers cannot let a library allocate device memory while they step:
-// code that records the step into a CUDA graph with stream capture (an
-// allocation inside the capture region fails or ends the capture), programs
-// that reserve their whole device memory budget up front, and real-time
-// control loops that must not wait on the allocator.  This entry point lets
-// them step a sim whose state lives in their own buffers, and allocates
-// nothing on any call.
+// Who cannot allocate: a training program that hands all free device memory
+// to its own caching allocator at start-up (an RL trainer that reserves the
+// GPU for its replay buffers and networks) finds cudaMalloc failing or
+// fragmenting its pool; a real-time control loop cannot wait on cudaMalloc /
+// cudaFree, which may synchronise the device and take milliseconds; a host
+// process that fixes its device-memory budget when it starts may not let a
+// library grow it later.  This entry point steps a sim whose state lives in
+// the caller's own device buffers and allocates nothing on any call.
 //
-// Scratch: the kernel's variant with the persistent work queue needs a queue
-// head and six per-env statistics arrays.  They live in the file-scope device
-// array below, sized for MJB200_NOALLOC_MAX_ENVS envs (about 1.5 MB per GPU,
-// part of the library image, held until the process exits).  A sim with more
-// envs is rejected with an error; it never reads or writes past the array.
+// Scratch: the step kernel needs a work-queue head (independent-warp launch
+// mode) and six per-env statistics arrays.  They live in the file-scope
+// device array below, sized for MJB200_NOALLOC_MAX_ENVS envs (about 1.5 MB
+// per GPU, part of the library image, held by every GPU that loads the
+// library until the process exits).  A sim with more envs is rejected with an
+// error; the kernel never reads or writes past the array.
 //
-// Set-up: the array's device address is looked up with cudaGetSymbolAddress
-// once per device, on the first call made on that device, and cached.  That
-// first lookup may initialise the CUDA context, so make the first call on
-// each device before any stream capture begins.
+// Set-up: in host code the array's name is a host-side stand-in, not a
+// device address.  The device address is looked up with cudaGetSymbolAddress
+// on the first call made on each device (with that device current) and
+// cached; that lookup may initialise the device's CUDA context, so make the
+// first call on each device before any stream capture begins.
 //
-// What must start at zero: only the work-queue head; every call clears it on
-// the caller's stream before the launch.  The statistics are overwritten by
-// each launch.
+// What must start at zero: only the work-queue head; every call that uses
+// the queue clears it on the caller's stream before the launch.  The
+// statistics are overwritten by each launch, and the array keeps the last
+// call's contents.
 //
 // Concurrency: the scratch is shared by every sim on the device.  Two calls
-// whose kernels overlap (different streams, different threads, different
-// sims) race on the queue head and the statistics; order them on one stream
-// or synchronise between them.
+// whose kernels overlap on the GPU (different streams, different threads,
+// different sims) race on the queue head and the statistics; order them on
+// one stream or synchronise between them.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -38,7 +42,6 @@
 #include "step_params.h"
 
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
-cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int convex, int* blocks_per_sm);
 
 #define MJB200_NOALLOC_MAX_ENVS 65536
 #define MJB200_NOALLOC_HEAD_WORDS 64  // queue head, padded to 256 bytes
@@ -48,7 +51,6 @@ static __device__ __align__(256) int g_mjb200_noalloc_scratch[MJB200_NOALLOC_HEA
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr int kWarpsPerBlock = 4;
 std::mutex g_scratch_mutex;
 int* g_scratch_addr[kMaxDevices] = {};
 
@@ -94,18 +96,17 @@ extern "C" MJMLX_API int mjb200_batched_step_noalloc(MjmlxBatchedSim* sim, float
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* scratch = nullptr;
   cudaError_t e = scratch_address(&scratch);
-  const size_t smem = (size_t)kWarpsPerBlock * (E.desc_words() + E.ws_stride()) * 4;
-  int bps = 0;
-  if (e == cudaSuccess) e = mjb_occupancy(kWarpsPerBlock, smem, E.convex() ? 1 : 0, &bps);
-  if (e == cudaSuccess && bps < 1) e = cudaErrorInvalidConfiguration;
-  if (e == cudaSuccess) e = cudaMemsetAsync(scratch, 0, sizeof(int), s);
   if (e == cudaSuccess) {
-    const int groups = (E.num_envs() + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    int grid = E.sm_count() * bps;
-    if (grid > groups) grid = groups;
-    if (grid < 1) grid = 1;
-    StepParams P = E.external_params(qpos, qvel, ctrl, qacc_warmstart, n, scratch, scratch + MJB200_NOALLOC_HEAD_WORDS);
-    e = mjb_launch_step(P, grid, kWarpsPerBlock, smem, s);
+    // the sim's own launch shape (chosen, and its shared-memory limit set,
+    // when the sim was created): the same stage code in the same mapping as
+    // the regular step, so the results are the same
+    int grid = 1, warps = 1, smem = 0, persistent = 0;
+    E.launch_shape(&grid, &warps, &smem, &persistent);
+    const bool queue = persistent && !E.lockstep();
+    StepParams P = E.external_params(qpos, qvel, ctrl, qacc_warmstart, n, queue ? scratch : nullptr, scratch + MJB200_NOALLOC_HEAD_WORDS);
+    P.lockstep = E.lockstep();
+    if (queue) e = cudaMemsetAsync(scratch, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = mjb_launch_step(P, grid, warps, (size_t)smem, s);
   }
   if (e != cudaSuccess) {
     mjb::set_error(std::string("mjb200_batched_step_noalloc: ") + cudaGetErrorString(e));

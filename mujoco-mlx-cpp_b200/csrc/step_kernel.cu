@@ -7,6 +7,8 @@
 // (src/batched.cpp:980-1228).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "dev_solver.cuh"
 #include "step_params.h"
 
@@ -608,13 +610,36 @@ __global__ void __launch_bounds__(512) mjb_geom_pose_kernel(StepParams P, float*
   }
 }
 
+namespace {
+
+// The dynamic shared-memory limit of a kernel is a function attribute of the
+// current device.  Every launch and occupancy query goes through this helper,
+// which only ever raises the attribute and remembers, per device and kernel,
+// the largest value set so far; a sim created later with a smaller workspace
+// therefore never lowers the limit below what an earlier sim launches with.
+constexpr int kAttrDevices = 64;
+enum { kAttrStep = 0, kAttrStepConvex = 1, kAttrGeomPose = 2, kAttrKernels = 3 };
+std::mutex g_attr_mutex;
+size_t g_attr_smem[kAttrDevices][kAttrKernels];
+
+template <class Kernel>
+cudaError_t raise_smem_limit(Kernel kernel, int slot, size_t smem_bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kAttrDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  if (smem_bytes <= g_attr_smem[dev][slot]) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  if (e == cudaSuccess) g_attr_smem[dev][slot] = smem_bytes;
+  return e;
+}
+
+}  // namespace
+
 cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
-  static size_t configured = 0;
-  if (smem_bytes > configured) {
-    cudaError_t e = cudaFuncSetAttribute(mjb_geom_pose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (e != cudaSuccess) return e;
-    configured = smem_bytes;
-  }
+  cudaError_t e = raise_smem_limit(mjb_geom_pose_kernel, kAttrGeomPose, smem_bytes);
+  if (e != cudaSuccess) return e;
   int grid = (P.num_envs + warps_per_block - 1) / warps_per_block;
   if (P.gws && grid > P.gws_blocks) grid = P.gws_blocks;   // one HBM workspace per resident warp
   mjb_geom_pose_kernel<<<grid, warps_per_block * 32, smem_bytes, stream>>>(P, gpose, ng_max);
@@ -624,26 +649,21 @@ cudaError_t mjb_launch_geom_pose(const StepParams& P, float* gpose, int ng_max, 
 // P.convex selects the instance with the GJK / EPA collider (models with
 // general convex pairs); both instances share every other stage.
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream) {
-  static size_t configured[2] = {0, 0};
-  const int k = P.convex ? 1 : 0;
-  if (smem_bytes > configured[k]) {
-    cudaError_t e = k ? cudaFuncSetAttribute(mjb_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes)
-                      : cudaFuncSetAttribute(mjb_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-    if (e != cudaSuccess) return e;
-    configured[k] = smem_bytes;
-  }
-  if (k) mjb_step_kernel<true><<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
+  cudaError_t e = P.convex ? raise_smem_limit(mjb_step_kernel<true>, kAttrStepConvex, smem_bytes)
+                           : raise_smem_limit(mjb_step_kernel<false>, kAttrStep, smem_bytes);
+  if (e != cudaSuccess) return e;
+  if (P.convex) mjb_step_kernel<true><<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
   else mjb_step_kernel<false><<<grid, warps_per_block * 32, smem_bytes, stream>>>(P);
   return cudaGetLastError();
 }
 
 cudaError_t mjb_occupancy(int warps_per_block, size_t smem_bytes, int convex, int* blocks_per_sm) {
   if (convex) {
-    cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    cudaError_t e = raise_smem_limit(mjb_step_kernel<true>, kAttrStepConvex, smem_bytes);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel<true>, warps_per_block * 32, smem_bytes);
   }
-  cudaError_t e = cudaFuncSetAttribute(mjb_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  cudaError_t e = raise_smem_limit(mjb_step_kernel<false>, kAttrStep, smem_bytes);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, mjb_step_kernel<false>, warps_per_block * 32, smem_bytes);
 }

@@ -1,10 +1,14 @@
 """The allocation-free step (mjb200_batched_step_noalloc) against the regular
 device step (mjb200_batched_step_device_ctrl) on the same inputs.
 
-Both paths run the same stage code; only the launch mapping (persistent work
-queue vs block lockstep) and the buffers differ, so after each of two calls in
-a row the states must agree to max |d| <= 1e-5.  The file name keeps it last
-in collection order so that it also runs after every other GPU test.
+The allocation-free step exists for callers that cannot have the library
+allocate device memory while they step: trainers that give all free device
+memory to their own caching allocator, real-time loops that cannot wait on
+cudaMalloc / cudaFree, hosts with a fixed device-memory budget.  It runs the
+same stage code with the sim's own launch shape, so after each of two calls
+in a row the states must agree with the regular step's to max |d| <= 1e-5
+(they are bitwise equal in practice).  The file name keeps it last in
+collection order so that it also runs after every other GPU test.
 """
 import numpy as np
 import pytest
@@ -13,32 +17,30 @@ import mjb200
 
 pytestmark = pytest.mark.gpu
 
-B = 96
 NSUB = 4
 
 
-def test_noalloc_matches_regular_step_twice(quad_model):
+def _compare_two_calls(model, qpos, qvel, ctrls):
     import torch
 
-    qpos, qvel = mjb200.models.quadruped_initial_state(B)
-    qpos = qpos.astype(np.float32)
-    qvel = qvel.astype(np.float32)
-    ctrls = [mjb200.models.quadruped_controls(B, k).astype(np.float32) for k in range(2)]
-
-    ref = mjb200.BatchedSim(quad_model, B)
+    B = qpos.shape[0]
+    ref = mjb200.BatchedSim(model, B)
     ref.set_state(qpos, qvel)
-    sim = mjb200.BatchedSim(quad_model, B)
+    sim = mjb200.BatchedSim(model, B)
     dev = torch.device("cuda:0")
     qp_t = torch.from_numpy(qpos.reshape(-1).copy()).to(dev)
     qv_t = torch.from_numpy(qvel.reshape(-1).copy()).to(dev)
     warm_t = torch.zeros(qvel.size, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    for k in range(2):
-        ctrl_t = torch.from_numpy(ctrls[k].reshape(-1).copy()).to(dev)
+    for k, c in enumerate(ctrls):
+        ctrl_t = torch.from_numpy(c.reshape(-1).copy()).to(dev) if c is not None else None
         torch.cuda.synchronize()
-        ref.step_device_ctrl(ctrl_t.data_ptr(), NSUB)
+        if ctrl_t is not None:
+            ref.step_device_ctrl(ctrl_t.data_ptr(), NSUB)
+        else:
+            ref.step_device(NSUB)
         ref.sync()
-        rc = sim.step_noalloc(qp_t.data_ptr(), qv_t.data_ptr(), ctrl_t.data_ptr(), warm_t.data_ptr(), NSUB, stream)
+        rc = sim.step_noalloc(qp_t.data_ptr(), qv_t.data_ptr(), ctrl_t.data_ptr() if ctrl_t is not None else 0, warm_t.data_ptr(), NSUB, stream)
         assert rc == 0, mjb200.capi.last_error()
         torch.cuda.synchronize()
         rq, rv = ref.state()
@@ -48,7 +50,54 @@ def test_noalloc_matches_regular_step_twice(quad_model):
         assert np.abs(gq - rq).max() <= 1e-5, f"call {k}: qpos differs by {np.abs(gq - rq).max():.3g}"
         assert np.abs(gv - rv).max() <= 1e-5 * max(1.0, np.abs(rv).max()), f"call {k}: qvel differs by {np.abs(gv - rv).max():.3g}"
         # the state moved: the comparison is not between two untouched copies
-        assert np.abs(gq - qpos).max() > 1e-4
+        assert np.abs(gq - qpos.reshape(gq.shape)).max() > 1e-4
+    ref.close()
+    sim.close()
+
+
+def test_noalloc_matches_regular_step_twice(quad_model):
+    B = 96
+    qpos, qvel = mjb200.models.quadruped_initial_state(B)
+    ctrls = [mjb200.models.quadruped_controls(B, k).astype(np.float32) for k in range(2)]
+    _compare_two_calls(quad_model, qpos.astype(np.float32), qvel.astype(np.float32), ctrls)
+
+
+def test_noalloc_convex_pile_matches_regular_step_twice():
+    """Kernel instance with the GJK / EPA collider (mixed convex bodies)."""
+    model = mjb200.load_model_from_string(mjb200.models.convex_pile_xml(6, seed=1))
+    q, v = mjb200.models.box_pile_state(model, 32, seed=4)
+    _compare_two_calls(model, q.astype(np.float32), v.astype(np.float32), [None, None])
+
+
+def test_noalloc_keeps_other_sims_launchable(quad_model):
+    """A large-workspace sim, then the allocation-free step of a sim with a
+    smaller workspace, then the large sim again: the shared-memory limit the
+    first sim launches with must still be in place."""
+    import torch
+
+    B = 64
+    big = mjb200.BatchedSim(quad_model, B)
+    qpos, qvel = mjb200.models.quadruped_initial_state(B)
+    ctrl = mjb200.models.quadruped_controls(B, 0).astype(np.float32)
+    big.set_state(qpos.astype(np.float32), qvel.astype(np.float32))
+    big.step(ctrl, NSUB)
+    small_model = mjb200.load_model_from_string(mjb200.models.chain_xml(2, "free"))
+    small = mjb200.BatchedSim(small_model, 8)
+    assert small.launch_shape()["smem_bytes"] < big.launch_shape()["smem_bytes"]
+    qp, qv, c, w = small.device_state()
+    assert small.step_noalloc(qp, qv, c, w, 2, small.stream()) == 0, mjb200.capi.last_error()
+    small.sync()
+    big.step(ctrl, NSUB)
+    q2, v2 = big.state()
+    assert np.isfinite(q2).all() and np.all(big.stats()["status"] == 0)
+    # the same two steps on a fresh sim give the same state
+    again = mjb200.BatchedSim(quad_model, B)
+    again.set_state(qpos.astype(np.float32), qvel.astype(np.float32))
+    again.step(ctrl, NSUB)
+    again.step(ctrl, NSUB)
+    q3, v3 = again.state()
+    assert np.array_equal(q2, q3) and np.array_equal(v2, v3)
+    torch.cuda.synchronize()
 
 
 def test_noalloc_rejects_oversized_sim(quad_model):
@@ -57,3 +106,13 @@ def test_noalloc_rejects_oversized_sim(quad_model):
     rc = sim.step_noalloc(qp, qv, ctrl, warm, 1, sim.stream())
     assert rc == -2
     assert "65536" in mjb200.capi.last_error()
+
+
+def test_noalloc_rejects_hbm_workspace_model():
+    """The 64-body bin needs the regular step's HBM workspace: refused with -1."""
+    model = mjb200.load_model_from_string(mjb200.models.bin_xml(64, seed=0))
+    sim = mjb200.BatchedSim(model, 2)
+    qp, qv, ctrl, warm = sim.device_state()
+    rc = sim.step_noalloc(qp, qv, ctrl, warm, 1, sim.stream())
+    assert rc == -1
+    assert "HBM workspace" in mjb200.capi.last_error()
