@@ -121,6 +121,8 @@ void oracle_collide(const OModel* m, OData* d);
 void oracle_make_constraints(const OModel* m, OData* d, const ORand* r);
 void oracle_solve(const OModel* m, OData* d, int max_iter);
 void oracle_integrate(const OModel* m, OData* d);
+/* contact wrench per body (cfrc_ext) from the solved contact rows */
+void oracle_cfrc_ext(const OModel* m, OData* d, const ORand* r);
 
 /* one full physics step (mj_step with the Euler integrator); max_iter <= 0
  * uses the model's iteration count */

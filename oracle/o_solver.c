@@ -634,6 +634,60 @@ static void reset_env(const OModel* m, OData* d) {
   memset(d->qacc_warmstart, 0, m->nv * sizeof(double));
 }
 
+/* Contact wrench per body after the solve, cfrc_ext[6 nb] = (torque, force)
+ * in com-based coordinates: torque about the subtree COM of the body's root.
+ * Follows the reference's mjmlx_cfrc_ext aggregation
+ * (src/compat/mkx_kernels/solver.hpp:906-929: per contact, geom 2's body gets
+ * +F and geom 1's body -F) with MuJoCo's contact wrench (mj_contactForce /
+ * mj_rnePostConstraint semantics, unverified vs MuJoCo C until
+ * cross-checked) where the reference keeps only the normal force and no
+ * torque: pyramidal rows decode to the normal force sum f_n = sum_k f_k and
+ * per direction mu_d (f_2d - f_2d+1); elliptic rows are the normal and
+ * friction forces themselves; world force F = f_n n + f_1 t1 + f_2 t2,
+ * torsional / rolling torque T = f_3 n + f_4 t1 + f_5 t2; each side adds
+ * (p - subtree_com[root]) x F + T to the torque. */
+void oracle_cfrc_ext(const OModel* m, OData* d, const ORand* rnd) {
+  memset(d->cfrc_ext, 0, 6 * m->nbody * sizeof(double));
+  const double fs = rnd ? rnd->friction_scale : 1.0;
+  for (int c = 0; c < d->ncon; c++) {
+    const double* con = &d->contact[ORACLE_CONTACT_STRIDE * c];
+    const int r = (int)con[19];
+    if (r < 0) continue;
+    const int pair = (int)con[13];
+    const int* pi = &m->pair_int[6 * pair];
+    const double* pr = &m->pair_real[16 * pair];
+    const int dim = pi[4];
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    if (d->efc_type[r] == T_ELLIPTIC) {
+      for (int k = 0; k < dim; k++) f[k] = d->efc_force[r + k];
+    } else if (dim == 1) {
+      f[0] = d->efc_force[r];
+    } else {
+      for (int k = 0; k < 2 * (dim - 1); k++) f[0] += d->efc_force[r + k];
+      for (int k = 0; k + 1 < dim; k++) f[1 + k] = pr[2 + k] * fs * (d->efc_force[r + 2 * k] - d->efc_force[r + 2 * k + 1]);
+    }
+    const double* n = con + 3;
+    const double* t1 = con + 6;
+    const double* t2 = con + 9;
+    double F[3], T[3];
+    for (int k = 0; k < 3; k++) {
+      F[k] = f[0] * n[k] + f[1] * t1[k] + f[2] * t2[k];
+      T[k] = f[3] * n[k] + f[4] * t1[k] + f[5] * t2[k];
+    }
+    for (int side = 0; side < 2; side++) {
+      const int body = side == 0 ? pi[3] : pi[2];
+      const double sg = side == 0 ? 1.0 : -1.0;
+      const double* rc = &d->subtree_com[3 * m->body_rootid[body]];
+      double off[3] = {con[0] - rc[0], con[1] - rc[1], con[2] - rc[2]}, tq[3];
+      o_cross(off, F, tq);
+      for (int k = 0; k < 3; k++) {
+        d->cfrc_ext[6 * body + k] += sg * (tq[k] + T[k]);
+        d->cfrc_ext[6 * body + 3 + k] += sg * F[k];
+      }
+    }
+  }
+}
+
 void oracle_step(const OModel* m, OData* d, const ORand* r, int max_iter) {
   if (max_iter <= 0) max_iter = m->iterations;
   d->status = 0;
@@ -649,6 +703,7 @@ void oracle_step(const OModel* m, OData* d, const ORand* r, int max_iter) {
   oracle_collide(m, d);
   oracle_make_constraints(m, d, r);
   oracle_solve(m, d, max_iter);
+  oracle_cfrc_ext(m, d, r);
   for (int i = 0; i < m->nv; i++)
     if (bad(d->qacc[i])) {
       reset_env(m, d);

@@ -117,6 +117,50 @@ def test_resting_sphere_supports_its_weight():
     # the pyramid rows' forces sum to the normal force
     assert env.efc()["force"].sum() == pytest.approx(m_ * G, rel=1e-4)
     assert -2e-3 < env.a["qpos"][2] - 0.1 < 0
+    # the contact wrench on the sphere is its weight upward through its COM,
+    # and the world body takes the opposite force
+    cf = env.a["cfrc_ext"].reshape(-1, 6)
+    assert cf[1, 3:] == pytest.approx([0.0, 0.0, m_ * G], rel=1e-4, abs=1e-6)
+    assert np.abs(cf[1, :3]).max() < 1e-9
+    assert cf[0, 3:] == pytest.approx([0.0, 0.0, -m_ * G], rel=1e-4, abs=1e-6)
+
+
+def test_cfrc_ext_sliding_box_friction_and_torque():
+    """A resting box on a plane, then kicked sideways: at rest the contact
+    wrench is the box's weight; after the kick the force is the decoded
+    pyramid force sum, F = sum_c (f_n n + mu (f_0 - f_1) t1 + mu (f_2 - f_3) t2),
+    with friction against the sliding direction, the torque is sum_c (p_c -
+    com) x F_c about the box's COM (its subtree COM), and the world body
+    takes the opposite force.  The pair's friction is the larger of the
+    plane's (1.0) and the box's."""
+    mu, mass = 1.0, 1.0
+    xml = wrap(PLANE + '<body pos="0 0 0.05"><freejoint/><geom type="box" size="0.05 0.05 0.05" mass="%g" friction="%g 0.005 0.0001"/></body>'
+               % (mass, mu))
+    om, env = env_from_xml(xml)
+    for _ in range(200):
+        env.step()
+    cf = env.a["cfrc_ext"].reshape(-1, 6)
+    assert cf[1, 3:] == pytest.approx([0.0, 0.0, mass * G], rel=1e-3, abs=1e-6)
+    env.a["qvel"][0] = 1.0
+    env.step()
+    cf = env.a["cfrc_ext"].reshape(-1, 6)
+    con = env.contacts()
+    assert env.d.ncon == 4
+    assert cf[1, 3:] == pytest.approx(-cf[0, 3:], abs=1e-9)
+    com = env.a["subtree_com"][3:6]
+    efc = env.efc()
+    F_sum, T = np.zeros(3), np.zeros(3)
+    for c in con:
+        r = int(c[19])
+        f = efc["force"][r:r + 4]
+        n, t1, t2 = c[3:6], c[6:9], c[9:12]
+        F = f.sum() * n + mu * (f[0] - f[1]) * t1 + mu * (f[2] - f[3]) * t2
+        F_sum += F
+        T += np.cross(c[:3] - com, F)
+    assert cf[1, 3:] == pytest.approx(F_sum, abs=1e-9)
+    assert cf[1, :3] == pytest.approx(T, abs=1e-9)
+    assert cf[1, 3] < -0.1 * cf[1, 5]   # friction opposes the +x slide
+    assert abs(cf[1, 1]) > 1e-3         # friction below the COM tips the box about y
 
 
 def test_joint_limit_and_frictionloss_rows():
