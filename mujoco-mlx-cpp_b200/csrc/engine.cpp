@@ -25,6 +25,9 @@ void check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// The zero fill runs on the legacy default stream, which the engine's
+// non-blocking streams are not ordered after; it is waited for here, so a
+// copy or kernel issued next on any stream cannot be overtaken by it.
 template <class T>
 void DevBuf<T>::alloc(size_t count) {
   release();
@@ -32,6 +35,7 @@ void DevBuf<T>::alloc(size_t count) {
   if (count) {
     check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
     check(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+    check(cudaStreamSynchronize(nullptr), "cudaMemset sync");
   }
 }
 template <class T>
@@ -431,12 +435,16 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
   desc_words_ = (int)(sizeof(DevModelDesc) / 4);
   std::vector<DevModelDesc> descs;
   for (auto& L : layouts_) descs.push_back(L.desc);
+  // copies ordered on the sim's stream (a blocking cudaMemcpy from pageable
+  // memory may return before its DMA lands, and the non-blocking stream is
+  // not ordered after the legacy stream it runs on)
   d_models_.alloc(descs.size());
-  check(cudaMemcpy(d_models_.p, descs.data(), descs.size() * sizeof(DevModelDesc), cudaMemcpyHostToDevice), "upload models");
+  check(cudaMemcpyAsync(d_models_.p, descs.data(), descs.size() * sizeof(DevModelDesc), cudaMemcpyHostToDevice, stream_), "upload models");
   d_itab_.alloc(h_itab_.size());
-  check(cudaMemcpy(d_itab_.p, h_itab_.data(), h_itab_.size() * 4, cudaMemcpyHostToDevice), "upload itab");
+  check(cudaMemcpyAsync(d_itab_.p, h_itab_.data(), h_itab_.size() * 4, cudaMemcpyHostToDevice, stream_), "upload itab");
   d_ftab_.alloc(h_ftab_.size());
-  check(cudaMemcpy(d_ftab_.p, h_ftab_.data(), h_ftab_.size() * 4, cudaMemcpyHostToDevice), "upload ftab");
+  check(cudaMemcpyAsync(d_ftab_.p, h_ftab_.data(), h_ftab_.size() * 4, cudaMemcpyHostToDevice, stream_), "upload ftab");
+  check(cudaStreamSynchronize(stream_), "upload sync");
 }
 
 void Engine::alloc_state() {
@@ -907,8 +915,8 @@ void Engine::get_qacc_warmstart(float* out) {
 }
 
 void Engine::set_qacc_warmstart(const float* in) {
+  check(cudaMemcpyAsync(warm_.p, in, sizeof(float) * tot_v_, cudaMemcpyHostToDevice, stream_), "set warm start");
   sync();
-  check(cudaMemcpy(warm_.p, in, sizeof(float) * tot_v_, cudaMemcpyHostToDevice), "set warm start");
 }
 
 void Engine::step_with_warmstart(const float* qacc, int n) {
@@ -935,20 +943,22 @@ void Engine::get_state(float* qpos, float* qvel) {
   sync();
 }
 
+// State setters copy on the sim's stream and wait: the next launch on that
+// stream is ordered after the copy, and the caller's buffer is free on return.
 void Engine::set_state(const float* qpos, const float* qvel) {
-  sync();
   feat_valid_ = false;
-  if (qpos) check(cudaMemcpy(qpos_.p, qpos, sizeof(float) * tot_q_, cudaMemcpyHostToDevice), "set qpos");
-  if (qvel) check(cudaMemcpy(qvel_.p, qvel, sizeof(float) * tot_v_, cudaMemcpyHostToDevice), "set qvel");
+  if (qpos) check(cudaMemcpyAsync(qpos_.p, qpos, sizeof(float) * tot_q_, cudaMemcpyHostToDevice, stream_), "set qpos");
+  if (qvel) check(cudaMemcpyAsync(qvel_.p, qvel, sizeof(float) * tot_v_, cudaMemcpyHostToDevice, stream_), "set qvel");
+  sync();
 }
 
 void Engine::set_env_state(int env, const float* qpos, const float* qvel) {
   if (env < 0 || env >= B_) return;
   feat_valid_ = false;
   const Model& m = *models_[h_model_[env]];
+  if (qpos) check(cudaMemcpyAsync(qpos_.p + h_qadr_[env], qpos, sizeof(float) * m.nq, cudaMemcpyHostToDevice, stream_), "set env qpos");
+  if (qvel) check(cudaMemcpyAsync(qvel_.p + h_vadr_[env], qvel, sizeof(float) * m.nv, cudaMemcpyHostToDevice, stream_), "set env qvel");
   sync();
-  if (qpos) check(cudaMemcpy(qpos_.p + h_qadr_[env], qpos, sizeof(float) * m.nq, cudaMemcpyHostToDevice), "set env qpos");
-  if (qvel) check(cudaMemcpy(qvel_.p + h_vadr_[env], qvel, sizeof(float) * m.nv, cudaMemcpyHostToDevice), "set env qvel");
 }
 
 void Engine::reset(const int* mask) {
@@ -1081,14 +1091,19 @@ int Engine::set_free_drag(const int* env_idx, int n, const float* drag_k) {
 void Engine::stage_timing(int enable, unsigned long long* out8) {
   sync();
   if (out8) {
-    if (timing_) check(cudaMemcpy(out8, stage_cycles_.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "stage cycles");
-    else std::memset(out8, 0, 8 * sizeof(unsigned long long));
+    if (timing_) {
+      check(cudaMemcpyAsync(out8, stage_cycles_.p, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_), "stage cycles");
+      sync();
+    } else {
+      std::memset(out8, 0, 8 * sizeof(unsigned long long));
+    }
   }
   if (enable >= 0) {
     bool on = enable != 0;
     if (on) {
       if (!stage_cycles_.p) stage_cycles_.alloc(16);
-      check(cudaMemset(stage_cycles_.p, 0, 16 * sizeof(unsigned long long)), "stage cycles reset");
+      check(cudaMemsetAsync(stage_cycles_.p, 0, 16 * sizeof(unsigned long long), stream_), "stage cycles reset");
+      sync();
     }
     if (on != timing_) invalidate_graphs();
     timing_ = on;

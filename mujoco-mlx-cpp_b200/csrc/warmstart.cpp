@@ -64,7 +64,8 @@ WarmStartNet::WarmStartNet(int in_raw, int nout, uint64_t seed) : in_raw_(in_raw
   wtb_.alloc(nweight_);
   err_.alloc(1);
   loss_.alloc(1);
-  check(cudaMemset(err_.p, 0, sizeof(int)), "warm start err");
+  check(cudaMemsetAsync(err_.p, 0, sizeof(int), stream_), "warm start err");
+  check(cudaStreamSynchronize(stream_), "warm start sync");
   // initial parameters: U(+-1/sqrt(fan_in)) on real inputs, output layer x0.1,
   // zero biases, zero weights on padded inputs / outputs
   std::vector<float> h(nparam_, 0.f);
@@ -86,20 +87,25 @@ WarmStartNet::~WarmStartNet() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
+// Copies and fills run on the net's own stream and are waited for (the
+// stream is non-blocking, so legacy-stream copies would not be ordered with
+// its kernels).
 int WarmStartNet::error_word() {
   int e = 0;
-  cudaMemcpy(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (cudaMemcpyAsync(&e, err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_) != cudaSuccess) return -1;
+  cudaStreamSynchronize(stream_);
   return e;
 }
 
 void WarmStartNet::get_params(float* host) const {
-  check(cudaMemcpy(host, params_.p, sizeof(float) * nparam_, cudaMemcpyDeviceToHost), "warm start get params");
+  check(cudaMemcpyAsync(host, params_.p, sizeof(float) * nparam_, cudaMemcpyDeviceToHost, stream_), "warm start get params");
+  check(cudaStreamSynchronize(stream_), "warm start sync");
 }
 
 void WarmStartNet::set_params(const float* host) {
-  check(cudaMemcpy(params_.p, host, sizeof(float) * nparam_, cudaMemcpyHostToDevice), "warm start set params");
-  check(cudaMemset(adam_m_.p, 0, sizeof(float) * nparam_), "adam m");
-  check(cudaMemset(adam_v_.p, 0, sizeof(float) * nparam_), "adam v");
+  check(cudaMemcpyAsync(params_.p, host, sizeof(float) * nparam_, cudaMemcpyHostToDevice, stream_), "warm start set params");
+  check(cudaMemsetAsync(adam_m_.p, 0, sizeof(float) * nparam_, stream_), "adam m");
+  check(cudaMemsetAsync(adam_v_.p, 0, sizeof(float) * nparam_, stream_), "adam v");
   adam_t_ = 0;
   for (int l = 0; l < kLayers; l++) check(cast_weights(rows_[l], cols_[l], P(l), W(l), WT(l), stream_), "cast weights");
   check(cudaStreamSynchronize(stream_), "warm start sync");
@@ -175,7 +181,8 @@ void WarmStartNet::ensure_batch(int n) {
   t_.alloc((size_t)cap * nout_);
   yf_.alloc((size_t)cap * kOutPad);
   zero_prev_.alloc((size_t)cap * nout_);
-  check(cudaMemset(zero_prev_.p, 0, sizeof(float) * cap * nout_), "zero prev");
+  check(cudaMemsetAsync(zero_prev_.p, 0, sizeof(float) * cap * nout_, stream_), "zero prev");
+  check(cudaStreamSynchronize(stream_), "warm start sync");
   cap_ = cap;
   maps_n_ = -1;
 }

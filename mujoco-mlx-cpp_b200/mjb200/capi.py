@@ -87,6 +87,8 @@ def _load():
         "mjb200_batched_set_warmstart": (C.c_int, [C.c_void_p, C.c_void_p]),
         "mjb200_warmstart_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+        "mjb200_gemm_bf16_gated": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_void_p,
+                                             C.c_void_p]),
         "mjb200_batched_get_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_pack_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -451,6 +453,15 @@ class BatchedSim:
         qp = None if qpos is None else np.ascontiguousarray(qpos, np.float32).reshape(-1)
         qv = None if qvel is None else np.ascontiguousarray(qvel, np.float32).reshape(-1)
         lib.mjmlx_batched_set_state(self.handle, _fp(qp), _fp(qv))
+
+    def set_env_state(self, env: int, qpos=None, qvel=None):
+        """One env's qpos / qvel (mjmlx_batched_set_env_qpos / _qvel)."""
+        if qpos is not None:
+            a = np.ascontiguousarray(qpos, np.float32).reshape(-1)
+            lib.mjmlx_batched_set_env_qpos(self.handle, env, _fp(a), a.size)
+        if qvel is not None:
+            a = np.ascontiguousarray(qvel, np.float32).reshape(-1)
+            lib.mjmlx_batched_set_env_qvel(self.handle, env, _fp(a), a.size)
 
     def reset(self, mask):
         m = np.ascontiguousarray(mask, np.int32)

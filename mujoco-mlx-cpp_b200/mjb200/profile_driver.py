@@ -5,12 +5,15 @@
     python -m mjb200.profile_driver learned --envs 4096 --ctrl 3
     python -m mjb200.profile_driver gemm    --rows 16384
     python -m mjb200.profile_driver sensitivity --envs 4096
+    python -m mjb200.profile_driver aux --envs 16384
 
 `step`: the quadruped workload (4 substeps per control step, seeded random
 position targets) on the plain solver; `learned`: the same after a short
 warm-start training (collect + 2 epochs) with the net attached; `gemm`: the
 MLP's forward GEMM shapes (rows x 192 -> 256 -> 256 -> 256 -> 64) and one
 weight-gradient shape (256 x 256, K = 4096), each launched `--repeat` times;
+`aux`: the small kernels (pack, reset, geom poses and rays, the training
+kernels around the GEMMs) at sizes above L2;
 `sensitivity`: Newton iterations of one substep from warm starts at known
 distances from the converged solution x* (x* + eps (previous - x*)), which
 bounds what any predicted warm start can save.
@@ -72,7 +75,7 @@ def _sensitivity(mjb200, m, B):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["step", "learned", "gemm", "sensitivity", "bin", "convex"])
+    ap.add_argument("what", choices=["step", "learned", "gemm", "sensitivity", "bin", "convex", "aux"])
     ap.add_argument("--envs", type=int, default=4096)
     ap.add_argument("--ctrl", type=int, default=3, help="control steps (4 substeps each)")
     ap.add_argument("--rows", type=int, default=16384)
@@ -103,6 +106,45 @@ def main(argv=None):
                     raise RuntimeError(mjb200.capi.last_error())
             torch.cuda.synchronize()
         print("gemm done")
+        return
+
+    if a.what == "aux":
+        # the engine's small kernels, each a few times at sizes above L2
+        # where the kernel scales: packed read-back (16384 envs), masked
+        # reset (16384 envs), geom poses + ray casts (4096 envs x 64 rays),
+        # and the training kernels (feature gather, column statistics, bias
+        # gradient sums, Adam) on 262144 rows of 129 inputs
+        m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
+        B = a.envs
+        sim = mjb200.BatchedSim(m, B)
+        q, v = mjb200.models.quadruped_initial_state_fast(B, seed=1000)
+        sim.set_state(q.astype(np.float32), v.astype(np.float32))
+        sim.step(mjb200.models.quadruped_controls_fast(B, 0, seed=2000).astype(np.float32), 4)
+        sim.set_pack_spec([4, 7, 10, 13], 6, 12)
+        for _ in range(a.repeat):
+            sim.pack_device()
+        sim.sync()
+        for _ in range(a.repeat):
+            sim.reset(np.ones(B, np.int32))
+        nb = min(B, 4096)
+        rs = mjb200.BatchedSim(m, nb)
+        g = np.random.default_rng(0)
+        pnt = np.zeros((nb, 64, 3), np.float32)
+        pnt[:, :, 2] = 1.0
+        pnt[:, :, :2] = g.uniform(-0.4, 0.4, size=(nb, 64, 2))
+        vec = np.zeros((nb, 64, 3), np.float32)
+        vec[:, :, 2] = -1.0
+        for _ in range(a.repeat):
+            rs.raycast(pnt, vec)
+        rows, width = 262144, 129
+        x = torch.randn(rows, width, device="cuda")
+        t = torch.randn(rows, m.nv, device="cuda")
+        net = mjb200.WarmStart(width, m.nv, seed=3)
+        torch.cuda.synchronize()
+        net.fit_normalization(x.data_ptr(), t.data_ptr(), rows)
+        net.train(x.data_ptr(), t.data_ptr(), rows, epochs=1, batch=4096, lr=1e-3, seed=4)
+        torch.cuda.synchronize()
+        print("aux done")
         return
 
     if a.what in ("bin", "convex"):
