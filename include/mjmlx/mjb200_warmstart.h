@@ -95,6 +95,17 @@ MJMLX_API int mjb200_warmstart_predict(MjbWarmStart* net, const float* feat_dev,
  * 0, -1 bad arguments, -3 CUDA error. */
 MJMLX_API int mjb200_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, void* stream);
 
+/* The same GEMM with its failure path exposed, for tests of the bounded
+ * waits (no counterpart in the reference).  Before its first MMA each CTA
+ * waits for the device word *gate_dev to become nonzero; every wait of the
+ * kernel gives up after wait_limit_s seconds (0 < wait_limit_s <= 2).  A
+ * CTA whose wait gave up writes nothing to C, sets *err_dev (device int) to
+ * 1, lets its own TMA copies and MMAs finish, frees its TMEM and returns, so
+ * the context stays usable.  N 64, 128, 192 or 256.  Returns 0, -1 bad
+ * arguments, -3 CUDA error (the launch, not the wait: read *err_dev). */
+MJMLX_API int mjb200_gemm_bf16_gated(const void* A, const void* B, float* C, int M, int N, int K, const int* gate_dev, double wait_limit_s,
+                                     int* err_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -192,4 +192,34 @@ MJMLX_API int mjb200_gemm_bf16(const void* A, const void* B, float* C, int M, in
   return 0;
 }
 
+MJMLX_API int mjb200_gemm_bf16_gated(const void* A, const void* B, float* C, int M, int N, int K, const int* gate_dev, double wait_limit_s,
+                                     int* err_dev, void* stream) {
+  if (!A || !B || !C || !gate_dev || !err_dev || M <= 0 || K <= 0 || K % 64 != 0 || !(wait_limit_s > 0) || wait_limit_s > 2.0 ||
+      !(N == 64 || N == 128 || N == 192 || N == 256)) {
+    set_error("mjb200_gemm_bf16_gated: bad arguments");
+    return -1;
+  }
+  CUtensorMap ma, mb;
+  if (!mjb::make_tmap_bf16(&ma, A, M, K, 128) || !mjb::make_tmap_bf16(&mb, B, N, K, N)) {
+    set_error("mjb200_gemm_bf16_gated: tensor map encode failed (alignment or driver)");
+    return -1;
+  }
+  mjb::GemmArgs a{};
+  a.M = M;
+  a.N = N;
+  a.K = K;
+  a.mode = mjb::EPI_F32;
+  a.ldo = N;
+  a.out_f32 = C;
+  a.err = err_dev;
+  a.gate = gate_dev;
+  a.wait_limit_ns = (unsigned long long)(wait_limit_s * 1e9);
+  cudaError_t e = mjb::gemm_tn(ma, mb, a, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) {
+    set_error(std::string("mjb200_gemm_bf16_gated: ") + cudaGetErrorString(e));
+    return -3;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -40,9 +40,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Waits for the phase with the given parity; false when the CTA aborted or
 // the time limit passed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, unsigned long long limit_ns = kWaitLimitNs) {
   const uint32_t addr = smem_u32(bar);
   unsigned long long t0 = 0;
   for (uint32_t it = 0;; it++) {
@@ -59,8 +63,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     if ((it & 63) == 0) {
       unsigned long long t = global_ns();
       if (it == 0) t0 = t;
-      else if (t - t0 > kWaitLimitNs) return false;
+      else if (t - t0 > limit_ns) return false;
     }
+  }
+}
+
+// Waits until the device word *flag is nonzero; false when the CTA aborted
+// or the time limit passed.
+__device__ __forceinline__ bool flag_wait(const volatile int* flag, volatile int* abort_flag, unsigned long long limit_ns) {
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (*flag != 0) return true;
+    if (*abort_flag) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -139,6 +154,7 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int nk = a.K / BK;
+  const unsigned long long limit = a.wait_limit_ns ? a.wait_limit_ns : kWaitLimitNs;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -162,7 +178,7 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
   if (warp == 0 && lane == 0) {
     for (int kc = 0; kc < nk; kc++) {
       const int s = kc % STAGES;
-      if (kc >= STAGES && !mbar_wait(&empty[s], ((kc / STAGES) - 1) & 1, abort_flag)) {
+      if (kc >= STAGES && !mbar_wait(&empty[s], ((kc / STAGES) - 1) & 1, abort_flag, limit)) {
         *abort_flag = 1;
         break;
       }
@@ -173,9 +189,13 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
       issued = kc + 1;
     }
   } else if (warp == 1 && lane == 0) {
-    for (int kc = 0; kc < nk; kc++) {
+    int nmma = 0;
+    // test hook (a.gate): the first MMA waits for a device word; a word that
+    // nothing sets makes this bounded wait run out and the CTA abort
+    if (a.gate && !flag_wait(a.gate, abort_flag, limit)) *abort_flag = 1;
+    for (int kc = 0; kc < nk && !*abort_flag; kc++) {
       const int s = kc % STAGES;
-      if (!mbar_wait(&full[s], (kc / STAGES) & 1, abort_flag)) {
+      if (!mbar_wait(&full[s], (kc / STAGES) & 1, abort_flag, limit)) {
         *abort_flag = 1;
         break;
       }
@@ -185,11 +205,15 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
 #pragma unroll
       for (int k = 0; k < BK / 16; k++) mma_bf16(tmem, sw128_desc(sa + 32 * k), sw128_desc(sb + 32 * k), IDESC, (kc | k) != 0);
       mma_commit(&empty[s]);
+      nmma++;
     }
-    mma_commit(done);
+    // done completes once every MMA issued here has finished (a plain
+    // arrive when none was issued)
+    if (nmma) mma_commit(done);
+    else mbar_arrive(done);
   }
   __syncwarp();
-  const bool ok = mbar_wait(done, 0, abort_flag) && !*abort_flag;
+  const bool ok = mbar_wait(done, 0, abort_flag, limit) && !*abort_flag;
   __syncwarp();
   tc_fence_after();
 
@@ -280,10 +304,12 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
     }
   } else if (threadIdx.x == 0) {
     if (a.err) atomicExch(a.err, 1);
-    // let the TMA copies this thread issued land before the CTA's shared
-    // memory is released (each wait again bounded by the time limit)
+    // let the TMA copies this thread issued land, and the MMAs already
+    // issued finish, before the CTA's shared memory and TMEM are released
+    // (each wait again bounded by the time limit)
     volatile int no_abort = 0;
-    for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; kc++) mbar_wait(&full[kc % STAGES], (kc / STAGES) & 1, &no_abort);
+    for (int kc = issued > STAGES ? issued - STAGES : 0; kc < issued; kc++) mbar_wait(&full[kc % STAGES], (kc / STAGES) & 1, &no_abort, limit);
+    mbar_wait(done, 0, &no_abort, limit);
   }
   tc_fence_before();
   __syncthreads();
@@ -605,6 +631,8 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const __grid_constant
   const uint32_t tmem = *tmem_slot;
 
   int g = 0;  // K-chunk counter over all layers (ring stage and phase)
+  int issued = 0;   // chunks whose TMA load thread 0 issued (thread 0 only)
+  int lfail = 0;    // layer whose wait gave up
   bool ok = true;
 #pragma unroll 1
   for (int l = 0; l < 4 && ok; l++) {
@@ -619,8 +647,10 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const __grid_constant
         }
         mbar_expect_tx(&full[s], (uint32_t)(N * 128));
         tma_load_2d(ring + s * INF_STAGE_BYTES, maps[l], &full[s], c * 64, 0);
+        issued = gc + 1;
       }
     } else if (warp == 1 && lane == 0) {
+      int nmma = 0;
       for (int c = 0; c < nk; c++) {
         const int gc = g + c, s = gc % INF_STAGES;
         if (!mbar_wait(&full[s], (gc / INF_STAGES) & 1, abort_flag)) {
@@ -633,15 +663,22 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const __grid_constant
 #pragma unroll
         for (int k = 0; k < 4; k++) mma_bf16(tmem, sw128_desc(sa + 32 * k), sw128_desc(sb + 32 * k), idesc, (c | k) != 0);
         mma_commit(&empty[s]);
+        nmma++;
       }
-      mma_commit(done);
+      // this layer's phase of done completes once its MMAs have finished
+      // (a plain arrive when none was issued)
+      if (nmma) mma_commit(done);
+      else mbar_arrive(done);
     }
     g += nk;
     __syncwarp();
     ok = mbar_wait(done, l & 1, abort_flag) && !*abort_flag;
     __syncwarp();
     tc_fence_after();
-    if (!ok) break;
+    if (!ok) {
+      lfail = l;
+      break;
+    }
     // epilogue: TMEM lanes of this warp = its 32 rows
     const int r = warp * 32 + lane, env = m0 + r;
     const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
@@ -676,7 +713,16 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_kernel(const __grid_constant
     __syncthreads();
     tc_fence_after();
   }
-  if (!ok && threadIdx.x == 0 && a.err) atomicExch(a.err, 2);
+  if (!ok && threadIdx.x == 0) {
+    if (a.err) atomicExch(a.err, 2);
+    // let the TMA copies this thread issued land, and the layer's MMAs
+    // finish, before the CTA's shared memory and TMEM are released (each
+    // wait bounded by the time limit)
+    volatile int no_abort = 0;
+    for (int gc = issued > INF_STAGES ? issued - INF_STAGES : 0; gc < issued; gc++)
+      mbar_wait(&full[gc % INF_STAGES], (gc / INF_STAGES) & 1, &no_abort);
+    mbar_wait(done, lfail & 1, &no_abort);
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {

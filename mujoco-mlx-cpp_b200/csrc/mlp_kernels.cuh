@@ -37,6 +37,8 @@ struct GemmArgs {
   const float* ostd;
   float* pred;
   int* err;             // set to a nonzero code when a bounded wait gives up
+  const volatile int* gate;       // test hook (null in production): the first MMA waits, bounded, for *gate != 0
+  unsigned long long wait_limit_ns;  // limit of each bounded wait (0: 2 s)
 };
 
 // Encodes a 2-D bf16 row-major [rows][cols] tensor map with a box of

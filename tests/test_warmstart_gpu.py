@@ -222,3 +222,42 @@ def test_fused_inference_matches_unfused(B):
     assert np.isfinite(outs[0]).all()
     scale = np.abs(outs[1] - prev.cpu().numpy()).max()
     assert np.abs(outs[0] - outs[1]).max() <= 1e-3 * scale + 1e-6, np.abs(outs[0] - outs[1]).max() / scale
+
+
+def test_gemm_bounded_wait_gives_up_and_context_survives():
+    """Every mbarrier / flag wait of the tcgen05 GEMM is bounded.  A gate
+    word that nothing sets makes the first MMA's wait run out (limit 50 ms):
+    the kernel returns with the error word set and C untouched, and the next
+    GEMM on the same context is correct.  With the gate open the gated GEMM
+    gives the plain result."""
+    import time
+
+    M, N, K = 300, 256, 512
+    g = torch.Generator().manual_seed(5)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16).cuda()
+    B = torch.randn(N, K, generator=g).to(torch.bfloat16).cuda()
+    C = torch.full((M, N), float("nan"), device="cuda")
+    gate = torch.zeros(1, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = mjb200.capi.lib.mjb200_gemm_bf16_gated(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, gate.data_ptr(), 0.05, err.data_ptr(), None)
+    assert rc == 0, mjb200.capi.last_error()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    assert int(err.item()) == 1
+    assert torch.isnan(C).all()
+    assert dt < 5.0
+    ref = (A.double() @ B.double().T)
+    C2 = torch.full((M, N), float("nan"), device="cuda")
+    assert mjb200.gemm_bf16(A.data_ptr(), B.data_ptr(), C2.data_ptr(), M, N, K) == 0
+    torch.cuda.synchronize()
+    assert (C2.double() - ref).abs().max().item() <= 1e-5 * ref.abs().max().item()
+    gate.fill_(1)
+    err.zero_()
+    C3 = torch.full((M, N), float("nan"), device="cuda")
+    torch.cuda.synchronize()
+    assert mjb200.capi.lib.mjb200_gemm_bf16_gated(A.data_ptr(), B.data_ptr(), C3.data_ptr(), M, N, K, gate.data_ptr(), 0.5, err.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(C3, C2)
