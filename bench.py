@@ -178,25 +178,38 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_models():
+    """The workload generators (mjb200/models.py, plain numpy), loaded by file
+    path so that the CPU arm does not import the package, which loads the
+    product library."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("mjb200_workload_models", os.path.join(ROOT, "mujoco-mlx-cpp_b200", "mjb200", "models.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def cpu_reference(B, cpu_seconds, warmup=1):
-    """FP64 oracle on all host threads: env-steps/s over a bounded sample."""
+    """FP64 oracle on all host threads: env-steps/s over a bounded sample.
+    The model comes from the committed dump oracle/models/quadruped12.dump,
+    so this arm never loads libmjb200.so."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import mjb200
     import oracle
 
+    models = workload_models()
     nthread = os.cpu_count() or 1
-    m = mjb200.load_model_from_string(mjb200.models.quadruped_xml())
-    om = oracle.OracleModel(m.dump())
+    om = oracle.OracleModel(oracle.load_dump("quadruped12.dump"))
     Bs = min(B, 4096)
     ob = oracle.OracleBatch(om, Bs)
-    q, v = mjb200.models.quadruped_initial_state_fast(Bs)
+    q, v = models.quadruped_initial_state_fast(Bs)
     ob.set_state(q, v)
     for w in range(warmup):
-        ob.set_ctrl(mjb200.models.quadruped_controls_fast(Bs, w))
+        ob.set_ctrl(models.quadruped_controls_fast(Bs, w))
         ob.step(SUBSTEPS, nthread=nthread)
     n, t = 0, 0.0
     while t < cpu_seconds:
-        ob.set_ctrl(mjb200.models.quadruped_controls_fast(Bs, warmup + n))
+        ob.set_ctrl(models.quadruped_controls_fast(Bs, warmup + n))
         t0 = time.perf_counter()
         ob.step(SUBSTEPS, nthread=nthread)
         t += time.perf_counter() - t0
@@ -336,7 +349,10 @@ def run_ours(args, world, rank, local):
         e2e_s = replicas.reduce_over_ranks(time_e2e(sim, host_ctrl, K, W, flush, world), "max", device="cuda")
         # iteration statistics of the last timed env-step (per env: mean over
         # its 4 substeps; p99 over envs of the per-substep maximum)
+        q10, q50, q90 = np.percentile(step_ms, [10, 50, 90])
         res[mode] = {"value": world * B * K / total_s, "ms_per_step": 1e3 * total_s / K, "kernel_ms": statistics.mean(kern_ms),
+                     "ms_per_step_median": float(q50), "ms_per_step_p10": float(q10), "ms_per_step_p90": float(q90),
+                     "kernel_ms_median": float(np.median(kern_ms)),
                      "e2e": world * B * K / e2e_s, "newton_iter_mean": float(st["niter_sum"].mean() / SUBSTEPS),
                      "newton_iter_p99": float(np.percentile(st["niter_max"], 99)),
                      "predicted_warmstart_share": float(np.mean(st["warm_choice"] == 2)), "launch": sim.launch_shape()}
@@ -361,7 +377,8 @@ def run_ours(args, world, rank, local):
         return
     L, P = res["learned"], res["plain"]
     line = {"metric": METRIC, "value": L["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": L["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step": L["ms_per_step"], "ms_per_step_median": L["ms_per_step_median"], "ms_per_step_p10": L["ms_per_step_p10"],
+            "ms_per_step_p90": L["ms_per_step_p90"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(B),
             "e2e": {"value": L["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,

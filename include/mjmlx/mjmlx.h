@@ -165,6 +165,25 @@ MJMLX_API int mjmlx_batched_raycast(MjmlxBatchedSim* sim, const float* pnt, cons
 /* Wait for the last step.  Replaces mjmlx.h:252. */
 MJMLX_API void mjmlx_batched_eval_state(const MjmlxBatchedSim* sim);
 
+/* Camera sensor (replaces mjmlx.h:272-295, the reference's Vulkan renderer).
+ * Rendering needs a graphics stack, which this CUDA engine does not have:
+ * the functions are exported so that callers built against the reference's
+ * API (its Python RL binding among them) link unchanged, and they refuse at
+ * run time.  mjmlx_camera_create returns NULL with a message
+ * (mjb200_last_error); the int functions return -1 (count, draw-call count
+ * and gpu_supported return 0); free accepts NULL. */
+typedef struct MjmlxCameraRenderer MjmlxCameraRenderer;
+MJMLX_API MjmlxCameraRenderer* mjmlx_camera_create(MjmlxBatchedSim* sim, int width, int height);
+MJMLX_API void mjmlx_camera_free(MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_count(const MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_render(MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_draw_call_count(const MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_get_rgb(MjmlxCameraRenderer* r, uint8_t* out);
+MJMLX_API int mjmlx_camera_get_depth(MjmlxCameraRenderer* r, float* out);
+MJMLX_API int mjmlx_camera_gpu_supported(const MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_gpu_copy(MjmlxCameraRenderer* r);
+MJMLX_API int mjmlx_camera_gpu_export_fd(MjmlxCameraRenderer* r, int which, uint64_t* alloc_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -109,6 +109,26 @@ def _ptr(a, kind):
     return a.ctypes.data_as(_ip if kind == "i" else _dp)
 
 
+def parse_dump(text: str) -> dict:
+    """Arrays of a compiled-model dump (the text of mjb200_model_dump: per
+    line name, kind i / f, count, values)."""
+    out = {}
+    for line in text.splitlines():
+        parts = line.split()
+        if not parts:
+            continue
+        name, kind, n = parts[0], parts[1], int(parts[2])
+        vals = parts[3:3 + n]
+        out[name] = np.array([int(v) for v in vals], np.int64) if kind == "i" else np.array([float(v) for v in vals], np.float64)
+    return out
+
+
+def load_dump(name: str) -> dict:
+    """A committed model dump from oracle/models/ (see make_model_dumps.py)."""
+    with open(os.path.join(HERE, "models", name)) as f:
+        return parse_dump(f.read())
+
+
 class OracleModel:
     """OModel built from a model dump (dict of numpy arrays)."""
 

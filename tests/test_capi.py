@@ -92,3 +92,21 @@ def test_model_info_and_null_handling(quad_model):
     null = capi.lib.mjmlx_model_info(None)
     assert (null.nq, null.nv) == (0, 0)
     assert capi.lib.mjmlx_name2id(None, 1, b"trunk") == -1
+
+
+def test_camera_api_is_exported_and_refuses():
+    """The reference's camera renderer is graphics (Vulkan); the entry points
+    exist so its callers link, and they refuse with a message."""
+    lib = C.CDLL(capi.LIB_PATH)
+    lib.mjmlx_camera_create.restype = C.c_void_p
+    lib.mjmlx_camera_create.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    assert lib.mjmlx_camera_create(None, 64, 48) is None
+    assert "graphics" in capi.last_error()
+    for fn in ("mjmlx_camera_render", "mjmlx_camera_gpu_copy"):
+        getattr(lib, fn).argtypes = [C.c_void_p]
+        assert getattr(lib, fn)(None) == -1
+    lib.mjmlx_camera_count.argtypes = [C.c_void_p]
+    lib.mjmlx_camera_gpu_supported.argtypes = [C.c_void_p]
+    assert lib.mjmlx_camera_count(None) == 0 and lib.mjmlx_camera_gpu_supported(None) == 0
+    lib.mjmlx_camera_free.argtypes = [C.c_void_p]
+    lib.mjmlx_camera_free(None)

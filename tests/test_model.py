@@ -108,3 +108,16 @@ def test_dump_roundtrip_sizes(quad_model):
     assert d["qpos0"].size == nq and d["dof_armature"].size == nv
     assert d["body_mass"].size == nbody and d["jnt_type"].size == njnt and d["geom_type"].size == ngeom
     assert d["body_mass"][1:].sum() == pytest.approx(6.0 + 4 * (3 * 0.7) + 4 * 0.0, rel=0.2)
+
+
+def test_committed_oracle_dump_matches_compiler(quad_model):
+    """The bench's CPU arm steps oracle/models/quadruped12.dump (so it never
+    loads the product library); the committed dump must be what the
+    compiler produces today (regenerate with oracle/make_model_dumps.py)."""
+    import oracle
+
+    want = quad_model.dump()
+    got = oracle.load_dump("quadruped12.dump")
+    assert sorted(got) == sorted(want)
+    for k in want:
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
