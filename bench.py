@@ -8,18 +8,19 @@ FP32, condim 3 pyramidal, self-collision on, Newton 16 iterations at
 tolerance 1e-8, seeded uniform random position targets resampled every control
 step.  Data are synthetic (seeded Philox), there is no dataset.
 
-  value   whole-job env-steps/s of the learned-warm-start engine with the
-          per-step controls already resident in HBM (device-to-device copy
-          into the sim, then per substep: the fused tcgen05 inference kernel
-          (feature gather and the MLP's 4 layers) + the step kernel), CUDA events on the sim's stream, L2
-          flushed (256 MB write) before every timed step.  The net is trained
-          first, on the GPU, from plain rollouts with disjoint seeds
-          (--train-ctrl-steps x 4 substeps x envs pairs, --train-epochs).
-          solver.plain holds the same numbers for the plain solver
-          (previous-step warm start, one fused launch of 4 substeps), and
-          solver.learned / iteration_reduction the comparison at the same
-          tolerance.
-  e2e     the same metric through the public C ABI with host buffers:
+  value   whole-job env-steps/s of the engine (plain solver: previous-step
+          warm start, one fused launch of 4 substeps) with the per-step
+          controls already resident in HBM (device-to-device copy into the
+          sim, then the launch), CUDA events on the sim's stream, L2 flushed
+          (256 MB write) before every timed step.  solver.learned holds the
+          same numbers with the learned warm start attached (the step kernel
+          runs the MLP itself after every substep's constraint build, on bf16
+          mma.sync tiles shared by the CTA's warps), and learned_over_plain /
+          iteration_reduction the comparison at the same tolerance.  The net
+          is trained first, on the GPU, from plain rollouts with disjoint
+          seeds (--train-ctrl-steps x 4 substeps x envs pairs,
+          --train-epochs).
+  e2e     the same metric (plain solver) through the public C ABI with host buffers:
           mjmlx_batched_step_n(ctrl host array, 4) + mjmlx_batched_get_state
           (qpos, qvel to host) every step, wall clock.
   roofline  the plain step kernel: algorithmic 488 B per env-substep (qpos,
@@ -233,7 +234,9 @@ def run_reference(args, world, rank):
 def train_warmstart(m, B, nctrl, epochs, seed=50000):
     """Learned warm start for the bench: plain rollouts of B envs for nctrl
     control steps (seeds disjoint from the timed workload) give
-    B * (4 * nctrl - 1) training pairs; the net trains on the GPU."""
+    B * 4 * nctrl training pairs (one per env and substep: the features the
+    fused inference sees after the constraint build, and the converged qacc
+    minus the previous one); the net trains on the GPU."""
     import numpy as np
     import torch
 
@@ -245,7 +248,7 @@ def train_warmstart(m, B, nctrl, epochs, seed=50000):
     sim.set_state(q.astype(np.float32), v.astype(np.float32))
     ctrl = torch.from_numpy(np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed + 1) for c in range(nctrl)]).astype(np.float32)).cuda()
     width = sim.warmstart_input_width()
-    rows = B * (SUBSTEPS * nctrl - 1)
+    rows = B * SUBSTEPS * nctrl
     xraw = torch.empty(rows, width, device="cuda")
     traw = torch.empty(rows, m.nv, device="cuda")
     torch.cuda.synchronize()
@@ -334,11 +337,8 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
     res = {}
-    for mode in ("plain", "learned", "learned_first"):
-        # learned_first: the prediction only at the first substep of each
-        # env-step (where the controls change), the other 3 substeps in one
-        # launch with the previous-step warm start
-        sim = mjb200.BatchedSim(m, B, record=0, predict_every=SUBSTEPS if mode == "learned_first" else 1)
+    for mode in ("plain", "learned"):
+        sim = mjb200.BatchedSim(m, B, record=0)
         if mode != "plain":
             sim.set_warmstart(net)
         stream = torch.cuda.ExternalStream(sim.stream())
@@ -376,18 +376,17 @@ def run_ours(args, world, rank, local):
     if rank != 0:
         return
     L, P = res["learned"], res["plain"]
-    line = {"metric": METRIC, "value": L["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": L["ms_per_step"], "ms_per_step_median": L["ms_per_step_median"], "ms_per_step_p10": L["ms_per_step_p10"],
-            "ms_per_step_p90": L["ms_per_step_p90"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+    line = {"metric": METRIC, "value": P["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": P["ms_per_step"], "ms_per_step_median": P["ms_per_step_median"], "ms_per_step_p10": P["ms_per_step_p10"],
+            "ms_per_step_p90": P["ms_per_step_p90"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(B),
-            "e2e": {"value": L["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": P["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,
-            # learned path: per substep one fused inference kernel (mlp_infer_kernel) and one step kernel
-            "gpu_launches": K * SUBSTEPS * 2,
-            "solver": {"value_is": "learned warm start (previous-step and qacc_smooth candidates kept as fallback), same tolerance 1e-8",
+            # one step-kernel launch per env-step (the learned path runs its inference inside it)
+            "gpu_launches": K,
+            "solver": {"value_is": "plain solver (previous-step warm start, MuJoCo's); learned: the same engine with the fused learned "
+                                   "warm start as a third candidate (previous-step and qacc_smooth kept as fallback), same tolerance 1e-8",
                        "learned": L, "plain": P, "learned_over_plain": L["value"] / P["value"],
-                       "learned_first_substep": res["learned_first"],
-                       "learned_first_over_plain": res["learned_first"]["value"] / P["value"],
                        "iteration_reduction": 1.0 - L["newton_iter_mean"] / max(P["newton_iter_mean"], 1e-9), "training": train_info},
             "clocks": clocks}
     if world == 1:

@@ -2,13 +2,18 @@
  * mjb200 learned Newton warm start.  No counterpart in the reference, whose
  * Newton solver starts from qacc = 0 (src/compat/mkx_kernels/solver.hpp:592).
  *
- * A 3 x 256 GELU MLP maps the state an env reaches at the end of a substep
- * (qpos without the free root's x, y; qvel; the converged qacc; normal and
- * distance of up to 16 contacts) plus the controls of the next substep to the
- * change of the converged acceleration over that substep.  Attached to a sim,
- * its prediction is a third warm-start candidate of the Newton solver next to
- * qacc_smooth and the previous qacc; the solver keeps the lowest Gauss cost
- * and iterates to the same tolerance as without it.
+ * A 3 x 256 GELU MLP predicts the converged acceleration of a substep as a
+ * change from the previous substep's.  Per-env models: the step kernel runs
+ * the net itself, after the constraint build of every substep, on that
+ * substep's features (qpos without the free root's x, y; qvel; qacc_smooth;
+ * the previous converged qacc; ctrl; normal and distance of up to 16
+ * contacts), with bf16 tensor-core tiles shared by the warps of a lockstep
+ * CTA (8 or 16 warps).  Models made only of free bodies with nv > 64: one
+ * feature row per body from the end of the previous substep, inferred by a
+ * separate launch.  Attached to a sim, the prediction is a third warm-start
+ * candidate of the Newton solver next to qacc_smooth and the previous qacc;
+ * the solver keeps the lowest Gauss cost and iterates to the same tolerance
+ * as without it.
  *
  * All arrays named *_dev are device pointers (float, row-major).  Functions
  * return 0 on success and -1 on error (message in mjb200_last_error), unless
@@ -30,7 +35,7 @@ typedef struct MjbWarmStart MjbWarmStart;
 MJMLX_API MjbWarmStart* mjb200_warmstart_create(int in_raw, int nout, unsigned long long seed);
 MJMLX_API void mjb200_warmstart_free(MjbWarmStart* net);
 
-/* Input width (features + controls) the sim's learned warm start expects, or -1. */
+/* Input width the sim's learned warm start expects, or -1. */
 MJMLX_API int mjb200_warmstart_input_width(const MjmlxBatchedSim* sim);
 
 /* The net shape a sim expects: input width, output width and rows per env.
@@ -71,15 +76,24 @@ MJMLX_API int mjb200_warmstart_train(MjbWarmStart* net, const float* xraw_dev, c
 
 /* Training data from a plain rollout of the sim (learned warm start off):
  * ctrl_dev holds nctrl control sets of total_u floats, each applied for
- * substeps_per_ctrl substeps; every substep after the first writes
- * num_envs x rows_per_env rows xraw_dev[.][in_raw] and traw_dev[.][nout]
- * (mjb200_warmstart_layout) while max_rows allows.  Returns the number of
- * rows written, or -1. */
+ * substeps_per_ctrl substeps.  Per-env models: every substep writes num_envs
+ * rows xraw_dev[.][in_raw] (the features the fused inference sees) and
+ * traw_dev[.][nv] (the substep's converged qacc minus the previous one);
+ * per-body models: every substep after the first writes num_envs x
+ * rows_per_env rows (mjb200_warmstart_layout).  Rows are written while
+ * max_rows allows.  Returns the number of rows written, or -1. */
 MJMLX_API int mjb200_batched_warmstart_collect(MjmlxBatchedSim* sim, const float* ctrl_dev, int nctrl, int substeps_per_ctrl, float* xraw_dev,
                                                float* traw_dev, int max_rows);
 /* Attaches a net to the sim (NULL detaches).  The net must outlive the
- * attachment and serves one sim batch size. */
+ * attachment and serves one sim batch size.  Per-env models need lockstep
+ * CTAs of 8 or 16 warps with the workspaces in shared memory and nv * nv >=
+ * 256; the sim switches to 8-warp CTAs when it can, else -1. */
 MJMLX_API int mjb200_batched_set_warmstart(MjmlxBatchedSim* sim, MjbWarmStart* net);
+/* Debug capture of the fused warm start (mjb200_batched_set_debug enabled, a
+ * per-env net attached): the input features features[num_envs][in_raw] and
+ * the predictions pred[total_v] of the last substep of the last step (either
+ * may be NULL).  Returns in_raw, or -1 when nothing was captured. */
+MJMLX_API int mjb200_batched_get_warmstart_debug(MjmlxBatchedSim* sim, float* features, float* pred);
 
 /* Prediction for B envs from device arrays feat_dev[B][fstride] (first nfeat
  * used), ctrl_dev[B][nu] and the previous qacc prev_dev[B][nout]:

@@ -48,7 +48,7 @@ MJMLX_API int mjb200_warmstart_input_width(const MjmlxBatchedSim* sim) {
   if (!sim || !sim->engine) return -1;
   return guarded("mjb200_warmstart_input_width", [&] {
     if (!sim->engine->uniform()) throw std::runtime_error("needs a single-model batch");
-    return sim->engine->feature_count() + sim->engine->model(0).nu;
+    return sim->engine->warmstart_input_width();
   });
 }
 
@@ -57,7 +57,7 @@ MJMLX_API int mjb200_warmstart_layout(const MjmlxBatchedSim* sim, int* in_raw, i
   return guarded("mjb200_warmstart_layout", [&] {
     const auto& e = *sim->engine;
     if (!e.uniform()) throw std::runtime_error("needs a single-model batch");
-    if (in_raw) *in_raw = e.feature_count() + (e.feature_per_body() ? 0 : e.model(0).nu);
+    if (in_raw) *in_raw = e.warmstart_input_width();
     if (nout) *nout = e.warmstart_outputs();
     if (rows_per_env) *rows_per_env = e.rows_per_env();
     return 0;
@@ -149,6 +149,11 @@ MJMLX_API int mjb200_batched_set_warmstart(MjmlxBatchedSim* sim, MjbWarmStart* w
     sim->engine->set_warmstart(w ? w->net.get() : nullptr);
     return 0;
   });
+}
+
+MJMLX_API int mjb200_batched_get_warmstart_debug(MjmlxBatchedSim* sim, float* features, float* pred) {
+  if (!sim || !sim->engine) return -1;
+  return guarded("mjb200_batched_get_warmstart_debug", [&] { return sim->engine->get_warmstart_debug(features, pred); });
 }
 
 MJMLX_API int mjb200_warmstart_predict(MjbWarmStart* w, const float* feat, int fstride, int nfeat, const float* ctrl, int nu, const float* prev,

@@ -537,6 +537,7 @@ void Engine::choose_launch() {
   const int per_warp = (desc_words_ + (gws_mode_ ? 0 : ws_stride_)) * 4;
   if (cfg_.warps_per_block > 0) warps_ = cfg_.warps_per_block;
   else if (gws_mode_) warps_ = 4;
+  else if (lockstep_ && 16 * per_warp <= 227 * 1024) warps_ = 16;   // one lockstep CTA of 16 warps per SM (measured ~3 % faster than two of 8)
   else if (lockstep_) warps_ = std::max(1, std::min(8, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs of up to 8 warps per SM
   else warps_ = 4;
   smem_ = warps_ * per_warp;
@@ -559,11 +560,31 @@ void Engine::choose_launch() {
 
 void Engine::configure(const EngineConfig& cfg) {
   bool rebuild = cfg.ncon_max != cfg_.ncon_max || cfg.nefc_max != cfg_.nefc_max || cfg.tolerance != cfg_.tolerance || cfg.max_iter != cfg_.max_iter;
+  const EngineConfig old = cfg_;
   cfg_ = cfg;
   sync();
   if (rebuild) build_tables(cfg_, 0);
   choose_launch();
   invalidate_graphs();
+  if (fused_warmstart()) {
+    const std::string why = fused_blocker();
+    if (!why.empty()) {
+      cfg_ = old;
+      if (rebuild) build_tables(cfg_, 0);
+      choose_launch();
+      throw std::runtime_error("configure: the attached learned warm start " + why);
+    }
+  }
+}
+
+std::string Engine::fused_blocker() const {
+  const Model& m = *models_[0];
+  if (!lockstep_) return "needs lockstep CTAs (engine config lockstep = 1)";
+  if (warps_ != 8 && warps_ != 16) return "needs CTAs of 8 or 16 warps (engine config warps_per_block)";
+  if (gws_mode_) return "needs the workspaces in shared memory";
+  if (convex_) return "is not built into the kernel instance for general convex pairs and elliptic cones";
+  if (m.nv * m.nv < 256) return "needs nv * nv >= 256 (its activation rows use the Hessian slot of the workspace)";
+  return "";
 }
 
 std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
@@ -589,10 +610,12 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
   check(cudaEventCreate(&e0), "event");
   check(cudaEventCreate(&e1), "event");
   const bool feat_valid = feat_valid_;
+  const bool fused = fused_warmstart();
   for (int lock : {1, 0}) {
     for (int w : {2, 4, 8, 16}) {
       TuneCandidate c{w, lock, 0, -1.f};
-      if (w * per_warp > 227 * 1024) {
+      // an attached per-env net runs inside the kernel: lockstep, 8 or 16 warps
+      if (w * per_warp > 227 * 1024 || (fused && (!lock || (w != 8 && w != 16)))) {
         out.push_back(c);
         continue;
       }
@@ -708,6 +731,14 @@ StepParams Engine::params(int n, bool record) {
       P.env_fadr = d_fadr_.p;
     }
   }
+  if (fused_warmstart()) {
+    net_->fill_fused(P);
+    P.feat_qskip = feature_qskip();
+    if (record && dbg_ncon_ > 0 && dbg_feat_.p) {
+      P.nn_feat_out = dbg_feat_.p;
+      P.nn_pred_out = dbg_pred_.p;
+    }
+  }
   if (tot_s_ > 0) {
     if (record) P.sensordata = sensordata_.p;
     P.env_sadr = d_sadr_.p;
@@ -816,7 +847,7 @@ void Engine::launch_learned(int n, bool record) {
 
 void Engine::launch(int n, bool record) {
   if (n <= 0) return;
-  if (net_) {
+  if (net_ && feature_per_body()) {
     launch_learned(n, record);
     return;
   }
@@ -924,6 +955,7 @@ void Engine::step_with_warmstart(const float* qacc, int n) {
   check(cudaMemcpyAsync(pred_.p, qacc, sizeof(float) * tot_v_, cudaMemcpyDeviceToDevice, stream_), "warm start copy");
   StepParams P = params(1, cfg_.record != 0 && n == 1);
   P.qacc_pred = pred_.p;
+  P.nn_w[0] = nullptr;   // the caller's candidate, not the fused net's, for this substep
   if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
   check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
   feat_valid_ = false;
@@ -1028,8 +1060,20 @@ void Engine::set_debug(int ncon_max, int nefc_max) {
     dbg_con_.alloc((size_t)B_ * dbg_ncon_ * MJB_CONTACT_FLOATS);
     dbg_efc_.alloc((size_t)B_ * std::max(1, dbg_nefc_) * 4);
     dbg_vec_.alloc((size_t)B_ * 4 * nv_max_);
+    if (uniform()) {
+      dbg_feat_.alloc((size_t)B_ * warmstart_input_width());
+      dbg_pred_.alloc(std::max(tot_v_, 1));
+    }
   }
   invalidate_graphs();
+}
+
+int Engine::get_warmstart_debug(float* features, float* pred) {
+  if (dbg_ncon_ <= 0 || !dbg_feat_.p || !fused_warmstart()) return -1;
+  if (features) check(cudaMemcpyAsync(features, dbg_feat_.p, sizeof(float) * dbg_feat_.n, cudaMemcpyDeviceToHost, stream_), "dbg copy");
+  if (pred) check(cudaMemcpyAsync(pred, dbg_pred_.p, sizeof(float) * tot_v_, cudaMemcpyDeviceToHost, stream_), "dbg copy");
+  sync();
+  return warmstart_input_width();
 }
 
 void Engine::get_debug(float* contacts, float* efc, float* vec) {
@@ -1121,6 +1165,12 @@ int Engine::feature_count() const {
   return m.nq - feature_qskip() + 2 * m.nv + 4 * MJB_FEAT_CONTACTS;
 }
 
+int Engine::warmstart_input_width() const {
+  const Model& m = *models_[0];
+  if (feature_per_body()) return MJB_FEAT_BODY;
+  return m.nq - feature_qskip() + 3 * m.nv + m.nu + 4 * MJB_FEAT_CONTACTS;   // the step kernel's nn_feature layout
+}
+
 bool Engine::feature_per_body() const {
   const Model& m = *models_[0];
   if (m.nv <= WarmStartNet::kOutPad || m.nu != 0 || m.njnt != m.nbody - 1) return false;
@@ -1144,17 +1194,68 @@ void Engine::ensure_features() {
 void Engine::set_warmstart(WarmStartNet* net) {
   sync();
   if (net) {
-    ensure_features();
-    const Model& m = *models_[0];
-    if (net->in_raw() != feature_count() + (feature_per_body() ? 0 : m.nu) || net->nout() != warmstart_outputs())
+    if (!uniform()) throw std::runtime_error("learned warm start: needs a single-model batch");
+    if (net->in_raw() != warmstart_input_width() || net->nout() != warmstart_outputs())
       throw std::runtime_error("learned warm start: the net's input / output widths do not match this model");
-    net->prepare_inference(B_ * rows_per_env());
+    if (feature_per_body()) {
+      ensure_features();
+      net->prepare_inference(B_ * rows_per_env());
+    } else {
+      if (net->in_pad() > 256) throw std::runtime_error("learned warm start: inputs past 256 do not fit the fused inference");
+      net_ = net;
+      if (!fused_blocker().empty() && lockstep_ && !gws_mode_) {
+        // 8-warp lockstep CTAs (one per SM when the workspaces are large)
+        EngineConfig c = cfg_;
+        c.warps_per_block = 8;
+        c.lockstep = 1;
+        const EngineConfig prev = cfg_;
+        cfg_ = c;
+        choose_launch();
+        if (!fused_blocker().empty() || smem_ > 227 * 1024) {
+          cfg_ = prev;
+          choose_launch();
+        }
+      }
+      const std::string why = fused_blocker();
+      if (!why.empty()) {
+        net_ = nullptr;
+        throw std::runtime_error("learned warm start (fused into the step kernel): " + why);
+      }
+    }
   }
   net_ = net;
   invalidate_graphs();
 }
 
 int Engine::collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows) {
+  if (!uniform()) throw std::runtime_error("learned warm start: needs a single-model batch");
+  if (!feature_per_body()) {
+    // per-env: the step kernel writes (features after the constraint build,
+    // converged qacc minus the previous one) for every env and substep
+    const Model& m = *models_[0];
+    const int F = warmstart_input_width();
+    WarmStartNet* saved = net_;
+    net_ = nullptr;
+    int rows = 0;
+    for (int c = 0; c < nctrl; c++) {
+      int n = sub_per_ctrl;
+      if (rows + (long long)n * B_ > max_rows) n = (max_rows - rows) / B_;
+      if (n <= 0) break;
+      if (m.nu > 0) check(cudaMemcpyAsync(ctrl_.p, ctrl_seq + (size_t)c * tot_u_, sizeof(float) * tot_u_, cudaMemcpyDeviceToDevice, stream_), "collect ctrl");
+      StepParams P = params(n, false);
+      P.pair_x = xraw + (size_t)rows * F;
+      P.pair_t = traw + (size_t)rows * m.nv;
+      P.nn_in_raw = F;
+      P.feat_qskip = feature_qskip();
+      if (persistent_ && !lockstep_) check(cudaMemsetAsync(counter_.p, 0, sizeof(int), stream_), "reset work counter");
+      check(mjb_launch_step(P, grid_, warps_, smem_, stream_), "mjb_step_kernel launch");
+      rows += n * B_;
+      if (n < sub_per_ctrl) break;
+    }
+    sync();
+    net_ = saved;
+    return rows;
+  }
   ensure_features();
   const Model& m = *models_[0];
   const bool per_body = feature_per_body();

@@ -90,6 +90,11 @@ class Engine {
   void stats(int* status, int* niter_sum, int* niter_max, int* ncon, int* nefc, int* choice);
   void set_debug(int ncon_max, int nefc_max);
   void get_debug(float* contacts, float* efc, float* vec);
+  // Debug capture of the fused learned warm start (last substep of the last
+  // recorded step): input features [B][warmstart_input_width()] and
+  // predictions [total_v].  Returns the feature width, or -1 when nothing
+  // was captured.
+  int get_warmstart_debug(float* features, float* pred);
   int dbg_ncon_max() const { return dbg_ncon_; }
   int dbg_nefc_max() const { return dbg_nefc_; }
   int dbg_nv_max() const { return nv_max_; }
@@ -103,10 +108,17 @@ class Engine {
   bool domain_rand() const { return rand_on_; }
 
   // learned warm start
-  // Raw features per env written after each substep (qpos minus the leading
-  // free-joint x, y; qvel; converged qacc; 16 x contact normal and distance).
+  // Input width of the net for this sim: per-env models, the fused layout of
+  // the substep after its constraint build (qpos minus the leading free-joint
+  // x, y; qvel; qacc_smooth; previous converged qacc; ctrl; 16 x contact
+  // normal and distance); per-body models, MJB_FEAT_BODY.
+  int warmstart_input_width() const;
+  // Per-body mode: floats per body row written after each substep.
   int feature_count() const;
   int feature_qskip() const;
+  // A per-env net is attached: the step kernel runs it (lockstep CTAs of 8
+  // or 16 warps, workspaces in shared memory, nv * nv >= 256).
+  bool fused_warmstart() const { return net_ && !feature_per_body(); }
   // Per-body mode: models made only of free bodies (children of the world)
   // with more dofs than a per-env net serves (nv > 64) and no controls get
   // one feature row and 6 outputs per body (rows_per_env = nbody - 1);
@@ -114,16 +126,20 @@ class Engine {
   bool feature_per_body() const;
   int rows_per_env() const { return feature_per_body() ? models_[0]->nbody - 1 : 1; }
   int warmstart_outputs() const { return feature_per_body() ? 6 : models_[0]->nv; }
-  // Attaches a trained net (null detaches): every substep then first runs the
-  // net on the features of the previous substep and the current controls and
-  // offers its prediction to the Newton solver as a warm-start candidate.
+  // Attaches a trained net (null detaches): every substep then offers the
+  // net's prediction to the Newton solver as a warm-start candidate.  Per-env
+  // models switch the sim to 8-warp lockstep CTAs when its launch shape
+  // cannot run the fused inference; throws when no shape can.
   void set_warmstart(class WarmStartNet* net);
   class WarmStartNet* warmstart() const { return net_; }
-  // Plain rollout that records training pairs: for each substep after the
-  // first, xraw row = [features of the previous substep | controls] and traw
-  // row = converged qacc of the substep minus that of the previous one.
-  // ctrl_seq: nctrl device control sets of total_u floats, each held for
-  // sub_per_ctrl substeps.  Returns the number of rows written (<= max_rows).
+  // Plain rollout that records training pairs.  Per-env models: for every
+  // substep, B rows of xraw = the fused input features of the substep and
+  // traw = its converged qacc minus the previous one (written by the step
+  // kernel).  Per-body models: for each substep after the first, B *
+  // (nbody - 1) body rows of the previous substep's features and the
+  // change of the bodies' converged accelerations.  ctrl_seq: nctrl device
+  // control sets of total_u floats, each held for sub_per_ctrl substeps.
+  // Returns the number of rows written (<= max_rows).
   int collect(const float* ctrl_seq, int nctrl, int sub_per_ctrl, float* xraw, float* traw, int max_rows);
   // n substeps; the first offers qacc[total_v] (device) to the Newton
   // solver as an extra warm-start candidate (kept when its cost is lowest).
@@ -183,6 +199,8 @@ class Engine {
   void ensure_features();
   void invalidate_graphs();
   StepParams params(int n, bool record);
+  // why the current launch shape cannot run the fused inference ("" = it can)
+  std::string fused_blocker() const;
 
   std::vector<const Model*> models_;
   std::vector<int> counts_;
@@ -208,7 +226,7 @@ class Engine {
   DevBuf<float> qpos_, qvel_, ctrl_, warm_, pred_, qpos0_;
   DevBuf<int> status_, niter_sum_, niter_max_, ncon_, nefc_, choice_, counter_;
   DevBuf<float> rec_xpos_, rec_xquat_, rec_scom_, rec_cinert_, rec_cvel_, rec_qfa_, rec_cfrc_, rec_qacc_;
-  DevBuf<float> dbg_con_, dbg_efc_, dbg_vec_;
+  DevBuf<float> dbg_con_, dbg_efc_, dbg_vec_, dbg_feat_, dbg_pred_;
   int dbg_ncon_ = 0, dbg_nefc_ = 0;
   DevBuf<float> rand_mass_, rand_fric_, rand_gain_, rand_com_, rand_drag_;
   std::vector<float> h_rand_mass_, h_rand_fric_, h_rand_gain_, h_rand_com_, h_rand_drag_;

@@ -9,6 +9,7 @@
 
 #include <mutex>
 
+#include "dev_nn.cuh"
 #include "dev_solver.cuh"
 #include "step_params.h"
 
@@ -387,6 +388,28 @@ __device__ __noinline__ bool check_state(Env& E) {
 
 }  // namespace
 
+namespace {
+
+// Feature row of the env (training pairs and / or the MLP's input row), then
+// with fused = true the MLP over the CTA's envs.  Every warp of a lockstep
+// CTA calls it with fused = true (block barriers inside); rows use warp 0's
+// descriptor, which always belongs to a valid env.
+__device__ __noinline__ void d_nn_stage(const Env& E, const StepParams& P, int ncon, bool valid, int s, bool last, bool fused) {
+  float* raw = (P.pair_x && valid) ? P.pair_x + ((size_t)s * P.num_envs + E.env) * P.nn_in_raw
+                                   : (last && P.nn_feat_out && valid) ? P.nn_feat_out + (size_t)E.env * P.nn_in_raw : nullptr;
+  if (!fused) {
+    d_nn_features(E, P, ncon, true, raw);
+    return;
+  }
+  const int W = blockDim.x >> 5, warp = threadIdx.x >> 5;
+  Env En = E;
+  En.md = reinterpret_cast<const DevModelDesc*>(mjb_smem);
+  d_nn_features(En, P, ncon, valid, raw);
+  d_nn_infer(P, *En.md, mjb_smem + W * P.desc_words, W, warp, E.lane);
+}
+
+}  // namespace
+
 // Two execution modes share the stage functions:
 //  * independent warps (P.lockstep == 0): each warp takes envs from the
 //    persistent queue and runs all stages on its own;
@@ -399,6 +422,9 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = blockDim.x >> 5;
   const bool lockstep = P.lockstep != 0;
+  // the fused warm start is compiled into the instance without the GJK / EPA
+  // collider and elliptic solver only (the host refuses it for those models)
+  const bool nnfused = !CVX && lockstep && P.nn_w[0] != nullptr && P.gws == nullptr;
   int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
   float* ws = P.gws ? P.gws + ((size_t)blockIdx.x * W + warp) * P.ws_stride : mjb_smem + W * P.desc_words + warp * P.ws_stride;
   // optional per-stage timing: thread 0 of each CTA accumulates the clock
@@ -516,11 +542,34 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       STAGE_SYNC();
       if (valid) nefc = d_constraints<CVX>(E, P, ncon);
       STAGE_SYNC();
+      // fused learned warm start: feature rows of this substep, then the MLP
+      // over the CTA's envs (block barriers inside: every warp takes part)
+      if constexpr (!CVX) {
+        if (nnfused || (P.pair_x && valid)) {
+          const long long tn = timing ? clock64() : 0;
+          d_nn_stage(E, P, ncon, valid, s, last, nnfused);
+          if (timing && nnfused) {   // stage clock bucket 6: the fused inference, barrier to barrier
+            const long long t_ = clock64();
+            tstage[6] += (unsigned long long)(t_ - tn);
+            tlast = t_;
+          }
+        }
+      }
       if (valid) {
-        const float* xpred = (P.qacc_pred && s == 0) ? P.qacc_pred + vadr : nullptr;   // a prediction serves the launch's first substep
+        // a caller / separately inferred prediction serves the launch's first substep; the fused one every substep
+        const float* xpred = nnfused ? ws + E.md->w_vec + 7 * nv : (P.qacc_pred && s == 0) ? P.qacc_pred + vadr : nullptr;
         int it = d_newton<CVX>(E, P, nefc, max_iter, xpred, choice);
         nsum += it;
         nmax = it > nmax ? it : nmax;
+        if (P.pair_t) {
+          float* tr = P.pair_t + ((size_t)s * P.num_envs + env) * nv;
+#pragma unroll 1
+          for (int k = lane; k < nv; k += 32) tr[k] = ws[E.md->w_x + k] - ws[E.md->w_xwarm + k];
+        }
+        if (last && nnfused && P.nn_pred_out) {
+#pragma unroll 1
+          for (int k = lane; k < nv; k += 32) P.nn_pred_out[vadr + k] = ws[E.md->w_vec + 7 * nv + k];
+        }
       }
       // no barrier here: warps whose Newton solve ends early go on through
       // integration and the next substep's kinematics while the slowest

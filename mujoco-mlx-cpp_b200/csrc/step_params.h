@@ -94,6 +94,30 @@ struct StepParams {
   int feat_stride;
   int feat_qskip;
   int feat_body;
+  // fused learned warm start (per-env models, lockstep CTAs of 4, 8 or 16
+  // warps; nn_w[0] null = off): after the constraint build of every substep
+  // the CTA evaluates a 4-layer GELU MLP on the feature rows of its envs
+  // (qpos[feat_qskip:], qvel, qacc_smooth, previous qacc, ctrl, first
+  // MJB_FEAT_CONTACTS contacts as normal and distance; nn_in_raw values) and
+  // offers qacc_prev + out_mean + out_std * y to the Newton solver.  Weights
+  // are bf16 [nn_rows][nn_cols] per layer (K contiguous), biases fp32.
+  const uint16_t* nn_w[4];
+  const float* nn_b[4];
+  int nn_rows[4], nn_cols[4];
+  const float* nn_in_mean;
+  const float* nn_in_istd;
+  const float* nn_out_mean;
+  const float* nn_out_std;
+  int nn_in_raw;
+  int nn_nout;
+  // training pairs of the fused warm start written by the kernel (nullable):
+  // row s * num_envs + env holds the nn_in_raw features of substep s (taken
+  // after its constraint build) and the converged qacc minus the previous
+  // one (nv floats); single-model batches
+  float* pair_x;
+  float* pair_t;
+  float* nn_pred_out;          // debug capture (nullable): the fused prediction of the last substep, at env_vadr
+  float* nn_feat_out;          // debug capture (nullable): the fused input features of the last substep, [B][nn_in_raw]
   int stats_accumulate;        // 1: add this launch's Newton iterations to niter_sum / max into niter_max
   int poison_workspace;        // 1: fill each env's shared workspace with NaN before its first stage (test aid)
 };

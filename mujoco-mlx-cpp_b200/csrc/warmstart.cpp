@@ -111,6 +111,21 @@ void WarmStartNet::set_params(const float* host) {
   check(cudaStreamSynchronize(stream_), "warm start sync");
 }
 
+void WarmStartNet::fill_fused(StepParams& P) const {
+  for (int l = 0; l < kLayers; l++) {
+    P.nn_w[l] = wb_.p + woff_[l] - layer_base_[l];
+    P.nn_b[l] = params_.p + boff_[l];
+    P.nn_rows[l] = rows_[l];
+    P.nn_cols[l] = cols_[l];
+  }
+  P.nn_in_mean = in_mean_.p;
+  P.nn_in_istd = in_istd_.p;
+  P.nn_out_mean = out_mean_.p;
+  P.nn_out_std = out_std_.p;
+  P.nn_in_raw = in_raw_;
+  P.nn_nout = nout_;
+}
+
 void WarmStartNet::set_normalization(const float* in_mean, const float* in_std, const float* out_mean, const float* out_std) {
   h_in_mean_.assign(in_mean, in_mean + in_raw_);
   h_in_std_.assign(in_std, in_std + in_raw_);

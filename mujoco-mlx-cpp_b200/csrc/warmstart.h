@@ -1,14 +1,21 @@
-// Learned Newton warm start: a 3 x 256 GELU MLP that maps the features of an
-// env at the end of a physics substep (plus the controls of the next one) to
-// the change of the converged acceleration over the next substep.  The
-// prediction qacc_prev + mean + std * y enters the Newton solver as a third
-// warm-start candidate next to qacc_smooth and the previous qacc; the solver
-// keeps the cheapest by the Gauss cost and iterates to the same tolerance, so
-// a poor prediction costs nothing but the inference.  No counterpart in the
+// Learned Newton warm start: a 3 x 256 GELU MLP that predicts the change of
+// the converged acceleration from the previous substep's.  The prediction
+// qacc_prev + mean + std * y enters the Newton solver as a third warm-start
+// candidate next to qacc_smooth and the previous qacc; the solver keeps the
+// cheapest by the Gauss cost and iterates to the same tolerance, so a poor
+// prediction costs nothing but the inference.  No counterpart in the
 // reference (its solver cold-starts, solver.hpp:592).
 //
-// Training and inference run on the GPU through BF16 tcgen05 GEMMs with FP32
-// accumulation (mlp_kernels.cu); parameters are kept in FP32 with Adam.
+// Per-env models: the step kernel evaluates the net itself after the
+// constraint build of every substep, on that substep's features (state,
+// unconstrained acceleration, previous converged acceleration, controls,
+// contacts; dev_nn.cuh), with bf16 mma.sync tiles shared by the CTA's warps.
+// Per-body models (free bodies only, nv > 64): one row per body from the end
+// of the previous substep, inferred by a separate tcgen05 launch.
+//
+// Training, and the per-body inference, run on the GPU through BF16 tcgen05
+// GEMMs with FP32 accumulation (mlp_kernels.cu); parameters are kept in FP32
+// with Adam.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -18,6 +25,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "step_params.h"
 
 namespace mjb {
 
@@ -68,6 +76,10 @@ class WarmStartNet {
   void prepare_inference(int B);
 
   int error_word();
+
+  // Device pointers of the weights (bf16 [rows][cols] per layer), biases and
+  // normalisation for the step kernel's fused inference (StepParams nn_*).
+  void fill_fused(StepParams& P) const;
 
  private:
   void ensure_batch(int n);

@@ -85,6 +85,7 @@ def _load():
         "mjb200_warmstart_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _f32p]),
         "mjb200_batched_warmstart_collect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_set_warmstart": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "mjb200_batched_get_warmstart_debug": (C.c_int, [C.c_void_p, _f32p, _f32p]),
         "mjb200_warmstart_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
         "mjb200_gemm_bf16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
         "mjb200_gemm_bf16_gated": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_void_p,
@@ -437,6 +438,16 @@ class BatchedSim:
         if lib.mjb200_batched_set_warmstart(self.handle, net.handle if net is not None else None) != 0:
             raise RuntimeError(last_error())
 
+    def warmstart_debug(self):
+        """(features [num_envs, in_raw], prediction [total_v]) the fused
+        inference used on the last substep (debug capture on)."""
+        width = lib.mjb200_warmstart_input_width(self.handle)
+        f = np.zeros((self.num_envs, width), np.float32)
+        p = np.zeros(self.total_v, np.float32)
+        if lib.mjb200_batched_get_warmstart_debug(self.handle, _fp(f), _fp(p)) < 0:
+            raise RuntimeError("warmstart_debug: " + last_error())
+        return f, p
+
     def sync(self):
         lib.mjmlx_batched_eval_state(self.handle)
 
@@ -535,7 +546,8 @@ class BatchedSim:
         if lib.mjb200_batched_configure(self.handle, C.byref(c)) != 0:
             raise RuntimeError(last_error())
 
-    STAGES = ("kinematics", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "newton_finish_kin", "x7", "x8", "x9", "x10", "x11", "x12", "x13", "x14", "x15")
+    STAGES = ("newton_finish_kin", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "fused_warmstart", "x7", "x8", "x9", "x10", "x11",
+              "x12", "x13", "x14", "x15")
 
     def stage_timing(self, enable: int = -1):
         out = (C.c_ulonglong * 16)()

@@ -33,7 +33,7 @@ def _quick_warmstart(mjb200, torch, m, B, nctrl=8, epochs=2, seed=50000):
     col.set_state(q.astype(np.float32), v.astype(np.float32))
     ctrl = torch.from_numpy(np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed + 1) for c in range(nctrl)]).astype(np.float32)).cuda()
     width = col.warmstart_input_width()
-    rows = B * (4 * nctrl - 1)
+    rows = B * 4 * nctrl
     x = torch.empty(rows, width, device="cuda")
     t = torch.empty(rows, m.nv, device="cuda")
     torch.cuda.synchronize()

@@ -1,7 +1,7 @@
 """Oracle parity at the benchmarked configuration: the 12-DoF quadruped at
 4096 and 16384 envs with the bench's inputs (seeded initial states, random
 position targets resampled every control step), stepped with the default
-launch (lockstep CTAs, persistent grid: 296 CTAs x 8 warps = 2368 envs per
+launch (lockstep CTAs, persistent grid: 148 CTAs x 16 warps = 2368 envs per
 wave, so 2 and 7 waves pass through the grid-stride loop), then one
 recorded substep compared with the FP64 oracle on 256 sampled envs
 (env = k B / 256), from the same FP32 state, controls and warm start.
@@ -125,7 +125,7 @@ def test_config2_learned_path_sampled_parity(quad_model):
     nctrl = 4
     ctrl = torch.from_numpy(np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed0 + 1) for c in range(nctrl)]).astype(np.float32)).cuda()
     width = col.warmstart_input_width()
-    rows = B * (NSUB * nctrl - 1)
+    rows = B * NSUB * nctrl
     xraw = torch.empty(rows, width, device="cuda")
     traw = torch.empty(rows, quad_model.nv, device="cuda")
     torch.cuda.synchronize()

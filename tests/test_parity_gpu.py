@@ -175,12 +175,13 @@ def test_rollout_drift_1000_steps(quad_model):
 
 def test_rollout_bitwise_deterministic_across_launch_modes(quad_model):
     """2048 envs x 24 control steps give bit-identical states and iteration
-    counts in lockstep, graph-free and work-queue launches and on repeats."""
+    counts in lockstep (16- and 8-warp CTAs), graph-free and work-queue
+    launches and on repeats."""
     B = 2048
     q, v = mjb200.models.quadruped_initial_state_fast(B, seed=777)
     ctrls = [mjb200.models.quadruped_controls_fast(B, c, seed=778).astype(np.float32) for c in range(24)]
     out = []
-    for kw in (dict(), dict(), dict(use_graph=0), dict(lockstep=0)):
+    for kw in (dict(), dict(), dict(use_graph=0), dict(lockstep=0), dict(warps_per_block=8)):
         sim = mjb200.BatchedSim(quad_model, B, **kw)
         sim.set_state(q.astype(np.float32), v.astype(np.float32))
         its = 0

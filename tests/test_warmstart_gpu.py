@@ -116,7 +116,7 @@ def _collect_and_train(model, B, nctrl, epochs, seed0=50000):
     ctrl = np.stack([mjb200.models.quadruped_controls_fast(B, c, seed=seed0 + 1) for c in range(nctrl)]).astype(np.float32)
     ctrl_d = torch.from_numpy(ctrl).cuda()
     width = sim.warmstart_input_width()
-    rows = B * (nctrl * 4 - 1)
+    rows = B * nctrl * 4
     xraw = torch.empty(rows, width, device="cuda")
     traw = torch.empty(rows, model.nv, device="cuda")
     torch.cuda.synchronize()
@@ -261,3 +261,40 @@ def test_gemm_bounded_wait_gives_up_and_context_survives():
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     assert torch.equal(C3, C2)
+
+
+def test_fused_kernel_inference_matches_tcgen05_inference(quad_model, trained_quad_net):
+    """The step kernel's own inference (bf16 mma.sync tiles shared by the
+    CTA's warps) against the net's tcgen05 inference on the features the
+    kernel captured: same bf16 rounding points, FP32 sums in another order,
+    so agreement to 1e-3 of the prediction's scale.  1003 envs leave a last
+    CTA with 3 valid warps, whose rows must not disturb the others."""
+    net, _ = trained_quad_net
+    B = 1003
+    sim = mjb200.BatchedSim(quad_model, B)
+    sim.set_warmstart(net)
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=5150)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    for c in range(3):
+        sim.step(mjb200.models.quadruped_controls_fast(B, c, seed=5151).astype(np.float32), 4)
+    sim.set_debug(24, 64)
+    sim.step(mjb200.models.quadruped_controls_fast(B, 3, seed=5151).astype(np.float32), 4)
+    feat, pred = sim.warmstart_debug()
+    nv = quad_model.nv
+    pred = pred.reshape(B, nv)
+    nqf = quad_model.nq - 2
+    prev = np.ascontiguousarray(feat[:, nqf + 2 * nv: nqf + 3 * nv])
+    assert np.isfinite(feat).all() and np.isfinite(pred).all()
+    f_d = torch.from_numpy(feat).cuda()
+    p_d = torch.from_numpy(prev).cuda()
+    out = torch.full((B, nv), float("nan"), device="cuda")
+    torch.cuda.synchronize()
+    net.predict(f_d.data_ptr(), feat.shape[1], feat.shape[1], 0, 0, p_d.data_ptr(), out.data_ptr(), B, True)
+    ref = out.cpu().numpy()
+    scale = np.abs(ref - prev).max()
+    err = np.abs(pred - ref).max()
+    print("fused in-kernel vs tcgen05 prediction: max diff %.3g, scale %.3g" % (err, scale))
+    assert scale > 0 and err <= 1e-3 * scale + 1e-6
+    st = sim.stats()
+    assert np.all(st["status"] == 0)
+    assert np.mean(st["warm_choice"] == 2) > 0.1
