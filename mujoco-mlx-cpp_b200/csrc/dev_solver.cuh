@@ -48,49 +48,44 @@ __device__ __noinline__ void d_chol_smem(float* A, int n, int lane, float* idiag
   }
 }
 
-// Cholesky for n <= 32 with the pivot column in registers: lane i holds
-// A[i][k] of the current column k, the pivot comes from lane k by shuffle,
-// each l_jk is broadcast by shuffle to the rows below it, and lane i keeps
-// its updated A[i][k+1] in a register for the next step.  Same arithmetic in
-// the same order as d_chol_smem (bitwise identical factors), with the pivot
-// and column round trips through shared memory and two warp barriers per
-// step removed.
-__device__ __noinline__ void d_chol_reg(float* A, int n, int lane, float* idiag) {
+// Cholesky for n <= 32 with rows padded to ld floats (a multiple of 4) and
+// col[32] (16-byte aligned) of scratch.  At step k lane i > k scales its
+// entry k and posts it to col[i]; every lane then updates its own row's
+// entries k+1..i four at a time with 16-byte loads and stores, reading the
+// posted column with broadcast loads instead of one shuffle per entry.  The
+// last group of a row may reach past its diagonal into the padded upper
+// triangle, which nothing reads.  Same arithmetic in the same order as
+// d_chol_smem (bitwise identical factors).
+__device__ __noinline__ void d_chol_vec(float* A, int n, int ld, int lane, float* idiag, float* col) {
   const bool own = lane < n;
-  float c = own ? A[lane * n] : 0.f;
+  float* row = A + lane * ld;
 #pragma unroll 1
   for (int k = 0; k < n; k++) {
-    const float akk = __shfl_sync(FULL_MASK, c, k);
-    const float d = sqrtf(fmaxf(akk, 1e-30f)), id = 1.f / d;
+    const float d = sqrtf(fmaxf(A[k * ld + k], 1e-30f)), id = 1.f / d;
     const bool below = own && lane > k;
-    const float l = below ? c * id : 0.f;
+    float l = 0.f;
+    if (below) {
+      l = row[k] * id;
+      row[k] = l;
+      col[lane] = l;
+    }
     if (lane == k) {
-      A[k * n + k] = d;
+      row[k] = d;
       idiag[k] = id;
     }
-    if (below) A[lane * n + k] = l;
-    float nc = below ? A[lane * n + k + 1] : 0.f;
-    const float l1 = __shfl_sync(FULL_MASK, l, (k + 1) & 31);
-    if (below) nc -= l * l1;
-    int j = k + 2;
+    __syncwarp();
+    if (below) {
 #pragma unroll 1
-    for (; j + 3 < n; j += 4) {
-      const float a0 = __shfl_sync(FULL_MASK, l, j), a1 = __shfl_sync(FULL_MASK, l, j + 1);
-      const float a2 = __shfl_sync(FULL_MASK, l, j + 2), a3 = __shfl_sync(FULL_MASK, l, j + 3);
-      if (own) {
-        float* r = A + lane * n;
-        if (lane >= j) r[j] -= l * a0;
-        if (lane >= j + 1) r[j + 1] -= l * a1;
-        if (lane >= j + 2) r[j + 2] -= l * a2;
-        if (lane >= j + 3) r[j + 3] -= l * a3;
+      for (int j = (k + 1) & ~3; j <= lane; j += 4) {
+        float4 a = *reinterpret_cast<float4*>(row + j);
+        const float4 c = *reinterpret_cast<const float4*>(col + j);
+        if (j > k) a.x -= l * c.x;
+        if (j + 1 > k) a.y -= l * c.y;
+        if (j + 2 > k) a.z -= l * c.z;
+        a.w -= l * c.w;   // j + 3 > k always (j >= k - 2)
+        *reinterpret_cast<float4*>(row + j) = a;
       }
     }
-#pragma unroll 1
-    for (; j < n; j++) {
-      const float a0 = __shfl_sync(FULL_MASK, l, j);
-      if (own && lane >= j) A[lane * n + j] -= l * a0;
-    }
-    c = nc;
     __syncwarp();
   }
 }
@@ -141,8 +136,10 @@ __device__ __noinline__ void d_chol_sparse(float* A, int n, int lane, float* idi
   }
 }
 
-__device__ __forceinline__ void d_chol(float* A, int n, int lane, float* idiag, int* nz = nullptr) {
-  if (n <= 32) d_chol_reg(A, n, lane, idiag);
+// ld: row stride of A (n rounded up to 4 for n <= 32, then col = A + n * ld
+// is the vector path's column scratch; n otherwise)
+__device__ __forceinline__ void d_chol(float* A, int n, int ld, int lane, float* idiag, int* nz = nullptr) {
+  if (n <= 32) d_chol_vec(A, n, ld, lane, idiag, A + n * ld);
   else if (n > 64 && nz) d_chol_sparse(A, n, lane, idiag, nz);
   else d_chol_smem(A, n, lane, idiag);
 }
@@ -172,7 +169,7 @@ __device__ __noinline__ void d_chol_solve_mem(const float* L, const float* idiag
   }
 }
 
-__device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, int n, float* x, int lane) {
+__device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, int n, int ld, float* x, int lane) {
   if (n > 64) {
     d_chol_solve_mem(L, idiag, n, x, lane);
     return;
@@ -187,8 +184,8 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
       if (k < 32) x0 = xk;
       else x1 = xk;
     }
-    if (lane > k && lane < n) x0 -= L[lane * n + k] * xk;
-    if (lane + 32 > k && lane + 32 < n) x1 -= L[(lane + 32) * n + k] * xk;
+    if (lane > k && lane < n) x0 -= L[lane * ld + k] * xk;
+    if (lane + 32 > k && lane + 32 < n) x1 -= L[(lane + 32) * ld + k] * xk;
   }
 #pragma unroll 1
   for (int k = n - 1; k >= 0; k--) {
@@ -198,8 +195,8 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
       if (k < 32) x0 = xk;
       else x1 = xk;
     }
-    if (lane < k && lane < n) x0 -= L[k * n + lane] * xk;
-    if (lane + 32 < k && lane + 32 < n) x1 -= L[k * n + lane + 32] * xk;
+    if (lane < k && lane < n) x0 -= L[k * ld + lane] * xk;
+    if (lane + 32 < k && lane + 32 < n) x1 -= L[k * ld + lane + 32] * xk;
   }
   if (lane < n) x[lane] = x0;
   if (lane + 32 < n) x[lane + 32] = x1;
@@ -235,7 +232,7 @@ __device__ __forceinline__ float cone_entry(const float* J, const float* hau, in
 }
 
 __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
-                                           int n, int lane, const int* it, int i_tri, float* L, float* idiag,
+                                           int n, int ld, int lane, const int* it, int i_tri, float* L, float* idiag,
                                            const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0) {
   const int ntri = n * (n + 1) / 2;
 #pragma unroll 1
@@ -259,10 +256,10 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
       s0 += eD[r0] * J[r0 * n + i] * J[r0 * n + j];
     }
     if (ncone) s1 += cone_entry(J, hau, ne, cones, ncone, n, i, j);
-    L[i * n + j] = (s0 + s1) + (s2 + s3);
+    L[i * ld + j] = (s0 + s1) + (s2 + s3);
   }
   __syncwarp();
-  d_chol(L, n, lane, idiag);
+  d_chol(L, n, ld, lane, idiag);
 }
 
 // Row-sparse variant for large models (nv > 64, HBM workspaces): a contact
@@ -335,7 +332,7 @@ __device__ __noinline__ void d_factor_sparse(const float* M, const float* J, con
     }
     __syncwarp();
   }
-  d_chol(L, n, lane, idiag, nz);
+  d_chol(L, n, n, lane, idiag, nz);
 }
 
 // ell: rows weigh with HD instead of D, plus the middle-zone cones
@@ -349,7 +346,7 @@ __device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const
   const float* eD = efc + (ell ? EFC_HD : EFC_D) * ne;
   const float* hau = efc + EFC_HA * ne;
   if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag, cones, ncone, hau, ne);
-  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne);
+  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, m.ldh, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne);
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
@@ -1121,7 +1118,7 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
 #pragma unroll 1
     for (int i = lane; i < nv; i += 32) p[i] = -grad[i];
     __syncwarp();
-    d_chol_solve(H, idiag, nv, p, lane);
+    d_chol_solve(H, idiag, nv, m.ldh, p, lane);
     // line-search coefficients A = p'Mp, B = p'Md, q = J p
     float A = 0, B = 0, gp = 0;
 #pragma unroll 1

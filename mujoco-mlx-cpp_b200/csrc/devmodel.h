@@ -10,7 +10,9 @@
 
 #define MJB_CONTACT_FLOATS 16  // pos3 frame9 dist pair(bits) dim includemargin
 
-struct DevModelDesc {
+// alignas(16): the per-warp shared-memory copies of the descriptor precede
+// the workspaces, which need 16-byte alignment for vector loads
+struct alignas(16) DevModelDesc {
   // sizes
   int nq, nv, nu, nbody, njnt, ngeom, npair, nlimit, nfloss, nlevel, nmesh;
   int ncon_max, nefc_max, ntri;
@@ -70,6 +72,8 @@ struct DevModelDesc {
   // phase region K (kinematics / dynamics), aliased by region S (solver)
   int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;
   int w_J, w_efc, w_H, w_active, w_nz;   // w_nz: nv ints, nonzero columns of one row (row-sparse H build)
+  int ldh;       // leading dimension of H / its factor at w_H: nv rounded up to 4 for nv <= 32 (then 32 floats of
+                 // 16-byte aligned column scratch follow the nv x ldh matrix), nv otherwise
 };
 
 // per-tendon floats: range lo, hi, margin, frictionloss, stiffness, damping,

@@ -261,7 +261,7 @@ __device__ __noinline__ void d_qacc_smooth(Env& E) {
   __syncwarp();
   float* idiag = ws + m.w_vec + 8 * nv;
   d_factor(E, nullptr, 0, nullptr, 0.f, H, idiag);
-  d_chol_solve(H, idiag, nv, ws + m.w_qas, lane);
+  d_chol_solve(H, idiag, nv, m.ldh, ws + m.w_qas, lane);
 }
 
 // bad-acceleration check, implicit-damping solve, warm-start save, integration.
@@ -287,7 +287,7 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
     __syncwarp();
     float* idiag = ws + m.w_vec + 8 * nv;
     d_factor(E, nullptr, 0, E.ft + m.f_dof_damping_implicit, m.timestep, H, idiag);
-    d_chol_solve(H, idiag, nv, acc, lane);
+    d_chol_solve(H, idiag, nv, m.ldh, acc, lane);
     a = acc;
   }
 #pragma unroll 1
