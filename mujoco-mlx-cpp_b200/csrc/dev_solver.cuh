@@ -54,14 +54,20 @@ __device__ __noinline__ void d_chol_smem(float* A, int n, int lane, float* idiag
 // entries k+1..i four at a time with 16-byte loads and stores, reading the
 // posted column with broadcast loads instead of one shuffle per entry.  The
 // last group of a row may reach past its diagonal into the padded upper
-// triangle, which nothing reads.  Same arithmetic in the same order as
-// d_chol_smem (bitwise identical factors).
+// triangle, which nothing reads.  The updates are d_chol_smem's in the same
+// order; the pivot's 1 / sqrt is the hardware estimate refined by one Newton
+// step instead of IEEE sqrt and division.
 __device__ __noinline__ void d_chol_vec(float* A, int n, int ld, int lane, float* idiag, float* col) {
   const bool own = lane < n;
   float* row = A + lane * ld;
 #pragma unroll 1
   for (int k = 0; k < n; k++) {
-    const float d = sqrtf(fmaxf(A[k * ld + k], 1e-30f)), id = 1.f / d;
+    // pivot: 1 / sqrt from the hardware estimate plus one Newton step
+    // (about 1 ulp), d = akk / sqrt(akk)
+    const float akk = fmaxf(A[k * ld + k], 1e-30f);
+    float id = rsqrtf(akk);
+    id = id * fmaf(-0.5f * akk * id, id, 1.5f);
+    const float d = akk * id;
     const bool below = own && lane > k;
     float l = 0.f;
     if (below) {
@@ -235,10 +241,15 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
                                            int n, int ld, int lane, const int* it, int i_tri, float* L, float* idiag,
                                            const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0) {
   const int ntri = n * (n + 1) / 2;
+  (void)it;
+  (void)i_tri;
 #pragma unroll 1
   for (int t = lane; t < ntri; t += 32) {
-    int packed = ldi(it, i_tri + t);
-    int i = packed >> 16, j = packed & 0xffff;
+    // entry t of the lower triangle in row-major order (row i, column j)
+    int i = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+    if ((i + 1) * (i + 2) / 2 <= t) i++;
+    else if (i * (i + 1) / 2 > t) i--;
+    const int j = t - i * (i + 1) / 2;
     float s0 = M[i * n + j], s1 = 0, s2 = 0, s3 = 0;
     if (i == j && ddiag) s0 += dscale * ldf(ddiag, i);
     int a = 0;
