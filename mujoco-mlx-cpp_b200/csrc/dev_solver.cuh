@@ -175,9 +175,60 @@ __device__ __noinline__ void d_chol_solve_mem(const float* L, const float* idiag
   }
 }
 
+// n <= 32 with rows padded to ld (a multiple of 4): the substitutions go
+// four columns per group, loading the group's factor entries (one 16-byte
+// row load forward, four row loads backward) and pivots before its four
+// dependent shuffle steps, so the chain waits on shuffles only.  Same
+// arithmetic in the same order as the general version.
+__device__ __noinline__ void d_chol_solve32(const float* L, const float* idiag, int n, int ld, float* x, int lane) {
+  const bool own = lane < n;
+  float x0 = own ? x[lane] : 0.f;
+  const float* Lr = L + lane * ld;
+#pragma unroll 1
+  for (int k0 = 0; k0 < n; k0 += 4) {
+    const float4 lr = own ? *reinterpret_cast<const float4*>(Lr + k0) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float lq[4] = {lr.x, lr.y, lr.z, lr.w};
+    float dg[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) dg[q] = k0 + q < n ? idiag[k0 + q] : 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int k = k0 + q;
+      if (k >= n) break;
+      const float xk = __shfl_sync(FULL_MASK, x0, k) * dg[q];
+      if (lane == k) x0 = xk;
+      else if (lane > k) x0 -= lq[q] * xk;
+    }
+  }
+#pragma unroll 1
+  for (int k0 = n - 1; k0 >= 0; k0 -= 4) {
+    float lk[4], dg[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int k = k0 - q;
+      lk[q] = k >= 0 && lane < k ? L[k * ld + lane] : 0.f;
+      dg[q] = k >= 0 ? idiag[k] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int k = k0 - q;
+      if (k < 0) break;
+      const float xk = __shfl_sync(FULL_MASK, x0, k) * dg[q];
+      if (lane == k) x0 = xk;
+      else if (lane < k) x0 -= lk[q] * xk;
+    }
+  }
+  if (own) x[lane] = x0;
+  __syncwarp();
+}
+
 __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, int n, int ld, float* x, int lane) {
   if (n > 64) {
     d_chol_solve_mem(L, idiag, n, x, lane);
+    return;
+  }
+  if (n <= 32) {
+    d_chol_solve32(L, idiag, n, ld, x, lane);
     return;
   }
   float x0 = lane < n ? x[lane] : 0.f;
