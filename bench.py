@@ -313,6 +313,69 @@ def time_e2e(sim, host_ctrl, K, W, flush, world):
     return e2e_s
 
 
+def mixed_batch(K, W, flush, B=8192, seed=8100):
+    """The mixed workload: 8192 envs drawn 50/30/20 from the quadruped, the
+    21-DoF capsule humanoid and the 7-hinge arm with gripper and free box in
+    one persistent launch, mass x U[0.8, 1.2] and friction x U[0.5, 1.25]
+    per env, seeded random controls every env-step, the launch shape from
+    the autotuner (its cached choice).  Plain solver; env-steps/s over
+    min(K, 20) timed env-steps of 4 substeps, CUDA events, L2 flushed."""
+    import numpy as np
+    import torch
+
+    import mjb200
+
+    mods = [mjb200.load_model_from_string(f()) for f in (mjb200.models.quadruped_xml, mjb200.models.humanoid_xml, mjb200.models.arm_xml)]
+    counts = [int(B * f) for f in (0.5, 0.3, 0.2)]
+    counts[0] += B - sum(counts)
+    sim = mjb200.BatchedSim(mods, counts, domain_rand=1, record=0)
+    rng = np.random.default_rng(seed)
+    e0 = 0
+    for m, n in zip(mods, counts):
+        nb = int(m.dump()["sizes"][3])
+        sim.set_env_params(np.arange(e0, e0 + n), mass_scale=rng.uniform(0.8, 1.2, size=(n, nb)), friction_scale=rng.uniform(0.5, 1.25, size=n))
+        e0 += n
+    qs, vs = [], []
+    for i, (m, n) in enumerate(zip(mods, counts)):
+        h = (0.28, 0.34) if i == 0 else (1.25, 1.35) if i == 1 else None
+        q, v = mjb200.models.random_state(m, n, seed=seed + i, height=h)
+        qs.append(q.reshape(-1))
+        vs.append(v.reshape(-1))
+    q0 = np.concatenate(qs).astype(np.float32)
+    v0 = np.concatenate(vs).astype(np.float32)
+    nt = min(K, 20)
+    steps = W + nt
+    ctrl = np.stack([np.concatenate([mjb200.models.random_controls(m, n, s, seed=seed + 10 + i).reshape(-1) for i, (m, n) in enumerate(zip(mods, counts))])
+                     for s in range(steps)]).astype(np.float32)
+    cdev = torch.from_numpy(ctrl).cuda()
+    sim.set_state(q0, v0)
+    cached = sim.autotune_cached(nsub=SUBSTEPS, reps=2)
+    sim.set_state(q0, v0)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    for w in range(W):
+        sim.step_device_ctrl(cdev[w].data_ptr(), SUBSTEPS)
+    sim.sync()
+    ms = []
+    for k in range(nt):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step_device_ctrl(cdev[W + k].data_ptr(), SUBSTEPS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    st = sim.stats()
+    out = {"workload": "mixed: 8192 envs, quadruped 4097 / capsule humanoid (nv 23) 2457 / 7-hinge arm with gripper and free box 1638, "
+                       "mass x U[0.8, 1.2], friction x U[0.5, 1.25], 4 substeps x dt per model, plain solver",
+           "value": B * 1e3 / float(np.median(ms)), "unit": UNIT, "ms_per_step_median": float(np.median(ms)), "steps": nt,
+           "launch": sim.launch_shape(), "autotune_cached": bool(cached), "contacts_per_env_mean": float(st["ncon"].mean()),
+           "contacts_per_env_max": int(st["ncon"].max()), "newton_iter_mean": float(st["niter_sum"].mean() / SUBSTEPS),
+           "status_nonzero": int((st["status"] != 0).sum())}
+    sim.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -357,6 +420,7 @@ def run_ours(args, world, rank, local):
                      "newton_iter_p99": float(np.percentile(st["niter_max"], 99)),
                      "predicted_warmstart_share": float(np.mean(st["warm_choice"] == 2)), "launch": sim.launch_shape()}
         sim.close()
+    cfg3 = mixed_batch(K, W, flush)
     clocks = sampler.stop()
     h2d = B * nu * 4
     d2h = B * (m.nq + m.nv) * 4
@@ -388,6 +452,7 @@ def run_ours(args, world, rank, local):
                                    "warm start as a third candidate (previous-step and qacc_smooth kept as fallback), same tolerance 1e-8",
                        "learned": L, "plain": P, "learned_over_plain": L["value"] / P["value"],
                        "iteration_reduction": 1.0 - L["newton_iter_mean"] / max(P["newton_iter_mean"], 1e-9), "training": train_info},
+            "config3_mixed": cfg3,
             "clocks": clocks}
     if world == 1:
         line["cpu_baseline"] = cpu_reference(B, args.cpu_seconds)

@@ -58,12 +58,21 @@ MJMLX_API MjmlxBatchedSim* mjb200_batched_create_multi(const MjmlxModel* const* 
 MJMLX_API int mjb200_batched_configure(MjmlxBatchedSim* sim, const MjbEngineConfig* ecfg);
 MJMLX_API int mjb200_batched_get_config(const MjmlxBatchedSim* sim, MjbEngineConfig* out);
 /* Launch-shape autotuner: times envs-per-CTA 2/4/8/16 with lockstep CTAs and
- * with the independent-warp work queue, reps launches of nsub substeps each,
- * from the sim's current state (restored before every candidate and at the
- * end), and keeps the fastest.  Per candidate i (at most max_candidates):
- * warps[i], lockstep[i], ms[i] (mean per launch, -1 if it cannot launch);
- * any array may be NULL.  Returns the number of candidates, or -1. */
+ * with the independent-warp work queue (CTAs per SM at the occupancy
+ * limit), and lockstep CTAs of 4 and 8 warps at one CTA per SM; reps
+ * launches of nsub substeps each, from the sim's current state (restored
+ * before every candidate and at the end), and keeps the fastest.  Per
+ * candidate i (at most max_candidates): warps[i], lockstep[i], ms[i] (mean
+ * per launch, -1 if it cannot launch); any array may be NULL.  Returns the
+ * number of candidates, or -1.  No counterpart in the reference (its
+ * per-kernel workgroup sizes are fixed, src/batched.cpp:53-57). */
 MJMLX_API int mjb200_batched_autotune(MjmlxBatchedSim* sim, int nsub, int reps, int max_candidates, int* warps, int* lockstep, float* ms);
+/* The autotuner's choice for the sim, cached per process by the compiled
+ * model tables, per-model env counts and capacities (and whether a learned
+ * net is attached): a sim of an already tuned batch takes the cached launch
+ * shape without timing anything.  Returns 1 when the cached choice was
+ * applied, 0 when it tuned now and stored the choice, -1 on error. */
+MJMLX_API int mjb200_batched_autotune_cached(MjmlxBatchedSim* sim, int nsub, int reps);
 
 /* Record layout: num_envs, sum of nq / nv / nu over envs, and the per-env
  * offsets (arrays of num_envs, each may be NULL). */

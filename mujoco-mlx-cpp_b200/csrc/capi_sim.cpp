@@ -258,6 +258,11 @@ MJMLX_API int mjb200_batched_autotune(MjmlxBatchedSim* sim, int nsub, int reps, 
   }, -1);
 }
 
+MJMLX_API int mjb200_batched_autotune_cached(MjmlxBatchedSim* sim, int nsub, int reps) {
+  if (!sim || !sim->engine || nsub <= 0 || reps <= 0) return -1;
+  return guard("mjb200_batched_autotune_cached", [&]() { return sim->engine->autotune_cached(nsub, reps) ? 1 : 0; }, -1);
+}
+
 MJMLX_API int mjb200_batched_layout(const MjmlxBatchedSim* sim, int* num_envs, int* total_q, int* total_v, int* total_u, int* qadr, int* vadr, int* uadr) {
   if (!sim) return -1;
   Engine& e = *sim->engine;

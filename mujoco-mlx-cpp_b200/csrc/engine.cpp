@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 cudaError_t mjb_launch_step(const StepParams& P, int grid, int warps_per_block, size_t smem_bytes, cudaStream_t stream);
@@ -613,9 +614,20 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
   check(cudaEventCreate(&e1), "event");
   const bool feat_valid = feat_valid_;
   const bool fused = fused_warmstart();
-  for (int lock : {1, 0}) {
-    for (int w : {2, 4, 8, 16}) {
-      TuneCandidate c{w, lock, 0, -1.f};
+  // CTA shapes: warps per CTA x lockstep, at the occupancy limit of CTAs
+  // per SM, plus lockstep CTAs of 4 and 8 warps at one CTA per SM
+  struct Shape {
+    int w, lock, bps;
+  };
+  std::vector<Shape> shapes;
+  for (int lock : {1, 0})
+    for (int w : {2, 4, 8, 16}) shapes.push_back({w, lock, 0});
+  shapes.push_back({4, 1, 1});
+  shapes.push_back({8, 1, 1});
+  for (const Shape& sh : shapes) {
+    const int w = sh.w, lock = sh.lock;
+    {
+      TuneCandidate c{w, lock, sh.bps, -1.f};
       // an attached per-env net runs inside the kernel: lockstep, 8 or 16 warps
       if (w * per_warp > 227 * 1024 || (fused && (!lock || (w != 8 && w != 16)))) {
         out.push_back(c);
@@ -625,7 +637,7 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
       cfg.warps_per_block = w;
       cfg.lockstep = lock;
       cfg.persistent = 1;
-      cfg.blocks_per_sm = 0;
+      cfg.blocks_per_sm = sh.bps;
       try {
         configure(cfg);
       } catch (const std::exception&) {
@@ -654,6 +666,7 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
   if (best) {
     cfg.warps_per_block = best->warps_per_block;
     cfg.lockstep = best->lockstep;
+    cfg.blocks_per_sm = best->blocks_per_sm;
     cfg.persistent = 1;
   }
   configure(cfg);
@@ -661,6 +674,50 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
   sync();
   feat_valid_ = feat_valid;
   return out;
+}
+
+namespace {
+std::mutex g_tune_mutex;
+std::map<uint64_t, Engine::TuneCandidate> g_tune_cache;
+
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; i++) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+}  // namespace
+
+bool Engine::autotune_cached(int nsub, int reps) {
+  uint64_t key = 1469598103934665603ull;
+  key = fnv1a(key, h_itab_.data(), h_itab_.size() * sizeof(int));
+  key = fnv1a(key, h_ftab_.data(), h_ftab_.size() * sizeof(float));
+  key = fnv1a(key, counts_.data(), counts_.size() * sizeof(int));
+  for (const auto& L : layouts_) key = fnv1a(key, &L.desc, sizeof(L.desc));
+  const int fused = fused_warmstart() ? 1 : 0;
+  key = fnv1a(key, &fused, sizeof(fused));
+  TuneCandidate hit{0, 0, 0, -1.f};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) hit = it->second;
+  }
+  if (hit.warps_per_block > 0) {
+    EngineConfig cfg = cfg_;
+    cfg.warps_per_block = hit.warps_per_block;
+    cfg.lockstep = hit.lockstep;
+    cfg.blocks_per_sm = hit.blocks_per_sm;
+    cfg.persistent = 1;
+    configure(cfg);
+    return true;
+  }
+  autotune(nsub, reps);
+  TuneCandidate chosen{warps_, lockstep_, cfg_.blocks_per_sm, 0.f};
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache[key] = chosen;
+  return false;
 }
 
 void Engine::launch_shape(int* grid, int* warps, int* smem, int* persistent) const {

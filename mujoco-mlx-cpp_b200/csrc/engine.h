@@ -162,6 +162,11 @@ class Engine {
     float ms;  // mean per launch; < 0 when the shape cannot launch
   };
   std::vector<TuneCandidate> autotune(int nsub, int reps);
+  // The autotuner's choice for this sim's batch, from a process-wide cache
+  // keyed by the compiled model tables, the per-model env counts and the
+  // contact / row capacities (a learned net attached counts too); tunes and
+  // stores it on a miss.  Returns true when the cached choice was applied.
+  bool autotune_cached(int nsub, int reps);
   const EngineConfig& config() const { return cfg_; }
   void launch_shape(int* grid, int* warps, int* smem_bytes, int* persistent) const;
   int lockstep() const { return lockstep_; }

@@ -94,6 +94,7 @@ def _load():
         "mjb200_batched_set_qacc_warmstart": (C.c_int, [C.c_void_p, _f32p]),
         "mjb200_batched_pack_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
         "mjb200_batched_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p]),
+        "mjb200_batched_autotune_cached": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "mjb200_batched_step_warmstart": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
         "mjb200_batched_step_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
         "mjb200_batched_device_state": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
@@ -365,6 +366,14 @@ class BatchedSim:
         if n < 0:
             raise RuntimeError(last_error())
         return [(int(w[i]), int(l[i]), float(t[i])) for i in range(n)]
+
+    def autotune_cached(self, nsub: int = 4, reps: int = 3) -> bool:
+        """The autotuner's choice from the process-wide cache (True) or tuned
+        now and stored (False)."""
+        r = lib.mjb200_batched_autotune_cached(self.handle, nsub, reps)
+        if r < 0:
+            raise RuntimeError(last_error())
+        return r == 1
 
     def step_warmstart(self, qacc_ptr: int, n: int = 1):
         if lib.mjb200_batched_step_warmstart(self.handle, C.c_void_p(qacc_ptr), n) != 0:

@@ -136,3 +136,73 @@ def test_autotuner_choice_keeps_results():
             sim.step(c, 4)
         out.append(sim.state())
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_config3_8192_mixed_sampled_parity():
+    """The mixed workload at its stated size: 8192 envs drawn 50/30/20 from
+    the quadruped, the capsule humanoid and the arm with gripper and free
+    box, mass x U[0.8, 1.2] and friction x U[0.5, 1.25] per env, in one
+    persistent launch; after 8 control steps, one recorded substep compared
+    with the oracle on 64 sampled envs per model (contacts, rows, qacc)."""
+    models = _models()
+    B = 8192
+    counts = _counts(B)
+    assert counts == [4097, 2457, 1638]
+    sim = mjb200.BatchedSim(models, counts, domain_rand=1, ncon_max=32, nefc_max=96)
+    scales = _randomise(sim, models, counts, np.random.default_rng(8192))
+    qs, vs = _states(models, counts, 170)
+    sim.set_state(_flat(qs), _flat(vs))
+    for c in range(8):
+        sim.step(_flat(_ctrls(models, counts, c, 170)), 4)
+    assert np.all(sim.stats()["status"] == 0)
+    qp, qv = sim.state()
+    ctrl = _ctrls(models, counts, 8, 170)
+    sim.set_debug(32, 96)
+    sim.step(_flat(ctrl), 1)
+    con, efc, vec = sim.get_debug()
+    st = sim.stats()
+    qps, qvs = _split(qp, models, counts, "nq"), _split(qv, models, counts, "nv")
+    e0, nbound = 0, 0
+    for k, (m, n) in enumerate(zip(models, counts)):
+        om = oracle.OracleModel(m.dump())
+        ms, fs = scales[k]
+        errs, ncons = [], []
+        for i in range(0, n, n // 64)[:64]:
+            e = e0 + i
+            env = oracle.OracleEnv(om, 32, 96)
+            env.a["qpos"][:] = qps[k][i]
+            env.a["qvel"][:] = qvs[k][i]
+            env.a["ctrl"][: om.nu] = ctrl[k][i].astype(np.float32)
+            mass = np.ascontiguousarray(ms[i].astype(np.float32), np.float64)
+            rand = oracle.ORand(mass.ctypes.data_as(C.POINTER(C.c_double)), float(np.float32(fs[i])), None)
+            env.step(0, rand)
+            ok, nb = contact_sets_match(con[e], env.contacts(), st["ncon"][e])
+            assert ok, (k, i)
+            nbound += nb
+            ncons.append(int(st["ncon"][e]))
+            if nb == 0:
+                assert st["nefc"][e] == env.d.nefc, (k, i)
+                errs.append(rel_err(vec[e, 2, : om.nv], env.a["qacc"]))
+        errs = np.array(errs)
+        print("config 3 model", k, "envs", n, "contacts per env: mean %.1f max %d" % (np.mean(ncons), max(ncons)),
+              "qacc rel err median %.2e max %.2e" % (np.median(errs), errs.max()))
+        assert np.median(errs) <= 1e-4 and errs.max() <= 2e-3, (k, np.median(errs), errs.max())
+        e0 += n
+    assert nbound <= 3
+
+
+def test_autotune_cache_reuses_choice():
+    """A second sim of the same mixed batch takes the first sim's tuned
+    launch shape from the cache without timing anything."""
+    models = _models()
+    counts = _counts(512)
+    qs, vs = _states(models, counts, 95)
+    a = mjb200.BatchedSim(models, counts)
+    a.set_state(_flat(qs), _flat(vs))
+    first = a.autotune_cached(nsub=2, reps=1)
+    b = mjb200.BatchedSim(models, counts)
+    b.set_state(_flat(qs), _flat(vs))
+    assert b.autotune_cached(nsub=2, reps=1)
+    assert b.launch_shape() == a.launch_shape()
+    c = mjb200.BatchedSim(models, _counts(600))          # another batch: not cached yet
+    assert not c.autotune_cached(nsub=2, reps=1) or first is False
