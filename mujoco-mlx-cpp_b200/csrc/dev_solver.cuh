@@ -260,6 +260,109 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
   __syncwarp();
 }
 
+// Explicit inverses N = A^-1 for n <= 32 (full storage, rows padded to
+// ld, a multiple of 4, with zeros past column n; row i on lane i).
+
+// In-place inversion by the symmetric sweep operator on every pivot.  Step
+// k: d = a_kk; every row i != k becomes a_i - (a_ik / d) a_k with entry k set
+// to -a_ik / d; row k becomes a_k / d with entry k = 1 / d.  After all n
+// steps A holds A^-1.  The pivots are Schur complements of an SPD matrix,
+// so they stay positive and no pivoting is needed.  The pivot row is first
+// copied to col (16-byte aligned, ld floats), so every lane, its owner
+// included (factor 1 - 1/d gives a_k / d), updates its own row from the
+// copy with 16-byte loads and stores.
+__device__ __noinline__ void d_sweep(float* A, int n, int ld, int lane, float* col) {
+  const bool own = lane < n;
+  float* row = A + lane * ld;
+#pragma unroll 1
+  for (int k = 0; k < n; k++) {
+    __syncwarp();
+    if (lane < ld) col[lane] = A[k * ld + lane];
+    __syncwarp();
+    const float id = __frcp_rn(col[k]);
+    if (own) {
+      const float f = lane == k ? 1.f - id : row[k] * id;
+#pragma unroll 2
+      for (int j = 0; j < ld; j += 4) {
+        float4 a = *reinterpret_cast<float4*>(row + j);
+        const float4 c = *reinterpret_cast<const float4*>(col + j);
+        a.x = fmaf(-f, c.x, a.x);
+        a.y = fmaf(-f, c.y, a.y);
+        a.z = fmaf(-f, c.z, a.z);
+        a.w = fmaf(-f, c.w, a.w);
+        *reinterpret_cast<float4*>(row + j) = a;
+      }
+      row[k] = lane == k ? id : -f;
+    }
+  }
+  __syncwarp();
+}
+
+// sum_j a[j] x[j] over ld floats (both 16-byte aligned)
+__device__ __forceinline__ float row_dot4(const float* a, const float* x, int ld) {
+  float s0 = 0.f, s1 = 0.f;
+#pragma unroll 2
+  for (int j = 0; j < ld; j += 4) {
+    const float4 p = *reinterpret_cast<const float4*>(a + j);
+    const float4 q = *reinterpret_cast<const float4*>(x + j);
+    s0 = fmaf(p.x, q.x, s0);
+    s1 = fmaf(p.y, q.y, s1);
+    s0 = fmaf(p.z, q.z, s0);
+    s1 = fmaf(p.w, q.w, s1);
+  }
+  return s0 + s1;
+}
+
+// y = N v for the inverse N (lane i returns y_i; lanes >= n return 0).
+// col: 16-byte aligned scratch of ld floats, v: n floats.
+__device__ __noinline__ float d_inv_apply(const float* N, int n, int ld, float* col, const float* v, int lane) {
+  __syncwarp();
+  if (lane < ld) col[lane] = lane < n ? v[lane] : 0.f;
+  __syncwarp();
+  const float y = lane < n ? row_dot4(N + lane * ld, col, ld) : 0.f;
+  __syncwarp();
+  return y;
+}
+
+// N = A^-1 updated for A + sgn x x' with x = w J_r (one constraint row),
+// by Sherman-Morrison: u = N x, s = x'u, N -= sgn u u' / (1 + sgn s).  For
+// an update the denominator is 1 + x'A^-1 x >= 1; for a downdate it is
+// 1 - x'A^-1 x in (0, 1], and below 0.02 (the row carries nearly all of A
+// along x, so the subtraction cancels and rounding errors grow by up to the
+// reciprocal) the call returns false with N unchanged and the caller
+// rebuilds the inverse.  Measured on the quadruped, bounds of 0.1 and 0.3
+// rebuild more often and cost more time than the extra Newton iterations
+// that the looser bound brings.
+__device__ __noinline__ bool d_inv_rank1(float* N, int n, int ld, float* col, const float* Jr, float w, float sgn, int lane) {
+  const bool own = lane < n;
+  float* row = N + lane * ld;
+  __syncwarp();
+  const float x = own ? w * Jr[lane] : 0.f;
+  if (lane < ld) col[lane] = x;
+  __syncwarp();
+  const float u = own ? row_dot4(row, col, ld) : 0.f;
+  const float den = 1.f + sgn * warp_sum(x * u);
+  if (!(den > 0.02f)) return false;
+  const float gu = -sgn * __frcp_rn(den) * u;
+  __syncwarp();
+  if (lane < ld) col[lane] = u;
+  __syncwarp();
+  if (own) {
+#pragma unroll 2
+    for (int j = 0; j < ld; j += 4) {
+      float4 a = *reinterpret_cast<float4*>(row + j);
+      const float4 c = *reinterpret_cast<const float4*>(col + j);
+      a.x = fmaf(gu, c.x, a.x);
+      a.y = fmaf(gu, c.y, a.y);
+      a.z = fmaf(gu, c.z, a.z);
+      a.w = fmaf(gu, c.w, a.w);
+      *reinterpret_cast<float4*>(row + j) = a;
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
 // A = M + sum over the listed rows r of D_r J_r' J_r + dscale * diag(ddiag),
 // built in shared memory from the lower-triangle entry table (entries spread
 // over the lanes), then factored by the right-looking shared-memory Cholesky
@@ -288,9 +391,11 @@ __device__ __forceinline__ float cone_entry(const float* J, const float* hau, in
   return s;
 }
 
+// inv = true (n <= 32, no cones): both triangles and zero padding are
+// written and L receives N = A^-1 from the sweep instead of the factor.
 __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
                                            int n, int ld, int lane, const int* it, int i_tri, float* L, float* idiag,
-                                           const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0) {
+                                           const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0, bool inv = false) {
   const int ntri = n * (n + 1) / 2;
   (void)it;
   (void)i_tri;
@@ -319,6 +424,15 @@ __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const
     }
     if (ncone) s1 += cone_entry(J, hau, ne, cones, ncone, n, i, j);
     L[i * ld + j] = (s0 + s1) + (s2 + s3);
+    if (inv) L[j * ld + i] = (s0 + s1) + (s2 + s3);
+  }
+  if (inv) {
+#pragma unroll 1
+    for (int i = lane; i < n; i += 32)
+      for (int j = n; j < ld; j++) L[i * ld + j] = 0.f;
+    __syncwarp();
+    d_sweep(L, n, ld, lane, L + n * ld);
+    return;
   }
   __syncwarp();
   d_chol(L, n, ld, lane, idiag);
@@ -398,8 +512,9 @@ __device__ __noinline__ void d_factor_sparse(const float* M, const float* J, con
 }
 
 // ell: rows weigh with HD instead of D, plus the middle-zone cones
+// inv = true (nv <= 32, no cones): L receives N = A^-1 instead of the factor
 __device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const float* ddiag, float dscale, float* L, float* idiag,
-                                         bool ell = false, const int* cones = nullptr, int ncone = 0) {
+                                         bool ell = false, const int* cones = nullptr, int ncone = 0, bool inv = false) {
   const DevModelDesc& m = *E.md;
   const int nv = m.nv, ne = m.nefc_max;
   const float* M = E.ws + m.w_M;
@@ -408,7 +523,7 @@ __device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const
   const float* eD = efc + (ell ? EFC_HD : EFC_D) * ne;
   const float* hau = efc + EFC_HA * ne;
   if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag, cones, ncone, hau, ne);
-  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, m.ldh, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne);
+  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, m.ldh, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne, inv);
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {
@@ -1076,16 +1191,78 @@ __device__ __forceinline__ float grad_update(const float* J, const float* force,
 
 // Newton solve from the warm start; x (w_x) holds the result.  Returns the
 // iteration count.  vec: Md, grad, p, Mp, tmp, -, -, -, idiag.
-// The Hessian factor is rebuilt only when the set of rows in their quadratic
-// zone changed since the last factorisation.  Termination: improvement or
-// gradient below tolerance * meaninertia * nv, where the gradient test also
-// accepts the FP32 round-off floor of the gradient (16 eps times the norm of
-// the terms it is summed from) -- below that floor FP32 cannot resolve it.
-template <bool EXT>
-__device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int max_iter, const float* xpred, int& choice) {
+// The Hessian changes only when the set of rows in their quadratic zone
+// does.  INV = true (for nv <= 32 without elliptic cones and nefc <= 128;
+// the caller checks) keeps the inverse N = H^-1 instead of a factor, and
+// updates it
+// incrementally (MuJoCo's Newton solver keeps its factor incrementally the
+// same way): rows that entered the set since the last rebuild are added and
+// rows that left are removed by Sherman-Morrison rank-1 steps, as long as at
+// most kMaxRank1 rows changed; more changes, or a removal that cancels,
+// rebuild N from H by the sweep.  The direction is then p = -N g, one
+// matrix-vector product instead of two triangular solves.  hm = true says
+// H still holds M^-1 from the unconstrained solve, which then serves as
+// the starting inverse (no active rows: no rebuild at all).
+// Termination: improvement or gradient below tolerance * meaninertia * nv,
+// where the gradient test also accepts the FP32 round-off floor of the
+// gradient (16 eps times the norm of the terms it is summed from) -- below
+// that floor FP32 cannot resolve it.
+constexpr int kMaxRank1 = 32;
+
+// Inverse mode of the Newton solver (nv <= 32, no elliptic cones, nefc <=
+// 128): bring N = H^-1 in the H slot up to the rows now in their quadratic
+// zone, then the direction p = -N grad (solver vectors 2 and 1).  The row-set words are in the sparse-index slot: words 0-3 the rows
+// N includes, words 4-7 the rows active now.  have = false: N holds nothing
+// usable (rebuild).  Otherwise up to kMaxRank1 changed rows go in by
+// Sherman-Morrison (additions first), and more, or a cancelling removal,
+// rebuild N from M and the listed active rows by the sweep.
+__device__ __noinline__ void d_hinv_direction(Env& E, const int* act_list, int nact, bool have) {
+  const DevModelDesc& m = *E.md;
+  const int nv = m.nv, lane = E.lane;
+  float* ws = E.ws;
+  float* H = ws + m.w_H;
+  float* hcol = H + nv * m.ldh;
+  unsigned* wd = reinterpret_cast<unsigned*>(ws + m.w_nz);
+  const float* J = ws + m.w_J;
+  const float* eD = ws + m.w_efc + EFC_D * m.nefc_max;
+  int nch = 0;
+#pragma unroll
+  for (int c = 0; c < 4; c++) nch += __popc(wd[c] ^ wd[4 + c]);
+  bool full = !have || nch > kMaxRank1;
+  if (!full && nch > 0) {
+#pragma unroll 1
+    for (int c = 0; c < 4; c++) {
+      unsigned b = wd[4 + c] & ~wd[c];
+      while (b) {
+        const int r = 32 * c + __ffs(b) - 1;
+        b &= b - 1;
+        d_inv_rank1(H, nv, m.ldh, hcol, J + r * nv, sqrtf(eD[r]), 1.f, lane);
+      }
+    }
+#pragma unroll 1
+    for (int c = 0; c < 4 && !full; c++) {
+      unsigned b = wd[c] & ~wd[4 + c];
+      while (b && !full) {
+        const int r = 32 * c + __ffs(b) - 1;
+        b &= b - 1;
+        full = !d_inv_rank1(H, nv, m.ldh, hcol, J + r * nv, sqrtf(eD[r]), -1.f, lane);
+      }
+    }
+  }
+  if (full) d_factor(E, act_list, nact, nullptr, 0.f, H, nullptr, false, nullptr, 0, true);
+  __syncwarp();
+  if (lane < 4) wd[lane] = wd[4 + lane];
+  float* vec = ws + m.w_vec;
+  const float pi = d_inv_apply(H, nv, m.ldh, hcol, vec + nv, lane);
+  if (lane < nv) vec[2 * nv + lane] = -pi;
+  __syncwarp();
+}
+
+template <bool EXT, bool INV>
+__device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int max_iter, const float* xpred, int& choice, bool hm) {
   (void)P;
   const DevModelDesc& m = *E.md;
-  const bool ell = EXT && m.cone == 1;
+  const bool ell = !INV && EXT && m.cone == 1;
   const int nv = m.nv, ne = m.nefc_max, lane = E.lane, ls_iter = m.ls_iterations;
   float* ws = E.ws;
   const float* M = ws + m.w_M;
@@ -1145,16 +1322,27 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
   if (nefc == 0 || scale * sqrtf(gn) < tol || gn <= eps_floor * eps_floor * terms) return 0;
   int nact_prev = -1;
   int niter = 0;
+  // inverse mode (INV: the caller checked nv <= 32, nefc <= 128, no
+  // elliptic cones): the row-set words live in the sparse-index slot (words
+  // 0-3: rows in N, 4-7: rows in their quadratic zone; bit r % 32 of word
+  // r / 32), written by lane 0
+  constexpr bool inc = INV;
+  bool have = hm;
+  if (inc && lane == 0)
+    for (int c = 0; c < 8; c++) reinterpret_cast<unsigned*>(ws + m.w_nz)[c] = 0u;
 #pragma unroll 1
   for (int iter = 0; iter < max_iter; iter++) {
     // compact list of rows in their quadratic zone (order preserved)
     int nact = 0;
     bool changed = false;
+    if (inc && lane == 0)
+      for (int c = 4; c < 8; c++) reinterpret_cast<unsigned*>(ws + m.w_nz)[c] = 0u;
 #pragma unroll 1
     for (int base = 0; base < nefc; base += 32) {
       int r = base + lane;
       bool q = r < nefc && (ell ? eHD[r] > 0.f : row_quad((int)eT[r], eD[r], eL[r], eY[r]));
       unsigned b = __ballot_sync(FULL_MASK, q);
+      if (inc && lane == 0) reinterpret_cast<unsigned*>(ws + m.w_nz)[4 + (base >> 5)] = b;
       int pos = nact + __popc(b & ((1u << lane) - 1u));
       if (q) {
         if (nact_prev < 0 || pos >= nact_prev || act_list[pos] != r) changed = true;
@@ -1173,14 +1361,19 @@ __device__ __noinline__ int d_newton(Env& E, const StepParams& P, int nefc, int 
     int* cones = act_list + ne - 1;
     const int ncone = ell ? d_cone_list(E, nefc, cones) : 0;
     if (ncone) changed = true;
-    if (changed) {
-      d_factor(E, act_list, nact, nullptr, 0.f, H, idiag, ell, cones, ncone);
-      nact_prev = nact;
-    }
+    if constexpr (INV) {
+      d_hinv_direction(E, act_list, nact, have);
+      have = true;
+    } else {
+      if (changed) {
+        d_factor(E, act_list, nact, nullptr, 0.f, H, idiag, ell, cones, ncone);
+        nact_prev = nact;
+      }
 #pragma unroll 1
-    for (int i = lane; i < nv; i += 32) p[i] = -grad[i];
-    __syncwarp();
-    d_chol_solve(H, idiag, nv, m.ldh, p, lane);
+      for (int i = lane; i < nv; i += 32) p[i] = -grad[i];
+      __syncwarp();
+      d_chol_solve(H, idiag, nv, m.ldh, p, lane);
+    }
     // line-search coefficients A = p'Mp, B = p'Md, q = J p
     float A = 0, B = 0, gp = 0;
 #pragma unroll 1

@@ -71,7 +71,8 @@ struct alignas(16) DevModelDesc {
   int w_con, w_rowcon;
   // phase region K (kinematics / dynamics), aliased by region S (solver)
   int w_xpos, w_xquat, w_xmat, w_xipos, w_xanchor, w_xaxis, w_gxpos, w_gxmat, w_cinert, w_crb, w_cvel, w_cdofdot, w_cacc, w_tmp;
-  int w_J, w_efc, w_H, w_active, w_nz;   // w_nz: nv ints, nonzero columns of one row (row-sparse H build)
+  int w_J, w_efc, w_H, w_active, w_nz;   // w_nz: max(nv, 8) ints: nonzero columns of one row (row-sparse H build,
+                                         // nv > 64), or the Newton inverse mode's row-set words (nv <= 32)
   int ldh;       // leading dimension of H / its factor at w_H: nv rounded up to 4 for nv <= 32 (then 32 floats of
                  // 16-byte aligned column scratch follow the nv x ldh matrix), nv otherwise
 };

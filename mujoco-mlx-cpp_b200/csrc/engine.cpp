@@ -425,7 +425,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     d.ldh = nv <= 32 ? (nv + 3) & ~3 : nv;
     d.w_J = take(d.nefc_max * nv); d.w_efc = take((m.cone == CONE_ELLIPTIC ? MJB_EFC_FIELDS_ELLIPTIC : MJB_EFC_FIELDS) * d.nefc_max);
     d.w_H = take(nv <= 32 ? nv * d.ldh + 32 : nv * nv); d.w_active = take(d.nefc_max);
-    d.w_nz = take(nv);
+    d.w_nz = take(std::max(nv, 8));
     int send = off;
     d.ws_size = std::max(kend, send);
     ws_stride_ = std::max(ws_stride_, d.ws_size);

@@ -260,6 +260,15 @@ __device__ __noinline__ void d_qacc_smooth(Env& E) {
   for (int k = lane; k < nv; k += 32) ws[m.w_qas + k] = ws[m.w_qfs + k];
   __syncwarp();
   float* idiag = ws + m.w_vec + 8 * nv;
+  if (nv <= 32) {
+    // explicit inverse: H <- M^-1 (the Newton solver starts from it),
+    // qacc_smooth = M^-1 qfrc_smooth
+    d_factor(E, nullptr, 0, nullptr, 0.f, H, idiag, false, nullptr, 0, true);
+    const float a = d_inv_apply(H, nv, m.ldh, H + nv * m.ldh, ws + m.w_qfs, lane);
+    if (lane < nv) ws[m.w_qas + lane] = a;
+    __syncwarp();
+    return;
+  }
   d_factor(E, nullptr, 0, nullptr, 0.f, H, idiag);
   d_chol_solve(H, idiag, nv, m.ldh, ws + m.w_qas, lane);
 }
@@ -558,7 +567,12 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       if (valid) {
         // a caller / separately inferred prediction serves the launch's first substep; the fused one every substep
         const float* xpred = nnfused ? ws + E.md->w_vec + 7 * nv : (P.qacc_pred && s == 0) ? P.qacc_pred + vadr : nullptr;
-        int it = d_newton<CVX>(E, P, nefc, max_iter, xpred, choice);
+        // inverse mode for small models without elliptic cones; H still
+        // holds the unconstrained solve's M^-1 (nv <= 32) unless the learned
+        // warm start's features took its slot
+        const bool inv = !(CVX && E.md->cone == 1) && nv <= 32 && nefc <= 128;
+        const bool hm = P.nn_w[0] == nullptr;
+        int it = inv ? d_newton<CVX, true>(E, P, nefc, max_iter, xpred, choice, hm) : d_newton<CVX, false>(E, P, nefc, max_iter, xpred, choice, hm);
         nsum += it;
         nmax = it > nmax ? it : nmax;
         if (P.pair_t) {
