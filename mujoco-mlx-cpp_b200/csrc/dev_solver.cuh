@@ -266,8 +266,14 @@ __device__ __noinline__ void d_chol_solve(const float* L, const float* idiag, in
 // In-place inversion by the symmetric sweep operator on every pivot.  Step
 // k: d = a_kk; every row i != k becomes a_i - (a_ik / d) a_k with entry k set
 // to -a_ik / d; row k becomes a_k / d with entry k = 1 / d.  After all n
-// steps A holds A^-1.  The pivots are Schur complements of an SPD matrix,
-// so they stay positive and no pivoting is needed.  The pivot row is first
+// steps A holds A^-1 whatever the pivot order.  The pivots are Schur
+// complements of an SPD matrix, so they stay positive and no pivoting is
+// needed.  Pivots go from the last dof to the first: in the depth-first
+// dof order of a kinematic tree that sweeps leaves before their ancestors,
+// and a row with a_ik = 0 (a dof on another branch) is left as it is, so M
+// and Hessians with the tree's pattern keep the branches apart until their
+// common ancestors' pivots (for the quadruped a leg pivot touches the 9 rows
+// of the free joint and its own leg instead of 18).  The pivot row is first
 // copied to col (16-byte aligned, ld floats), so every lane, its owner
 // included (factor 1 - 1/d gives a_k / d), updates its own row from the
 // copy with 16-byte loads and stores.
@@ -275,13 +281,14 @@ __device__ __noinline__ void d_sweep(float* A, int n, int ld, int lane, float* c
   const bool own = lane < n;
   float* row = A + lane * ld;
 #pragma unroll 1
-  for (int k = 0; k < n; k++) {
+  for (int k = n - 1; k >= 0; k--) {
     __syncwarp();
     if (lane < ld) col[lane] = A[k * ld + lane];
     __syncwarp();
     const float id = __frcp_rn(col[k]);
-    if (own) {
-      const float f = lane == k ? 1.f - id : row[k] * id;
+    const float aik = own ? row[k] : 0.f;
+    if (own && (aik != 0.f || lane == k)) {
+      const float f = lane == k ? 1.f - id : aik * id;
 #pragma unroll 2
       for (int j = 0; j < ld; j += 4) {
         float4 a = *reinterpret_cast<float4*>(row + j);

@@ -419,6 +419,16 @@ __device__ __noinline__ void d_nn_stage(const Env& E, const StepParams& P, int n
 
 }  // namespace
 
+// SM cycle counter read that the compiler keeps in place relative to the
+// memory operations and barriers around it (clock64() alone may be
+// scheduled across the stage barrier, which moves a stage's barrier wait
+// into the next stage's bucket).
+__device__ __forceinline__ long long stage_clock() {
+  long long t;
+  asm volatile("mov.u64 %0, %%clock64;" : "=l"(t) : : "memory");
+  return t;
+}
+
 // Two execution modes share the stage functions:
 //  * independent warps (P.lockstep == 0): each warp takes envs from the
 //    persistent queue and runs all stages on its own;
@@ -440,7 +450,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
   // between consecutive stage barriers
   const bool timing = lockstep && P.stage_cycles != nullptr && threadIdx.x == 0;
   unsigned long long tstage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  long long tlast = timing ? clock64() : 0;
+  long long tlast = timing ? stage_clock() : 0;
   int stage_id = 0;
 #define STAGE_SYNC()                                  \
   do {                                                \
@@ -449,7 +459,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       __syncthreads();                                \
     }                                                 \
     if (timing) {                                     \
-      long long t_ = clock64();                       \
+      long long t_ = stage_clock();                   \
       tstage[stage_id & 7] += (unsigned long long)(t_ - tlast); \
       tlast = t_;                                     \
     }                                                 \
@@ -555,10 +565,10 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
       // over the CTA's envs (block barriers inside: every warp takes part)
       if constexpr (!CVX) {
         if (nnfused || (P.pair_x && valid)) {
-          const long long tn = timing ? clock64() : 0;
+          const long long tn = timing ? stage_clock() : 0;
           d_nn_stage(E, P, ncon, valid, s, last, nnfused);
           if (timing && nnfused) {   // stage clock bucket 6: the fused inference, barrier to barrier
-            const long long t_ = clock64();
+            const long long t_ = stage_clock();
             tstage[6] += (unsigned long long)(t_ - tn);
             tlast = t_;
           }
