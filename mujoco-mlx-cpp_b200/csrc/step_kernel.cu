@@ -437,7 +437,7 @@ __device__ __forceinline__ long long stage_clock() {
 //    the CTA execute the same stage code at the same time (instruction-cache
 //    locality); envs whose Newton solve ends early wait at the barrier.
 template <bool CVX>
-__global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
+__global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ StepParams P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int W = blockDim.x >> 5;
   const bool lockstep = P.lockstep != 0;
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(StepParams P) {
 // Geom poses of every env at its current qpos (kinematics only), for ray
 // casting: gpose[env][g][12] = world position (3), rotation matrix (9, row
 // major).  One warp per env; the workspace layout is the step kernel's.
-__global__ void __launch_bounds__(512) mjb_geom_pose_kernel(StepParams P, float* gpose, int ng_max) {
+__global__ void __launch_bounds__(512) mjb_geom_pose_kernel(const __grid_constant__ StepParams P, float* gpose, int ng_max) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, W = blockDim.x >> 5;
   int* dsm = reinterpret_cast<int*>(mjb_smem) + warp * P.desc_words;
   float* ws = P.gws ? P.gws + ((size_t)blockIdx.x * W + warp) * P.ws_stride : mjb_smem + W * P.desc_words + warp * P.ws_stride;
