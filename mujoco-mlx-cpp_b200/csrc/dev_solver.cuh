@@ -841,7 +841,7 @@ __device__ __noinline__ int d_constraints(Env& E, const StepParams& P, int ncon)
       if (stop) break;
     }
   }
-  if (stop) E.status |= MJB_STATUS_EFC_OVERFLOW;
+  if (stop) env_status(E, MJB_STATUS_EFC_OVERFLOW);
   __syncwarp();
   // Jacobian rows of the contacts: one lane per dof
   if (nefc > row0) {

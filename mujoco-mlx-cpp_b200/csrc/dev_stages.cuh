@@ -14,15 +14,30 @@
 
 namespace mjbdev {
 
+// The lane index, read from the thread index wherever E.lane is used
+// (it converts to int), so the rest of the context can live in one
+// per-warp shared-memory slot.
+struct LaneId {
+  __device__ __forceinline__ operator int() const { return (int)(threadIdx.x & 31u); }
+};
+
+// Per-env context of a warp.  The step kernels keep it in the warp's
+// shared-memory slot after the model descriptor copy, and the stage
+// functions take it by reference, so reading a field is a shared-memory
+// load rather than a stack load.  Status bits are set with atomicOr
+// (env_status), which is safe from any subset of the warp's lanes.
 struct Env {
   const DevModelDesc* md;  // shared-memory copy
   const int* it;
   const float* ft;
   float* ws;
-  int lane;
   int env;
   int status;
+  LaneId lane;
 };
+
+__device__ __forceinline__ void env_status(Env& E, int bits) { atomicOr(&E.status, bits); }
+static_assert(sizeof(Env) <= 4 * MJB_ENV_SLOT_WORDS, "env context exceeds its shared-memory slot");
 
 __device__ __forceinline__ float msc(const StepParams& P, const Env& E, int b) {
   return P.rand_mass ? P.rand_mass[P.env_badr[E.env] + b] : 1.f;
@@ -170,7 +185,7 @@ __device__ __noinline__ int d_collide(Env& E) {
                          s2, ldf(ft, m.f_geom_rbound + g2), mesh2, nvert2, margin, cs);
       if (n < 0) { unsup = true; n = 0; }
     }
-    if (__any_sync(FULL_MASK, unsup)) E.status |= MJB_STATUS_UNSUPPORTED_PAIR;
+    if (__any_sync(FULL_MASK, unsup)) env_status(E, MJB_STATUS_UNSUPPORTED_PAIR);
     int incl = warp_incl_scan(n, E.lane);
     int total = __shfl_sync(FULL_MASK, incl, 31);
     int off = ncon + incl - n;
@@ -189,7 +204,7 @@ __device__ __noinline__ int d_collide(Env& E) {
     ncon += total;
   }
   if (ncon > m.ncon_max) {
-    E.status |= MJB_STATUS_CONTACT_OVERFLOW;
+    env_status(E, MJB_STATUS_CONTACT_OVERFLOW);
     ncon = m.ncon_max;
   }
   __syncwarp();

@@ -10,6 +10,12 @@
 
 #define MJB_CONTACT_FLOATS 16  // pos3 frame9 dist pair(bits) dim includemargin
 
+// per-warp shared-memory slot of the step kernels: the model descriptor copy
+// (MJB_DESC_COPY_WORDS 32-bit words), then the warp's env context
+// (MJB_ENV_SLOT_WORDS words)
+#define MJB_DESC_COPY_WORDS ((int)(sizeof(DevModelDesc) / 4))
+#define MJB_ENV_SLOT_WORDS 16
+
 // alignas(16): the per-warp shared-memory copies of the descriptor precede
 // the workspaces, which need 16-byte alignment for vector loads
 struct alignas(16) DevModelDesc {

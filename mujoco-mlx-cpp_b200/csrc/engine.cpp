@@ -435,7 +435,7 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     L.nq = m.nq; L.nv = m.nv; L.nu = m.nu; L.nbody = m.nbody;
     layouts_.push_back(L);
   }
-  desc_words_ = (int)(sizeof(DevModelDesc) / 4);
+  desc_words_ = MJB_DESC_COPY_WORDS + MJB_ENV_SLOT_WORDS;
   std::vector<DevModelDesc> descs;
   for (auto& L : layouts_) descs.push_back(L.desc);
   // copies ordered on the sim's stream (a blocking cudaMemcpy from pageable

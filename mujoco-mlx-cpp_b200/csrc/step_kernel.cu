@@ -284,7 +284,7 @@ __device__ __noinline__ bool d_finish(Env& E, const float* qfc, float* acc) {
 #pragma unroll 1
   for (int i = lane; i < nv; i += 32) badacc |= badval(x[i]);
   if (__any_sync(FULL_MASK, badacc)) {
-    E.status |= MJB_STATUS_BADQACC;
+    env_status(E, MJB_STATUS_BADQACC);
     reset_env(E);
     return false;
   }
@@ -388,7 +388,7 @@ __device__ __noinline__ bool check_state(Env& E) {
 #pragma unroll 1
   for (int i = E.lane; i < m.nv; i += 32) bad |= badval(ws[m.w_qvel + i]);
   if (__any_sync(FULL_MASK, bad)) {
-    E.status |= MJB_STATUS_BADSTATE;
+    env_status(E, MJB_STATUS_BADSTATE);
     reset_env(E);
     return true;
   }
@@ -481,14 +481,19 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
       break;
     }
     const bool valid = env < P.num_envs;
-    Env E;
-    E.it = P.itab;
-    E.ft = P.ftab;
-    E.ws = ws;
-    E.lane = lane;
-    E.env = env;
-    E.status = 0;
-    E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+    // the warp's context lives in its shared-memory slot after the
+    // descriptor copy; lane 0 fills it for this env
+    Env& E = *reinterpret_cast<Env*>(dsm + MJB_DESC_COPY_WORDS);
+    __syncwarp();
+    if (lane == 0) {
+      E.it = P.itab;
+      E.ft = P.ftab;
+      E.ws = ws;
+      E.env = env;
+      E.status = 0;
+      E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+    }
+    __syncwarp();
     int qadr = 0, vadr = 0, badr = 0, nv = 0;
     if (P.poison_workspace) {
       // test aid: any read of the workspace before it is written in this
@@ -500,7 +505,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
     if (valid) {
       const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
 #pragma unroll 1
-      for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
+      for (int k = lane; k < MJB_DESC_COPY_WORDS; k += 32) dsm[k] = __ldg(src + k);
       __syncwarp();
       const DevModelDesc& m = *E.md;
       nv = m.nv;
@@ -657,16 +662,17 @@ __global__ void __launch_bounds__(512) mjb_geom_pose_kernel(const __grid_constan
   for (int env = blockIdx.x * W + warp; env < P.num_envs; env += gridDim.x * W) {
     const int* src = reinterpret_cast<const int*>(P.models + P.env_model[env]);
 #pragma unroll 1
-    for (int k = lane; k < P.desc_words; k += 32) dsm[k] = __ldg(src + k);
+    for (int k = lane; k < MJB_DESC_COPY_WORDS; k += 32) dsm[k] = __ldg(src + k);
+    Env& E = *reinterpret_cast<Env*>(dsm + MJB_DESC_COPY_WORDS);
+    if (lane == 0) {
+      E.it = P.itab;
+      E.ft = P.ftab;
+      E.ws = ws;
+      E.env = env;
+      E.status = 0;
+      E.md = reinterpret_cast<const DevModelDesc*>(dsm);
+    }
     __syncwarp();
-    Env E;
-    E.it = P.itab;
-    E.ft = P.ftab;
-    E.ws = ws;
-    E.lane = lane;
-    E.env = env;
-    E.status = 0;
-    E.md = reinterpret_cast<const DevModelDesc*>(dsm);
     const DevModelDesc& m = *E.md;
     const int qadr = P.env_qadr[env];
 #pragma unroll 1

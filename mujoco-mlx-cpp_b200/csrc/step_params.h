@@ -35,7 +35,7 @@ struct StepParams {
   float* gws;               // non-null: workspaces in HBM (ws_stride floats per resident warp, by global warp index)
                             // for models whose workspace exceeds shared memory; shared memory then holds the descriptors only
   int gws_blocks;           // CTAs the HBM workspaces cover
-  int desc_words;           // 32-bit words of DevModelDesc copied into shared memory
+  int desc_words;           // 32-bit words of each warp's shared-memory slot: the DevModelDesc copy, then the env context
 
   // per-env statistics of this launch
   int* status;
