@@ -531,24 +531,28 @@ void Engine::alloc_state() {
   check(cudaStreamSynchronize(stream_), "init sync");
 }
 
+// Dynamic shared memory available to one step-kernel CTA: the 227 KB a CTA
+// can hold on sm_100, less the kernel's few static bytes (stage-clock slots).
+constexpr int kStepSmemMax = 227 * 1024 - 64;
+
 void Engine::choose_launch() {
   lockstep_ = cfg_.lockstep ? 1 : 0;
   // a workspace that does not fit shared memory (large models: the bin of
   // free bodies, nv in the hundreds) lives in HBM, one per resident warp;
   // shared memory then holds the model descriptors only
-  gws_mode_ = (desc_words_ + ws_stride_) * 4 > 227 * 1024;
+  gws_mode_ = (desc_words_ + ws_stride_) * 4 > kStepSmemMax;
   const int per_warp = (desc_words_ + (gws_mode_ ? 0 : ws_stride_)) * 4;
   if (cfg_.warps_per_block > 0) warps_ = cfg_.warps_per_block;
   else if (gws_mode_) warps_ = 4;
-  else if (lockstep_ && 16 * per_warp <= 227 * 1024) warps_ = 16;   // one lockstep CTA of 16 warps per SM (measured ~3 % faster than two of 8)
-  else if (lockstep_) warps_ = std::max(1, std::min(8, (227 * 1024 / 2) / per_warp));  // two lockstep CTAs of up to 8 warps per SM
+  else if (lockstep_ && 16 * per_warp <= kStepSmemMax) warps_ = 16;   // one lockstep CTA of 16 warps per SM (measured ~3 % faster than two of 8)
+  else if (lockstep_) warps_ = std::max(1, std::min(8, (kStepSmemMax / 2) / per_warp));  // two lockstep CTAs of up to 8 warps per SM
   else warps_ = 4;
   smem_ = warps_ * per_warp;
-  if (smem_ > 227 * 1024) {
-    warps_ = std::max(1, (227 * 1024) / per_warp);
+  if (smem_ > kStepSmemMax) {
+    warps_ = std::max(1, kStepSmemMax / per_warp);
     smem_ = warps_ * per_warp;
   }
-  if (smem_ > 227 * 1024) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
+  if (smem_ > kStepSmemMax) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
   int bps = 0;
   check(mjb_occupancy(warps_, smem_, convex_, &bps), "occupancy");
   if (bps < 1) throw std::runtime_error("engine: kernel cannot be resident with this configuration");
@@ -629,7 +633,7 @@ std::vector<Engine::TuneCandidate> Engine::autotune(int nsub, int reps) {
     {
       TuneCandidate c{w, lock, sh.bps, -1.f};
       // an attached per-env net runs inside the kernel: lockstep, 8 or 16 warps
-      if (w * per_warp > 227 * 1024 || (fused && (!lock || (w != 8 && w != 16)))) {
+      if (w * per_warp > kStepSmemMax || (fused && (!lock || (w != 8 && w != 16)))) {
         out.push_back(c);
         continue;
       }
@@ -1270,7 +1274,7 @@ void Engine::set_warmstart(WarmStartNet* net) {
         const EngineConfig prev = cfg_;
         cfg_ = c;
         choose_launch();
-        if (!fused_blocker().empty() || smem_ > 227 * 1024) {
+        if (!fused_blocker().empty() || smem_ > kStepSmemMax) {
           cfg_ = prev;
           choose_launch();
         }

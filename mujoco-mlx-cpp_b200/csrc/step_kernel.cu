@@ -420,9 +420,7 @@ __device__ __noinline__ void d_nn_stage(const Env& E, const StepParams& P, int n
 }  // namespace
 
 // SM cycle counter read that the compiler keeps in place relative to the
-// memory operations and barriers around it (clock64() alone may be
-// scheduled across the stage barrier, which moves a stage's barrier wait
-// into the next stage's bucket).
+// memory operations around it.
 __device__ __forceinline__ long long stage_clock() {
   long long t;
   asm volatile("mov.u64 %0, %%clock64;" : "=l"(t) : : "memory");
@@ -448,22 +446,40 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
   float* ws = P.gws ? P.gws + ((size_t)blockIdx.x * W + warp) * P.ws_stride : mjb_smem + W * P.desc_words + warp * P.ws_stride;
   // optional per-stage timing: thread 0 of each CTA accumulates the clock
   // between consecutive stage barriers
-  const bool timing = lockstep && P.stage_cycles != nullptr && threadIdx.x == 0;
+  // Stage clocks: each warp's lane 0 posts its arrival time at a stage
+  // barrier into tarr[tpar] (atomicMax), so after the barrier the slot holds
+  // the moment the last warp arrived, i.e. when the barrier completed.  (A
+  // clock read placed after the barrier can be issued before the barrier
+  // completes, which moves barrier waits into the next stage's bucket.)
+  // The two slots alternate; each is cleared by thread 0 right after it is
+  // read, one barrier before its next use.
+  __shared__ unsigned long long tarr[2];
+  const bool stimed = lockstep && P.stage_cycles != nullptr;
+  const bool timing = stimed && threadIdx.x == 0;
   unsigned long long tstage[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   long long tlast = timing ? stage_clock() : 0;
-  int stage_id = 0;
-#define STAGE_SYNC()                                  \
-  do {                                                \
-    if (lockstep) {                                   \
-      __syncwarp();                                   \
-      __syncthreads();                                \
-    }                                                 \
-    if (timing) {                                     \
-      long long t_ = stage_clock();                   \
-      tstage[stage_id & 7] += (unsigned long long)(t_ - tlast); \
-      tlast = t_;                                     \
-    }                                                 \
-    stage_id++;                                       \
+  int stage_id = 0, tpar = 0;
+  if (stimed) {
+    if (threadIdx.x == 0) tarr[0] = tarr[1] = 0ull;
+    __syncthreads();
+  }
+#define TIMED_BARRIER(bucket)                                                        \
+  do {                                                                               \
+    __syncwarp();                                                                    \
+    if (stimed && lane == 0) atomicMax(&tarr[tpar], (unsigned long long)stage_clock()); \
+    __syncthreads();                                                                 \
+    if (timing) {                                                                    \
+      const long long t_ = (long long)tarr[tpar];                                    \
+      tstage[(bucket) & 7] += (unsigned long long)(t_ - tlast);                      \
+      tlast = t_;                                                                    \
+      tarr[tpar] = 0ull;                                                             \
+    }                                                                                \
+    tpar ^= 1;                                                                       \
+  } while (0)
+#define STAGE_SYNC()                 \
+  do {                               \
+    if (lockstep) TIMED_BARRIER(stage_id); \
+    stage_id++;                      \
   } while (0)
 
   int group = blockIdx.x;
@@ -570,13 +586,9 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
       // over the CTA's envs (block barriers inside: every warp takes part)
       if constexpr (!CVX) {
         if (nnfused || (P.pair_x && valid)) {
-          const long long tn = timing ? stage_clock() : 0;
           d_nn_stage(E, P, ncon, valid, s, last, nnfused);
-          if (timing && nnfused) {   // stage clock bucket 6: the fused inference, barrier to barrier
-            const long long t_ = stage_clock();
-            tstage[6] += (unsigned long long)(t_ - tn);
-            tlast = t_;
-          }
+          // stage clock bucket 6: the fused inference (one more barrier, only while timing)
+          if (nnfused && stimed) TIMED_BARRIER(6);
         }
       }
       if (valid) {
@@ -649,6 +661,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
   if (timing)
     for (int k = 0; k < 8; k++) atomicAdd(P.stage_cycles + k, tstage[k]);
 #undef STAGE_SYNC
+#undef TIMED_BARRIER
 }
 
 // Geom poses of every env at its current qpos (kinematics only), for ray
