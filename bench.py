@@ -295,11 +295,16 @@ def time_device(sim, ctrl_dev, stride, K, W, flush, stream, world):
 
 
 def time_e2e(sim, host_ctrl, K, W, flush, world):
+    """End to end through the public API: each step uploads that step's
+    controls from page-locked host memory and reads the new state back into
+    page-locked host arrays (the D2H is a direct DMA)."""
     import torch
 
+    out = (torch.empty(sim.total_q, dtype=torch.float32, pin_memory=True).numpy(),
+           torch.empty(sim.total_v, dtype=torch.float32, pin_memory=True).numpy())
     for w in range(W):
         sim.step(host_ctrl[w], SUBSTEPS)
-        sim.state()
+        sim.state(out)
     if world > 1:
         torch.distributed.barrier()
     e2e_s = 0.0
@@ -308,7 +313,7 @@ def time_e2e(sim, host_ctrl, K, W, flush, world):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         sim.step(host_ctrl[W + k], SUBSTEPS)
-        sim.state()
+        sim.state(out)
         e2e_s += time.perf_counter() - t0
     return e2e_s
 
@@ -395,7 +400,9 @@ def run_ours(args, world, rank, local):
     nu = m.nu
     ctrl_all = np.stack([mjb200.models.quadruped_controls_fast(B, s, seed=seed_ctrl) for s in range(K + W)]).astype(np.float32)
     ctrl_dev = torch.from_numpy(ctrl_all).cuda()
-    host_ctrl = [np.ascontiguousarray(ctrl_all[s]) for s in range(K + W)]
+    ctrl_pinned = torch.empty(ctrl_all.shape, dtype=torch.float32, pin_memory=True).numpy()
+    ctrl_pinned[...] = ctrl_all
+    host_ctrl = [ctrl_pinned[s] for s in range(K + W)]   # page-locked, as the e2e contract asks
     stride = B * nu
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 

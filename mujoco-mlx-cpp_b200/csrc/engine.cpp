@@ -111,6 +111,7 @@ Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   invalidate_graphs();
   if (h_ctrl_pinned_) cudaFreeHost(h_ctrl_pinned_);
+  if (ctrl_done_) cudaEventDestroy(ctrl_done_);
   for (auto& kv : h_stage_) cudaFreeHost(kv.second);
   if (stream_) cudaStreamDestroy(stream_);
 }
@@ -941,7 +942,20 @@ void Engine::launch(int n, bool record) {
 void Engine::step(const float* ctrl_host, int n) {
   if (tot_u_ > 0) {
     if (ctrl_host) {
-      // stage through pinned memory so the copy is a true async DMA
+      cudaPointerAttributes pa{};
+      const bool pinned = cudaPointerGetAttributes(&pa, ctrl_host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+      if (pinned) {
+        // page-locked caller buffer: DMA straight from it, and return once
+        // the copy has landed so the caller may reuse the buffer
+        check(cudaMemcpyAsync(ctrl_.p, ctrl_host, sizeof(float) * tot_u_, cudaMemcpyHostToDevice, stream_), "ctrl upload");
+        if (!ctrl_done_) check(cudaEventCreateWithFlags(&ctrl_done_, cudaEventDisableTiming), "ctrl event");
+        check(cudaEventRecord(ctrl_done_, stream_), "ctrl event record");
+        launch(n, cfg_.record != 0);
+        check(cudaEventSynchronize(ctrl_done_), "ctrl upload wait");
+        return;
+      }
+      // pageable caller buffer: stage through pinned memory so the copy is
+      // a true async DMA
       check(cudaStreamSynchronize(stream_), "ctrl staging sync");
       std::memcpy(h_ctrl_pinned_, ctrl_host, sizeof(float) * tot_u_);
       check(cudaMemcpyAsync(ctrl_.p, h_ctrl_pinned_, sizeof(float) * tot_u_, cudaMemcpyHostToDevice, stream_), "ctrl upload");

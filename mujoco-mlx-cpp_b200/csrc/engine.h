@@ -248,6 +248,7 @@ class Engine {
   class WarmStartNet* net_ = nullptr;
 
   float* h_ctrl_pinned_ = nullptr;
+  cudaEvent_t ctrl_done_ = nullptr;   // set after a direct upload from a page-locked ctrl buffer
   std::map<std::string, float*> h_stage_;
   std::map<std::string, size_t> h_stage_n_;
 

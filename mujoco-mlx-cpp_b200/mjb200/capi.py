@@ -461,9 +461,18 @@ class BatchedSim:
         lib.mjmlx_batched_eval_state(self.handle)
 
     # ---- state
-    def state(self):
-        qpos = np.zeros(self.total_q, np.float32)
-        qvel = np.zeros(self.total_v, np.float32)
+    def state(self, out=None):
+        """(qpos, qvel) of every env.  out: optional preallocated contiguous
+        float32 arrays (qpos, qvel) of total_q / total_v values to copy into,
+        e.g. page-locked ones for a direct device-to-host DMA."""
+        if out is None:
+            qpos = np.zeros(self.total_q, np.float32)
+            qvel = np.zeros(self.total_v, np.float32)
+        else:
+            qpos, qvel = out
+            if qpos.dtype != np.float32 or qvel.dtype != np.float32 or not (qpos.flags.c_contiguous and qvel.flags.c_contiguous) \
+                    or qpos.size != self.total_q or qvel.size != self.total_v:
+                raise ValueError("out must be contiguous float32 arrays of total_q and total_v values")
         lib.mjmlx_batched_get_state(self.handle, _fp(qpos), _fp(qvel), None, None)
         if self.uniform:
             return qpos.reshape(self.num_envs, -1), qvel.reshape(self.num_envs, -1)

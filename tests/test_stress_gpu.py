@@ -84,3 +84,34 @@ def test_sims_created_and_freed_with_mixed_setters(quad_model):
             got = _sequence(quad_model, B, 7000 + B)
             for a, b in zip(got, ref[B]):
                 assert np.array_equal(a, b), (rep, B)
+
+
+def test_pinned_ctrl_and_state_buffers_match_pageable(quad_model):
+    """Controls from a page-locked buffer go up by direct DMA (the step waits
+    for that copy before returning, so the buffer may be refilled at once),
+    and state(out=...) fills page-locked arrays: the results are the same
+    bits as with pageable buffers, also when the pinned control buffer is
+    overwritten right after each step."""
+    import torch
+
+    B = 4096
+    q, v = mjb200.models.quadruped_initial_state_fast(B, seed=8810)
+    q, v = q.astype(np.float32), v.astype(np.float32)
+    ref = mjb200.BatchedSim(quad_model, B, record=0)
+    pin = mjb200.BatchedSim(quad_model, B, record=0)
+    ref.set_state(q, v)
+    pin.set_state(q, v)
+    cbuf = torch.empty((B, quad_model.nu), dtype=torch.float32, pin_memory=True).numpy()
+    out = (torch.empty(pin.total_q, dtype=torch.float32, pin_memory=True).numpy(),
+           torch.empty(pin.total_v, dtype=torch.float32, pin_memory=True).numpy())
+    for k in range(6):
+        c = _ctrl(B, k)
+        ref.step(c.copy(), 4)
+        cbuf[...] = c
+        pin.step(cbuf, 4)
+        cbuf[...] = np.nan   # refilled at once: the upload has already landed
+        qr, vr = ref.state()
+        qp, vp = pin.state(out)
+        assert np.array_equal(qr, qp) and np.array_equal(vr, vp), k
+    ref.close()
+    pin.close()
