@@ -153,7 +153,11 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int nk = a.K / BK;
+  // this CTA's K chunks: all of them, or slice blockIdx.z of ksplit
+  const int nks = a.ksplit > 1 ? a.ksplit : 1;
+  const int kc0 = (a.K / BK) * (int)blockIdx.z / nks;
+  const int nk = (a.K / BK) * ((int)blockIdx.z + 1) / nks - kc0;
+  float* const out_f32 = a.ksplit > 1 ? a.split_ws + (size_t)blockIdx.z * a.M * a.ldo : a.out_f32;
   const unsigned long long limit = a.wait_limit_ns ? a.wait_limit_ns : kWaitLimitNs;
 
   if (threadIdx.x == 0) {
@@ -184,8 +188,8 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
       }
       uint8_t* sa = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_2d(sa, &tmA, &full[s], kc * BK, m0);
-      tma_load_2d(sa + A_BYTES, &tmB, &full[s], kc * BK, n0);
+      tma_load_2d(sa, &tmA, &full[s], (kc0 + kc) * BK, m0);
+      tma_load_2d(sa + A_BYTES, &tmB, &full[s], (kc0 + kc) * BK, n0);
       issued = kc + 1;
     }
   } else if (warp == 1 && lane == 0) {
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(128, 1) gemm_tn_kernel(const __grid_constant__
       // tcgen05.ld (a .sync.aligned instruction)
       if (rv) switch (a.mode) {
         case EPI_F32: {
-          float4* d = reinterpret_cast<float4*>(a.out_f32 + (size_t)row * a.ldo + col0);
+          float4* d = reinterpret_cast<float4*>(out_f32 + (size_t)row * a.ldo + col0);
 #pragma unroll
           for (int i = 0; i < 4; i++) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
           break;
@@ -331,9 +335,29 @@ cudaError_t launch_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const Ge
   static cudaError_t attr_err = cudaSuccess;
   std::call_once(once, [&] { attr_err = cudaFuncSetAttribute(gemm_tn_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); });
   if (attr_err != cudaSuccess) return attr_err;
-  dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN);
+  dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.ksplit > 1 ? a.ksplit : 1);
   gemm_tn_kernel<BN><<<grid, 128, smem, s>>>(tmA, tmB, a);
   return cudaGetLastError();
+}
+
+// out[r * ldo + c] = sum over z < nsplit, in order, of ws[z * M * ldo + r * ldo + c]
+// for r < M, c < N (N a multiple of 4; one thread per 4 columns)
+__global__ void __launch_bounds__(256) splitk_reduce_kernel(const float* ws, int nsplit, int M, int N, int ldo, float* out) {
+  const int nq = N >> 2;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M * nq) return;
+  const int r = t / nq, c = (t - r * nq) << 2;
+  const size_t o = (size_t)r * ldo + c, slice = (size_t)M * ldo;
+  float4 acc = *reinterpret_cast<const float4*>(ws + o);
+#pragma unroll 1
+  for (int z = 1; z < nsplit; z++) {
+    const float4 v = *reinterpret_cast<const float4*>(ws + z * slice + o);
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+    acc.w += v.w;
+  }
+  *reinterpret_cast<float4*>(out + o) = acc;
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -367,11 +391,27 @@ bool make_tmap_bf16(CUtensorMap* map, const void* base, int rows, int cols, int 
 
 cudaError_t gemm_tn(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmArgs& a, cudaStream_t s) {
   if (a.M <= 0 || a.K <= 0 || a.K % BK != 0 || a.N <= 0 || a.N % 16 != 0) return cudaErrorInvalidValue;
-  if (a.N == 64) return launch_gemm<64>(tmA, tmB, a, s);
-  if (a.N == 128) return launch_gemm<128>(tmA, tmB, a, s);
-  if (a.N == 192) return launch_gemm<192>(tmA, tmB, a, s);
-  if (a.N % 256 == 0) return launch_gemm<256>(tmA, tmB, a, s);
-  return cudaErrorInvalidValue;
+  if (a.ksplit > 1 && (a.mode != EPI_F32 || a.bias || !a.split_ws || !a.out_f32 || a.ksplit > a.K / BK || a.ldo % 4 != 0))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaErrorInvalidValue;
+  if (a.N == 64) e = launch_gemm<64>(tmA, tmB, a, s);
+  else if (a.N == 128) e = launch_gemm<128>(tmA, tmB, a, s);
+  else if (a.N == 192) e = launch_gemm<192>(tmA, tmB, a, s);
+  else if (a.N % 256 == 0) e = launch_gemm<256>(tmA, tmB, a, s);
+  if (e != cudaSuccess || a.ksplit <= 1) return e;
+  const int threads = a.M * (a.N / 4);
+  splitk_reduce_kernel<<<(threads + 255) / 256, 256, 0, s>>>(a.split_ws, a.ksplit, a.M, a.N, a.ldo, a.out_f32);
+  return cudaGetLastError();
+}
+
+int gemm_ksplit(int M, int N, int K) {
+  // enough CTAs to spread the K loop over the SMs, at least 4 K chunks
+  // (of 64) each so the 3-stage load ring still fills
+  const int tiles = ((M + BM - 1) / BM) * ((N + 255) / 256);
+  const int nk = K / BK;
+  int ks = 1;
+  while (ks * 2 * tiles <= 148 && nk / (ks * 2) >= 4) ks *= 2;
+  return ks;
 }
 
 }  // namespace mjb

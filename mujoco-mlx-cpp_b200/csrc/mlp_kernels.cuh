@@ -39,6 +39,13 @@ struct GemmArgs {
   int* err;             // set to a nonzero code when a bounded wait gives up
   const volatile int* gate;       // test hook (null in production): the first MMA waits, bounded, for *gate != 0
   unsigned long long wait_limit_ns;  // limit of each bounded wait (0: 2 s)
+  // split K (EPI_F32 without bias only): ksplit > 1 CTAs share each output
+  // tile, each over a contiguous range of the K chunks, writing FP32 partial
+  // tiles into split_ws (ksplit slices of M x ldo floats); a second kernel
+  // sums the slices in slice order into out_f32, so results do not depend
+  // on scheduling.  Used for the weight gradients, whose K is the batch.
+  int ksplit;
+  float* split_ws;
 };
 
 // Encodes a 2-D bf16 row-major [rows][cols] tensor map with a box of
@@ -49,6 +56,9 @@ bool make_tmap_bf16(CUtensorMap* map, const void* base, int rows, int cols, int 
 // rows 128; tmB: B [N][K] with box rows = the CTA's N tile (N <= 256 in one
 // tile, else 256-column tiles).
 cudaError_t gemm_tn(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmArgs& a, cudaStream_t s);
+// Split of the K loop gemm_tn should use for an EPI_F32 C[M x N] with this
+// K (a power of two, 1 when the tiles alone fill the GPU).
+int gemm_ksplit(int M, int N, int K);
 
 }  // namespace mjb
 

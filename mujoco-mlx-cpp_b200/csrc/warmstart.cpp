@@ -268,12 +268,24 @@ void WarmStartNet::forward_batch(int n, bool train, const float* target, float* 
   check(gemm_tn(*a_map, m_w_[3], a, s), "warm start output gemm");
 }
 
+// Weight gradients have K = the batch (thousands) and only one or two
+// output tiles: split K over enough CTAs to spread the loop over the SMs.
+void WarmStartNet::split_k(GemmArgs& g) {
+  const int ks = gemm_ksplit(g.M, g.N, g.K);
+  if (ks <= 1) return;
+  const size_t need = (size_t)ks * g.M * g.ldo;
+  if (splitk_.n < need) splitk_.alloc(need);
+  g.ksplit = ks;
+  g.split_ws = splitk_.p;
+}
+
 void WarmStartNet::backward_batch(int n, cudaStream_t s) {
   const int H = kHidden;
   // output layer: dW3 = dY^T H2, db3 = colsum dY, dZ2 = (dY W3) * gelu'(Z2)
   {
     GemmArgs a = gemm_args(kOutPad, H, n, EPI_F32, H, err_.p);
     a.out_f32 = grads_.p + woff_[3];
+    split_k(a);
     check(gemm_tn(m_dyt_, m_ht_[2], a, s), "dW3");
     check(rowsum_bf16(bf(dyt_), kOutPad, n, n, grads_.p + boff_[3], s), "db3");
     GemmArgs b = gemm_args(n, H, kOutPad, EPI_BWD_GELU, H, err_.p);
@@ -295,6 +307,7 @@ void WarmStartNet::backward_batch(int n, cudaStream_t s) {
   for (int l = 2; l >= 1; l--) {
     GemmArgs a = gemm_args(H, H, n, EPI_F32, H, err_.p);
     a.out_f32 = grads_.p + woff_[l];
+    split_k(a);
     check(gemm_tn(*m_dzt, m_ht_[l - 1], a, s), "dW hidden");
     check(rowsum_bf16(bf(*dzt), H, n, n, grads_.p + boff_[l], s), "db hidden");
     GemmArgs b = gemm_args(n, H, H, EPI_BWD_GELU, H, err_.p);
@@ -311,6 +324,7 @@ void WarmStartNet::backward_batch(int n, cudaStream_t s) {
   // input layer: dW0 = dZ0^T X, db0
   GemmArgs a = gemm_args(H, in_pad_, n, EPI_F32, in_pad_, err_.p);
   a.out_f32 = grads_.p + woff_[0];
+  split_k(a);
   check(gemm_tn(*m_dzt, m_xt_, a, s), "dW0");
   check(rowsum_bf16(bf(*dzt), H, n, n, grads_.p + boff_[0], s), "db0");
 }

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "mlp_kernels.cuh"
 #include "step_params.h"
 
 namespace mjb {
@@ -83,6 +84,7 @@ class WarmStartNet {
 
  private:
   void ensure_batch(int n);
+  void split_k(GemmArgs& g);
   void build_maps(int n);
   void forward_batch(int n, bool train, const float* target, float* loss, float* y_f32, const float* prev, float* pred, cudaStream_t s,
                      bool inference_buffers = false);
@@ -104,6 +106,7 @@ class WarmStartNet {
   std::vector<float> h_in_mean_, h_in_std_, h_out_mean_, h_out_std_;
   DevBuf<int> err_;
   DevBuf<float> loss_;
+  DevBuf<float> splitk_;   // split-K partial tiles of the weight-gradient GEMMs
 
   // batch scratch (capacity cap_)
   int cap_ = 0, maps_n_ = -1;

@@ -72,8 +72,10 @@ def test_forward_matches_cpu_reference():
     assert _rel(got, exact) <= 6e-2
 
 
-def test_gradients_match_cpu_reference():
-    n = 256
+@pytest.mark.parametrize("n", [256, 4096])
+def test_gradients_match_cpu_reference(n):
+    """n = 4096 runs the weight-gradient GEMMs with K split over 16 CTAs per
+    output tile (64 K chunks) and the ordered reduction of the partials."""
     net, p, xraw, traw, (im, is_, om, os_) = _net_and_data(n, seed=2, out_scale=10.0)
     x = torch.from_numpy(xraw).cuda()
     t = torch.from_numpy(traw).cuda()
