@@ -161,13 +161,13 @@ MJMLX_API int mjb200_batched_pack_device(MjmlxBatchedSim* sim, float** pack_dev)
  * each step) and its float count; NULL / 0 without sensors. */
 MJMLX_API int mjb200_batched_sensordata_device(MjmlxBatchedSim* sim, float** sensordata_dev, int* n);
 
-/* Per-stage SM clock totals of the lockstep step kernel, thread 0 of each
- * CTA measuring from one stage barrier to the next, summed over CTAs:
- * 0 state check + kinematics (plus the previous substep's Newton solve,
- * integration and waiting, which have no barrier of their own), 1
- * collision, 2 COM + CRB, 3 RNE + forces, 4 unconstrained solve, 5
- * constraint build, 6 the fused learned warm start (features and MLP, when a
- * per-env net is attached), 7 unused.  enable 1 starts (and zeroes) the
+/* Per-stage SM clock totals of the lockstep step kernel, summed over CTAs.
+ * A stage runs from one stage barrier to the next and ends when the CTA's
+ * last warp arrives: 0 constraint force, integration, state check and the
+ * next substep's kinematics, 1 collision, 2 COM + CRB, 3 RNE + forces, 4
+ * unconstrained solve, 5 constraint build, 6 the fused learned warm start
+ * (features and MLP, when a per-env net is attached), 7 the Newton solve
+ * (until the CTA's slowest solve ends).  enable 1 starts (and zeroes) the
  * counters, 0 stops them, -1 leaves them; cycles8 (may be NULL) receives the
  * totals accumulated so far.  Returns 0 / -1. */
 MJMLX_API int mjb200_batched_stage_timing(MjmlxBatchedSim* sim, int enable, unsigned long long* cycles8);

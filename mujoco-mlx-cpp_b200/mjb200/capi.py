@@ -564,7 +564,7 @@ class BatchedSim:
         if lib.mjb200_batched_configure(self.handle, C.byref(c)) != 0:
             raise RuntimeError(last_error())
 
-    STAGES = ("newton_finish_kin", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "fused_warmstart", "x7", "x8", "x9", "x10", "x11",
+    STAGES = ("finish_kin", "collision", "com_crb", "rne_forces", "qacc_smooth", "constraints", "fused_warmstart", "newton", "x8", "x9", "x10", "x11",
               "x12", "x13", "x14", "x15")
 
     def stage_timing(self, enable: int = -1):
