@@ -393,8 +393,12 @@ cudaError_t gemm_tn(const CUtensorMap& tmA, const CUtensorMap& tmB, const GemmAr
   if (a.M <= 0 || a.K <= 0 || a.K % BK != 0 || a.N <= 0 || a.N % 16 != 0) return cudaErrorInvalidValue;
   if (a.ksplit > 1 && (a.mode != EPI_F32 || a.bias || !a.split_ws || !a.out_f32 || a.ksplit > a.K / BK || a.ldo % 4 != 0))
     return cudaErrorInvalidValue;
+  if (a.bn && (a.bn != 64 && a.bn != 128 && a.bn != 256)) return cudaErrorInvalidValue;
+  if (a.bn && a.N % a.bn != 0) return cudaErrorInvalidValue;
   cudaError_t e = cudaErrorInvalidValue;
-  if (a.N == 64) e = launch_gemm<64>(tmA, tmB, a, s);
+  if (a.bn == 64) e = launch_gemm<64>(tmA, tmB, a, s);
+  else if (a.bn == 128) e = launch_gemm<128>(tmA, tmB, a, s);
+  else if (a.N == 64) e = launch_gemm<64>(tmA, tmB, a, s);
   else if (a.N == 128) e = launch_gemm<128>(tmA, tmB, a, s);
   else if (a.N == 192) e = launch_gemm<192>(tmA, tmB, a, s);
   else if (a.N % 256 == 0) e = launch_gemm<256>(tmA, tmB, a, s);

@@ -46,6 +46,10 @@ struct GemmArgs {
   // on scheduling.  Used for the weight gradients, whose K is the batch.
   int ksplit;
   float* split_ws;
+  // N tile width of the launch: 0 picks the widest N allows (one CTA per 256
+  // columns); 64 or 128 give more, narrower CTAs (for small M).  tmB's box
+  // must have this many rows.
+  int bn;
 };
 
 // Encodes a 2-D bf16 row-major [rows][cols] tensor map with a box of

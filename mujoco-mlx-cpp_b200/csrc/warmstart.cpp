@@ -202,13 +202,37 @@ void WarmStartNet::ensure_batch(int n) {
   maps_n_ = -1;
 }
 
+void WarmStartNet::build_weight_maps() {
+  for (int l = 0; l < kLayers; l++) {
+    map_or_throw(&m_w_[l], W(l), rows_[l], cols_[l], rows_[l]);
+    w64_[l] = rows_[l] > 64 && rows_[l] % 64 == 0;
+    if (w64_[l]) map_or_throw(&m_w64_[l], W(l), rows_[l], cols_[l], 64);
+  }
+  for (int l = 1; l < kLayers; l++) {
+    map_or_throw(&m_wt_[l], WT(l), cols_[l], rows_[l], cols_[l]);
+    wt64_[l] = cols_[l] > 64 && cols_[l] % 64 == 0;
+    if (wt64_[l]) map_or_throw(&m_wt64_[l], WT(l), cols_[l], rows_[l], 64);
+  }
+}
+
+// B operand of a GEMM whose N is the weight's row count: 64-column tiles
+// (four CTAs per 256 columns) when one CTA per 256 columns would use under
+// half the SMs, as for a 4096-row training batch (32 row tiles).
+const CUtensorMap& WarmStartNet::pick_b(GemmArgs& g, const CUtensorMap& wide, const CUtensorMap& narrow, bool has_narrow) const {
+  const int ctas = (g.M + 127) / 128 * ((g.N + 255) / 256);
+  if (has_narrow && g.N > 64 && g.N % 64 == 0 && 2 * ctas <= 148) {
+    g.bn = 64;
+    return narrow;
+  }
+  return wide;
+}
+
 void WarmStartNet::build_maps(int n) {
   if (n == maps_n_) return;
   const int H = kHidden;
   map_or_throw(&m_x_, x_.p, n, in_pad_, 128);
   for (int i = 0; i < 3; i++) map_or_throw(&m_h_[i], h_[i].p, n, H, 128);
-  for (int l = 0; l < kLayers; l++) map_or_throw(&m_w_[l], W(l), rows_[l], cols_[l], rows_[l]);
-  for (int l = 1; l < kLayers; l++) map_or_throw(&m_wt_[l], WT(l), cols_[l], rows_[l], cols_[l]);
+  build_weight_maps();
   map_or_throw(&m_dy_, dy_.p, n, kOutPad, 128);
   map_or_throw(&m_dza_, dza_.p, n, H, 128);
   map_or_throw(&m_dzb_, dzb_.p, n, H, 128);
@@ -241,7 +265,7 @@ void WarmStartNet::forward_batch(int n, bool train, const float* target, float* 
       a.out_t = bf(ht_[l]);
       a.ldt = n;
     }
-    check(gemm_tn(*a_map, m_w_[l], a, s), "warm start forward gemm");
+    check(gemm_tn(*a_map, pick_b(a, m_w_[l], m_w64_[l], w64_[l]), a, s), "warm start forward gemm");
     a_map = inference_buffers ? &m_hi_[l] : &m_h_[l];
     K = H;
   }
@@ -293,7 +317,7 @@ void WarmStartNet::backward_batch(int n, cudaStream_t s) {
     b.out = bf(dza_);
     b.out_t = bf(dzat_);
     b.ldt = n;
-    check(gemm_tn(m_dy_, m_wt_[3], b, s), "dH2");
+    check(gemm_tn(m_dy_, pick_b(b, m_wt_[3], m_wt64_[3], wt64_[3]), b, s), "dH2");
   }
   // hidden layers 2, 1 (dZ ping-pongs between the a and b buffers)
   DevBuf<uint16_t>* dz = &dza_;
@@ -315,7 +339,7 @@ void WarmStartNet::backward_batch(int n, cudaStream_t s) {
     b.out = bf(*nz);
     b.out_t = bf(*nzt);
     b.ldt = n;
-    check(gemm_tn(*m_dz, m_wt_[l], b, s), "dH hidden");
+    check(gemm_tn(*m_dz, pick_b(b, m_wt_[l], m_wt64_[l], wt64_[l]), b, s), "dH hidden");
     std::swap(dz, nz);
     std::swap(dzt, nzt);
     std::swap(m_dz, m_nz);
@@ -412,9 +436,7 @@ void WarmStartNet::prepare_inference(int B) {
   for (int i = 0; i < 3; i++) hi_[i].alloc((size_t)B * kHidden);
   map_or_throw(&m_xi_, xi_.p, B, in_pad_, 128);
   for (int i = 0; i < 3; i++) map_or_throw(&m_hi_[i], hi_[i].p, B, kHidden, 128);
-  if (maps_n_ < 0) {
-    for (int l = 0; l < kLayers; l++) map_or_throw(&m_w_[l], W(l), rows_[l], cols_[l], rows_[l]);
-  }
+  if (maps_n_ < 0) build_weight_maps();
   inf_B_ = B;
 }
 

@@ -85,6 +85,8 @@ class WarmStartNet {
  private:
   void ensure_batch(int n);
   void split_k(GemmArgs& g);
+  void build_weight_maps();
+  const CUtensorMap& pick_b(GemmArgs& g, const CUtensorMap& wide, const CUtensorMap& narrow, bool has_narrow) const;
   void build_maps(int n);
   void forward_batch(int n, bool train, const float* target, float* loss, float* y_f32, const float* prev, float* pred, cudaStream_t s,
                      bool inference_buffers = false);
@@ -114,6 +116,10 @@ class WarmStartNet {
   DevBuf<float> t_, yf_, zero_prev_;
   DevBuf<int> idx_;
   CUtensorMap m_x_, m_h_[3], m_w_[kLayers], m_wt_[kLayers], m_dy_, m_dyt_, m_xt_, m_ht_[3], m_dza_, m_dzb_, m_dzat_, m_dzbt_;
+  // the same weights with 64-row boxes, for GEMMs whose M is too small to
+  // fill the GPU with one CTA per 256 output columns (w64_ / wt64_: which exist)
+  CUtensorMap m_w64_[kLayers], m_wt64_[kLayers];
+  bool w64_[kLayers] = {}, wt64_[kLayers] = {};
   int adam_t_ = 0;
   // inference buffers (batch inf_B_)
   int inf_B_ = 0;
