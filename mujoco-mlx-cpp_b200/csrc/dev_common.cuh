@@ -124,7 +124,9 @@ __device__ __forceinline__ float dot_s(const float* a, int stride, const float* 
 }
 
 // read-only model table access (L1/L2 cached, tables are shared by every env)
-__device__ __forceinline__ int ldi(const int* t, int i) { return __ldg(t + i); }
+// t may be the shared-memory copy of the int table or the global one: a
+// generic load serves both
+__device__ __forceinline__ int ldi(const int* t, int i) { return t[i]; }
 __device__ __forceinline__ float ldf(const float* t, int i) { return __ldg(t + i); }
 
 }  // namespace mjbdev

@@ -554,6 +554,16 @@ void Engine::choose_launch() {
     smem_ = warps_ * per_warp;
   }
   if (smem_ > kStepSmemMax) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
+  // the model int table in shared memory too, when it fits after the
+  // workspaces: the stages walk it in dependent chains (tree levels, parents,
+  // dof and joint indices), and from global memory each link can miss the
+  // small L1 left beside the workspaces
+  const int itab_bytes = (int)((h_itab_.size() * 4 + 15) & ~size_t(15));
+  itab_smem_ = 0;
+  if (!h_itab_.empty() && smem_ + itab_bytes <= kStepSmemMax) {
+    itab_smem_ = (int)h_itab_.size();
+    smem_ += itab_bytes;
+  }
   int bps = 0;
   check(mjb_occupancy(warps_, smem_, convex_, &bps), "occupancy");
   if (bps < 1) throw std::runtime_error("engine: kernel cannot be resident with this configuration");
@@ -756,6 +766,7 @@ StepParams Engine::params(int n, bool record) {
   P.stage_cycles = timing_ ? stage_cycles_.p : nullptr;
   P.ws_stride = ws_stride_;
   P.desc_words = desc_words_;
+  P.itab_smem = itab_smem_;
   if (gws_mode_) {
     P.gws = gws_.p;
     P.gws_blocks = grid_;
@@ -837,6 +848,7 @@ StepParams Engine::external_params(float* qpos, float* qvel, const float* ctrl, 
   P.lockstep = 0;
   P.ws_stride = ws_stride_;
   P.desc_words = desc_words_;
+  P.itab_smem = itab_smem_;
   P.status = stats6;
   P.niter_sum = stats6 + B_;
   P.niter_max = stats6 + 2 * B_;

@@ -214,6 +214,7 @@ class Engine {
   bool rand_on_ = false;
   bool convex_ = false;   // some model has a pair for the GJK / EPA collider or an elliptic cone (extended kernel instance)
   bool gws_mode_ = false; // workspaces in HBM (too large for shared memory)
+  int itab_smem_ = 0;      // words of the int table the step kernel copies into shared memory (0: none)
   DevBuf<float> gws_;
   cudaStream_t stream_ = nullptr;
 

@@ -482,6 +482,16 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
     stage_id++;                      \
   } while (0)
 
+  // the model int table, copied into shared memory after the workspaces when
+  // the host left room for it (P.itab_smem words)
+  const int* itab = P.itab;
+  if (P.itab_smem) {
+    int* its = reinterpret_cast<int*>(mjb_smem + W * P.desc_words + (P.gws ? 0 : W * P.ws_stride));
+#pragma unroll 1
+    for (int k = threadIdx.x; k < P.itab_smem; k += blockDim.x) its[k] = __ldg(P.itab + k);
+    __syncthreads();
+    itab = its;
+  }
   int group = blockIdx.x;
   int env = blockIdx.x * W + warp;
   if (!lockstep && P.work_counter) {
@@ -502,7 +512,7 @@ __global__ void __launch_bounds__(512) mjb_step_kernel(const __grid_constant__ S
     Env& E = *reinterpret_cast<Env*>(dsm + MJB_DESC_COPY_WORDS);
     __syncwarp();
     if (lane == 0) {
-      E.it = P.itab;
+      E.it = itab;
       E.ft = P.ftab;
       E.ws = ws;
       E.env = env;

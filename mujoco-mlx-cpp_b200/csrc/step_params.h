@@ -36,6 +36,8 @@ struct StepParams {
                             // for models whose workspace exceeds shared memory; shared memory then holds the descriptors only
   int gws_blocks;           // CTAs the HBM workspaces cover
   int desc_words;           // 32-bit words of each warp's shared-memory slot: the DevModelDesc copy, then the env context
+  int itab_smem;            // words of the model int table (itab) copied into shared memory after the workspaces, read by
+                            // every stage in place of itab; 0: the stages read itab from global memory
 
   // per-env statistics of this launch
   int* status;
