@@ -371,8 +371,9 @@ __device__ __noinline__ bool d_inv_rank1(float* N, int n, int ld, float* col, co
 }
 
 // A = M + sum over the listed rows r of D_r J_r' J_r + dscale * diag(ddiag),
-// built in shared memory from the lower-triangle entry table (entries spread
-// over the lanes), then factored by the right-looking shared-memory Cholesky
+// built in shared memory entry by entry of the lower triangle (entries spread
+// over the lanes, row and column computed from the entry index), then
+// factored by the right-looking shared-memory Cholesky
 // into the row-major lower triangle of L with idiag = 1 / L_jj.
 // Middle-zone elliptic cones add A A' - W W' per cone (A = sum_a HA_a J_a,
 // W = sum_a HU_a J_a over the cone's rows); their tangent rows' own terms
@@ -401,11 +402,9 @@ __device__ __forceinline__ float cone_entry(const float* J, const float* hau, in
 // inv = true (n <= 32, no cones): both triangles and zero padding are
 // written and L receives N = A^-1 from the sweep instead of the factor.
 __device__ __noinline__ void d_factor_smem(const float* M, const float* J, const float* eD, const int* act, int nact, const float* ddiag, float dscale,
-                                           int n, int ld, int lane, const int* it, int i_tri, float* L, float* idiag,
+                                           int n, int ld, int lane, float* L, float* idiag,
                                            const int* cones = nullptr, int ncone = 0, const float* hau = nullptr, int ne = 0, bool inv = false) {
   const int ntri = n * (n + 1) / 2;
-  (void)it;
-  (void)i_tri;
 #pragma unroll 1
   for (int t = lane; t < ntri; t += 32) {
     // entry t of the lower triangle in row-major order (row i, column j)
@@ -530,7 +529,7 @@ __device__ __forceinline__ void d_factor(Env& E, const int* act, int nact, const
   const float* eD = efc + (ell ? EFC_HD : EFC_D) * ne;
   const float* hau = efc + EFC_HA * ne;
   if (nv > 64) d_factor_sparse(M, J, eD, act, nact, ddiag, dscale, nv, E.lane, reinterpret_cast<int*>(E.ws + m.w_nz), L, idiag, cones, ncone, hau, ne);
-  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, m.ldh, E.lane, E.it, m.i_tri, L, idiag, cones, ncone, hau, ne, inv);
+  else d_factor_smem(M, J, eD, act, nact, ddiag, dscale, nv, m.ldh, E.lane, L, idiag, cones, ncone, hau, ne, inv);
 }
 
 __device__ __noinline__ void impedance(const DevModelDesc& m, float sr0, float sr1, const float* si, float pos, float& k, float& b, float& imp) {

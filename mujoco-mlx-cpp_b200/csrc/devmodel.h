@@ -21,7 +21,7 @@
 struct alignas(16) DevModelDesc {
   // sizes
   int nq, nv, nu, nbody, njnt, ngeom, npair, nlimit, nfloss, nlevel, nmesh;
-  int ncon_max, nefc_max, ntri;
+  int ncon_max, nefc_max;
   int cone, disableflags, iterations, ls_iterations, implicit;
   float timestep, gravity[3], tolerance, impratio, scale;  // scale = 1/(meaninertia*max(1,nv))
 
@@ -47,7 +47,6 @@ struct alignas(16) DevModelDesc {
   int nfree, i_free;     // free joints in MJCF order (dof address of each)
   int nsensor, nsensordata, nsens_acc;
   int i_sensor;  // MJB_SENSOR_INTS per sensor: mjtSensor type (-1 = reads zero), adr, dim, body, root body, a, b, accelerometer slot
-  int i_tri;     // lower-triangle (i,j) pairs packed as i*65536+j
   int i_mesh;    // 2 per mesh: vertadr vertnum
 
   // float table offsets

@@ -355,11 +355,6 @@ void Engine::build_tables(const EngineConfig& cfg, int solver_iterations) {
     }
     d.i_act = tb.ai(ai);
     d.f_act = tb.af(af);
-    std::vector<int> tri;
-    for (int i = 0; i < m.nv; i++)
-      for (int j = 0; j <= i; j++) tri.push_back((i << 16) | j);
-    d.ntri = (int)tri.size();
-    d.i_tri = tb.ai(tri);
     std::vector<int> mi;
     for (int k = 0; k < m.nmesh; k++) mi.insert(mi.end(), {m.mesh_vertadr[k], m.mesh_vertnum[k]});
     d.i_mesh = tb.ai(mi);
@@ -554,15 +549,22 @@ void Engine::choose_launch() {
     smem_ = warps_ * per_warp;
   }
   if (smem_ > kStepSmemMax) throw std::runtime_error("engine: per-env workspace exceeds shared memory (" + std::to_string(ws_stride_ * 4) + " bytes)");
-  // the model int table in shared memory too, when it fits after the
-  // workspaces: the stages walk it in dependent chains (tree levels, parents,
-  // dof and joint indices), and from global memory each link can miss the
-  // small L1 left beside the workspaces
+  // the model int table in shared memory too, when the workspaces are there
+  // and the table fits after them without costing a resident CTA: the
+  // stages walk it in dependent chains (tree levels, parents, dof and joint
+  // indices), and from global memory each link can miss the small L1 left
+  // beside the workspaces.  (With HBM workspaces several small CTAs share an
+  // SM, and a table copy in each halved the 64-body bin's throughput.)
   const int itab_bytes = (int)((h_itab_.size() * 4 + 15) & ~size_t(15));
   itab_smem_ = 0;
-  if (!h_itab_.empty() && smem_ + itab_bytes <= kStepSmemMax) {
-    itab_smem_ = (int)h_itab_.size();
-    smem_ += itab_bytes;
+  if (!gws_mode_ && !h_itab_.empty() && smem_ + itab_bytes <= kStepSmemMax) {
+    int b0 = 0, b1 = 0;
+    check(mjb_occupancy(warps_, smem_, convex_, &b0), "occupancy");
+    check(mjb_occupancy(warps_, smem_ + itab_bytes, convex_, &b1), "occupancy");
+    if (b1 >= b0) {
+      itab_smem_ = (int)h_itab_.size();
+      smem_ += itab_bytes;
+    }
   }
   int bps = 0;
   check(mjb_occupancy(warps_, smem_, convex_, &bps), "occupancy");
