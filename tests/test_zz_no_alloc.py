@@ -69,6 +69,57 @@ def test_noalloc_convex_pile_matches_regular_step_twice():
     _compare_two_calls(model, q.astype(np.float32), v.astype(np.float32), [None, None])
 
 
+def test_noalloc_replays_in_a_cuda_graph(quad_model):
+    """One call outside capture (the first call on a device looks up the
+    scratch address), then two calls captured into a CUDA graph on a side
+    stream.  Replaying the graph on fresh inputs written into the captured
+    buffers gives the regular step's state after two steps."""
+    import torch
+
+    B = 96
+    dev = torch.device("cuda:0")
+    qpos, qvel = mjb200.models.quadruped_initial_state(B)
+    qpos, qvel = qpos.astype(np.float32), qvel.astype(np.float32)
+    ctrls = [mjb200.models.quadruped_controls(B, k).astype(np.float32) for k in range(2)]
+    sim = mjb200.BatchedSim(quad_model, B)
+    qp_t = torch.from_numpy(qpos.reshape(-1).copy()).to(dev)
+    qv_t = torch.from_numpy(qvel.reshape(-1).copy()).to(dev)
+    warm_t = torch.zeros(qvel.size, dtype=torch.float32, device=dev)
+    c_t = [torch.from_numpy(c.reshape(-1).copy()).to(dev) for c in ctrls]
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    assert sim.step_noalloc(qp_t.data_ptr(), qv_t.data_ptr(), c_t[0].data_ptr(), warm_t.data_ptr(), NSUB, side.cuda_stream) == 0, mjb200.capi.last_error()
+    torch.cuda.synchronize()
+
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        rc0 = sim.step_noalloc(qp_t.data_ptr(), qv_t.data_ptr(), c_t[0].data_ptr(), warm_t.data_ptr(), NSUB, side.cuda_stream)
+        rc1 = sim.step_noalloc(qp_t.data_ptr(), qv_t.data_ptr(), c_t[1].data_ptr(), warm_t.data_ptr(), NSUB, side.cuda_stream)
+    assert rc0 == 0 and rc1 == 0, mjb200.capi.last_error()
+
+    # capture ran nothing: write the start state again, then replay
+    qp_t.copy_(torch.from_numpy(qpos.reshape(-1).copy()))
+    qv_t.copy_(torch.from_numpy(qvel.reshape(-1).copy()))
+    warm_t.zero_()
+    graph.replay()
+    torch.cuda.synchronize()
+
+    ref = mjb200.BatchedSim(quad_model, B)
+    ref.set_state(qpos, qvel)
+    for c in ctrls:
+        ref.step(c, NSUB)
+    rq, rv = ref.state()
+    gq = qp_t.cpu().numpy().reshape(rq.shape)
+    gv = qv_t.cpu().numpy().reshape(rv.shape)
+    assert np.isfinite(gq).all() and np.isfinite(gv).all()
+    assert np.abs(gq - rq).max() <= 1e-5, f"qpos differs by {np.abs(gq - rq).max():.3g}"
+    assert np.abs(gv - rv).max() <= 1e-5 * max(1.0, np.abs(rv).max()), f"qvel differs by {np.abs(gv - rv).max():.3g}"
+    assert np.abs(gq - qpos.reshape(gq.shape)).max() > 1e-4
+    del graph
+    ref.close()
+    sim.close()
+
+
 def test_noalloc_keeps_other_sims_launchable(quad_model):
     """A large-workspace sim, then the allocation-free step of a sim with a
     smaller workspace, then the large sim again: the shared-memory limit the
