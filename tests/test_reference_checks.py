@@ -10,7 +10,9 @@ gravity compensation hovers, frictionloss adds one row per dof and slows the
 joint, an excluded body pair yields no pair and no contact, a joint
 equality adds one row, the implicit integrators differ from Euler where the
 velocity derivative of an actuator matters, identity per-env parameters
-change nothing.  Each test names the reference test it follows (file:line
+change nothing, an explicit pair collides geoms that filtering skips and
+sets the contact's friction, a spherical ellipsoid behaves as a sphere, and
+every primitive dropped on the floor is caught.  Each test names the reference test it follows (file:line
 within the reference's tests/ folder) and, where the mechanics allow,
 replaces the reference's loose bound with the closed-form answer.  The
 models are written here, in the spirit of the reference's, not copied.
@@ -374,3 +376,97 @@ def test_env_params_change_the_result():
     assert np.abs(qm[:3] - q0[:3]).max() < 1e-12   # the box does not see the arm's mass
     assert np.abs(qf[0] - q0[0]) > 1e-3      # box slide along x
     assert np.abs(qg[7] - q0[7]) > 1e-3
+
+
+# ------------------------------------------------------------------ collision
+
+# contact record fields (oracle layout): pos 0-2, frame 3-11, dist 12,
+# pair 13, geom1 14, geom2 15, condim 16, mu0 17
+_DIST, _G1, _G2, _MU0 = 12, 14, 15, 17
+
+
+def test_explicit_pair_collides_geoms_that_filtering_skips():
+    """test_collision_full.cpp:114-122 and 142-150: a geom with contype =
+    conaffinity = 0 gets no pair and no contact, unless an explicit <pair>
+    names it; then it touches the floor, 1 cm deep as placed."""
+    scene = ('<geom name="floor" type="plane" size="5 5 0.1"/><body pos="0 0 0.09"><freejoint/>'
+             '<geom name="ball" type="sphere" size="0.1" mass="1" contype="0" conaffinity="0"/></body>')
+    _, om, env = env_from_xml(doc(scene))
+    assert om.npair == 0
+    env.step()
+    assert env.d.ncon == 0
+    _, om, env = env_from_xml(doc(scene, extra='<contact><pair geom1="ball" geom2="floor"/></contact>'))
+    assert om.npair == 1
+    env.step()
+    assert env.d.ncon == 1
+    c = env.contacts()[0]
+    assert c[_DIST] == pytest.approx(-0.01, abs=1e-12)
+    assert sorted((int(c[_G1]), int(c[_G2]))) == [0, 1]
+
+
+def test_explicit_pair_friction_sets_the_contact_friction():
+    """test_collision_full.cpp:170-178 (pairs with friction 0.5 and 2.0
+    produce contacts): each contact carries its pair's friction, and the
+    box on the low-friction pair slides farther."""
+    scene = ('<geom name="floor" type="plane" size="5 5 0.1" contype="0" conaffinity="0"/>'
+             '<body pos="0 0 0.099"><freejoint/><geom name="a" type="box" size="0.1 0.1 0.1" mass="1" contype="0" conaffinity="0"/></body>'
+             '<body pos="0 1 0.099"><freejoint/><geom name="b" type="box" size="0.1 0.1 0.1" mass="1" contype="0" conaffinity="0"/></body>')
+    pairs = ('<contact><pair geom1="a" geom2="floor" friction="0.5 0.5 0.005 0.0001 0.0001"/>'
+             '<pair geom1="b" geom2="floor" friction="2.0 2.0 0.005 0.0001 0.0001"/></contact>')
+    _, om, env = env_from_xml(doc(scene, extra=pairs))
+    env.a["qvel"][0] = 1.0
+    env.a["qvel"][6] = 1.0
+    env.step()
+    mu = {}
+    for c in env.contacts():
+        g = max(int(c[_G1]), int(c[_G2]))
+        mu.setdefault(g, set()).add(round(float(c[_MU0]), 12))
+    assert mu == {1: {0.5}, 2: {2.0}}
+    for _ in range(150):
+        env.step()
+    xa, xb = env.a["qpos"][0], env.a["qpos"][7]
+    assert xa > xb + 0.02 and xb > 0
+
+
+def test_spherical_ellipsoid_matches_sphere():
+    """test_collision_ellipsoid.cpp:177-199 (an ellipsoid with three equal
+    radii stays within 1 of a sphere): a tumbling ellipsoid with equal radii
+    and a sphere of the same mass bounce on the floor identically, to
+    1e-9 over 300 steps."""
+    out = []
+    for g in ('type="sphere" size="0.1"', 'type="ellipsoid" size="0.1 0.1 0.1"'):
+        _, om, env = env_from_xml(doc(FLOOR + f'<body pos="0 0 0.2"><freejoint/><geom {g} mass="1.2"/></body>'))
+        env.a["qvel"][:] = [0.5, -0.2, -1.0, 3.0, -2.0, 1.0]
+        hist = []
+        for _ in range(300):
+            env.step()
+            hist.append(np.concatenate([env.a["qpos"], env.a["qvel"], [env.d.ncon]]))
+        out.append(np.array(hist))
+    assert out[0][:, -1].max() == 1
+    np.testing.assert_allclose(out[1], out[0], atol=1e-9)
+
+
+@pytest.mark.parametrize("geom", ['type="sphere" size="0.1"', 'type="capsule" size="0.06 0.12"', 'type="box" size="0.1 0.08 0.06"',
+                                  'type="ellipsoid" size="0.12 0.08 0.06"', 'type="cylinder" size="0.08 0.1"'])
+def test_dropped_primitive_is_caught(geom):
+    """test_batched_collision_primitives.cpp:111-124 (each primitive dropped
+    on the floor stays within |qpos| < 2 after 200 steps) and
+    test_collision_full.cpp:221-232 (no fall through): tilted, dropped from
+    0.4 m, the body hits the floor at about 2.8 m/s, sinks less than 3 cm
+    into it on impact (the soft contact's default 20 ms time constant) and
+    then stays on it: in contact and below 0.2 m for each of the last 300
+    of 1500 steps, less than 1 cm deep.  (The sphere, capsule and box come
+    to rest; the ellipsoid keeps rocking and the cylinder rolls on its
+    side, as condim 3 models no rolling friction.)"""
+    _, om, env = env_from_xml(doc(FLOOR + f'<body pos="0 0 0.4" euler="20 35 0"><freejoint/><geom {geom} mass="1"/></body>'))
+    lowest = np.inf
+    for i in range(1500):
+        env.step()
+        cs = env.contacts()
+        for c in cs:
+            lowest = min(lowest, c[_DIST])
+        if i >= 1200:
+            assert len(cs) >= 1 and cs[:, _DIST].min() > -0.01
+            assert 0 < env.a["qpos"][2] < 0.2
+    assert lowest > -0.03
+    assert np.isfinite(env.a["qpos"]).all() and np.isfinite(env.a["qvel"]).all()
