@@ -384,6 +384,55 @@ def mixed_batch(K, W, flush, B=8192, seed=8100):
     return out
 
 
+def bin_stress(K, W, flush, B=2048, seed=5):
+    """The collision-heavy workload: 2048 envs, each a 1 m bin of 64 free
+    bodies (boxes, capsules, ellipsoids and convex hulls of 32 noisy points
+    on a 5 cm sphere) dropped from seeded poses; condim 6, elliptic cone,
+    GJK / EPA, HBM workspaces.  Plain solver (previous-step warm start);
+    median env-steps/s over min(K, 8) timed env-steps of 4 substeps after
+    20 settling substeps and min(W, 2) warm-up env-steps (the bodies are
+    still piling up: contacts grow over the timed steps), CUDA events on
+    the sim's stream, L2 flushed before each."""
+    import numpy as np
+    import torch
+
+    import mjb200
+
+    m = mjb200.load_model_from_string(mjb200.models.bin_xml(64, 1.0, seed=1, condim=6, cone="elliptic"))
+    ncon = 400
+    sim = mjb200.BatchedSim(m, B, record=0, ncon_max=ncon, nefc_max=ncon * 6)
+    q, v = mjb200.models.box_pile_state(m, B, seed=seed)
+    sim.set_state(q.astype(np.float32), v.astype(np.float32))
+    sim.step(None, 20)
+    for _ in range(min(W, 2)):
+        sim.step(None, SUBSTEPS)
+    sim.sync()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    nt = min(K, 8)
+    ms, its, itmax = [], [], []
+    for _ in range(nt):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(None, SUBSTEPS)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        st = sim.stats()
+        its.append(st["niter_sum"] / SUBSTEPS)
+        itmax.append(st["niter_max"])
+    its = np.concatenate(its)
+    out = {"workload": f"bin: {B} envs x 64 free bodies (boxes, capsules, ellipsoids, convex hulls), nv 384, condim 6, elliptic cone, "
+                       "GJK / EPA, 4 substeps of 4 ms, 30 Newton iterations, tol 1e-8, plain solver",
+           "value": B * 1e3 / float(np.median(ms)), "unit": UNIT, "ms_per_step_median": float(np.median(ms)), "steps": nt,
+           "newton_iter_mean": float(its.mean()), "newton_iter_p99": float(np.percentile(its, 99)), "newton_iter_max": int(np.max(itmax)),
+           "contacts_per_env_mean": float(st["ncon"].mean()), "rows_per_env_mean": float(st["nefc"].mean()),
+           "status_nonzero": int((st["status"] != 0).sum()), "launch": sim.launch_shape()}
+    sim.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -431,6 +480,7 @@ def run_ours(args, world, rank, local):
                      "predicted_warmstart_share": float(np.mean(st["warm_choice"] == 2)), "launch": sim.launch_shape()}
         sim.close()
     cfg3 = mixed_batch(K, W, flush)
+    cfg5 = bin_stress(K, W, flush)
     clocks = sampler.stop()
     h2d = B * nu * 4
     d2h = B * (m.nq + m.nv) * 4
@@ -463,6 +513,7 @@ def run_ours(args, world, rank, local):
                        "learned": L, "plain": P, "learned_over_plain": L["value"] / P["value"],
                        "iteration_reduction": 1.0 - L["newton_iter_mean"] / max(P["newton_iter_mean"], 1e-9), "training": train_info},
             "config3_mixed": cfg3,
+            "config5_bin": cfg5,
             "clocks": clocks}
     if world == 1:
         line["cpu_baseline"] = cpu_reference(B, args.cpu_seconds)
