@@ -502,7 +502,8 @@ def run_ours(args, world, rank, local):
     L, P = res["learned"], res["plain"]
     line = {"metric": METRIC, "value": P["value"], "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": P["ms_per_step"], "ms_per_step_median": P["ms_per_step_median"], "ms_per_step_p10": P["ms_per_step_p10"],
-            "ms_per_step_p90": P["ms_per_step_p90"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step_p90": P["ms_per_step_p90"], "substeps_per_s": P["value"] * SUBSTEPS, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(B),
             "e2e": {"value": P["e2e"], "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline,
