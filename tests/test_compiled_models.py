@@ -237,3 +237,77 @@ def test_pair_table_matches_filter_rules(model_xml):
     got = {frozenset((int(a), int(b))) for a, b in pi[:, :2]}
     assert len(got) == len(pi)
     assert got == expected_pairs(d, True)
+
+
+GEOM_TYPE = {"plane": 0, "hfield": 1, "sphere": 2, "capsule": 3, "ellipsoid": 4, "cylinder": 5, "box": 6, "mesh": 7}
+JOINT_TYPE = {"free": 0, "ball": 1, "slide": 2, "hinge": 3}
+
+
+@pytest.mark.parametrize("name", ["quadruped", "humanoid", "arm", "bin64"])
+def test_kinematic_tree_from_the_mjcf(name):
+    """Body frames, parents, joints and geom placement in the dump against
+    the MJCF text: body pos / quat relative to the parent, joint type, pos,
+    unit axis, range and armature, geom type, body, size, and for fromto
+    capsules the midpoint, the half-length and the z axis along the segment
+    (the oracle's kinematics reads all of these from the dump)."""
+    xml = mjb200.models.quadruped_xml() if name == "quadruped" else MODELS[name]()
+    d = mjb200.load_model_from_string(xml).dump()
+    wb = ET.fromstring(xml).find("worldbody")
+    bodies, parents = [wb], [-1]
+
+    def visit(b, parent):
+        bodies.append(b)
+        parents.append(parent)
+        me = len(bodies) - 1
+        for c in b.findall("body"):
+            visit(c, me)
+
+    for b in wb.findall("body"):
+        visit(b, 0)
+    nb = int(d["sizes"][3])
+    assert len(bodies) == nb
+    np.testing.assert_array_equal(d["body_parentid"][1:], parents[1:])
+    bpos, bquat = d["body_pos"].reshape(nb, 3), d["body_quat"].reshape(nb, 4)
+    joints, geoms = [], []
+    for i, b in enumerate(bodies):
+        if i:
+            np.testing.assert_allclose(bpos[i], nums(b.get("pos", "0 0 0")), atol=1e-12, err_msg=f"{name} body {i}")
+            q = nums(b.get("quat", "1 0 0 0"))
+            q /= np.linalg.norm(q)
+            assert min(np.abs(bquat[i] - q).max(), np.abs(bquat[i] + q).max()) < 1e-9, (name, i)
+        for el in b:
+            if el.tag in ("joint", "freejoint"):
+                joints.append((i, el))
+            elif el.tag == "geom":
+                geoms.append((i, el))
+    nj = int(d["sizes"][4])
+    assert len(joints) == nj
+    jpos, jaxis, jrng = d["jnt_pos"].reshape(nj, 3), d["jnt_axis"].reshape(nj, 3), d["jnt_range"].reshape(nj, 2)
+    for j, (bi, el) in enumerate(joints):
+        t = "free" if el.tag == "freejoint" else el.get("type", "hinge")
+        assert d["jnt_type"][j] == JOINT_TYPE[t] and d["jnt_bodyid"][j] == bi, (name, j)
+        if t in ("hinge", "slide"):
+            ax = nums(el.get("axis", "0 0 1"))
+            np.testing.assert_allclose(jaxis[j], ax / np.linalg.norm(ax), atol=1e-12, err_msg=f"{name} joint {j}")
+            np.testing.assert_allclose(jpos[j], nums(el.get("pos", "0 0 0")), atol=1e-12, err_msg=f"{name} joint {j}")
+            if el.get("range"):
+                np.testing.assert_allclose(jrng[j], nums(el.get("range")), atol=1e-12)
+                assert d["jnt_limited"][j] == 1
+            if el.get("armature"):
+                assert d["dof_armature"][d["jnt_dofadr"][j]] == pytest.approx(float(el.get("armature")))
+    ng = int(d["sizes"][5])
+    assert len(geoms) == ng
+    gpos, gquat, gsize = d["geom_pos"].reshape(ng, 3), d["geom_quat"].reshape(ng, 4), d["geom_size"].reshape(ng, 3)
+    for g, (bi, el) in enumerate(geoms):
+        t = el.get("type", "sphere")
+        assert d["geom_type"][g] == GEOM_TYPE[t] and d["geom_bodyid"][g] == bi, (name, g)
+        if el.get("fromto"):
+            ft = nums(el.get("fromto"))
+            seg = ft[3:] - ft[:3]
+            np.testing.assert_allclose(gpos[g], (ft[:3] + ft[3:]) / 2, atol=1e-12)
+            assert gsize[g, 0] == pytest.approx(nums(el.get("size"))[0]) and gsize[g, 1] == pytest.approx(np.linalg.norm(seg) / 2)
+            np.testing.assert_allclose(quat_mat(gquat[g])[:, 2], seg / np.linalg.norm(seg), atol=1e-9)
+        elif t in ("sphere", "box", "ellipsoid", "capsule", "cylinder"):
+            sz = nums(el.get("size"))
+            np.testing.assert_allclose(gsize[g, :len(sz)], sz, atol=1e-12)
+            np.testing.assert_allclose(gpos[g], nums(el.get("pos", "0 0 0")), atol=1e-12)
