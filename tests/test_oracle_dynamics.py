@@ -13,12 +13,15 @@ From those Jacobians alone:
     energy, sum over bodies of m g Jv_z;
   * for a fixed-base chain (hinges and slides only, where the coordinates
     are ordinary ones) the velocity part of the bias force is the
-    Christoffel term  dM/dt v - 1/2 d(v' M v)/dq,  from differences of M.
+    Christoffel term  dM/dt v - 1/2 d(v' M v)/dq,  from differences of M;
+  * each contact's pyramid rows are the normal and tangential components
+    of the relative velocity of the contact point on the two bodies, and
+    the normal row is the gradient of the contact distance.
 
 These do not involve the kernels, the compiler's inertia formulas (the
 body inertias are read from the same dump the oracle uses) or any MuJoCo
-code: they check the recursions (forward.hpp:143-397 of the reference) by
-an independent route.
+code: they check the recursions (forward.hpp:143-397 of the reference)
+and the contact Jacobians (solver.hpp:474-571) by an independent route.
 """
 import ctypes as C
 
@@ -163,3 +166,84 @@ def test_rne_velocity_terms_from_the_christoffel_symbols():
         want = Mdot_v - 0.5 * grad
         np.testing.assert_allclose((bias - bias0)[arm], want[arm], atol=1e-6 * max(1.0, np.abs(want).max()))
         assert np.abs(want[arm]).max() > 0.1          # the velocity terms are not negligible here
+
+
+def skew(r):
+    return np.array([[0, -r[2], r[1]], [r[2], 0, -r[0]], [-r[1], r[0], 0]])
+
+
+def test_contact_rows_from_the_motion_of_the_contact_point():
+    """The pyramid rows of every contact (reference solver.hpp:474-571)
+    against the material velocity of the contact point on each body, from
+    the finite-difference Jacobians: with Jrel = J_point(body2) -
+    J_point(body1), J_point = Jv - [p - xipos]x Jw, the rows' mean is
+    n' Jrel and their half-difference over mu is t' Jrel; the normal row is
+    also the gradient of the contact distance (same contacts, moved
+    configuration)."""
+    xml = ('<mujoco><option timestep="0.002"/><worldbody><geom type="plane" size="5 5 0.1"/>'
+           '<body pos="0 0 0.098"><freejoint/><geom type="sphere" size="0.1" mass="1"/></body>'
+           '<body pos="0.5 0 0.045" euler="0.3 0.2 0"><freejoint/><geom type="capsule" size="0.05 0.2" euler="0 1.5 0" mass="1"/></body>'
+           '<body pos="-0.5 0 0.097" euler="0.02 -0.03 0.4"><freejoint/><geom type="box" size="0.1 0.15 0.1" mass="2"/></body>'
+           '<body pos="0 0.6 0.3"><freejoint/><geom type="sphere" size="0.1" mass="1"/></body>'
+           '<body pos="0.05 0.62 0.49"><freejoint/><geom type="sphere" size="0.1" mass="0.5"/></body>'
+           '</worldbody></mujoco>')
+    p = Probe(xml)
+    d, om, env = p.d, p.om, p.env
+    rng = np.random.default_rng(3)
+    q = d["qpos0"].astype(float).copy()
+
+    def contacts_at(qq):
+        env.a["qpos"][:] = qq
+        env.a["qvel"][:] = 0
+        oracle.lib.oracle_kinematics(C.byref(om.c), C.byref(env.d))
+        for fn in ("oracle_com", "oracle_crb", "oracle_rne"):
+            getattr(oracle.lib, fn)(C.byref(om.c), C.byref(env.d), None)
+        oracle.lib.oracle_collide(C.byref(om.c), C.byref(env.d))
+        oracle.lib.oracle_make_constraints(C.byref(om.c), C.byref(env.d), None)
+        return env.contacts(), env.efc()
+
+    con, efc = contacts_at(q)
+    gtype = d["geom_type"]
+    kinds = {(int(gtype[int(c[14])]), int(gtype[int(c[15])])) for c in con}
+    assert kinds == {(0, 2), (0, 3), (0, 6), (2, 2)} and len(con) >= 6
+    _, R = p.fk(q)
+    xipos, _ = p.fk(q)
+    Jv, Jw = p.jacobians(q)
+    gbody = d["geom_bodyid"]
+    pr = d["pair_real"].reshape(-1, 16)
+    for c in con:
+        pos, n, t1, t2 = c[0:3], c[3:6], c[6:9], c[9:12]
+        b1, b2 = gbody[int(c[14])], gbody[int(c[15])]
+
+        def jpoint(b):
+            if b == 0:
+                return np.zeros((3, p.nv))
+            return Jv[b] - skew(pos - xipos[b]) @ Jw[b]
+
+        Jrel = jpoint(b2) - jpoint(b1)
+        r = int(c[19])
+        J = efc["J"][r:r + 4]
+        mu = pr[int(c[13]), 2:4]
+        scale = max(1.0, np.abs(J).max())
+        np.testing.assert_allclose((J[0] + J[1]) / 2, n @ Jrel, atol=1e-7 * scale)
+        np.testing.assert_allclose((J[0] - J[1]) / (2 * mu[0]), t1 @ Jrel, atol=1e-7 * scale / mu[0])
+        np.testing.assert_allclose((J[2] - J[3]) / (2 * mu[1]), t2 @ Jrel, atol=1e-7 * scale / mu[1])
+    # distance gradient of the contacts whose point is unique (sphere-plane,
+    # sphere-sphere): along a random velocity direction
+    v = rng.normal(size=p.nv)
+    h = 1e-6
+    cp, _ = contacts_at(integrate(d, q, h * v))
+    cm, _ = contacts_at(integrate(d, q, -h * v))
+    con, efc = contacts_at(q)
+    checked = 0
+    for k, c in enumerate(con):
+        t = (gtype[int(c[14])], gtype[int(c[15])])
+        if t not in ((0, 2), (2, 2)):
+            continue
+        same = [i for i in range(len(cp)) if int(cp[i, 13]) == int(c[13])], [i for i in range(len(cm)) if int(cm[i, 13]) == int(c[13])]
+        ddist = (cp[same[0][0], 12] - cm[same[1][0], 12]) / (2 * h)
+        r = int(c[19])
+        Jn = (efc["J"][r] + efc["J"][r + 1]) / 2
+        assert Jn @ v == pytest.approx(ddist, rel=1e-6, abs=1e-8)
+        checked += 1
+    assert checked == 2                        # the floor sphere and the sphere pair
