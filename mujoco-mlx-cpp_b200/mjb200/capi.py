@@ -42,6 +42,9 @@ def _load():
         "mjmlx_load_model_from_string": (C.c_void_p, [C.c_char_p]),
         "mjmlx_load_model_from_string_ex": (C.c_void_p, [C.c_char_p, C.POINTER(MjmlxModelOptions)]),
         "mjmlx_load_model": (C.c_void_p, [C.c_char_p]),
+        "mjmlx_load_model_ex": (C.c_void_p, [C.c_char_p, C.POINTER(MjmlxModelOptions)]),
+        "mjmlx_default_model_options": (MjmlxModelOptions, []),
+        "mjmlx_model_body_mass": (C.c_float, [C.c_void_p, C.c_int]),
         "mjmlx_free_model": (None, [C.c_void_p]),
         "mjmlx_model_info": (MjmlxModelInfo, [C.c_void_p]),
         "mjmlx_model_opt_timestep": (C.c_float, [C.c_void_p]),
@@ -58,6 +61,7 @@ def _load():
         "mjmlx_batched_set_env_qvel": (None, [C.c_void_p, C.c_int, _f32p, C.c_int]),
         "mjmlx_batched_set_env_params": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p, _f32p, _f32p, _f32p]),
         "mjmlx_batched_set_free_drag": (C.c_int, [C.c_void_p, _i32p, C.c_int, _f32p]),
+        "mjmlx_batched_num_free_joints": (C.c_int, [C.c_void_p]),
         "mjmlx_batched_grad_step": (None, [C.c_void_p, _f32p]),
         "mjmlx_batched_set_pack_spec": (C.c_int, [C.c_void_p, _i32p, C.c_int, C.c_int, C.c_int]),
         "mjmlx_batched_get_pack": (C.c_int, [C.c_void_p, _f32p]),
@@ -197,8 +201,9 @@ def load_model_from_string(xml: str, self_collision: int = 1, max_condim: int = 
     return Model(lib.mjmlx_load_model_from_string_ex(xml.encode(), C.byref(opt)))
 
 
-def load_model(path: str) -> Model:
-    return Model(lib.mjmlx_load_model(path.encode()))
+def load_model(path: str, self_collision: int = 1, max_condim: int = 0) -> Model:
+    opt = MjmlxModelOptions(self_collision, max_condim)
+    return Model(lib.mjmlx_load_model_ex(path.encode(), C.byref(opt)))
 
 
 def _fp(a):
@@ -388,11 +393,19 @@ class BatchedSim:
         self.pack_stride = stride
         return stride
 
-    def get_pack(self):
-        out = np.zeros((self.num_envs, self.pack_stride), np.float32)
+    def get_pack(self, out=None):
+        """Packed rows [num_envs, stride]; out: optional contiguous float32
+        array of that shape to fill (e.g. a page-locked one)."""
+        if out is None:
+            out = np.zeros((self.num_envs, self.pack_stride), np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.num_envs * self.pack_stride:
+            raise ValueError("out must be a contiguous float32 array of num_envs x stride values")
         if lib.mjmlx_batched_get_pack(self.handle, _fp(out)) != 0:
             raise RuntimeError("get_pack: " + last_error())
         return out
+
+    def num_free_joints(self) -> int:
+        return lib.mjmlx_batched_num_free_joints(self.handle)
 
     def pack_device(self) -> int:
         """Device pointer of the packed rows (num_envs x stride floats)."""
