@@ -247,3 +247,59 @@ def test_contact_rows_from_the_motion_of_the_contact_point():
         assert Jn @ v == pytest.approx(ddist, rel=1e-6, abs=1e-8)
         checked += 1
     assert checked == 2                        # the floor sphere and the sphere pair
+
+
+def mujoco_impedance(solref, solimp, pos, h, refsafe=True):
+    """MuJoCo's documented soft-constraint parameters, written from its
+    documentation: (k, b, imp) for signed distance pos."""
+    tc, dr = solref
+    dmin, dmax, width, mid, power = solimp
+    dmin, dmax = np.clip([dmin, dmax], 1e-4, 0.9999)
+    mid = np.clip(mid, 1e-4, 0.9999)
+    power = max(power, 1.0)
+    width = max(width, 1e-12)
+    if tc > 0:
+        if refsafe:
+            tc = max(tc, 2 * h)
+        k = 1 / (dmax * dmax * tc * tc * dr * dr)
+        b = 2 / (dmax * tc)
+    else:
+        k, b = -tc / (dmax * dmax), -dr / dmax
+    x = abs(pos) / width
+    if x >= 1:
+        imp = dmax
+    else:
+        y = x ** power / mid ** (power - 1) if x < mid else 1 - (1 - x) ** power / (1 - mid) ** (power - 1)
+        imp = dmin + y * (dmax - dmin)
+    return k, b, imp
+
+
+@pytest.mark.parametrize("solref,solimp,q,v", [
+    ((0.02, 1.0), (0.9, 0.95, 0.001, 0.5, 2), 0.7, 0.3),      # defaults, deep
+    ((0.02, 1.0), (0.9, 0.95, 0.1, 0.5, 2), 0.52, -0.4),      # inside the width, below mid
+    ((0.02, 1.0), (0.5, 0.99, 0.1, 0.3, 3), 0.58, 0.1),       # inside the width, above mid, power 3
+    ((0.001, 0.5), (0.9, 0.95, 0.001, 0.5, 2), 0.6, 0.0),     # time constant below 2 h: clamped
+    ((-2000.0, -30.0), (0.9, 0.95, 0.001, 0.5, 2), 0.6, 0.2),  # direct stiffness and damping
+])
+def test_limit_row_impedance_follows_the_documented_formulas(solref, solimp, q, v):
+    """A hinge past its upper limit 0.5: the limit row's D = imp / ((1 - imp)
+    invweight) and aref = -b J v - k imp pos with pos = 0.5 - q, against
+    MuJoCo's documented solref / solimp semantics restated above
+    (reference solver.hpp:122-138, 347-368)."""
+    h = 0.002
+    xml = (f'<mujoco><compiler angle="radian"/><option timestep="{h}"/><worldbody><body><joint type="hinge" axis="0 1 0" limited="true" range="-0.5 0.5" '
+           f'solreflimit="{solref[0]} {solref[1]}" solimplimit="{" ".join(str(x) for x in solimp)}"/>'
+           '<geom type="capsule" fromto="0 0 0 0.3 0 0" size="0.03" mass="1"/></body></worldbody></mujoco>')
+    p = Probe(xml)
+    env = p.env
+    env.a["qpos"][0] = q
+    env.a["qvel"][0] = v
+    env.step()
+    e = p.env.efc()
+    assert list(e["type"]) == [1]
+    pos = 0.5 - q
+    k, b, imp = mujoco_impedance(solref, solimp, pos, h)
+    invw = p.d["dof_invweight0"][0]
+    assert e["J"][0, 0] == -1.0
+    assert e["D"][0] == pytest.approx(imp / ((1 - imp) * invw), rel=1e-12)
+    assert e["aref"][0] == pytest.approx(-b * (-v) - k * imp * pos, rel=1e-12)
