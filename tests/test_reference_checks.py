@@ -470,3 +470,20 @@ def test_dropped_primitive_is_caught(geom):
             assert 0 < env.a["qpos"][2] < 0.2
     assert lowest > -0.03
     assert np.isfinite(env.a["qpos"]).all() and np.isfinite(env.a["qvel"]).all()
+
+
+@pytest.mark.parametrize("eulerdamp", [True, False])
+def test_euler_folds_joint_damping_unless_disabled(eulerdamp):
+    """test_implicit.cpp:199-223 (damped pendulum): MuJoCo's Euler
+    integrator puts the joint damping d on the mass matrix's diagonal,
+    v1 = v0 + h (-d v0) / (m + h d); with the eulerdamp flag disabled the
+    damping force is explicit, v1 = v0 + h (-d v0) / m.  A horizontal slide
+    with no gravity along it."""
+    h, m, d, v0 = 0.01, 0.5, 40.0, 2.0
+    flag = "" if eulerdamp else '<flag eulerdamp="disable"/>'
+    _, om, env = env_from_xml(doc(f'<body><joint type="slide" axis="1 0 0" damping="{d}"/><geom type="box" size="0.1 0.1 0.1" mass="{m}"/></body>',
+                                  option=f'<option timestep="{h}">{flag}</option>'))
+    env.a["qvel"][0] = v0
+    env.step()
+    want = v0 + h * (-d * v0) / (m + h * d) if eulerdamp else v0 + h * (-d * v0) / m
+    assert env.a["qvel"][0] == pytest.approx(want, rel=1e-12)
